@@ -1,0 +1,233 @@
+/*
+ * yafel_gpu.h -- C ABI of the B200 continuous-Galerkin assemble + solve path.
+ *
+ * The library (yafel_b200/libyafel_b200.so) replaces, for one GPU, the
+ * reference's path from the DoF numbering through element assembly, Dirichlet
+ * conditions, sparse storage, SpMV, preconditioners and Krylov solvers.  Each
+ * entry point names the reference interface it replaces (paths relative to the
+ * YAFEL source tree).  Plain pointers and sizes only; all handles are opaque;
+ * every call returns a yg_status and never throws.  Host arrays are copied; the
+ * library owns all device memory behind a handle.  Calls on one context are
+ * not thread-safe (the reference's objects are not either); use one context per
+ * thread.
+ */
+#ifndef YAFEL_GPU_H
+#define YAFEL_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+/* Symbols of the shared library; hidden-by-default builds export only these. */
+#if defined(YG_BUILD) && defined(__GNUC__)
+#define YG_API __attribute__((visibility("default")))
+#else
+#define YG_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum yg_status {
+    YG_OK = 0,
+    YG_NOT_CONVERGED = 1, /* iteration cap reached (the reference returns silently: cg_solve.hpp:56) */
+    YG_BREAKDOWN = 2,     /* p.Ap <= 0, rho = 0 or omega = 0 in a Krylov recurrence */
+    YG_NAN = 3,           /* a non-finite scalar appeared */
+    YG_TIMEOUT = 4,       /* a bounded device wait expired */
+    YG_OUT_OF_MEMORY = 5,
+    YG_OVER_BUDGET = 6,   /* the request exceeds the context's HBM budget */
+    YG_BAD_ARG = 7,
+    YG_CUDA_ERROR = 8,
+    YG_UNSUPPORTED = 9,
+    YG_ZERO_PIVOT = 10    /* reported, not fatal: the reference warns and continues */
+} yg_status;
+
+typedef struct yg_context_t *yg_context;
+typedef struct yg_dofmap_t *yg_dofmap;
+typedef struct yg_matrix_t *yg_matrix;
+typedef struct yg_vector_t *yg_vector;
+typedef struct yg_precond_t *yg_precond;
+
+/* ------------------------------------------------------------------ context */
+
+/* One CUDA device, one stream, an HBM budget (0 = no limit).  No reference
+ * counterpart: the reference runs in one host process. */
+YG_API yg_status yg_context_create(int32_t device, uint64_t hbm_budget_bytes, yg_context *out);
+YG_API yg_status yg_context_destroy(yg_context ctx);
+YG_API yg_status yg_context_synchronize(yg_context ctx);
+YG_API yg_status yg_context_memory(yg_context ctx, uint64_t *in_use, uint64_t *budget);
+/* Kernels this context has launched so far (instrumentation for benchmarks). */
+YG_API int64_t yg_context_launches(yg_context ctx);
+/* Message of the last failed call on this thread; never NULL. */
+YG_API const char *yg_last_error(void);
+YG_API const char *yg_status_string(yg_status s);
+
+/* ------------------------------------------------------------------ vectors */
+
+/* Device FP64 vector.  Replaces Vector<double> (include/old_handmade_linalg/Vector.hpp:9-158). */
+YG_API yg_status yg_vector_create(yg_context ctx, int64_t n, yg_vector *out);
+YG_API yg_status yg_vector_destroy(yg_vector v);
+YG_API int64_t yg_vector_size(yg_vector v);
+YG_API yg_status yg_vector_upload(yg_vector v, const double *host, int64_t n);
+YG_API yg_status yg_vector_download(yg_vector v, double *host, int64_t n);
+YG_API yg_status yg_vector_fill(yg_vector v, double value);
+YG_API yg_status yg_vector_copy(yg_vector dst, yg_vector src);
+/* Deterministic dot product; replaces VectorExpression::dot (VectorExpression.hpp:33-54). */
+YG_API yg_status yg_vector_dot(yg_vector a, yg_vector b, double *out);
+/* y += alpha*x; replaces Vector::operator+= of a scaled expression (Vector.hpp:48-150). */
+YG_API yg_status yg_vector_axpy(double alpha, yg_vector x, yg_vector y);
+
+/* ------------------------------------------------------------------ DoFManager */
+
+/* Mesh cell types use the reference's CellType codes (include/mesh/mesh_typedefs.hpp:42-50). */
+enum { YG_CELL_LINE2 = 0, YG_CELL_TRI3 = 1, YG_CELL_TET4 = 2, YG_CELL_QUAD4 = 3, YG_CELL_HEX8 = 4, YG_CELL_POINT1 = 5 };
+/* Element topologies (include/element/ElementType.hpp:22-27). */
+enum { YG_TOPO_TENSOR = 0, YG_TOPO_SIMPLEX = 1, YG_TOPO_NONE = 2 };
+
+/* DoFManager(const Mesh&, ManagerType::CG, polyOrder, dof_per_node)
+ * (include/utils/DoFManager.hpp:25, src/utils/DoFManager.cpp:11-36,143-229,340-414).
+ * nodes_xyz: 3 per node; cells as in Mesh(DefinitionScheme::Explicit, ...)
+ * (include/mesh/Mesh.hpp:48-53).  Numbering is identical to the reference's:
+ * p=1 keeps the mesh numbering; p>1 merges coincident element nodes sorted on
+ * snapped (z,y,x).  Fails with YG_BAD_ARG for polyOrder < 1, as the reference
+ * throws (DoFManager.cpp:162).  ctx may be NULL: the numbering is then built on
+ * the host only (no device memory) and the dofmap cannot be assembled. */
+YG_API yg_status yg_dofmap_create(yg_context ctx, const double *nodes_xyz, int32_t n_nodes,
+                           const int32_t *cell_nodes, const int32_t *cell_offsets,
+                           const int32_t *cell_types, int32_t n_cells, int32_t poly_order,
+                           int32_t dof_per_node, yg_dofmap *out);
+YG_API yg_status yg_dofmap_destroy(yg_dofmap d);
+/* Sizes of dof_nodes, cells, the elements array, and dofs = dof_nodes*dof_per_node. */
+YG_API yg_status yg_dofmap_sizes(yg_dofmap d, int32_t *n_dof_nodes, int32_t *n_cells,
+                          int64_t *n_element_nodes, int64_t *n_dofs);
+/* Copies of dof_nodes, element_offsets, elements and element_types
+ * (DoFManager.hpp:67-73); any pointer may be NULL. */
+YG_API yg_status yg_dofmap_get(yg_dofmap d, double *dof_nodes_xyz, int32_t *element_offsets,
+                        int32_t *elements, int8_t *topology, int8_t *topo_dim, int8_t *poly_order);
+
+/* ------------------------------------------------------------------ assembly */
+
+/* Device physics registered for CGAssembly<Physics>; a host-side Physics struct
+ * cannot run on the GPU, so each is a kernel with parameters.
+ *  YG_POISSON     params = {sign, f}: K_AB += sign*gradN_A.gradN_B*jxw, R_A += f*N_A*jxw
+ *                 (apps/BasicPoisson/main.cpp:31-60 uses sign=-1; sign=+1 is the SPD form)
+ *  YG_ELASTICITY  params = {sign, lambda, mu, b0, b1, b2}: K_{Ai,Bk} += sign*C_ikjl
+ *                 dN_A/dx_j dN_B/dx_l jxw, R_{Ai} += b_i*N_A*jxw
+ *                 (apps/BasicLinearElasticity/main.cpp:41-113)
+ *  YG_SUPG        params = {k, h, U0, Q}: steady SUPG advection-diffusion with U=(U0,0,0)
+ *                 (apps/supg_learning/supg_advection.hpp:19-132) */
+enum { YG_POISSON = 0, YG_ELASTICITY = 1, YG_SUPG = 2 };
+typedef struct yg_physics {
+    int32_t kind;
+    int32_t nsd; /* Physics::nsd(); cells of another topological dimension are skipped */
+    double params[8];
+} yg_physics;
+
+/* AssemblyRequirement (include/assembly/AssemblyRequirement.hpp:12-19) as bits. */
+enum { YG_REQ_RESIDUAL = 1, YG_REQ_TANGENT = 2 };
+/* Storage of the assembled tangent: scalar CSR, or BCSR with dof_per_node-sized
+ * blocks (dof = node*dof_per_node + comp, so node blocks are natural). */
+enum { YG_FORMAT_CSR = 0, YG_FORMAT_BCSR = 1 };
+
+/* CGAssembly<Physics>(FESystem&, requirements) (include/assembly/CGAssembly.hpp:27-186).
+ * Tangent: if *K is NULL a new matrix (pattern built on the GPU) is returned; if
+ * *K came from an earlier call on the same dofmap and format, its values are
+ * replaced, like setFromTriplets (CGAssembly.hpp:185).  Residual: added into
+ * `residual` (length n_dofs), like GlobalResidual += private_residual
+ * (CGAssembly.hpp:181).  Duplicate summation is deterministic (element-coloured
+ * scatter, colours in ascending order). */
+YG_API yg_status yg_assemble(yg_dofmap d, const yg_physics *physics, uint32_t requirements,
+                      int32_t format, yg_matrix *K, yg_vector residual);
+
+/* DirichletBC::apply(A, rhs) for one BC object (src/boundary_conditions/DirichletBC.cpp:27-89):
+ * rhs -= A*g, zero the BC rows and columns, unit diagonal, rhs_bc = g.  bc_dofs
+ * are global dofs (node*dof_per_node + component), bc_values their g. */
+YG_API yg_status yg_dirichlet_apply(yg_matrix K, yg_vector rhs, const int64_t *bc_dofs,
+                             const double *bc_values, int64_t n_bc);
+
+/* ------------------------------------------------------------------ matrices */
+
+/* sparse_csr<T>(triplets) for block=1 (include/old_handmade_linalg/sparse_csr.hpp:90-149)
+ * and sparse_bcsr<B,T>(triplets) for block=B (sparse_bcsr.hpp:93-176): duplicates
+ * summed, rows/cols = max index + 1 (BCSR: rounded up to whole blocks).  Triplet
+ * indices are size_t in the reference (sparse_matrix.hpp:19). */
+YG_API yg_status yg_matrix_from_triplets(yg_context ctx, int32_t block, const uint64_t *rows,
+                                  const uint64_t *cols, const double *vals, uint64_t n,
+                                  yg_matrix *out);
+/* Import an already compressed matrix (row_ptr/col_index/_data of sparse_csr,
+ * sparse_csr.hpp:63-65, or brow_ptr/bcol_index/data of sparse_bcsr,
+ * sparse_bcsr.hpp:31-33). Column indices must be sorted within each row. */
+YG_API yg_status yg_matrix_from_csr(yg_context ctx, int32_t block, int64_t nbrows, int64_t nbcols,
+                             const int64_t *brow_ptr, const int64_t *bcol, const double *vals,
+                             yg_matrix *out);
+YG_API yg_status yg_matrix_destroy(yg_matrix A);
+/* rows(), cols(), nnz() (scalar entries) and the block size. */
+YG_API yg_status yg_matrix_sizes(yg_matrix A, int64_t *rows, int64_t *cols, int64_t *nnz, int32_t *block);
+/* Export in the reference layout (block row pointer, block columns, values with
+ * row-major blocks); any pointer may be NULL. */
+YG_API yg_status yg_matrix_get(yg_matrix A, int64_t *brow_ptr, int64_t *bcol, double *vals);
+/* Keep an FP32 copy of the values for mixed-precision SpMV (no reference counterpart). */
+YG_API yg_status yg_matrix_make_fp32(yg_matrix A);
+
+/* y = A*x: csr_spmv / bcsr_spmv via operator* (include/old_handmade_linalg/csr_spmv.hpp:25-56,
+ * bcsr_spmv.hpp:23-62, operators.hpp:117-131).  precision: YG_PREC_FP64 or
+ * YG_PREC_MIXED (FP32 values, FP64 vectors and accumulation). */
+enum { YG_PREC_FP64 = 0, YG_PREC_MIXED = 1 };
+YG_API yg_status yg_spmv(yg_matrix A, yg_vector x, yg_vector y);
+YG_API yg_status yg_spmv_ex(yg_matrix A, yg_vector x, yg_vector y, int32_t precision);
+
+/* ------------------------------------------------------------------ preconditioners */
+
+/* IdentityPreconditioner (IdentityPreconditioner.hpp:20-29), JacobiPreconditioner
+ * (JacobiPreconditioner.hpp:11-54: z_i = r_i / a_ii, a zero diagonal gives inf as
+ * in the reference), ILUPreconditioner (ILUPreconditioner.hpp:96-329: ILU(0) on
+ * the pattern of A, no pivoting, zero pivots skipped; solve = forward
+ * substitution with unit L then backward substitution with U). */
+enum { YG_PRECOND_IDENTITY = 0, YG_PRECOND_JACOBI = 1, YG_PRECOND_ILU0 = 2 };
+YG_API yg_status yg_precond_create(yg_matrix A, int32_t kind, yg_precond *out);
+/* M.solve(z) in place (Preconditioner.hpp:9-21). */
+YG_API yg_status yg_precond_apply(yg_precond M, yg_vector z);
+YG_API yg_status yg_precond_destroy(yg_precond M);
+/* Number of zero pivots skipped while factoring (ILU(0)) or zero diagonals (Jacobi). */
+YG_API int64_t yg_precond_zero_pivots(yg_precond M);
+
+/* ------------------------------------------------------------------ solvers */
+
+/* Stopping criteria.  REFERENCE reproduces the reference's own test:
+ *   cg_solve:   r.r / r0.r0 < tol, at most N iterations (cg_solve.hpp:45-69)
+ *   pcg_solve:  r.z / r0.z0 < tol, at most N iterations (pcg_solve.hpp:141-167)
+ *   bicgstab:   ||Ax-b||^2/||b||^2 < tol checked every max(N/100,1) iterations
+ *               (bicgstab_solve.hpp:227-272)
+ * RELRES stops when ||b - A x|| <= tol ||b||, recomputed in FP64 on the GPU
+ * before returning (the recursive residual is only a trigger). */
+enum { YG_CRIT_REFERENCE = 0, YG_CRIT_RELRES = 1 };
+typedef struct yg_solve_opts {
+    int32_t criterion;  /* YG_CRIT_* */
+    int32_t precision;  /* YG_PREC_FP64, or YG_PREC_MIXED: FP32 matrix inside FP64 iterative refinement */
+    double tol;         /* see criterion */
+    int64_t maxiter;    /* 0 = the reference's default (N for CG) */
+    int32_t check_every;/* iterations between host convergence checks (0 = automatic) */
+    int32_t reserved;
+} yg_solve_opts;
+typedef struct yg_solve_stats {
+    int64_t iterations;       /* Krylov iterations (inner iterations summed for MIXED) */
+    double rel_residual;      /* ||b - A x|| / ||b|| recomputed in FP64 */
+    int32_t status;           /* yg_status of the solve */
+    int32_t refinements;      /* outer FP64 refinement steps (MIXED) */
+    double device_ms;         /* device time of the solve (CUDA events) */
+} yg_solve_stats;
+
+/* cg_solve(A, rhs, x0, TOL) / pcg_solve(A, rhs, M, x0, TOL)
+ * (solver/iterative/cg_solve.hpp:23-81, pcg_solve.hpp:115-178).  M may be NULL
+ * (plain CG).  x holds x0 on entry and the solution on return. */
+YG_API yg_status yg_cg(yg_matrix A, yg_precond M, yg_vector b, yg_vector x, const yg_solve_opts *opts,
+                yg_solve_stats *stats);
+/* bicgstab_solve(A, rhs, x0) (solver/iterative/bicgstab_solve.hpp:207-283), with an
+ * optional right preconditioner and an iteration cap (the reference has none). */
+YG_API yg_status yg_bicgstab(yg_matrix A, yg_precond M, yg_vector b, yg_vector x,
+                      const yg_solve_opts *opts, yg_solve_stats *stats);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,404 @@
+"""ctypes front end of the checker libraries (test infrastructure only).
+
+``liboracle.so`` is the C restatement of the reference path (oracle/yafel_oracle.c);
+``_ref/libyafel_ref.so`` is the reference's own handmade linear algebra and
+quadrature compiled in place (oracle/Makefile).  Only tests, the smoke check
+and the bench's CPU-baseline leg import this module.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+_REF = None
+
+i8p = np.ctypeslib.ndpointer(np.int8, flags="C_CONTIGUOUS")
+u8p = np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS")
+i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+i64p = np.ctypeslib.ndpointer(np.int64, flags="C_CONTIGUOUS")
+f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+
+TENSOR, SIMPLEX, NONE = 0, 1, 2
+POISSON, ELASTICITY, SUPG = 0, 1, 2
+PRECOND_NONE, PRECOND_JACOBI, PRECOND_ILU0 = 0, 1, 2
+CRIT_REFERENCE, CRIT_RELRES = 0, 1
+
+
+class _Csr(C.Structure):
+    _fields_ = [("nrows", C.c_int64), ("ncols", C.c_int64), ("nnz", C.c_int64),
+                ("row_ptr", C.POINTER(C.c_int64)), ("col", C.POINTER(C.c_int64)),
+                ("val", C.POINTER(C.c_double))]
+
+
+class _Bcsr(C.Structure):
+    _fields_ = [("block", C.c_int32), ("nbrows", C.c_int64), ("nbcols", C.c_int64),
+                ("nnzb", C.c_int64), ("brow_ptr", C.POINTER(C.c_int64)),
+                ("bcol", C.POINTER(C.c_int64)), ("val", C.POINTER(C.c_double))]
+
+
+class _Dofmap(C.Structure):
+    _fields_ = [("n_nodes", C.c_int32), ("nodes", C.POINTER(C.c_double)),
+                ("n_cells", C.c_int32), ("offsets", C.POINTER(C.c_int32)),
+                ("elements", C.POINTER(C.c_int32)), ("topology", C.POINTER(C.c_int8)),
+                ("topo_dim", C.POINTER(C.c_int8)), ("poly_order", C.POINTER(C.c_int8))]
+
+
+def build():
+    """Compile liboracle.so (and _ref when the reference tree is present)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(HERE, "liboracle.so")
+        if not os.path.exists(path):
+            build()
+        L = C.CDLL(path)
+        L.or_gauss_legendre_1d.argtypes = [C.c_int, f64p, f64p]
+        L.or_gauss_lobatto_1d.argtypes = [C.c_int, f64p, f64p]
+        L.or_tensor_rule.argtypes = [C.c_int, C.c_int, C.c_int, f64p, f64p]
+        L.or_triangle_rule.argtypes = [C.c_int, f64p, f64p]
+        L.or_local_nodes.argtypes = [C.c_int, C.c_int, C.c_int, f64p]
+        L.or_element_rule.argtypes = [C.c_int, C.c_int, C.c_int, f64p, f64p]
+        L.or_shape_functions.argtypes = [C.c_int, C.c_int, C.c_int, f64p, C.c_int, f64p, f64p]
+        L.or_dofmanager.argtypes = [f64p, C.c_int32, i32p, i32p, i32p, C.c_int32, C.c_int32]
+        L.or_dofmanager.restype = C.POINTER(_Dofmap)
+        L.or_free_dofmap.argtypes = [C.POINTER(_Dofmap)]
+        L.or_assemble.argtypes = [C.POINTER(_Dofmap), C.c_int32, C.c_int32, C.c_int32, f64p, C.c_void_p]
+        L.or_assemble.restype = C.POINTER(_Csr)
+        L.or_dirichlet_apply.argtypes = [C.POINTER(_Csr), f64p, u8p, f64p]
+        L.or_csr_from_triplets.argtypes = [i64p, i64p, f64p, C.c_int64]
+        L.or_csr_from_triplets.restype = C.POINTER(_Csr)
+        L.or_bcsr_from_triplets.argtypes = [C.c_int32, i64p, i64p, f64p, C.c_int64]
+        L.or_bcsr_from_triplets.restype = C.POINTER(_Bcsr)
+        L.or_free_csr.argtypes = [C.POINTER(_Csr)]
+        L.or_free_bcsr.argtypes = [C.POINTER(_Bcsr)]
+        L.or_csr_spmv.argtypes = [C.POINTER(_Csr), f64p, f64p]
+        L.or_bcsr_spmv.argtypes = [C.POINTER(_Bcsr), f64p, f64p]
+        L.or_ilu0.argtypes = [C.POINTER(_Csr)]
+        L.or_ilu0.restype = C.POINTER(_Csr)
+        L.or_ilu_solve.argtypes = [C.POINTER(_Csr), f64p]
+        L.or_cg.argtypes = [C.POINTER(_Csr), f64p, f64p, C.c_int32, C.c_int32, C.c_double,
+                            C.c_int64, C.POINTER(C.c_double)]
+        L.or_cg.restype = C.c_int64
+        L.or_bicgstab.argtypes = [C.POINTER(_Csr), f64p, f64p, C.c_int32, C.c_double, C.c_int64,
+                                  C.POINTER(C.c_double)]
+        L.or_bicgstab.restype = C.c_int64
+        L.or_true_relres.argtypes = [C.POINTER(_Csr), f64p, f64p]
+        L.or_true_relres.restype = C.c_double
+        L.or_num_threads.restype = C.c_int
+        _LIB = L
+    return _LIB
+
+
+def ref_available():
+    return os.path.exists(os.path.join(HERE, "_ref", "libyafel_ref.so"))
+
+
+def ref():
+    """The reference's own linear algebra / quadrature (compiled in place)."""
+    global _REF
+    if _REF is None:
+        path = os.path.join(HERE, "_ref", "libyafel_ref.so")
+        if not os.path.exists(path):
+            build()
+        R = C.CDLL(path)
+        R.ref_gauss_1d.argtypes = [C.c_int, C.c_int, f64p, f64p]
+        R.ref_tensor_rule.argtypes = [C.c_int, C.c_int, C.c_int, f64p, f64p]
+        R.ref_triangle_rule.argtypes = [C.c_int, f64p, f64p]
+        R.ref_csr_from_triplets.argtypes = [i64p, i64p, f64p, C.c_int64]
+        R.ref_csr_from_triplets.restype = C.c_void_p
+        R.ref_csr_info.argtypes = [C.c_void_p] + [C.POINTER(C.c_int64)] * 3
+        R.ref_csr_get.argtypes = [C.c_void_p, i64p, i64p, f64p]
+        R.ref_csr_free.argtypes = [C.c_void_p]
+        R.ref_csr_spmv.argtypes = [C.c_void_p, f64p, f64p]
+        R.ref_bcsr_from_triplets.argtypes = [C.c_int, i64p, i64p, f64p, C.c_int64]
+        R.ref_bcsr_from_triplets.restype = C.c_void_p
+        R.ref_bcsr_info.argtypes = [C.c_int, C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+        R.ref_bcsr_get.argtypes = [C.c_int, C.c_void_p, i64p, i64p, f64p]
+        R.ref_bcsr_spmv.argtypes = [C.c_int, C.c_void_p, f64p, f64p]
+        R.ref_bcsr_free.argtypes = [C.c_int, C.c_void_p]
+        R.ref_cg.argtypes = [C.c_void_p, f64p, f64p, C.c_double]
+        R.ref_bcsr_cg.argtypes = [C.c_int, C.c_void_p, f64p, f64p, C.c_double]
+        R.ref_pcg_jacobi.argtypes = [C.c_void_p, f64p, f64p, C.c_double]
+        R.ref_pcg_ilu.argtypes = [C.c_void_p, f64p, f64p, C.c_double]
+        R.ref_bicgstab.argtypes = [C.c_void_p, f64p, f64p]
+        R.ref_ilu_factor.argtypes = [C.c_void_p]
+        R.ref_ilu_factor.restype = C.c_void_p
+        R.ref_ilu_apply.argtypes = [C.c_void_p, f64p]
+        R.ref_jacobi_apply.argtypes = [C.c_void_p, f64p]
+        _REF = R
+    return _REF
+
+
+# ---------------------------------------------------------------- helpers
+
+class Csr:
+    """Host CSR (int64 indices, float64 values) owned by numpy."""
+
+    def __init__(self, nrows, ncols, row_ptr, col, val):
+        self.nrows, self.ncols = int(nrows), int(ncols)
+        self.row_ptr = np.ascontiguousarray(row_ptr, dtype=np.int64)
+        self.col = np.ascontiguousarray(col, dtype=np.int64)
+        self.val = np.ascontiguousarray(val, dtype=np.float64)
+
+    @property
+    def nnz(self):
+        return int(self.col.size)
+
+    def _struct(self):
+        s = _Csr(self.nrows, self.ncols, self.nnz,
+                 self.row_ptr.ctypes.data_as(C.POINTER(C.c_int64)),
+                 self.col.ctypes.data_as(C.POINTER(C.c_int64)),
+                 self.val.ctypes.data_as(C.POINTER(C.c_double)))
+        return s
+
+    def spmv(self, x):
+        y = np.empty(self.nrows)
+        s = self._struct()
+        lib().or_csr_spmv(C.byref(s), np.ascontiguousarray(x, dtype=np.float64), y)
+        return y
+
+    def copy(self):
+        return Csr(self.nrows, self.ncols, self.row_ptr.copy(), self.col.copy(), self.val.copy())
+
+    def diagonal(self):
+        d = np.zeros(self.nrows)
+        rows = np.repeat(np.arange(self.nrows), np.diff(self.row_ptr))
+        m = rows == self.col
+        d[rows[m]] = self.val[m]
+        return d
+
+
+def _csr_from_ptr(p):
+    s = p.contents
+    n, nnz = s.nrows, s.nnz
+    rp = np.ctypeslib.as_array(s.row_ptr, shape=(n + 1,)).copy()
+    col = np.ctypeslib.as_array(s.col, shape=(max(nnz, 1),))[:nnz].copy()
+    val = np.ctypeslib.as_array(s.val, shape=(max(nnz, 1),))[:nnz].copy()
+    out = Csr(n, s.ncols, rp, col, val)
+    lib().or_free_csr(p)
+    return out
+
+
+def gauss_1d(n, lobatto=False):
+    x, w = np.zeros(n), np.zeros(n)
+    (lib().or_gauss_lobatto_1d if lobatto else lib().or_gauss_legendre_1d)(n, x, w)
+    return x, w
+
+
+def tensor_rule(dim, order, lobatto=False):
+    pts, w = np.zeros(3 * 4096), np.zeros(4096)
+    nq = lib().or_tensor_rule(int(lobatto), dim, order, pts, w)
+    return pts[:3 * nq].reshape(nq, 3), w[:nq]
+
+
+def triangle_rule(order):
+    pts, w = np.zeros(3 * 4096), np.zeros(4096)
+    nq = lib().or_triangle_rule(order, pts, w)
+    return pts[:3 * nq].reshape(nq, 3), w[:nq]
+
+
+def element_rule(topology, dim, p):
+    pts, w = np.zeros(3 * 4096), np.zeros(4096)
+    nq = lib().or_element_rule(topology, dim, p, pts, w)
+    return pts[:3 * nq].reshape(nq, 3), w[:nq]
+
+
+def local_nodes(topology, dim, p):
+    pts = np.zeros(3 * 512)
+    n = lib().or_local_nodes(topology, dim, p, pts)
+    return pts[:3 * n].reshape(n, 3)
+
+
+def shape_functions(topology, dim, p, qpts):
+    qpts = np.ascontiguousarray(qpts, dtype=np.float64).reshape(-1, 3)
+    nq = qpts.shape[0]
+    nen = local_nodes(topology, dim, p).shape[0]
+    N, dN = np.zeros(nq * nen), np.zeros(nq * nen * dim)
+    r = lib().or_shape_functions(topology, dim, p, qpts.ravel(), nq, N, dN)
+    assert r == nen
+    return N.reshape(nq, nen), dN.reshape(nq, nen, dim)
+
+
+class DofMap:
+    def __init__(self, ptr):
+        self._p = ptr
+        s = ptr.contents
+        self.n_nodes, self.n_cells = s.n_nodes, s.n_cells
+        self.nodes = np.ctypeslib.as_array(s.nodes, shape=(max(1, 3 * s.n_nodes),))[:3 * s.n_nodes].reshape(-1, 3).copy()
+        self.offsets = np.ctypeslib.as_array(s.offsets, shape=(s.n_cells + 1,)).copy()
+        ne = int(self.offsets[-1])
+        self.elements = np.ctypeslib.as_array(s.elements, shape=(max(ne, 1),))[:ne].copy()
+        self.topology = np.ctypeslib.as_array(s.topology, shape=(max(1, s.n_cells),))[:s.n_cells].copy()
+        self.topo_dim = np.ctypeslib.as_array(s.topo_dim, shape=(max(1, s.n_cells),))[:s.n_cells].copy()
+
+    def __del__(self):
+        if getattr(self, "_p", None) is not None and _LIB is not None:
+            _LIB.or_free_dofmap(self._p)
+            self._p = None
+
+
+def dofmanager(mesh, p):
+    nodes = np.ascontiguousarray(mesh["nodes"], dtype=np.float64).ravel()
+    cn = np.ascontiguousarray(mesh["cell_nodes"], dtype=np.int32)
+    off = np.ascontiguousarray(mesh["offsets"], dtype=np.int32)
+    ct = np.ascontiguousarray(mesh["cell_types"], dtype=np.int32)
+    ptr = lib().or_dofmanager(nodes, nodes.size // 3, cn, off, ct, ct.size, p)
+    if not ptr:
+        raise RuntimeError("DoFManager: Invalid polynomial order")
+    return DofMap(ptr)
+
+
+def assemble(dm, dpn, nsd, physics, params, residual=True):
+    params = np.zeros(8) if params is None else np.ascontiguousarray(
+        np.pad(np.asarray(params, dtype=np.float64), (0, max(0, 8 - len(params)))), dtype=np.float64)
+    R = np.zeros(dm.n_nodes * dpn) if residual else None
+    p = lib().or_assemble(dm._p, dpn, nsd, physics, params,
+                          R.ctypes.data_as(C.c_void_p) if R is not None else None)
+    return _csr_from_ptr(p), R
+
+
+def dirichlet_apply(A, rhs, mask, vals):
+    s = A._struct()
+    lib().or_dirichlet_apply(C.byref(s), rhs, np.ascontiguousarray(mask, dtype=np.uint8),
+                             np.ascontiguousarray(vals, dtype=np.float64))
+
+
+def csr_from_triplets(r, c, v):
+    r = np.ascontiguousarray(r, dtype=np.int64)
+    c = np.ascontiguousarray(c, dtype=np.int64)
+    v = np.ascontiguousarray(v, dtype=np.float64)
+    return _csr_from_ptr(lib().or_csr_from_triplets(r, c, v, r.size))
+
+
+def bcsr_from_triplets(block, r, c, v):
+    r = np.ascontiguousarray(r, dtype=np.int64)
+    c = np.ascontiguousarray(c, dtype=np.int64)
+    v = np.ascontiguousarray(v, dtype=np.float64)
+    p = lib().or_bcsr_from_triplets(block, r, c, v, r.size)
+    s = p.contents
+    nb = s.nnzb
+    out = dict(block=block, nbrows=s.nbrows, nbcols=s.nbcols, nnzb=nb,
+               brow_ptr=np.ctypeslib.as_array(s.brow_ptr, shape=(s.nbrows + 1,)).copy(),
+               bcol=np.ctypeslib.as_array(s.bcol, shape=(max(nb, 1),))[:nb].copy(),
+               val=np.ctypeslib.as_array(s.val, shape=(max(nb * block * block, 1),))[:nb * block * block].copy())
+    lib().or_free_bcsr(p)
+    return out
+
+
+def bcsr_spmv(B, x):
+    s = _Bcsr(B["block"], B["nbrows"], B["nbcols"], B["nnzb"],
+              B["brow_ptr"].ctypes.data_as(C.POINTER(C.c_int64)),
+              B["bcol"].ctypes.data_as(C.POINTER(C.c_int64)),
+              B["val"].ctypes.data_as(C.POINTER(C.c_double)))
+    y = np.zeros(B["nbrows"] * B["block"])
+    lib().or_bcsr_spmv(C.byref(s), np.ascontiguousarray(x, dtype=np.float64), y)
+    return y
+
+
+def ilu0(A):
+    s = A._struct()
+    return _csr_from_ptr(lib().or_ilu0(C.byref(s)))
+
+
+def ilu_solve(F, z):
+    z = np.ascontiguousarray(z, dtype=np.float64).copy()
+    s = F._struct()
+    lib().or_ilu_solve(C.byref(s), z)
+    return z
+
+
+def cg(A, b, x0=None, precond=PRECOND_NONE, criterion=CRIT_RELRES, tol=1e-10, maxiter=0):
+    x = np.zeros(A.nrows) if x0 is None else np.ascontiguousarray(x0, dtype=np.float64).copy()
+    rr = C.c_double(0)
+    s = A._struct()
+    it = lib().or_cg(C.byref(s), np.ascontiguousarray(b, dtype=np.float64), x, precond, criterion,
+                     tol, maxiter, C.byref(rr))
+    return x, int(it), rr.value
+
+
+def bicgstab(A, b, x0=None, criterion=CRIT_RELRES, tol=1e-10, maxiter=0):
+    x = np.zeros(A.nrows) if x0 is None else np.ascontiguousarray(x0, dtype=np.float64).copy()
+    rr = C.c_double(0)
+    s = A._struct()
+    it = lib().or_bicgstab(C.byref(s), np.ascontiguousarray(b, dtype=np.float64), x, criterion,
+                           tol, maxiter, C.byref(rr))
+    return x, int(it), rr.value
+
+
+def true_relres(A, b, x):
+    s = A._struct()
+    return lib().or_true_relres(C.byref(s), np.ascontiguousarray(b, dtype=np.float64),
+                                np.ascontiguousarray(x, dtype=np.float64))
+
+
+# ------------------------------------------------- the reference itself (_ref)
+
+class RefCsr:
+    """The reference's sparse_csr<double>, built from triplets by its own ctor."""
+
+    def __init__(self, r, c, v):
+        R = ref()
+        self._r, self._c, self._v = (np.ascontiguousarray(r, dtype=np.int64),
+                                     np.ascontiguousarray(c, dtype=np.int64),
+                                     np.ascontiguousarray(v, dtype=np.float64))
+        self.h = R.ref_csr_from_triplets(self._r, self._c, self._v, self._r.size)
+        a, b, n = C.c_int64(), C.c_int64(), C.c_int64()
+        R.ref_csr_info(self.h, C.byref(a), C.byref(b), C.byref(n))
+        self.nrows, self.ncols, self.nnz = a.value, b.value, n.value
+
+    def arrays(self):
+        rp = np.zeros(self.nrows + 1, np.int64)
+        col = np.zeros(max(self.nnz, 1), np.int64)
+        val = np.zeros(max(self.nnz, 1))
+        ref().ref_csr_get(self.h, rp, col, val)
+        return rp, col[:self.nnz], val[:self.nnz]
+
+    def spmv(self, x):
+        y = np.zeros(self.nrows)
+        ref().ref_csr_spmv(self.h, np.ascontiguousarray(x, dtype=np.float64), y)
+        return y
+
+    def cg(self, b, x0, tol):
+        x = np.ascontiguousarray(x0, dtype=np.float64).copy()
+        ref().ref_cg(self.h, np.ascontiguousarray(b, dtype=np.float64), x, tol)
+        return x
+
+    def pcg_jacobi(self, b, x0, tol):
+        x = np.ascontiguousarray(x0, dtype=np.float64).copy()
+        ref().ref_pcg_jacobi(self.h, np.ascontiguousarray(b, dtype=np.float64), x, tol)
+        return x
+
+    def pcg_ilu(self, b, x0, tol):
+        x = np.ascontiguousarray(x0, dtype=np.float64).copy()
+        ref().ref_pcg_ilu(self.h, np.ascontiguousarray(b, dtype=np.float64), x, tol)
+        return x
+
+    def bicgstab(self, b, x0):
+        x = np.ascontiguousarray(x0, dtype=np.float64).copy()
+        ref().ref_bicgstab(self.h, np.ascontiguousarray(b, dtype=np.float64), x)
+        return x
+
+    def ilu_factor_values(self):
+        h = ref().ref_ilu_factor(self.h)
+        rp = np.zeros(self.nrows + 1, np.int64)
+        col = np.zeros(max(self.nnz, 1), np.int64)
+        val = np.zeros(max(self.nnz, 1))
+        ref().ref_csr_get(h, rp, col, val)
+        ref().ref_csr_free(h)
+        return val[:self.nnz]
+
+    def __del__(self):
+        if getattr(self, "h", None) and _REF is not None:
+            _REF.ref_csr_free(self.h)
+            self.h = None
+
+
+def csr_to_triplets(A):
+    rows = np.repeat(np.arange(A.nrows, dtype=np.int64), np.diff(A.row_ptr))
+    return rows, A.col.copy(), A.val.copy()

@@ -1,0 +1,146 @@
+"""Generate the golden fixtures in this directory from the reference's own code.
+
+Run here (where the reference tree exists and oracle/_ref is built):
+    python tests/golden/make_golden.py
+The fixtures hold outputs of the reference's handmade linear algebra and
+quadrature (compiled in place by oracle/Makefile), on the inputs its own tests
+use (test/test_sparse_csr.cpp, test_sparse_bcsr.cpp, test_cg_solve.cpp,
+test_bicgstab_solve.cpp, test_ILU.cpp) and on a small assembled Poisson system.
+They pin the oracle without the reference tree being present.
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from oracle import oracle as O  # noqa: E402
+from yafel_b200 import meshgen  # noqa: E402
+
+
+def quadrature():
+    R = O.ref()
+    out = {}
+    for lob in (0, 1):
+        for n in range(2, 10 if lob == 0 else 11):  # the reference's GL loop never ends at n=10
+            x, w = np.zeros(n), np.zeros(n)
+            R.ref_gauss_1d(lob, n, x, w)
+            out["g1d_%d_%d_x" % (lob, n)] = x
+            out["g1d_%d_%d_w" % (lob, n)] = w
+    for dim in (1, 2, 3):
+        for order in range(1, 10):
+            p, w = np.zeros(3 * 4096), np.zeros(4096)
+            nq = R.ref_tensor_rule(0, dim, order, p, w)
+            out["tp_%d_%d_p" % (dim, order)] = p[:3 * nq].reshape(nq, 3)
+            out["tp_%d_%d_w" % (dim, order)] = w[:nq]
+    for order in range(1, 7):
+        p, w = np.zeros(3 * 256), np.zeros(256)
+        nq = R.ref_triangle_rule(order, p, w)
+        out["tri_%d_p" % order] = p[:3 * nq].reshape(nq, 3)
+        out["tri_%d_w" % order] = w[:nq]
+    np.savez_compressed(os.path.join(HERE, "quadrature.npz"), **out)
+
+
+def laplace_5pt(N):
+    """2D five-point Laplacian of test/test_ILU.cpp:13-33 (diag -4, neighbours 1)."""
+    NN = N * N
+    r, c, v = [], [], []
+    for i in range(NN):
+        r.append(i); c.append(i); v.append(-4.0)
+        if i >= 1: r.append(i); c.append(i - 1); v.append(1.0)
+        if i >= N: r.append(i); c.append(i - N); v.append(1.0)
+        if i < NN - 1: r.append(i); c.append(i + 1); v.append(1.0)
+        if i < NN - N: r.append(i); c.append(i + N); v.append(1.0)
+    return np.array(r), np.array(c), np.array(v)
+
+
+def linalg():
+    out = {}
+    rng = np.random.Generator(np.random.PCG64(20261203))
+    # test_sparse_csr.cpp test_3: accumulation into two nonzeros
+    N = 10
+    r = np.array([N - 1, 0] * N); c = r.copy(); v = np.ones(2 * N)
+    A = O.RefCsr(r, c, v)
+    out["dup_in"] = np.stack([r, c, v])
+    out["dup_rp"], out["dup_col"], out["dup_val"] = A.arrays()
+    # test_sparse_csr.cpp test_4: random integer matrix, seeded here
+    r = rng.integers(0, 20, 500); c = rng.integers(0, 20, 500); v = rng.integers(-10, 11, 500).astype(float)
+    A = O.RefCsr(r, c, v)
+    out["rand_in"] = np.stack([r, c, v])
+    out["rand_rp"], out["rand_col"], out["rand_val"] = A.arrays()
+    # test_sparse_bcsr.cpp test_1: 60x60 dense fill read back through BCSR<3>
+    ii, jj = np.meshgrid(np.arange(60), np.arange(60), indexing="ij")
+    r, c, v = ii.ravel(), jj.ravel(), (ii * 60 + jj).ravel().astype(float)
+    R = O.ref()
+    h = R.ref_bcsr_from_triplets(3, np.ascontiguousarray(r, np.int64), np.ascontiguousarray(c, np.int64),
+                                 np.ascontiguousarray(v), r.size)
+    import ctypes as C
+    nb, nnzb = C.c_int64(), C.c_int64()
+    R.ref_bcsr_info(3, h, C.byref(nb), C.byref(nnzb))
+    brp = np.zeros(nb.value + 1, np.int64); bcol = np.zeros(nnzb.value, np.int64); bval = np.zeros(9 * nnzb.value)
+    R.ref_bcsr_get(3, h, brp, bcol, bval)
+    x = rng.standard_normal(60)
+    y = np.zeros(60)
+    R.ref_bcsr_spmv(3, h, x, y)
+    R.ref_bcsr_free(3, h)
+    out["bcsr60_rp"], out["bcsr60_col"], out["bcsr60_val"] = brp, bcol, bval
+    out["bcsr60_x"], out["bcsr60_y"] = x, y
+    # test_cg_solve.cpp / test_bicgstab_solve.cpp test_2: tridiag(1,-2,1), x_ref = i
+    N = 10
+    r = list(range(N)) + list(range(1, N)) + list(range(0, N - 1))
+    c = list(range(N)) + list(range(0, N - 1)) + list(range(1, N))
+    v = [-2.0] * N + [1.0] * (2 * (N - 1))
+    A = O.RefCsr(r, c, v)
+    b = A.spmv(np.arange(N, dtype=float))
+    out["lap_in"] = np.stack([np.array(r), np.array(c), np.array(v)])
+    out["lap_b"] = b
+    out["lap_cg"] = A.cg(b, np.zeros(N), 1e-14)
+    out["lap_bicgstab"] = A.bicgstab(b, np.zeros(N))
+    # test_cg_solve.cpp test_1: identity with integer rhs -> exact
+    rhs = rng.integers(0, 100, 10).astype(float)
+    A = O.RefCsr(np.arange(10), np.arange(10), np.ones(10))
+    out["ident_b"] = rhs
+    out["ident_cg"] = A.cg(rhs, np.zeros(10), 1e-14)
+    # test_ILU.cpp: ILU(0) factors of the 5x5-grid Laplacian
+    r, c, v = laplace_5pt(5)
+    A = O.RefCsr(r, c, v)
+    out["ilu5_in"] = np.stack([r, c, v])
+    out["ilu5_lu"] = A.ilu_factor_values()
+    z = rng.standard_normal(25)
+    out["ilu5_z"] = z
+    zz = z.copy(); O.ref().ref_ilu_apply(A.h, zz)
+    out["ilu5_apply"] = zz
+    np.savez_compressed(os.path.join(HERE, "linalg.npz"), **out)
+
+
+def poisson_system():
+    """8x8 Q1 Poisson (SPD sign, f=1), Dirichlet u=0 on the boundary, assembled by
+    the oracle; solved by the reference's pcg_solve (Jacobi and ILU) and cg_solve."""
+    m = meshgen.structured_quad(8, 8, order="tensor")
+    dm = O.dofmanager(m, 1)
+    K, R = O.assemble(dm, 1, 2, O.POISSON, [1.0, 1.0])
+    X = dm.nodes
+    mask = ((np.abs(X[:, 0]) < 1e-9) | (np.abs(X[:, 0] - 1) < 1e-9) |
+            (np.abs(X[:, 1]) < 1e-9) | (np.abs(X[:, 1] - 1) < 1e-9)).astype(np.uint8)
+    O.dirichlet_apply(K, R, mask, np.zeros(K.nrows))
+    r, c, v = O.csr_to_triplets(K)
+    A = O.RefCsr(r, c, v)
+    out = {"rp": K.row_ptr, "col": K.col, "val": K.val, "b": R, "mask": mask}
+    out["pcg_jacobi"] = A.pcg_jacobi(R, np.zeros(K.nrows), 1e-20)
+    out["pcg_ilu"] = A.pcg_ilu(R, np.zeros(K.nrows), 1e-20)
+    out["cg"] = A.cg(R, np.zeros(K.nrows), 1e-20)
+    out["ilu_lu"] = A.ilu_factor_values()
+    np.savez_compressed(os.path.join(HERE, "poisson8.npz"), **out)
+
+
+if __name__ == "__main__":
+    O.build()
+    if not O.ref_available():
+        sys.exit("oracle/_ref/libyafel_ref.so is missing: build it where the reference tree exists")
+    quadrature()
+    linalg()
+    poisson_system()
+    print("golden fixtures written to", HERE)

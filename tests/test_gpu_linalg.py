@@ -1,0 +1,201 @@
+"""GPU parity of the sparse linear algebra (CUDA path through the C ABI) against
+the oracle and the reference's own outputs."""
+import os
+
+import numpy as np
+import pytest
+
+import yafel_b200 as yb
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def gold(name):
+    return np.load(os.path.join(GOLD, name))
+
+
+def random_block_matrix(nb, B, per_row, seed):
+    rng = np.random.Generator(np.random.PCG64(seed))
+    rows, cols = [], []
+    for i in range(nb):
+        cs = np.unique(np.concatenate([[i], rng.integers(0, nb, per_row)]))
+        rows.append(np.full(cs.size, i))
+        cols.append(cs)
+    brow = np.concatenate(rows)
+    bcol = np.concatenate(cols)
+    rp = np.concatenate([[0], np.cumsum([c.size for c in cols])]).astype(np.int64)
+    val = rng.standard_normal(bcol.size * B * B)
+    return rp, bcol.astype(np.int64), val
+
+
+def bcsr_to_oracle_csr(rp, col, val, B):
+    nb = rp.size - 1
+    brow = np.repeat(np.arange(nb), np.diff(rp))
+    i = np.arange(B)
+    r = (brow[:, None, None] * B + i[None, :, None]).repeat(B, axis=2).ravel()
+    c = (col[:, None, None] * B + i[None, None, :]).repeat(B, axis=1).ravel()
+    return O.csr_from_triplets(r, c, val)
+
+
+@pytest.mark.parametrize("B,per_row", [(1, 3), (1, 40), (2, 9), (3, 5), (3, 70)])
+def test_spmv_matches_oracle(ctx, B, per_row):
+    rp, col, val = random_block_matrix(3000, B, per_row, seed=B * 100 + per_row)
+    A = yb.sparse_bcsr.from_bcsr(B, rp, col, val) if B > 1 else yb.sparse_csr.from_csr(rp, col, val)
+    Ao = bcsr_to_oracle_csr(rp, col, val, B)
+    x = np.random.Generator(np.random.PCG64(7)).standard_normal(A.cols())
+    y = A * x
+    yo = Ao.spmv(x)
+    scale = np.abs(val).max() * np.abs(x).max() * (per_row + 1) * B
+    assert np.abs(y - yo).max() <= 1e-14 * scale
+    # determinism: same bits twice
+    assert np.array_equal(y, A * x)
+
+
+@pytest.mark.parametrize("B", [1, 3])
+def test_spmv_mixed_precision(ctx, B):
+    rp, col, val = random_block_matrix(2000, B, 20, seed=3 + B)
+    A = yb.sparse_bcsr.from_bcsr(B, rp, col, val) if B > 1 else yb.sparse_csr.from_csr(rp, col, val)
+    x = np.random.Generator(np.random.PCG64(9)).standard_normal(A.cols())
+    y32 = A.spmv(x, precision=yb.PREC_MIXED).numpy()
+    Ao = bcsr_to_oracle_csr(rp, col, val.astype(np.float32).astype(np.float64), B)
+    yo = Ao.spmv(x)
+    assert np.abs(y32 - yo).max() <= 1e-13 * np.abs(yo).max()
+
+
+def test_sparse_csr_from_triplets_matches_reference(ctx):
+    g = gold("linalg.npz")
+    for key in ("dup", "rand"):
+        r, c, v = g[key + "_in"]
+        A = yb.sparse_csr((r.astype(np.uint64), c.astype(np.uint64), v))
+        rp, col, val = A.arrays()
+        assert np.array_equal(rp, g[key + "_rp"])
+        assert np.array_equal(col, g[key + "_col"])
+        assert np.array_equal(val, g[key + "_val"])
+    # test_sparse_csr.cpp test_1/test_3 sizes
+    A = yb.sparse_csr([(9, 9, 1.0), (0, 0, 1.0)] * 10)
+    assert A.rows() == 10 and A.cols() == 10 and A.nnz() == 2
+
+
+def test_sparse_bcsr_from_triplets_matches_reference(ctx):
+    g = gold("linalg.npz")
+    ii, jj = np.meshgrid(np.arange(60), np.arange(60), indexing="ij")
+    A = yb.sparse_bcsr(3, (ii.ravel().astype(np.uint64), jj.ravel().astype(np.uint64),
+                           (ii * 60 + jj).ravel().astype(float)))
+    rp, col, val = A.arrays()
+    assert np.array_equal(rp, g["bcsr60_rp"]) and np.array_equal(col, g["bcsr60_col"])
+    assert np.array_equal(val, g["bcsr60_val"])
+    y = A * g["bcsr60_x"]
+    assert np.allclose(y, g["bcsr60_y"], rtol=1e-14, atol=1e-10)
+    # sparse_bcsr.hpp: rows rounded to whole blocks (test_sparse_bcsr.cpp test_2/test_3)
+    B = yb.sparse_bcsr(3, [(59, 59, 1.0), (0, 0, 1.0)] * 60)
+    assert B.rows() == 60 and B.cols() == 60
+    rp, col, val = B.arrays()
+    assert val[0] == 60.0 and val[-1] == 60.0
+
+
+def test_cg_reference_tests(ctx):
+    g = gold("linalg.npz")
+    # test_cg_solve.cpp test_1: identity matrix returns the rhs exactly
+    I = yb.sparse_csr((np.arange(10, dtype=np.uint64), np.arange(10, dtype=np.uint64), np.ones(10)))
+    x = yb.cg_solve(I, g["ident_b"])
+    assert np.array_equal(x, g["ident_b"])
+    # test_2: tridiag(1,-2,1), ||x - x_ref||^2 < 1e-10
+    r, c, v = g["lap_in"]
+    A = yb.sparse_csr((r.astype(np.uint64), c.astype(np.uint64), v))
+    x = yb.cg_solve(A, g["lap_b"])
+    assert np.sum((x - np.arange(10)) ** 2) < 1e-10
+    assert np.allclose(x, g["lap_cg"], rtol=1e-10, atol=1e-10)
+    x = yb.bicgstab_solve(A, g["lap_b"])
+    assert np.sum((x - np.arange(10)) ** 2) < 1e-10
+
+
+def test_pcg_jacobi_ilu_match_reference_on_poisson(ctx):
+    g = gold("poisson8.npz")
+    A = yb.sparse_csr.from_csr(g["rp"], g["col"], g["val"])
+    M = yb.JacobiPreconditioner(A)
+    x = yb.pcg_solve(A, g["b"], M, np.zeros(A.rows()), 1e-20)
+    assert np.abs(x - g["pcg_jacobi"]).max() <= 1e-12 * np.abs(g["pcg_jacobi"]).max()
+    x = yb.cg_solve(A, g["b"], np.zeros(A.rows()), 1e-20)
+    assert np.abs(x - g["cg"]).max() <= 1e-12 * np.abs(g["cg"]).max()
+    L = yb.ILUPreconditioner(A)
+    x = yb.pcg_solve(A, g["b"], L, np.zeros(A.rows()), 1e-20)
+    assert np.abs(x - g["pcg_ilu"]).max() <= 1e-12 * np.abs(g["pcg_ilu"]).max()
+
+
+def test_ilu_apply_matches_reference(ctx):
+    g = gold("linalg.npz")
+    r, c, v = g["ilu5_in"]
+    A = yb.sparse_csr((r.astype(np.uint64), c.astype(np.uint64), v))
+    L = yb.ILUPreconditioner(A)
+    z = g["ilu5_z"].copy()
+    L.solve(z)
+    assert np.allclose(z, g["ilu5_apply"], rtol=1e-13, atol=1e-14)
+    assert L.zero_pivots == 0
+
+
+def test_jacobi_zero_diagonal_gives_inf_like_reference(ctx):
+    A = yb.sparse_csr([(0, 0, 2.0), (1, 1, 0.0), (0, 1, 1.0)])
+    M = yb.JacobiPreconditioner(A)
+    assert M.zero_pivots == 1
+    z = np.array([1.0, 1.0])
+    M.solve(z)
+    assert z[0] == 0.5 and np.isinf(z[1])
+
+
+@pytest.mark.parametrize("precond", [None, "jacobi", "ilu"])
+def test_relres_solve_reaches_1e10_and_matches_oracle(ctx, precond):
+    from yafel_b200 import meshgen
+    dm = O.dofmanager(meshgen.structured_quad(24, 24, order="tensor"), 1)
+    K, R = O.assemble(dm, 1, 2, O.POISSON, [1.0, 1.0])
+    X = dm.nodes
+    mask = ((X[:, 0] < 1e-9) | (X[:, 0] > 1 - 1e-9) | (X[:, 1] < 1e-9) | (X[:, 1] > 1 - 1e-9)).astype(np.uint8)
+    O.dirichlet_apply(K, R, mask, np.zeros(K.nrows))
+    A = yb.sparse_csr.from_csr(K.row_ptr, K.col, K.val)
+    M = None if precond is None else (yb.JacobiPreconditioner(A) if precond == "jacobi" else yb.ILUPreconditioner(A))
+    x, st = yb.solve(A, R, M=M, tol=1e-10)
+    assert st.status == 0 and st.rel_residual <= 1e-10
+    xs = x.numpy()
+    assert O.true_relres(K, R, xs) <= 1e-10
+    xo, _, _ = O.cg(K, R, precond={None: 0, "jacobi": 1, "ilu": 2}[precond], tol=1e-12)
+    assert np.linalg.norm(xs - xo) <= 1e-8 * np.linalg.norm(xo)
+
+
+def test_mixed_precision_refinement_reaches_1e10(ctx):
+    from yafel_b200 import meshgen
+    dm = O.dofmanager(meshgen.structured_hex(6, 6, 6, order="ccw"), 2)
+    K, _ = O.assemble(dm, 3, 3, O.ELASTICITY, [1.0, 0.5769230769230769, 0.3846153846153846])
+    X = dm.nodes
+    n = K.nrows
+    rng = np.random.Generator(np.random.PCG64(1))
+    b = rng.standard_normal(n)
+    mask = np.zeros(n, np.uint8)
+    clamp = np.nonzero(X[:, 0] < 1e-9)[0]
+    for c in range(3):
+        mask[clamp * 3 + c] = 1
+    O.dirichlet_apply(K, b, mask, np.zeros(n))
+    Bm = O.bcsr_from_triplets(3, *O.csr_to_triplets(K))
+    A = yb.sparse_bcsr.from_bcsr(3, Bm["brow_ptr"], Bm["bcol"], Bm["val"])
+    M = yb.JacobiPreconditioner(A)
+    x64, s64 = yb.solve(A, b, M=M, tol=1e-10)
+    xmx, smx = yb.solve(A, b, M=M, tol=1e-10, precision=yb.PREC_MIXED)
+    assert s64.status == 0 and smx.status == 0
+    assert s64.rel_residual <= 1e-10 and smx.rel_residual <= 1e-10
+    assert O.true_relres(K, b, xmx.numpy()) <= 1e-10
+    assert smx.refinements >= 1
+
+
+def test_bicgstab_relres_nonsymmetric(ctx):
+    from yafel_b200 import meshgen
+    dm = O.dofmanager(meshgen.structured_quad(20, 20, order="tensor"), 1)
+    K, R = O.assemble(dm, 1, 2, O.SUPG, [0.01, 0.05, 1.0, 0.0])
+    X = dm.nodes
+    b = np.sin(3 * X[:, 0]) + X[:, 1]
+    mask = ((X[:, 0] < 1e-9) | (X[:, 1] < 1e-9) | (X[:, 1] > 1 - 1e-9)).astype(np.uint8)
+    O.dirichlet_apply(K, b, mask, np.zeros(K.nrows))
+    A = yb.sparse_csr.from_csr(K.row_ptr, K.col, K.val)
+    for M in (None, yb.JacobiPreconditioner(A)):
+        x, st = yb.solve(A, b, M=M, method="bicgstab", tol=1e-10)
+        assert st.status == 0 and st.rel_residual <= 1e-10
+        assert O.true_relres(K, b, x.numpy()) <= 1e-10

@@ -1,0 +1,458 @@
+// capi.cu -- context, error reporting, device vectors and matrix import/export
+// of the C ABI declared in include/yafel_gpu.h.
+#include "internal.h"
+#include "device_common.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstring>
+#include <numeric>
+
+namespace yg {
+
+static thread_local std::string g_last_error;
+
+void set_error(const char *fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+}
+
+yg_status fail(yg_status s, const char *fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return s;
+}
+
+yg_status dev_alloc(yg_context ctx, void **p, size_t bytes) {
+    *p = nullptr;
+    if (bytes == 0) bytes = 16;
+    if (ctx->budget && ctx->in_use + bytes > ctx->budget)
+        return fail(YG_OVER_BUDGET, "allocation of %zu bytes exceeds the HBM budget (%llu of %llu in use)",
+                    bytes, (unsigned long long)ctx->in_use, (unsigned long long)ctx->budget);
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        *p = nullptr;
+        return fail(YG_OUT_OF_MEMORY, "cudaMalloc(%zu) failed: %s", bytes, cudaGetErrorString(e));
+    }
+    ctx->in_use += bytes;
+    ctx->allocs[*p] = bytes;
+    return YG_OK;
+}
+
+void dev_free(yg_context ctx, void *p) {
+    if (!p) return;
+    auto it = ctx->allocs.find(p);
+    if (it != ctx->allocs.end()) {
+        ctx->in_use -= it->second;
+        ctx->allocs.erase(it);
+    }
+    cudaFree(p);
+}
+
+// ------------------------------------------------------------ small kernels
+
+__global__ void k_fill(double *__restrict__ v, int64_t n, double val) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        v[i] = val;
+}
+
+__global__ void k_axpy(double alpha, const double *__restrict__ x, double *__restrict__ y, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        y[i] += alpha * x[i];
+}
+
+__global__ void __launch_bounds__(kThreads) k_dot_partials(const double *__restrict__ a, const double *__restrict__ b,
+                                                           int64_t n, double *__restrict__ partials) {
+    __shared__ double sm[kThreads / 32];
+    double s = 0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        s += a[i] * b[i];
+    s = block_sum<kThreads>(s, sm);
+    if (threadIdx.x == 0) partials[blockIdx.x] = s;
+}
+
+__global__ void __launch_bounds__(kThreads) k_sum_partials(const double *__restrict__ partials, int np,
+                                                           double *__restrict__ out) {
+    __shared__ double sm[kThreads / 32];
+    double s = 0;
+    for (int i = threadIdx.x; i < np; i += blockDim.x) s += partials[i];
+    s = block_sum<kThreads>(s, sm);
+    if (threadIdx.x == 0) out[0] = s;
+}
+
+__global__ void k_find_diag(int64_t nbrows, const int32_t *__restrict__ rowptr, const int32_t *__restrict__ col,
+                            int32_t *__restrict__ diag) {
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < nbrows; r += (int64_t)gridDim.x * blockDim.x) {
+        int lo = rowptr[r], hi = rowptr[r + 1] - 1, pos = -1;
+        while (lo <= hi) {
+            int mid = (lo + hi) >> 1;
+            int c = col[mid];
+            if (c == r) { pos = mid; break; }
+            if (c < r) lo = mid + 1; else hi = mid - 1;
+        }
+        diag[r] = pos;
+    }
+}
+
+__global__ void k_to_fp32(const double *__restrict__ v, float *__restrict__ o, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        o[i] = (float)v[i];
+}
+
+int stream_grid(yg_context ctx, int64_t n) {
+    int64_t g = (n + kThreads - 1) / kThreads;
+    int64_t cap = (int64_t)ctx->num_sms * 8;
+    if (g > cap) g = cap;
+    if (g < 1) g = 1;
+    return (int)g;
+}
+
+yg_status vector_dot(yg_context ctx, const double *a, const double *b, int64_t n, double *out) {
+    int g = stream_grid(ctx, n);
+    if (g > kMaxReduceBlocks) g = kMaxReduceBlocks;
+    k_dot_partials<<<g, kThreads, 0, ctx->stream>>>(a, b, n, ctx->d_partials);
+    YG_LAUNCHED(ctx);
+    k_sum_partials<<<1, kThreads, 0, ctx->stream>>>(ctx->d_partials, g, ctx->d_partials + kMaxReduceBlocks);
+    YG_LAUNCHED(ctx);
+    YG_CUDA(cudaGetLastError());
+    YG_CUDA(cudaMemcpyAsync(ctx->h_pinned, ctx->d_partials + kMaxReduceBlocks, sizeof(double),
+                            cudaMemcpyDeviceToHost, ctx->stream));
+    YG_CUDA(cudaStreamSynchronize(ctx->stream));
+    *out = ctx->h_pinned[0];
+    return YG_OK;
+}
+
+yg_status matrix_build_diag(yg_matrix A) {
+    yg_context ctx = A->ctx;
+    if (!A->d_diag) YG_TRY(dev_alloc_t(ctx, &A->d_diag, A->nbrows + 1));
+    k_find_diag<<<stream_grid(ctx, A->nbrows), kThreads, 0, ctx->stream>>>(A->nbrows, A->d_rowptr, A->d_col, A->d_diag);
+    YG_LAUNCHED(ctx);
+    YG_CUDA(cudaGetLastError());
+    return YG_OK;
+}
+
+// Upload a host block-CSR (int64 indices) into a new device matrix.
+static yg_status upload_bcsr(yg_context ctx, int32_t block, int64_t nbrows, int64_t nbcols,
+                             const std::vector<int64_t> &rp, const std::vector<int64_t> &col,
+                             const double *vals, yg_matrix *out) {
+    int64_t nnzb = rp[nbrows];
+    if (nnzb >= INT32_MAX || nbrows >= INT32_MAX || nbcols >= INT32_MAX)
+        return fail(YG_UNSUPPORTED, "matrix too large for 32-bit indices (nnzb=%lld)", (long long)nnzb);
+    if ((int64_t)nnzb * block * block >= ((int64_t)1 << 40))
+        return fail(YG_UNSUPPORTED, "matrix too large");
+    auto *A = new yg_matrix_t();
+    A->ctx = ctx;
+    A->block = block;
+    A->nbrows = nbrows;
+    A->nbcols = nbcols;
+    A->nnzb = nnzb;
+    std::vector<int32_t> rp32(nbrows + 1), col32(nnzb);
+    for (int64_t i = 0; i <= nbrows; ++i) rp32[i] = (int32_t)rp[i];
+    for (int64_t i = 0; i < nnzb; ++i) col32[i] = (int32_t)col[i];
+    yg_status s;
+    if ((s = dev_alloc_t(ctx, &A->d_rowptr, nbrows + 1)) != YG_OK ||
+        (s = dev_alloc_t(ctx, &A->d_col, nnzb)) != YG_OK ||
+        (s = dev_alloc_t(ctx, &A->d_val, nnzb * block * block)) != YG_OK) {
+        yg_matrix_destroy(A);
+        return s;
+    }
+    cudaMemcpyAsync(A->d_rowptr, rp32.data(), sizeof(int32_t) * (nbrows + 1), cudaMemcpyHostToDevice, ctx->stream);
+    cudaMemcpyAsync(A->d_col, col32.data(), sizeof(int32_t) * nnzb, cudaMemcpyHostToDevice, ctx->stream);
+    cudaMemcpyAsync(A->d_val, vals, sizeof(double) * nnzb * block * block, cudaMemcpyHostToDevice, ctx->stream);
+    if ((s = matrix_build_diag(A)) != YG_OK) { yg_matrix_destroy(A); return s; }
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) { yg_matrix_destroy(A); return fail(YG_CUDA_ERROR, "upload: %s", cudaGetErrorString(e)); }
+    spmv_autotune(A);
+    *out = A;
+    return YG_OK;
+}
+
+}  // namespace yg
+
+using namespace yg;
+
+// ================================================================ context
+
+extern "C" yg_status yg_context_create(int32_t device, uint64_t hbm_budget_bytes, yg_context *out) {
+    if (!out) return fail(YG_BAD_ARG, "yg_context_create: out is NULL");
+    *out = nullptr;
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0)
+        return fail(YG_CUDA_ERROR, "no CUDA device available (%s)", cudaGetErrorString(e));
+    if (device < 0 || device >= ndev) return fail(YG_BAD_ARG, "device %d out of range (%d devices)", device, ndev);
+    YG_CUDA(cudaSetDevice(device));
+    auto *ctx = new yg_context_t();
+    ctx->device = device;
+    ctx->budget = hbm_budget_bytes;
+    cudaDeviceProp prop;
+    YG_CUDA(cudaGetDeviceProperties(&prop, device));
+    ctx->num_sms = prop.multiProcessorCount;
+    ctx->reduce_blocks = ctx->num_sms * 4;
+    YG_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    yg_status s;
+    if ((s = dev_alloc_t(ctx, &ctx->d_partials, 8 * kMaxReduceBlocks)) != YG_OK ||
+        (s = dev_alloc_t(ctx, &ctx->d_scalars, 4)) != YG_OK) {
+        yg_context_destroy(ctx);
+        return s;
+    }
+    e = cudaMallocHost(&ctx->h_pinned, 64 * sizeof(double));
+    if (e != cudaSuccess) {
+        yg_context_destroy(ctx);
+        return fail(YG_OUT_OF_MEMORY, "cudaMallocHost: %s", cudaGetErrorString(e));
+    }
+    *out = ctx;
+    return YG_OK;
+}
+
+extern "C" yg_status yg_context_destroy(yg_context ctx) {
+    if (!ctx) return YG_OK;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    for (auto &kv : ctx->allocs) cudaFree(kv.first);
+    ctx->allocs.clear();
+    if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return YG_OK;
+}
+
+extern "C" yg_status yg_context_synchronize(yg_context ctx) {
+    if (!ctx) return fail(YG_BAD_ARG, "NULL context");
+    YG_CUDA(cudaStreamSynchronize(ctx->stream));
+    return YG_OK;
+}
+
+extern "C" yg_status yg_context_memory(yg_context ctx, uint64_t *in_use, uint64_t *budget) {
+    if (!ctx) return fail(YG_BAD_ARG, "NULL context");
+    if (in_use) *in_use = ctx->in_use;
+    if (budget) *budget = ctx->budget;
+    return YG_OK;
+}
+
+extern "C" int64_t yg_context_launches(yg_context ctx) { return ctx ? ctx->launches : 0; }
+
+extern "C" const char *yg_last_error(void) { return g_last_error.c_str(); }
+
+extern "C" const char *yg_status_string(yg_status s) {
+    switch (s) {
+    case YG_OK: return "ok";
+    case YG_NOT_CONVERGED: return "not converged";
+    case YG_BREAKDOWN: return "breakdown";
+    case YG_NAN: return "non-finite value";
+    case YG_TIMEOUT: return "timeout";
+    case YG_OUT_OF_MEMORY: return "out of memory";
+    case YG_OVER_BUDGET: return "over HBM budget";
+    case YG_BAD_ARG: return "bad argument";
+    case YG_CUDA_ERROR: return "CUDA error";
+    case YG_UNSUPPORTED: return "unsupported";
+    case YG_ZERO_PIVOT: return "zero pivot";
+    }
+    return "unknown status";
+}
+
+// ================================================================ vectors
+
+extern "C" yg_status yg_vector_create(yg_context ctx, int64_t n, yg_vector *out) {
+    if (!ctx || !out || n < 0) return fail(YG_BAD_ARG, "yg_vector_create: bad argument");
+    auto *v = new yg_vector_t();
+    v->ctx = ctx;
+    v->n = n;
+    yg_status s = dev_alloc_t(ctx, &v->d, n > 0 ? n : 1);
+    if (s != YG_OK) { delete v; return s; }
+    cudaMemsetAsync(v->d, 0, sizeof(double) * (n > 0 ? n : 1), ctx->stream);
+    *out = v;
+    return YG_OK;
+}
+
+extern "C" yg_status yg_vector_destroy(yg_vector v) {
+    if (!v) return YG_OK;
+    dev_free(v->ctx, v->d);
+    delete v;
+    return YG_OK;
+}
+
+extern "C" int64_t yg_vector_size(yg_vector v) { return v ? v->n : -1; }
+
+extern "C" yg_status yg_vector_upload(yg_vector v, const double *host, int64_t n) {
+    if (!v || (!host && n) || n != v->n) return fail(YG_BAD_ARG, "yg_vector_upload: size %lld != %lld", (long long)n, v ? (long long)v->n : -1LL);
+    YG_CUDA(cudaMemcpyAsync(v->d, host, sizeof(double) * n, cudaMemcpyHostToDevice, v->ctx->stream));
+    YG_CUDA(cudaStreamSynchronize(v->ctx->stream));
+    return YG_OK;
+}
+
+extern "C" yg_status yg_vector_download(yg_vector v, double *host, int64_t n) {
+    if (!v || (!host && n) || n != v->n) return fail(YG_BAD_ARG, "yg_vector_download: size mismatch");
+    YG_CUDA(cudaMemcpyAsync(host, v->d, sizeof(double) * n, cudaMemcpyDeviceToHost, v->ctx->stream));
+    YG_CUDA(cudaStreamSynchronize(v->ctx->stream));
+    return YG_OK;
+}
+
+extern "C" yg_status yg_vector_fill(yg_vector v, double value) {
+    if (!v) return fail(YG_BAD_ARG, "NULL vector");
+    k_fill<<<stream_grid(v->ctx, v->n), kThreads, 0, v->ctx->stream>>>(v->d, v->n, value);
+    YG_LAUNCHED(v->ctx);
+    YG_CUDA(cudaGetLastError());
+    return YG_OK;
+}
+
+extern "C" yg_status yg_vector_copy(yg_vector dst, yg_vector src) {
+    if (!dst || !src || dst->n != src->n) return fail(YG_BAD_ARG, "yg_vector_copy: size mismatch");
+    YG_CUDA(cudaMemcpyAsync(dst->d, src->d, sizeof(double) * src->n, cudaMemcpyDeviceToDevice, src->ctx->stream));
+    return YG_OK;
+}
+
+extern "C" yg_status yg_vector_dot(yg_vector a, yg_vector b, double *out) {
+    if (!a || !b || !out || a->n != b->n) return fail(YG_BAD_ARG, "yg_vector_dot: size mismatch");
+    return vector_dot(a->ctx, a->d, b->d, a->n, out);
+}
+
+extern "C" yg_status yg_vector_axpy(double alpha, yg_vector x, yg_vector y) {
+    if (!x || !y || x->n != y->n) return fail(YG_BAD_ARG, "yg_vector_axpy: size mismatch");
+    k_axpy<<<stream_grid(x->ctx, x->n), kThreads, 0, x->ctx->stream>>>(alpha, x->d, y->d, x->n);
+    YG_LAUNCHED(x->ctx);
+    YG_CUDA(cudaGetLastError());
+    return YG_OK;
+}
+
+// ================================================================ matrices
+
+extern "C" yg_status yg_matrix_from_triplets(yg_context ctx, int32_t block, const uint64_t *rows,
+                                             const uint64_t *cols, const double *vals, uint64_t n,
+                                             yg_matrix *out) {
+    if (!ctx || !out || block < 1 || block > 8 || (n && (!rows || !cols || !vals)))
+        return fail(YG_BAD_ARG, "yg_matrix_from_triplets: bad argument");
+    *out = nullptr;
+    if (n == 0) return fail(YG_BAD_ARG, "yg_matrix_from_triplets: empty triplet list (the reference does not support empty matrices)");
+    const int64_t B = block, B2 = B * B;
+    uint64_t maxr = 0, maxc = 0;
+    for (uint64_t i = 0; i < n; ++i) { maxr = std::max(maxr, rows[i]); maxc = std::max(maxc, cols[i]); }
+    int64_t nbrows = (int64_t)(maxr / B) + 1, nbcols = (int64_t)(maxc / B) + 1;
+    // Order: CSR sorts (row, col, value) so duplicates are summed in ascending
+    // value order (sparse_csr.hpp:103-104); BCSR sorts (I, J, i, j) and keeps
+    // the input order among duplicates.
+    std::vector<uint64_t> idx(n);
+    std::iota(idx.begin(), idx.end(), 0);
+    if (block == 1) {
+        std::sort(idx.begin(), idx.end(), [&](uint64_t a, uint64_t b) {
+            if (rows[a] != rows[b]) return rows[a] < rows[b];
+            if (cols[a] != cols[b]) return cols[a] < cols[b];
+            return vals[a] < vals[b];
+        });
+    } else {
+        std::stable_sort(idx.begin(), idx.end(), [&](uint64_t a, uint64_t b) {
+            uint64_t ka[4] = {rows[a] / B, cols[a] / B, rows[a] % B, cols[a] % B};
+            uint64_t kb[4] = {rows[b] / B, cols[b] / B, rows[b] % B, cols[b] % B};
+            for (int k = 0; k < 4; ++k) if (ka[k] != kb[k]) return ka[k] < kb[k];
+            return false;
+        });
+    }
+    std::vector<int64_t> rp(nbrows + 1, 0), col;
+    std::vector<double> val;
+    col.reserve(n);
+    val.reserve(n * (block == 1 ? 1 : 1));
+    int64_t curI = -1, curJ = -1;
+    for (uint64_t t = 0; t < n; ++t) {
+        uint64_t k = idx[t];
+        int64_t I = rows[k] / B, J = cols[k] / B;
+        if (I != curI || J != curJ) {
+            col.push_back(J);
+            val.resize(val.size() + B2, 0.0);
+            rp[I + 1]++;
+            curI = I; curJ = J;
+        }
+        val[(col.size() - 1) * B2 + (rows[k] % B) * B + (cols[k] % B)] += vals[k];
+    }
+    for (int64_t i = 0; i < nbrows; ++i) rp[i + 1] += rp[i];
+    return upload_bcsr(ctx, block, nbrows, nbcols, rp, col, val.data(), out);
+}
+
+extern "C" yg_status yg_matrix_from_csr(yg_context ctx, int32_t block, int64_t nbrows, int64_t nbcols,
+                                        const int64_t *brow_ptr, const int64_t *bcol, const double *vals,
+                                        yg_matrix *out) {
+    if (!ctx || !out || block < 1 || block > 8 || nbrows < 0 || !brow_ptr)
+        return fail(YG_BAD_ARG, "yg_matrix_from_csr: bad argument");
+    std::vector<int64_t> rp(brow_ptr, brow_ptr + nbrows + 1);
+    if (rp[0] != 0) return fail(YG_BAD_ARG, "yg_matrix_from_csr: row pointer must start at 0");
+    for (int64_t i = 0; i < nbrows; ++i)
+        if (rp[i + 1] < rp[i]) return fail(YG_BAD_ARG, "yg_matrix_from_csr: row pointer decreases at row %lld", (long long)i);
+    int64_t nnzb = rp[nbrows];
+    std::vector<int64_t> col(bcol, bcol + nnzb);
+    for (int64_t i = 0; i < nbrows; ++i)
+        for (int64_t k = rp[i]; k < rp[i + 1]; ++k) {
+            if (col[k] < 0 || col[k] >= nbcols) return fail(YG_BAD_ARG, "column %lld out of range in row %lld", (long long)col[k], (long long)i);
+            if (k > rp[i] && col[k] <= col[k - 1]) return fail(YG_BAD_ARG, "columns not strictly increasing in row %lld", (long long)i);
+        }
+    return upload_bcsr(ctx, block, nbrows, nbcols, rp, col, vals, out);
+}
+
+extern "C" yg_status yg_matrix_destroy(yg_matrix A) {
+    if (!A) return YG_OK;
+    yg_context ctx = A->ctx;
+    dev_free(ctx, A->d_rowptr);
+    dev_free(ctx, A->d_col);
+    dev_free(ctx, A->d_val);
+    dev_free(ctx, A->d_val32);
+    dev_free(ctx, A->d_diag);
+    delete A;
+    return YG_OK;
+}
+
+extern "C" yg_status yg_matrix_sizes(yg_matrix A, int64_t *rows, int64_t *cols, int64_t *nnz, int32_t *block) {
+    if (!A) return fail(YG_BAD_ARG, "NULL matrix");
+    if (rows) *rows = A->rows();
+    if (cols) *cols = A->cols();
+    if (nnz) *nnz = A->nnzb * A->block * A->block;
+    if (block) *block = A->block;
+    return YG_OK;
+}
+
+extern "C" yg_status yg_matrix_get(yg_matrix A, int64_t *brow_ptr, int64_t *bcol, double *vals) {
+    if (!A) return fail(YG_BAD_ARG, "NULL matrix");
+    yg_context ctx = A->ctx;
+    YG_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (brow_ptr) {
+        std::vector<int32_t> t(A->nbrows + 1);
+        YG_CUDA(cudaMemcpy(t.data(), A->d_rowptr, sizeof(int32_t) * (A->nbrows + 1), cudaMemcpyDeviceToHost));
+        for (int64_t i = 0; i <= A->nbrows; ++i) brow_ptr[i] = t[i];
+    }
+    if (bcol) {
+        std::vector<int32_t> t(A->nnzb);
+        YG_CUDA(cudaMemcpy(t.data(), A->d_col, sizeof(int32_t) * A->nnzb, cudaMemcpyDeviceToHost));
+        for (int64_t i = 0; i < A->nnzb; ++i) bcol[i] = t[i];
+    }
+    if (vals) YG_CUDA(cudaMemcpy(vals, A->d_val, sizeof(double) * A->nnzb * A->block * A->block, cudaMemcpyDeviceToHost));
+    return YG_OK;
+}
+
+extern "C" yg_status yg_matrix_make_fp32(yg_matrix A) {
+    if (!A) return fail(YG_BAD_ARG, "NULL matrix");
+    yg_context ctx = A->ctx;
+    int64_t n = A->nnzb * A->block * A->block;
+    if (!A->d_val32) YG_TRY(dev_alloc_t(ctx, &A->d_val32, n));
+    k_to_fp32<<<stream_grid(ctx, n), kThreads, 0, ctx->stream>>>(A->d_val, A->d_val32, n);
+    YG_LAUNCHED(ctx);
+    YG_CUDA(cudaGetLastError());
+    return YG_OK;
+}
+
+extern "C" yg_status yg_spmv_ex(yg_matrix A, yg_vector x, yg_vector y, int32_t precision) {
+    if (!A || !x || !y) return fail(YG_BAD_ARG, "yg_spmv: NULL argument");
+    if (x->n != A->cols() || y->n != A->rows())
+        return fail(YG_BAD_ARG, "yg_spmv: dimension mismatch (A %lldx%lld, x %lld, y %lld)", (long long)A->rows(),
+                    (long long)A->cols(), (long long)x->n, (long long)y->n);
+    if (precision == YG_PREC_MIXED && !A->d_val32) YG_TRY(yg_matrix_make_fp32(A));
+    return spmv_launch(A, x->d, y->d, precision, nullptr, nullptr, spmv_default_grid(A));
+}
+
+extern "C" yg_status yg_spmv(yg_matrix A, yg_vector x, yg_vector y) { return yg_spmv_ex(A, x, y, YG_PREC_FP64); }

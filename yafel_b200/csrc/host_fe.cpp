@@ -1,0 +1,491 @@
+// host_fe.cpp -- quadrature, reference elements, CG DoF numbering and element
+// colouring on the host.
+#include "host_fe.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+
+namespace yg {
+
+// Gauss-Legendre points: Newton on P_n from -cos(pi (i+0.75)/(n+0.5)) until
+// |P_n| <= 1e-15 (the reference's iteration, src/quadrature/QuadratureRule.cpp:66-106,
+// kept step for step so the points are bit-identical).
+void gauss_legendre_1d(int n, double *x, double *w) {
+    const double PI = std::atan2(1., 1.) * 4;
+    for (int i = 0; i < n; ++i) {
+        double xx = -std::cos(PI * (1 + i - 0.25) / (n + 0.5));
+        double Pold, Pn, Pnew, dP;
+        int guard = 0;
+        do {
+            Pold = 1;
+            Pn = xx;
+            for (int k = 2; k <= n; ++k) {
+                Pnew = ((2 * k - 1) * xx * Pn - (k - 1) * Pold) / k;
+                Pold = Pn;
+                Pn = Pnew;
+            }
+            dP = (n / (xx * xx - 1)) * (xx * Pn - Pold);
+            xx -= Pn / dP;
+        } while (std::fabs(Pn) > 1.0e-15 && ++guard < 200);
+        x[i] = xx;
+        w[i] = 2.0 / ((1 - xx * xx) * (dP * dP));
+    }
+}
+
+// Gauss-Lobatto points by the reference's fixed-point iteration
+// (src/quadrature/QuadratureRule.cpp:25-63).
+void gauss_lobatto_1d(int n, double *x, double *w) {
+    const double PI = std::atan2(1., 1.) * 4;
+    for (int i = 0; i < n; ++i) {
+        double xx = -std::cos((PI * i) / (n - 1));
+        double xold, Pold, Pn, Pnew;
+        int guard = 0;
+        do {
+            xold = xx;
+            Pold = 1;
+            Pn = xx;
+            for (int k = 2; k < n; ++k) {
+                Pnew = ((2 * k - 1) * xx * Pn - (k - 1) * Pold) / k;
+                Pold = Pn;
+                Pn = Pnew;
+            }
+            xx = xx - (xx - Pold / Pn) / n;
+        } while (std::fabs(xx - xold) > 1.0e-15 && ++guard < 200);
+        x[i] = xx;
+        w[i] = 2 / (n * (n - 1) * Pn * Pn);
+    }
+}
+
+// QuadratureRule::make_tensor_product (src/quadrature/QuadratureRule.cpp:109-175):
+// points per direction chosen for exactness `order`, x fastest.
+int tensor_rule(bool lobatto, int dim, int order, std::vector<double> &pts, std::vector<double> &w) {
+    pts.clear();
+    w.clear();
+    if (dim == 0) {
+        pts = {0, 0, 0};
+        w = {1};
+        return 1;
+    }
+    double x1[64], w1[64];
+    int n;
+    if (!lobatto) {
+        n = (order + 1) / 2 + (order + 1) % 2;
+        gauss_legendre_1d(n, x1, w1);
+    } else {
+        n = (order + 3) / 2 + (order + 3) % 2;
+        gauss_lobatto_1d(n, x1, w1);
+    }
+    if (dim == 1) {
+        for (int i = 0; i < n; ++i) { pts.insert(pts.end(), {x1[i], 0, 0}); w.push_back(w1[i]); }
+    } else if (dim == 2) {
+        for (int i = 0; i < n; ++i)
+            for (int j = 0; j < n; ++j) { pts.insert(pts.end(), {x1[j], x1[i], 0}); w.push_back(w1[i] * w1[j]); }
+    } else {
+        for (int i = 0; i < n; ++i)
+            for (int j = 0; j < n; ++j)
+                for (int k = 0; k < n; ++k) {
+                    pts.insert(pts.end(), {x1[k], x1[j], x1[i]});
+                    w.push_back(w1[i] * w1[j] * w1[k]);
+                }
+    }
+    return (int)w.size();
+}
+
+// Symmetric triangle rules on (0,0),(1,0),(0,1) of exactness 1..6: the published
+// Dunavant (1985) points and weights, which the reference tabulates for
+// QuadratureRule::get_triangle_quadrature (src/quadrature/TriangleQuadratureRules.cpp:9-85);
+// the same values keep assembled triangle matrices identical.
+int triangle_rule(int order, std::vector<double> &pts, std::vector<double> &w) {
+    struct P { double x, y, w; };
+    static const P r1[] = {{1. / 3., 1. / 3., 1. / 2.}};
+    static const P r2[] = {{1. / 6., 1. / 6., 1. / 6.}, {1. / 6., 2. / 3., 1. / 6.}, {2. / 3., 1. / 6., 1. / 6.}};
+    static const P r3[] = {{3.33333333333333333E-01, 3.33333333333333333E-01, -2.81250000000000000E-01},
+                           {6.00000000000000000E-01, 2.00000000000000000E-01, 2.60416666666666667E-01},
+                           {2.00000000000000000E-01, 6.00000000000000000E-01, 2.60416666666666667E-01},
+                           {2.00000000000000000E-01, 2.00000000000000000E-01, 2.60416666666666666E-01}};
+    static const P r4[] = {{1.081030181680700E-01, 4.459484909159650E-01, 1.116907948390055E-01},
+                           {4.459484909159650E-01, 1.081030181680700E-01, 1.116907948390055E-01},
+                           {4.459484909159650E-01, 4.459484909159650E-01, 1.116907948390055E-01},
+                           {8.168475729804590E-01, 9.157621350977100E-02, 5.497587182766100E-02},
+                           {9.157621350977100E-02, 8.168475729804590E-01, 5.497587182766100E-02},
+                           {9.157621350977100E-02, 9.157621350977100E-02, 5.497587182766100E-02}};
+    static const P r5[] = {{3.33333333333333E-01, 3.33333333333333E-01, 1.12500000000000E-01},
+                           {5.97158717897700E-02, 4.70142064105115E-01, 6.61970763942530E-02},
+                           {4.70142064105115E-01, 5.97158717897700E-02, 6.61970763942530E-02},
+                           {4.70142064105115E-01, 4.70142064105115E-01, 6.61970763942530E-02},
+                           {7.97426985353087E-01, 1.01286507323456E-01, 6.29695902724135E-02},
+                           {1.01286507323456E-01, 7.97426985353087E-01, 6.29695902724135E-02},
+                           {1.01286507323456E-01, 1.01286507323456E-01, 6.29695902724135E-02}};
+    static const P r6[] = {{5.01426509658179E-01, 2.49286745170910E-01, 5.83931378631895E-02},
+                           {2.49286745170910E-01, 5.01426509658179E-01, 5.83931378631895E-02},
+                           {2.49286745170910E-01, 2.49286745170910E-01, 5.83931378631895E-02},
+                           {8.73821971016996E-01, 6.30890144915020E-02, 2.54224531851035E-02},
+                           {6.30890144915020E-02, 8.73821971016996E-01, 2.54224531851035E-02},
+                           {6.30890144915020E-02, 6.30890144915020E-02, 2.54224531851035E-02},
+                           {5.31450498448170E-02, 3.10352451033784E-01, 4.14255378091870E-02},
+                           {6.36502499121399E-01, 5.31450498448170E-02, 4.14255378091870E-02},
+                           {3.10352451033784E-01, 6.36502499121399E-01, 4.14255378091870E-02},
+                           {5.31450498448170E-02, 6.36502499121399E-01, 4.14255378091870E-02},
+                           {6.36502499121399E-01, 3.10352451033784E-01, 4.14255378091870E-02},
+                           {3.10352451033784E-01, 5.31450498448170E-02, 4.14255378091870E-02}};
+    const P *r = nullptr;
+    int n = 0;
+    switch (order) {
+    case 1: r = r1; n = 1; break;
+    case 2: r = r2; n = 3; break;
+    case 3: r = r3; n = 4; break;
+    case 4: r = r4; n = 6; break;
+    case 5: r = r5; n = 7; break;
+    case 6: r = r6; n = 12; break;
+    default: return 0;
+    }
+    pts.clear();
+    w.clear();
+    for (int i = 0; i < n; ++i) { pts.insert(pts.end(), {r[i].x, r[i].y, 0.0}); w.push_back(r[i].w); }
+    return n;
+}
+
+// ------------------------------------------------------------ reference elements
+
+static double snap_to(double x, double s) { return std::round(x / s) * s; }
+
+// Local nodes: GLL tensor product, x fastest (make_tensorproduct_element.cpp:158-193);
+// triangle: Blyth-Pozrikidis warp of the GLL points snapped to 2^-21
+// (make_simplex_element.cpp:17-26,94-97,156-176).
+static int local_nodes(int topology, int dim, int p, std::vector<double> &pts) {
+    int n = p + 1;
+    double l[64], lw[64];
+    gauss_lobatto_1d(n, l, lw);
+    pts.clear();
+    if (topology == TOPO_TENSOR || dim == 1) {
+        if (dim == 1) for (int i = 0; i < n; ++i) pts.insert(pts.end(), {l[i], 0, 0});
+        else if (dim == 2) for (int i = 0; i < n; ++i) for (int j = 0; j < n; ++j) pts.insert(pts.end(), {l[j], l[i], 0});
+        else if (dim == 3)
+            for (int i = 0; i < n; ++i)
+                for (int j = 0; j < n; ++j)
+                    for (int k = 0; k < n; ++k) pts.insert(pts.end(), {l[k], l[j], l[i]});
+        return (int)pts.size() / 3;
+    }
+    if (topology == TOPO_SIMPLEX && dim == 2) {
+        const double snap = 1.0 / (2 << 20);
+        for (int i = 0; i < n; ++i)
+            for (int j = 0; j < n - i; ++j) {
+                int k = n - i - j - 1;
+                double vi = (l[i] + 1) / 2, vj = (l[j] + 1) / 2, vk = (l[k] + 1) / 2;
+                pts.insert(pts.end(), {snap_to((1 + 2 * vj - vi - vk) / 3, snap), snap_to((1 + 2 * vi - vj - vk) / 3, snap),
+                                       snap_to(0.0, snap)});
+            }
+        return (int)pts.size() / 3;
+    }
+    return 0;
+}
+
+// 1-D Lagrange basis on nodes x[0..n): values and derivatives at t.
+static void lagrange_1d(const double *x, int n, double t, double *v, double *dv) {
+    for (int j = 0; j < n; ++j) {
+        double num = 1, den = 1, d = 0;
+        for (int m = 0; m < n; ++m) {
+            if (m == j) continue;
+            den *= (x[j] - x[m]);
+        }
+        for (int m = 0; m < n; ++m) {
+            if (m == j) continue;
+            num *= (t - x[m]);
+            double prod = 1;
+            for (int q = 0; q < n; ++q)
+                if (q != j && q != m) prod *= (t - x[q]);
+            d += prod;
+        }
+        v[j] = num / den;
+        dv[j] = d / den;
+    }
+}
+
+// Dense LU with partial pivoting (row-major, in place) and solve.
+static void lu_factor(std::vector<double> &A, int n, std::vector<int> &piv) {
+    piv.resize(n);
+    std::iota(piv.begin(), piv.end(), 0);
+    for (int k = 0; k < n; ++k) {
+        int p = k;
+        for (int i = k + 1; i < n; ++i)
+            if (std::fabs(A[i * n + k]) > std::fabs(A[p * n + k])) p = i;
+        if (p != k) {
+            for (int j = 0; j < n; ++j) std::swap(A[k * n + j], A[p * n + j]);
+            std::swap(piv[k], piv[p]);
+        }
+        for (int i = k + 1; i < n; ++i) {
+            A[i * n + k] /= A[k * n + k];
+            for (int j = k + 1; j < n; ++j) A[i * n + j] -= A[i * n + k] * A[k * n + j];
+        }
+    }
+}
+static void lu_solve(const std::vector<double> &LU, int n, const std::vector<int> &piv, const double *b, double *x) {
+    std::vector<double> y(n);
+    for (int i = 0; i < n; ++i) {
+        double s = b[piv[i]];
+        for (int j = 0; j < i; ++j) s -= LU[i * n + j] * y[j];
+        y[i] = s;
+    }
+    for (int i = n - 1; i >= 0; --i) {
+        double s = y[i];
+        for (int j = i + 1; j < n; ++j) s -= LU[i * n + j] * x[j];
+        x[i] = s / LU[i * n + i];
+    }
+}
+
+// Monomial basis x^a y^b (a+b <= p) with derivatives.
+static void monomials_2d(int p, double x, double y, double *v, double *dx, double *dy) {
+    int c = 0;
+    for (int a = 0; a <= p; ++a)
+        for (int b = 0; a + b <= p; ++b) {
+            v[c] = std::pow(x, a) * std::pow(y, b);
+            dx[c] = a ? a * std::pow(x, a - 1) * std::pow(y, b) : 0.0;
+            dy[c] = b ? b * std::pow(x, a) * std::pow(y, b - 1) : 0.0;
+            ++c;
+        }
+}
+
+bool make_element_table(int topology, int dim, int p, ElementTable &T) {
+    T.topology = topology;
+    T.dim = dim;
+    T.p = p;
+    T.nen = local_nodes(topology, dim, p, T.local_nodes);
+    if (T.nen <= 0) return false;
+    if (topology == TOPO_TENSOR || dim == 1) {
+        // volume rule: Gauss-Legendre of exactness 2p (make_tensorproduct_element.cpp:127-128)
+        T.nq = tensor_rule(false, dim, 2 * p, T.qpts, T.qw);
+        // tensor-product Lagrange basis on the GLL points; node A = (i,j,k), x fastest
+        const int n = p + 1;
+        double l[64], lw[64];
+        gauss_lobatto_1d(n, l, lw);
+        T.N.assign((size_t)T.nq * T.nen, 0.0);
+        T.dN.assign((size_t)T.nq * T.nen * dim, 0.0);
+        for (int q = 0; q < T.nq; ++q) {
+            double v[3][64], dv[3][64];
+            for (int d = 0; d < dim; ++d) lagrange_1d(l, n, T.qpts[3 * q + d], v[d], dv[d]);
+            for (int A = 0; A < T.nen; ++A) {
+                int idx[3] = {A % n, (A / n) % n, A / (n * n)};
+                double val = 1;
+                for (int d = 0; d < dim; ++d) val *= v[d][idx[d]];
+                T.N[(size_t)q * T.nen + A] = val;
+                for (int g = 0; g < dim; ++g) {
+                    double dval = 1;
+                    for (int d = 0; d < dim; ++d) dval *= (d == g) ? dv[d][idx[d]] : v[d][idx[d]];
+                    T.dN[((size_t)q * T.nen + A) * dim + g] = dval;
+                }
+            }
+        }
+        return true;
+    }
+    if (topology == TOPO_SIMPLEX && dim == 2) {
+        // volume rule of exactness 2p (make_simplex_element.cpp:99-100)
+        T.nq = triangle_rule(std::max(1, 2 * p), T.qpts, T.qw);
+        if (T.nq == 0) return false;
+        // Nodal basis on the node set whose top vertex sits at y = 0.999999999, as
+        // the reference's Vandermonde uses (ShapeFunctionUtils.cpp:169-172): the
+        // Lagrange basis of a point set is unique, so any polynomial basis works.
+        const int nen = T.nen;
+        std::vector<double> nodes = T.local_nodes;
+        for (int i = 0; i < nen; ++i) nodes[3 * i + 1] = std::min(.999999999, nodes[3 * i + 1]);
+        std::vector<double> VT((size_t)nen * nen);
+        std::vector<double> v(nen), dx(nen), dy(nen);
+        for (int i = 0; i < nen; ++i) {
+            monomials_2d(p, nodes[3 * i], nodes[3 * i + 1], v.data(), dx.data(), dy.data());
+            for (int j = 0; j < nen; ++j) VT[(size_t)j * nen + i] = v[j];  // V(i,j) = phi_j(x_i), store V^T
+        }
+        std::vector<int> piv;
+        lu_factor(VT, nen, piv);
+        T.N.assign((size_t)T.nq * nen, 0.0);
+        T.dN.assign((size_t)T.nq * nen * 2, 0.0);
+        std::vector<double> sol(nen);
+        for (int q = 0; q < T.nq; ++q) {
+            monomials_2d(p, T.qpts[3 * q], T.qpts[3 * q + 1], v.data(), dx.data(), dy.data());
+            lu_solve(VT, nen, piv, v.data(), sol.data());
+            for (int A = 0; A < nen; ++A) T.N[(size_t)q * nen + A] = sol[A];
+            lu_solve(VT, nen, piv, dx.data(), sol.data());
+            for (int A = 0; A < nen; ++A) T.dN[((size_t)q * nen + A) * 2 + 0] = sol[A];
+            lu_solve(VT, nen, piv, dy.data(), sol.data());
+            for (int A = 0; A < nen; ++A) T.dN[((size_t)q * nen + A) * 2 + 1] = sol[A];
+        }
+        return true;
+    }
+    return false;
+}
+
+// ------------------------------------------------------------ DoF numbering
+
+static void cell_to_element(int ct, int &topo, int &tdim) {
+    switch (ct) {
+    case CELL_LINE2: topo = TOPO_TENSOR; tdim = 1; break;
+    case CELL_TRI3: topo = TOPO_SIMPLEX; tdim = 2; break;
+    case CELL_TET4: topo = TOPO_SIMPLEX; tdim = 3; break;
+    case CELL_QUAD4: topo = TOPO_TENSOR; tdim = 2; break;
+    case CELL_HEX8: topo = TOPO_TENSOR; tdim = 3; break;
+    default: topo = TOPO_NONE; tdim = 0; break;
+    }
+}
+
+// DoFManager::interpolate_from_corners (src/utils/DoFManager.cpp:296-338), with
+// the reference's operation order so the merged node set is the same.
+static void interpolate_from_corners(const double *xl, const double *c, int ct, double *out) {
+    const double x0 = xl[0], x1 = xl[1], x2 = xl[2];
+    for (int k = 0; k < 3; ++k) {
+        switch (ct) {
+        case CELL_TRI3: out[k] = (1 - x0 - x1) * c[k] + x0 * c[3 + k] + x1 * c[6 + k]; break;
+        case CELL_TET4: out[k] = (1 - x0 - x1 - x2) * c[k] + x0 * c[3 + k] + x1 * c[6 + k] + x2 * c[9 + k]; break;
+        case CELL_QUAD4:
+            out[k] = (1.0 / 4.0) * ((1 - x0) * (1 - x1) * c[k] + (1 + x0) * (1 - x1) * c[3 + k] +
+                                    (1 + x0) * (1 + x1) * c[6 + k] + (1 - x0) * (1 + x1) * c[9 + k]);
+            break;
+        case CELL_HEX8:
+            out[k] = (1.0 / 8.0) * ((1 - x0) * (1 - x1) * (1 - x2) * c[k] + (1 + x0) * (1 - x1) * (1 - x2) * c[3 + k] +
+                                    (1 + x0) * (1 + x1) * (1 - x2) * c[6 + k] + (1 - x0) * (1 + x1) * (1 - x2) * c[9 + k] +
+                                    (1 - x0) * (1 - x1) * (1 + x2) * c[12 + k] + (1 + x0) * (1 - x1) * (1 + x2) * c[15 + k] +
+                                    (1 + x0) * (1 + x1) * (1 + x2) * c[18 + k] + (1 - x0) * (1 + x1) * (1 + x2) * c[21 + k]);
+            break;
+        default: out[k] = 0; break;
+        }
+    }
+}
+
+bool build_dofmap(const double *xyz, int32_t n_nodes, const int32_t *cell_nodes, const int32_t *cell_offsets,
+                  const int32_t *cell_types, int32_t n_cells, int32_t p, int32_t dpn, HostDofmap &d) {
+    if (p < 1) return false;
+    d.dof_per_node = dpn;
+    d.poly_order = p;
+    d.offsets.assign(n_cells + 1, 0);
+    d.topology.resize(n_cells);
+    d.topo_dim.resize(n_cells);
+    d.porder.assign(n_cells, (int8_t)p);
+    for (int c = 0; c < n_cells; ++c) {
+        int t, td;
+        cell_to_element(cell_types[c], t, td);
+        d.topology[c] = (int8_t)t;
+        d.topo_dim[c] = (int8_t)td;
+    }
+    if (p == 1) {  // DoFManager.cpp:153-160
+        d.nodes.assign(xyz, xyz + 3 * (int64_t)n_nodes);
+        d.offsets.assign(cell_offsets, cell_offsets + n_cells + 1);
+        d.elements.assign(cell_nodes, cell_nodes + cell_offsets[n_cells]);
+        return true;
+    }
+    // make_raw_dofs (DoFManager.cpp:176-229)
+    std::vector<double> raw;
+    std::vector<double> loc;
+    std::vector<double> tabs[3][4];
+    int nloc[3][4] = {{0}};
+    int offset = 0;
+    for (int c = 0; c < n_cells; ++c) {
+        int t = d.topology[c], td = d.topo_dim[c];
+        if (t == TOPO_NONE) continue;
+        if (!nloc[t][td]) nloc[t][td] = local_nodes(t, td, p, tabs[t][td]);
+        const std::vector<double> &L = tabs[t][td];
+        int nl = nloc[t][td];
+        double corners[24] = {0};
+        int nc = cell_offsets[c + 1] - cell_offsets[c];
+        for (int i = 0; i < nc && i < 8; ++i)
+            for (int k = 0; k < 3; ++k) corners[3 * i + k] = xyz[3 * (int64_t)cell_nodes[cell_offsets[c] + i] + k];
+        for (int a = 0; a < nl; ++a) {
+            double o[3];
+            interpolate_from_corners(&L[3 * a], corners, cell_types[c], o);
+            raw.insert(raw.end(), o, o + 3);
+        }
+        d.offsets[c] = offset;
+        offset += nl;
+    }
+    d.offsets[n_cells] = offset;
+    const int64_t N = (int64_t)raw.size() / 3;
+    d.elements.resize(N);
+    // recombine_all_duplicates (DoFManager.cpp:340-414): sort on the snapped
+    // coordinates (z, y, x), merge neighbours closer than 1e-6.  The snapped value
+    // is k*s with k = round(x/s) an integer, so the order of the snapped doubles is
+    // the order of the integer triples, which pack into one 64-bit key.
+    if (N == 0) { d.nodes.clear(); return true; }
+    double bmin[3] = {raw[0], raw[1], raw[2]}, bmax[3] = {raw[0], raw[1], raw[2]};
+    for (int64_t i = 0; i < N; ++i)
+        for (int k = 0; k < 3; ++k) {
+            bmin[k] = std::min(bmin[k], raw[3 * i + k]);
+            bmax[k] = std::max(bmax[k], raw[3 * i + k]);
+        }
+    double max_dim = std::max(bmax[0] - bmin[0], std::max(bmax[1] - bmin[1], bmax[2] - bmin[2]));
+    double snapv = max_dim * 1.0e-6;
+    std::vector<int64_t> kq(3 * N);
+    int64_t kmin[3] = {INT64_MAX, INT64_MAX, INT64_MAX}, kmax[3] = {INT64_MIN, INT64_MIN, INT64_MIN};
+    for (int64_t i = 0; i < N; ++i)
+        for (int k = 0; k < 3; ++k) {
+            int64_t v = (snapv > 0) ? (int64_t)std::llround(std::round(raw[3 * i + k] / snapv)) : 0;
+            kq[3 * i + k] = v;
+            kmin[k] = std::min(kmin[k], v);
+            kmax[k] = std::max(kmax[k], v);
+        }
+    bool packable = true;
+    for (int k = 0; k < 3; ++k) packable &= (kmax[k] - kmin[k]) < (int64_t(1) << 21);
+    std::vector<int64_t> idx(N);
+    std::iota(idx.begin(), idx.end(), 0);
+    if (packable) {
+        std::vector<std::pair<uint64_t, int64_t>> keys(N);
+        for (int64_t i = 0; i < N; ++i) {
+            uint64_t key = ((uint64_t)(kq[3 * i + 2] - kmin[2]) << 42) | ((uint64_t)(kq[3 * i + 1] - kmin[1]) << 21) |
+                           (uint64_t)(kq[3 * i + 0] - kmin[0]);
+            keys[i] = {key, i};
+        }
+        std::sort(keys.begin(), keys.end());
+        for (int64_t i = 0; i < N; ++i) idx[i] = keys[i].second;
+    } else {
+        std::sort(idx.begin(), idx.end(), [&](int64_t a, int64_t b) {
+            for (int k = 2; k >= 0; --k)
+                if (kq[3 * a + k] != kq[3 * b + k]) return kq[3 * a + k] < kq[3 * b + k];
+            return a < b;
+        });
+    }
+    std::vector<int32_t> raw_to_new(N);
+    std::vector<int64_t> first;
+    first.reserve(N / 2 + 1);
+    for (int64_t i = 0; i < N; ++i) {
+        bool newg = true;
+        if (i > 0) {
+            const double *a = &raw[3 * idx[i]], *b = &raw[3 * idx[i - 1]];
+            double s = 0;
+            for (int k = 0; k < 3; ++k) s += (a[k] - b[k]) * (a[k] - b[k]);
+            if (std::sqrt(s) < 1.0e-6) newg = false;
+        }
+        if (newg) first.push_back(idx[i]);
+        raw_to_new[idx[i]] = (int32_t)(first.size() - 1);
+    }
+    d.nodes.resize(3 * first.size());
+    for (size_t g = 0; g < first.size(); ++g)
+        for (int k = 0; k < 3; ++k) d.nodes[3 * g + k] = raw[3 * first[g] + k];
+    for (int64_t i = 0; i < N; ++i) d.elements[i] = raw_to_new[i];
+    return true;
+}
+
+int color_cells(const HostDofmap &d, int nsd, int topology, std::vector<int32_t> &order, std::vector<int32_t> &ptr) {
+    const int32_t nc = d.n_cells();
+    std::vector<uint64_t> used(d.n_nodes(), 0);
+    std::vector<int8_t> color(nc, -1);
+    int ncolors = 0;
+    for (int32_t c = 0; c < nc; ++c) {
+        if (d.topo_dim[c] != nsd || d.topology[c] != topology) continue;
+        uint64_t mask = 0;
+        for (int32_t i = d.offsets[c]; i < d.offsets[c + 1]; ++i) mask |= used[d.elements[i]];
+        int col = 0;
+        while (col < 64 && (mask >> col) & 1) ++col;
+        if (col == 64) return -1;
+        color[c] = (int8_t)col;
+        for (int32_t i = d.offsets[c]; i < d.offsets[c + 1]; ++i) used[d.elements[i]] |= (uint64_t(1) << col);
+        ncolors = std::max(ncolors, col + 1);
+    }
+    ptr.assign(ncolors + 1, 0);
+    for (int32_t c = 0; c < nc; ++c)
+        if (color[c] >= 0) ptr[color[c] + 1]++;
+    for (int k = 0; k < ncolors; ++k) ptr[k + 1] += ptr[k];
+    order.resize(ptr[ncolors]);
+    std::vector<int32_t> fill(ptr.begin(), ptr.end() - 1);
+    for (int32_t c = 0; c < nc; ++c)
+        if (color[c] >= 0) order[fill[color[c]]++] = c;
+    return ncolors;
+}
+
+}  // namespace yg

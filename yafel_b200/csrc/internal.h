@@ -1,0 +1,132 @@
+// internal.h -- shared definitions of libyafel_b200 (not part of the C ABI).
+#pragma once
+
+#include "../../include/yafel_gpu.h"
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+#include <unordered_map>
+
+namespace yg {
+
+void set_error(const char *fmt, ...);
+yg_status fail(yg_status s, const char *fmt, ...);
+
+#define YG_CUDA(call)                                                                     \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess)                                                            \
+            return yg::fail(e_ == cudaErrorMemoryAllocation ? YG_OUT_OF_MEMORY : YG_CUDA_ERROR, \
+                            "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_),       \
+                            __FILE__, __LINE__);                                          \
+    } while (0)
+
+#define YG_TRY(expr)                                \
+    do {                                            \
+        yg_status s_ = (expr);                      \
+        if (s_ != YG_OK) return s_;                 \
+    } while (0)
+
+// Launch bookkeeping: every kernel launch goes through this so the context can
+// report how many of its kernels ran.
+#define YG_LAUNCHED(ctx) ((ctx)->launches++)
+
+constexpr int kThreads = 256;         // threads per block for streaming kernels
+constexpr int kMaxReduceBlocks = 4096;  // upper bound of partial sums per reduction
+
+}  // namespace yg
+
+// Solver scalars kept on the device so that a whole iteration (and a captured
+// sequence of iterations) never waits on the host.
+struct KrylovScalars {
+    double rz[2];     // r.z of the current iteration, double-buffered by parity
+    double rz0;       // r0.z0 (reference criterion)
+    double bb;        // b.b
+    double tol;       // criterion tolerance
+    double rr;        // last r.r
+    double rho[2], alpha, omega;  // BiCGSTAB recurrences (parity-buffered rho)
+    int64_t iter;     // completed iterations
+    int64_t maxiter;
+    int32_t flag;     // 0 running, 1 converged, 2 breakdown, 3 nan, 4 iteration cap
+    int32_t criterion;
+    int32_t check_freq;  // BiCGSTAB reference criterion: true-residual check period
+    int32_t pad;
+};
+
+struct yg_context_t {
+    int device = 0;
+    int num_sms = 148;
+    cudaStream_t stream = nullptr;
+    uint64_t budget = 0;
+    uint64_t in_use = 0;
+    int64_t launches = 0;
+    std::unordered_map<void *, size_t> allocs;
+    // reduction scratch (device) and pinned host mailbox
+    double *d_partials = nullptr;   // 8 * kMaxReduceBlocks doubles
+    double *h_pinned = nullptr;     // 64 doubles of pinned host memory
+    KrylovScalars *d_scalars = nullptr;
+    int reduce_blocks = 592;        // persistent grid for fused Krylov kernels
+};
+
+struct yg_vector_t {
+    yg_context ctx = nullptr;
+    int64_t n = 0;
+    double *d = nullptr;
+};
+
+struct DofmapDevice;
+
+struct yg_matrix_t {
+    yg_context ctx = nullptr;
+    int32_t block = 1;
+    int64_t nbrows = 0, nbcols = 0, nnzb = 0;
+    int32_t *d_rowptr = nullptr;  // nbrows+1
+    int32_t *d_col = nullptr;     // nnzb
+    double *d_val = nullptr;      // nnzb*block*block (row-major blocks)
+    float *d_val32 = nullptr;     // optional FP32 copy
+    int32_t *d_diag = nullptr;    // position of the diagonal block in each block row, -1 if absent
+    int lanes = 32;               // SpMV lanes per block row (autotuned)
+    const void *owner = nullptr;  // dofmap whose pattern this is (assembly re-use)
+    int32_t owner_format = -1;
+    int64_t rows() const { return nbrows * block; }
+    int64_t cols() const { return nbcols * block; }
+};
+
+struct yg_precond_t {
+    yg_matrix A = nullptr;
+    int32_t kind = 0;
+    double *d_dinv = nullptr;     // Jacobi: 1/a_ii (scalar diagonal)
+    int64_t zero_pivots = 0;
+    // ILU(0): factor values on A's pattern (scalar CSR view) + level schedules
+    double *d_lu = nullptr;
+    int32_t *d_lower_levels = nullptr, *d_upper_levels = nullptr;  // row lists grouped by level
+    std::vector<int32_t> lower_level_ptr, upper_level_ptr;
+    int32_t *d_csr_rowptr = nullptr, *d_csr_col = nullptr, *d_csr_diag = nullptr;  // scalar view
+    int64_t n = 0, nnz = 0;
+    double *d_tmp = nullptr;
+};
+
+namespace yg {
+
+yg_status dev_alloc(yg_context ctx, void **p, size_t bytes);
+void dev_free(yg_context ctx, void *p);
+template <typename T>
+yg_status dev_alloc_t(yg_context ctx, T **p, size_t count) {
+    return dev_alloc(ctx, reinterpret_cast<void **>(p), count * sizeof(T) + 16);
+}
+
+// ---- kernels-side entry points (implemented in .cu files) ----
+yg_status spmv_launch(yg_matrix A, const double *x, double *y, int precision, double *partials_dot,
+                      const int32_t *flag, int grid);
+yg_status spmv_launch_ex(yg_matrix A, const double *x, double *y, int precision, const double *w, double *partials,
+                         int dot_mode, const int32_t *flag, int grid);
+int spmv_default_grid(yg_matrix A);
+void spmv_autotune(yg_matrix A);
+yg_status vector_dot(yg_context ctx, const double *a, const double *b, int64_t n, double *out);
+yg_status matrix_build_diag(yg_matrix A);
+yg_status matrix_from_device_pattern(yg_matrix A);
+
+}  // namespace yg

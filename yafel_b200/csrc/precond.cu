@@ -1,0 +1,346 @@
+// precond.cu -- Jacobi and ILU(0) preconditioners.
+//
+// Jacobi replaces JacobiPreconditioner (solver/iterative/JacobiPreconditioner.hpp:11-54):
+// z_i = r_i / a_ii with the scalar diagonal; a zero diagonal gives inf, as the
+// reference computes 1/0 (its warning text says otherwise).  Inside PCG it is
+// fused into the vector kernels (krylov.cu) and never launched on its own.
+//
+// ILU(0) replaces ILUPreconditioner (ILUPreconditioner.hpp:96-329): incomplete
+// LU without pivoting on the scalar pattern of A (a BCSR matrix is expanded to
+// its full B*B entries per block), zero pivots skipped.  The reference walks
+// pivots (KIJ, O(N^2) row scans); here rows are factored in IKJ order, which
+// applies to every entry the same updates in the same order.  Rows are grouped
+// into dependency levels on the host (level = 1 + max level of the rows it
+// depends on); each level is one launch with a warp per row, for the
+// factorization and for both triangular solves.
+#include "internal.h"
+#include "device_common.cuh"
+
+#include <algorithm>
+#include <cmath>
+
+namespace yg {
+
+int stream_grid(yg_context ctx, int64_t n);
+
+__global__ void k_jacobi_build(int64_t nbrows, int B, const int32_t *__restrict__ diag, const double *__restrict__ val,
+                               double *__restrict__ dinv, int *__restrict__ zeros) {
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < nbrows * B; r += (int64_t)gridDim.x * blockDim.x) {
+        int64_t I = r / B, i = r % B;
+        int32_t d = diag[I];
+        double a = d >= 0 ? val[(int64_t)d * B * B + i * B + i] : 0.0;
+        dinv[r] = 1.0 / a;
+        if (a == 0) atomicAdd(zeros, 1);
+    }
+}
+
+__global__ void k_jacobi_apply(int64_t n, const double *__restrict__ dinv, const double *__restrict__ r,
+                               double *__restrict__ z) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        z[i] = r[i] * dinv[i];
+}
+
+// Scalar CSR expansion of a BCSR pattern: row I*B+i lists columns J*B+j.
+__global__ void k_expand_rowptr(int64_t nbrows, int B, const int32_t *__restrict__ brp, int32_t *__restrict__ rp) {
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r <= nbrows * B; r += (int64_t)gridDim.x * blockDim.x) {
+        if (r == nbrows * B) { rp[r] = brp[nbrows] * B * B; continue; }
+        int64_t I = r / B, i = r % B;
+        int32_t len = brp[I + 1] - brp[I];
+        rp[r] = brp[I] * B * B + (int32_t)i * len * B;
+    }
+}
+__global__ void k_expand_vals(int64_t nbrows, int B, const int32_t *__restrict__ brp, const int32_t *__restrict__ bcol,
+                              const double *__restrict__ bval, const int32_t *__restrict__ rp, int32_t *__restrict__ col,
+                              double *__restrict__ val) {
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < nbrows * B; r += (int64_t)gridDim.x * blockDim.x) {
+        int64_t I = r / B, i = r % B;
+        int32_t pos = rp[r];
+        for (int32_t k = brp[I]; k < brp[I + 1]; ++k)
+            for (int j = 0; j < B; ++j) {
+                col[pos] = bcol[k] * B + j;
+                val[pos] = bval[(int64_t)k * B * B + i * B + j];
+                ++pos;
+            }
+    }
+}
+
+__global__ void k_scalar_diag(int64_t n, const int32_t *__restrict__ rp, const int32_t *__restrict__ col,
+                              int32_t *__restrict__ diag) {
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
+        int lo = rp[r], hi = rp[r + 1] - 1, pos = -1;
+        while (lo <= hi) {
+            int mid = (lo + hi) >> 1;
+            if (col[mid] == r) { pos = mid; break; }
+            if (col[mid] < r) lo = mid + 1; else hi = mid - 1;
+        }
+        diag[r] = pos;
+    }
+}
+
+__device__ __forceinline__ int find_col(const int32_t *__restrict__ col, int lo, int hi, int c) {
+    --hi;
+    while (lo <= hi) {
+        int mid = (lo + hi) >> 1;
+        int v = col[mid];
+        if (v == c) return mid;
+        if (v < c) lo = mid + 1; else hi = mid - 1;
+    }
+    return -1;
+}
+
+// Factor the rows of one level: warp per row, pivots in ascending order, the
+// lanes share the updates of one pivot row.
+__global__ void k_ilu_factor_level(const int32_t *__restrict__ rows, int nrows, const int32_t *__restrict__ rp,
+                                   const int32_t *__restrict__ col, const int32_t *__restrict__ diag,
+                                   double *__restrict__ lu, int *__restrict__ zero_pivots) {
+    const int lane = threadIdx.x & 31;
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int t = w; t < nrows; t += nw) {
+        const int i = rows[t];
+        const int rs = rp[i], re = rp[i + 1];
+        for (int kk = rs; kk < re; ++kk) {
+            const int k = col[kk];
+            if (k >= i) break;
+            const int dk = diag[k];
+            const double piv = dk >= 0 ? lu[dk] : 0.0;
+            if (piv == 0) {
+                if (lane == 0) atomicAdd(zero_pivots, 1);
+                continue;
+            }
+            __syncwarp();
+            const double m = lu[kk] / piv;
+            const int ke = rp[k + 1];
+            for (int q = dk + 1 + lane; q < ke; q += 32) {
+                int pos = find_col(col, kk + 1, re, col[q]);
+                if (pos >= 0) lu[pos] -= m * lu[q];
+            }
+            __syncwarp();
+            if (lane == 0) lu[kk] = m;
+            __syncwarp();
+        }
+    }
+}
+
+// Forward substitution with unit L for one level (f_subst, ILUPreconditioner.hpp:201-221).
+__global__ void k_ilu_lower_level(const int32_t *__restrict__ rows, int nrows, const int32_t *__restrict__ rp,
+                                  const int32_t *__restrict__ col, const int32_t *__restrict__ diag,
+                                  const double *__restrict__ lu, double *__restrict__ z) {
+    const int lane = threadIdx.x & 31;
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int t = w; t < nrows; t += nw) {
+        const int i = rows[t];
+        const int rs = rp[i];
+        int re = diag[i] >= 0 ? diag[i] : rp[i + 1];
+        double s = 0;
+        for (int k = rs + lane; k < re; k += 32) {
+            int c = col[k];
+            if (c < i) s += lu[k] * z[c];
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) z[i] -= s;
+    }
+}
+
+// Backward substitution for one level (b_subst, ILUPreconditioner.hpp:226-253);
+// a row without a diagonal uses its first entry, as the reference does.
+__global__ void k_ilu_upper_level(const int32_t *__restrict__ rows, int nrows, const int32_t *__restrict__ rp,
+                                  const int32_t *__restrict__ col, const int32_t *__restrict__ diag,
+                                  const double *__restrict__ lu, double *__restrict__ z) {
+    const int lane = threadIdx.x & 31;
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int t = w; t < nrows; t += nw) {
+        const int i = rows[t];
+        const int id = diag[i] >= 0 ? diag[i] : rp[i];
+        const int re = rp[i + 1];
+        double s = 0;
+        for (int k = id + 1 + lane; k < re; k += 32) s += lu[k] * z[col[k]];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) z[i] = (z[i] - s) / lu[id];
+    }
+}
+
+static int level_grid(yg_context ctx, int64_t rows) {
+    int64_t warps_per_block = kThreads / 32;
+    int64_t g = (rows + warps_per_block - 1) / warps_per_block;
+    int64_t cap = (int64_t)ctx->num_sms * 8;
+    if (g > cap) g = cap;
+    if (g < 1) g = 1;
+    return (int)g;
+}
+
+static yg_status build_ilu(yg_precond M) {
+    yg_matrix A = M->A;
+    yg_context ctx = A->ctx;
+    const int B = A->block;
+    const int64_t n = A->rows();
+    const int64_t nnz = A->nnzb * B * B;
+    if (nnz >= INT32_MAX) return fail(YG_UNSUPPORTED, "ILU(0): too many entries for 32-bit indices");
+    M->n = n;
+    M->nnz = nnz;
+    YG_TRY(dev_alloc_t(ctx, &M->d_csr_rowptr, n + 1));
+    YG_TRY(dev_alloc_t(ctx, &M->d_csr_col, nnz));
+    YG_TRY(dev_alloc_t(ctx, &M->d_csr_diag, n));
+    YG_TRY(dev_alloc_t(ctx, &M->d_lu, nnz));
+    YG_TRY(dev_alloc_t(ctx, &M->d_tmp, 1));
+    cudaStream_t st = ctx->stream;
+    k_expand_rowptr<<<stream_grid(ctx, n + 1), kThreads, 0, st>>>(A->nbrows, B, A->d_rowptr, M->d_csr_rowptr);
+    YG_LAUNCHED(ctx);
+    k_expand_vals<<<stream_grid(ctx, n), kThreads, 0, st>>>(A->nbrows, B, A->d_rowptr, A->d_col, A->d_val,
+                                                            M->d_csr_rowptr, M->d_csr_col, M->d_lu);
+    YG_LAUNCHED(ctx);
+    k_scalar_diag<<<stream_grid(ctx, n), kThreads, 0, st>>>(n, M->d_csr_rowptr, M->d_csr_col, M->d_csr_diag);
+    YG_LAUNCHED(ctx);
+    YG_CUDA(cudaGetLastError());
+    // dependency levels on the host
+    std::vector<int32_t> rp(n + 1), col(nnz);
+    YG_CUDA(cudaMemcpyAsync(rp.data(), M->d_csr_rowptr, sizeof(int32_t) * (n + 1), cudaMemcpyDeviceToHost, st));
+    YG_CUDA(cudaMemcpyAsync(col.data(), M->d_csr_col, sizeof(int32_t) * nnz, cudaMemcpyDeviceToHost, st));
+    YG_CUDA(cudaStreamSynchronize(st));
+    std::vector<int32_t> lev(n, 0), ulev(n, 0);
+    int32_t maxl = 0, maxu = 0;
+    for (int64_t i = 0; i < n; ++i) {
+        int32_t l = 0;
+        for (int32_t k = rp[i]; k < rp[i + 1]; ++k) {
+            int32_t c = col[k];
+            if (c >= i) break;
+            l = std::max(l, lev[c] + 1);
+        }
+        lev[i] = l;
+        maxl = std::max(maxl, l);
+    }
+    for (int64_t i = n - 1; i >= 0; --i) {
+        int32_t l = 0;
+        for (int32_t k = rp[i + 1] - 1; k >= rp[i]; --k) {
+            int32_t c = col[k];
+            if (c <= i) break;
+            l = std::max(l, ulev[c] + 1);
+        }
+        ulev[i] = l;
+        maxu = std::max(maxu, l);
+    }
+    auto group = [&](const std::vector<int32_t> &L, int32_t nl, std::vector<int32_t> &ptr, std::vector<int32_t> &rows) {
+        ptr.assign(nl + 2, 0);
+        for (int64_t i = 0; i < n; ++i) ptr[L[i] + 1]++;
+        for (int32_t l = 0; l <= nl; ++l) ptr[l + 1] += ptr[l];
+        rows.resize(n);
+        std::vector<int32_t> fill(ptr.begin(), ptr.end() - 1);
+        for (int64_t i = 0; i < n; ++i) rows[fill[L[i]]++] = (int32_t)i;
+    };
+    std::vector<int32_t> lrows, urows;
+    group(lev, maxl, M->lower_level_ptr, lrows);
+    group(ulev, maxu, M->upper_level_ptr, urows);
+    YG_TRY(dev_alloc_t(ctx, &M->d_lower_levels, n));
+    YG_TRY(dev_alloc_t(ctx, &M->d_upper_levels, n));
+    YG_CUDA(cudaMemcpyAsync(M->d_lower_levels, lrows.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, st));
+    YG_CUDA(cudaMemcpyAsync(M->d_upper_levels, urows.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, st));
+    // factor level by level
+    int *d_zero = reinterpret_cast<int *>(M->d_tmp);
+    YG_CUDA(cudaMemsetAsync(d_zero, 0, sizeof(int), st));
+    for (size_t l = 0; l + 1 < M->lower_level_ptr.size(); ++l) {
+        int32_t a = M->lower_level_ptr[l], b = M->lower_level_ptr[l + 1];
+        if (b == a) continue;
+        k_ilu_factor_level<<<level_grid(ctx, b - a), kThreads, 0, st>>>(M->d_lower_levels + a, b - a, M->d_csr_rowptr,
+                                                                        M->d_csr_col, M->d_csr_diag, M->d_lu, d_zero);
+        YG_LAUNCHED(ctx);
+    }
+    YG_CUDA(cudaGetLastError());
+    int zeros = 0;
+    YG_CUDA(cudaMemcpyAsync(&zeros, d_zero, sizeof(int), cudaMemcpyDeviceToHost, st));
+    YG_CUDA(cudaStreamSynchronize(st));
+    M->zero_pivots = zeros;
+    return YG_OK;
+}
+
+yg_status precond_apply_dev(yg_precond M, const double *r, double *z) {
+    yg_context ctx = M->A->ctx;
+    cudaStream_t st = ctx->stream;
+    const int64_t n = M->A->rows();
+    if (M->kind == YG_PRECOND_IDENTITY) {
+        if (z != r) YG_CUDA(cudaMemcpyAsync(z, r, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+        return YG_OK;
+    }
+    if (M->kind == YG_PRECOND_JACOBI) {
+        k_jacobi_apply<<<stream_grid(ctx, n), kThreads, 0, st>>>(n, M->d_dinv, r, z);
+        YG_LAUNCHED(ctx);
+        return YG_OK;
+    }
+    if (z != r) YG_CUDA(cudaMemcpyAsync(z, r, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+    for (size_t l = 0; l + 1 < M->lower_level_ptr.size(); ++l) {
+        int32_t a = M->lower_level_ptr[l], b = M->lower_level_ptr[l + 1];
+        if (b == a) continue;
+        k_ilu_lower_level<<<level_grid(ctx, b - a), kThreads, 0, st>>>(M->d_lower_levels + a, b - a, M->d_csr_rowptr,
+                                                                       M->d_csr_col, M->d_csr_diag, M->d_lu, z);
+        YG_LAUNCHED(ctx);
+    }
+    for (size_t l = 0; l + 1 < M->upper_level_ptr.size(); ++l) {
+        int32_t a = M->upper_level_ptr[l], b = M->upper_level_ptr[l + 1];
+        if (b == a) continue;
+        k_ilu_upper_level<<<level_grid(ctx, b - a), kThreads, 0, st>>>(M->d_upper_levels + a, b - a, M->d_csr_rowptr,
+                                                                       M->d_csr_col, M->d_csr_diag, M->d_lu, z);
+        YG_LAUNCHED(ctx);
+    }
+    YG_CUDA(cudaGetLastError());
+    return YG_OK;
+}
+
+bool precond_fusable(yg_precond M) { return !M || M->kind == YG_PRECOND_IDENTITY || M->kind == YG_PRECOND_JACOBI; }
+const double *precond_dinv(yg_precond M) { return (M && M->kind == YG_PRECOND_JACOBI) ? M->d_dinv : nullptr; }
+
+}  // namespace yg
+
+using namespace yg;
+
+extern "C" yg_status yg_precond_create(yg_matrix A, int32_t kind, yg_precond *out) {
+    if (!A || !out) return fail(YG_BAD_ARG, "yg_precond_create: NULL argument");
+    if (A->rows() != A->cols()) return fail(YG_BAD_ARG, "preconditioner needs a square matrix");
+    *out = nullptr;
+    auto *M = new yg_precond_t();
+    M->A = A;
+    M->kind = kind;
+    yg_context ctx = A->ctx;
+    yg_status s = YG_OK;
+    if (kind == YG_PRECOND_JACOBI) {
+        const int64_t n = A->rows();
+        if ((s = dev_alloc_t(ctx, &M->d_dinv, n)) == YG_OK && (s = dev_alloc_t(ctx, &M->d_tmp, 1)) == YG_OK) {
+            int *d_zero = reinterpret_cast<int *>(M->d_tmp);
+            cudaMemsetAsync(d_zero, 0, sizeof(int), ctx->stream);
+            k_jacobi_build<<<stream_grid(ctx, n), kThreads, 0, ctx->stream>>>(A->nbrows, A->block, A->d_diag, A->d_val,
+                                                                             M->d_dinv, d_zero);
+            YG_LAUNCHED(ctx);
+            int zeros = 0;
+            cudaMemcpyAsync(&zeros, d_zero, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
+            cudaError_t e = cudaStreamSynchronize(ctx->stream);
+            if (e != cudaSuccess) s = fail(YG_CUDA_ERROR, "Jacobi build: %s", cudaGetErrorString(e));
+            M->zero_pivots = zeros;
+        }
+    } else if (kind == YG_PRECOND_ILU0) {
+        s = build_ilu(M);
+    } else if (kind != YG_PRECOND_IDENTITY) {
+        s = fail(YG_BAD_ARG, "unknown preconditioner kind %d", kind);
+    }
+    if (s != YG_OK) { yg_precond_destroy(M); return s; }
+    *out = M;
+    return YG_OK;
+}
+
+extern "C" yg_status yg_precond_apply(yg_precond M, yg_vector z) {
+    if (!M || !z || z->n != M->A->rows()) return fail(YG_BAD_ARG, "yg_precond_apply: size mismatch");
+    return precond_apply_dev(M, z->d, z->d);
+}
+
+extern "C" yg_status yg_precond_destroy(yg_precond M) {
+    if (!M) return YG_OK;
+    yg_context ctx = M->A->ctx;
+    for (void *p : {(void *)M->d_dinv, (void *)M->d_lu, (void *)M->d_lower_levels, (void *)M->d_upper_levels,
+                    (void *)M->d_csr_rowptr, (void *)M->d_csr_col, (void *)M->d_csr_diag, (void *)M->d_tmp})
+        dev_free(ctx, p);
+    delete M;
+    return YG_OK;
+}
+
+extern "C" int64_t yg_precond_zero_pivots(yg_precond M) { return M ? M->zero_pivots : -1; }
