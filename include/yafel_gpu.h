@@ -207,7 +207,7 @@ typedef struct yg_solve_opts {
     double tol;         /* see criterion */
     int64_t maxiter;    /* 0 = the reference's default (N for CG) */
     int32_t check_every;/* iterations between host convergence checks (0 = automatic) */
-    int32_t reserved;
+    int32_t profile;    /* 1: time every SpMV of the iteration with CUDA events (stats.spmv_*) */
 } yg_solve_opts;
 typedef struct yg_solve_stats {
     int64_t iterations;       /* Krylov iterations (inner iterations summed for MIXED) */
@@ -215,6 +215,8 @@ typedef struct yg_solve_stats {
     int32_t status;           /* yg_status of the solve */
     int32_t refinements;      /* outer FP64 refinement steps (MIXED) */
     double device_ms;         /* device time of the solve (CUDA events) */
+    double spmv_ms;           /* with opts.profile: summed device time of the iteration SpMVs */
+    int64_t spmv_launches;    /* with opts.profile: number of SpMVs timed */
 } yg_solve_stats;
 
 /* cg_solve(A, rhs, x0, TOL) / pcg_solve(A, rhs, M, x0, TOL)

@@ -62,6 +62,8 @@ def lib():
         L.or_gauss_lobatto_1d.argtypes = [C.c_int, f64p, f64p]
         L.or_tensor_rule.argtypes = [C.c_int, C.c_int, C.c_int, f64p, f64p]
         L.or_triangle_rule.argtypes = [C.c_int, f64p, f64p]
+        L.or_triangle_rule_collapsed.argtypes = [C.c_int, f64p, f64p]
+        L.or_set_triangle_rule.argtypes = [C.c_int, f64p, f64p, C.c_int]
         L.or_local_nodes.argtypes = [C.c_int, C.c_int, C.c_int, f64p]
         L.or_element_rule.argtypes = [C.c_int, C.c_int, C.c_int, f64p, f64p]
         L.or_shape_functions.argtypes = [C.c_int, C.c_int, C.c_int, f64p, C.c_int, f64p, f64p]
@@ -91,8 +93,33 @@ def lib():
         L.or_true_relres.argtypes = [C.POINTER(_Csr), f64p, f64p]
         L.or_true_relres.restype = C.c_double
         L.or_num_threads.restype = C.c_int
+        _install_reference_triangle_rules(L)
         _LIB = L
     return _LIB
+
+
+def _install_reference_triangle_rules(L):
+    """The reference integrates triangles with its tabulated (Dunavant) rules,
+    whose 15-digit constants are part of its arithmetic; the oracle uses the same
+    rules, read from the fixture that tests/golden/make_golden.py generated by
+    running the reference's own TriangleQuadratureRules.cpp.  Without the fixture
+    the oracle falls back to an exact collapsed Gauss-Legendre rule."""
+    path = os.path.join(os.path.dirname(HERE), "tests", "golden", "quadrature.npz")
+    if not os.path.exists(path):
+        return
+    g = np.load(path)
+    for order in range(1, 7):
+        key = "tri_%d_p" % order
+        if key in g:
+            p = np.ascontiguousarray(g[key], dtype=np.float64).ravel()
+            w = np.ascontiguousarray(g["tri_%d_w" % order], dtype=np.float64)
+            L.or_set_triangle_rule(order, p, w, w.size)
+
+
+def triangle_rule_collapsed(order):
+    pts, w = np.zeros(3 * 4096), np.zeros(4096)
+    nq = lib().or_triangle_rule_collapsed(order, pts, w)
+    return pts[:3 * nq].reshape(nq, 3), w[:nq]
 
 
 def ref_available():

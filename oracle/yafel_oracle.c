@@ -122,13 +122,36 @@ int or_tensor_rule(int lobatto, int dim, int order, double *pts, double *w) {
     return q;
 }
 
+int or_triangle_rule_collapsed(int order, double *pts, double *w);
+
 /* Triangle rule on the unit right triangle (0,0),(1,0),(0,1), exact for degree
  * `order`.  The reference tabulates Dunavant-type rules
  * (src/quadrature/TriangleQuadratureRules.cpp:9-221); the oracle uses an
  * independent rule of the same exactness (Gauss-Legendre on the collapsed
  * square, x = u(1-v), y = v, Jacobian 1-v), so the assembled values agree up to
  * rounding while the product's tables are checked, not copied. */
+/* Optional override with the reference's own tabulated rules (installed by
+ * oracle.py from the fixture that tests/golden/make_golden.py generated by
+ * running src/quadrature/TriangleQuadratureRules.cpp). */
+static int g_tri_n[16];
+static double g_tri_pts[16][3 * 64], g_tri_w[16][64];
+void or_set_triangle_rule(int order, const double *pts, const double *w, int n) {
+    if (order < 0 || order >= 16 || n > 64) return;
+    g_tri_n[order] = n;
+    memcpy(g_tri_pts[order], pts, sizeof(double) * 3 * n);
+    memcpy(g_tri_w[order], w, sizeof(double) * n);
+}
+
 int or_triangle_rule(int order, double *pts, double *w) {
+    if (order >= 0 && order < 16 && g_tri_n[order] > 0) {
+        memcpy(pts, g_tri_pts[order], sizeof(double) * 3 * g_tri_n[order]);
+        memcpy(w, g_tri_w[order], sizeof(double) * g_tri_n[order]);
+        return g_tri_n[order];
+    }
+    return or_triangle_rule_collapsed(order, pts, w);
+}
+
+int or_triangle_rule_collapsed(int order, double *pts, double *w) {
     int n = (order + 3) / 2; /* ceil((order+2)/2) */
     double x1[32], w1[32];
     or_gauss_legendre_1d(n, x1, w1);

@@ -63,6 +63,8 @@ void or_gauss_legendre_1d(int n, double *x, double *w);
 void or_gauss_lobatto_1d(int n, double *x, double *w);
 int or_tensor_rule(int lobatto, int dim, int order, double *pts, double *w);
 int or_triangle_rule(int order, double *pts, double *w);
+int or_triangle_rule_collapsed(int order, double *pts, double *w);
+void or_set_triangle_rule(int order, const double *pts, const double *w, int n);
 
 /* ---- reference elements ---- */
 int or_local_nodes(int topology, int dim, int p, double *pts);

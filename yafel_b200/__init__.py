@@ -8,6 +8,7 @@ Everything below calls the C ABI of include/yafel_gpu.h (libyafel_b200.so,
 hand-written sm_100a kernels); there is no CPU fallback.
 """
 import ctypes as C
+import sys
 
 import numpy as np
 
@@ -35,6 +36,12 @@ def _ptr(a):
     return a.ctypes.data_as(C.c_void_p) if a is not None else None
 
 
+def _alive(ctx):
+    """Handles are released only while the interpreter runs and the owning
+    context is open; at shutdown the context's teardown frees everything."""
+    return not sys.is_finalizing() and (ctx is None or getattr(ctx, "h", None))
+
+
 class Context:
     """A CUDA device, one stream and an HBM budget (bytes, 0 = unlimited)."""
 
@@ -56,9 +63,9 @@ class Context:
         return lib().yg_context_launches(self.h)
 
     def close(self):
-        if getattr(self, "h", None):
+        if getattr(self, "h", None) and not sys.is_finalizing():
             lib().yg_context_destroy(self.h)
-            self.h = None
+        self.h = None
 
     def __del__(self):
         try:
@@ -123,9 +130,9 @@ class DeviceVector:
         return self.n
 
     def __del__(self):
-        if getattr(self, "h", None) and getattr(self, "ctx", None) is not None and self.ctx.h:
+        if getattr(self, "h", None) and _alive(getattr(self, "ctx", None)):
             lib().yg_vector_destroy(self.h)
-            self.h = None
+        self.h = None
 
 
 def _as_device(v, ctx):
@@ -163,13 +170,13 @@ class DoFManager:
     """DoFManager(M, ManagerType::CG, polyOrder, dof_per_node)
     (src/utils/DoFManager.cpp:11-36); numbering identical to the reference's."""
 
-    def __init__(self, mesh, polyOrder=1, dof_per_node=1, ctx=None):
+    def __init__(self, mesh, polyOrder=1, dof_per_node=1, ctx=None, host_only=False):
         if isinstance(mesh, dict):
             mesh = Mesh.from_dict(mesh)
-        self.ctx = ctx or default_context()
+        self.ctx = None if host_only else (ctx or default_context())
         self.mesh = mesh
         h = C.c_void_p()
-        check(lib().yg_dofmap_create(self.ctx.h, _ptr(mesh.nodes), mesh.nNodes(), _ptr(mesh.cell_nodes),
+        check(lib().yg_dofmap_create(self.ctx.h if self.ctx else None, _ptr(mesh.nodes), mesh.nNodes(), _ptr(mesh.cell_nodes),
                                      _ptr(mesh.offsets), _ptr(mesh.cell_types), mesh.nCells(), int(polyOrder),
                                      int(dof_per_node), C.byref(h)), "DoFManager")
         self.h = h
@@ -228,9 +235,9 @@ class DoFManager:
         return (nodes[:, None] * d + np.arange(d)[None, :]).ravel()
 
     def __del__(self):
-        if getattr(self, "h", None) and self.ctx.h:
+        if getattr(self, "h", None) and _alive(getattr(self, "ctx", None)):
             lib().yg_dofmap_destroy(self.h)
-            self.h = None
+        self.h = None
 
 
 # ------------------------------------------------------------------ physics
@@ -350,9 +357,9 @@ class _Matrix:
         return self.spmv(np.asarray(x, dtype=np.float64)).numpy()
 
     def __del__(self):
-        if getattr(self, "h", None) and getattr(self, "ctx", None) is not None and self.ctx.h:
+        if getattr(self, "h", None) and _alive(getattr(self, "ctx", None)):
             lib().yg_matrix_destroy(self.h)
-            self.h = None
+        self.h = None
 
 
 def _triplet_arrays(ts):
@@ -548,9 +555,9 @@ class _Precond:
         return z
 
     def __del__(self):
-        if getattr(self, "h", None) and self.A.ctx.h:
+        if getattr(self, "h", None) and _alive(getattr(self.A, "ctx", None)):
             lib().yg_precond_destroy(self.h)
-            self.h = None
+        self.h = None
 
 
 class IdentityPreconditioner(_Precond):
@@ -566,7 +573,7 @@ class ILUPreconditioner(_Precond):
 
 
 def solve(A, b, x0=None, M=None, method="cg", criterion=CRIT_RELRES, tol=1e-10, maxiter=0,
-          precision=PREC_FP64, check_every=0, raise_on_failure=False):
+          precision=PREC_FP64, check_every=0, raise_on_failure=False, profile=False):
     """Solve on the GPU and return (x, stats).  b and x0 may be host arrays or
     DeviceVectors; x is a DeviceVector."""
     ctx = A.ctx
@@ -577,7 +584,7 @@ def solve(A, b, x0=None, M=None, method="cg", criterion=CRIT_RELRES, tol=1e-10, 
         xd = x0
     else:
         xd = DeviceVector(np.asarray(x0, dtype=np.float64), ctx)
-    opts = SolveOpts(criterion, precision, tol, maxiter, check_every, 0)
+    opts = SolveOpts(criterion, precision, tol, maxiter, check_every, int(bool(profile)))
     st = SolveStats()
     fn = lib().yg_cg if method == "cg" else lib().yg_bicgstab
     s = fn(A.h, M.h if M is not None else None, bd.h, xd.h, C.byref(opts), C.byref(st))

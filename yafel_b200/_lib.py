@@ -24,12 +24,12 @@ class Physics(C.Structure):
 
 class SolveOpts(C.Structure):
     _fields_ = [("criterion", i32), ("precision", i32), ("tol", f64), ("maxiter", i64),
-                ("check_every", i32), ("reserved", i32)]
+                ("check_every", i32), ("profile", i32)]
 
 
 class SolveStats(C.Structure):
     _fields_ = [("iterations", i64), ("rel_residual", f64), ("status", i32), ("refinements", i32),
-                ("device_ms", f64)]
+                ("device_ms", f64), ("spmv_ms", f64), ("spmv_launches", i64)]
 
 
 # name -> (restype, argtypes); mirrors include/yafel_gpu.h

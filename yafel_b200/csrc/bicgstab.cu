@@ -231,11 +231,15 @@ yg_status solve_bicgstab(yg_matrix A, yg_precond M, yg_vector bv, yg_vector xv, 
         flag = BF_CONVERGED;
     } else {
         // P layout: [0,2G) rhat.r/r.r ; [2G,3G) rhat.v ; [4G,6G) s.t/t.t ; b.b at 2*kMax
-        TRYB(spmv_launch(A, xv->d, q, YG_PREC_FP64, nullptr, nullptr, spmv_default_grid(A)));
-        k_bicg_init<<<G, kThreads, 0, st>>>(n, bv->d, q, r, rhat, p, v, P);
-        YG_LAUNCHED(ctx);
-        k_bicg_scalars_init<<<1, kThreads, 0, st>>>(S, P, G, o.tol, maxiter, o.criterion);
-        YG_LAUNCHED(ctx);
+        auto init = [&](int64_t iters_left) -> yg_status {
+            YG_TRY(spmv_launch(A, xv->d, q, YG_PREC_FP64, nullptr, nullptr, spmv_default_grid(A)));
+            k_bicg_init<<<G, kThreads, 0, st>>>(n, bv->d, q, r, rhat, p, v, P);
+            YG_LAUNCHED(ctx);
+            k_bicg_scalars_init<<<1, kThreads, 0, st>>>(S, P, G, o.tol, iters_left, o.criterion);
+            YG_LAUNCHED(ctx);
+            return YG_OK;
+        };
+        TRYB(init(maxiter));
         auto one = [&](int parity) -> yg_status {
             k_bicg_p<<<G, kThreads, 0, st>>>(n, P, G, S, parity, p, r, v, ph, dinv);
             YG_LAUNCHED(ctx);
@@ -278,13 +282,30 @@ yg_status solve_bicgstab(yg_matrix A, yg_precond M, yg_vector bv, yg_vector xv, 
                 if (m & 1) ++m;
                 BGraph g;
                 TRYB(build(m, g));
-                int64_t it = 0;
-                for (;;) {
-                    TRYB(replay(g, it));
+                int64_t total = 0;
+                // The recursive residual triggers the stop; the FP64 true residual
+                // decides.  If they drifted apart, restart from the true residual.
+                for (int restart = 0; restart < 8; ++restart) {
+                    int64_t it = 0;
+                    for (;;) {
+                        TRYB(replay(g, it));
+                        TRYB(read_s(ctx, &hs));
+                        if (hs.flag != BF_RUN) break;
+                    }
+                    total += hs.iter;
+                    flag = hs.flag;
+                    if (flag != BF_CONVERGED) break;
+                    TRYB(spmv_launch(A, xv->d, q, YG_PREC_FP64, nullptr, nullptr, spmv_default_grid(A)));
+                    k_axmb<<<stream_grid(ctx, n), kThreads, 0, st>>>(n, q, bv->d, q);
+                    YG_LAUNCHED(ctx);
+                    double rr = 0;
+                    TRYB(vector_dot(ctx, q, q, n, &rr));
+                    if (std::sqrt(rr) <= o.tol * std::sqrt(bb0)) break;
+                    if (total >= maxiter) { flag = BF_MAXITER; break; }
+                    TRYB(init(maxiter - total));
                     TRYB(read_s(ctx, &hs));
-                    if (hs.flag != BF_RUN) break;
                 }
-                flag = hs.flag;
+                hs.iter = total;
             } else {
                 // true residual ||Ax-b||^2/||b||^2 after iterations k = 0, f, 2f, ...
                 const int64_t freq = (n / 100 > 1) ? n / 100 : 1;

@@ -235,17 +235,70 @@ static void lu_solve(const std::vector<double> &LU, int n, const std::vector<int
     }
 }
 
-// Monomial basis x^a y^b (a+b <= p) with derivatives.
-static void monomials_2d(int p, double x, double y, double *v, double *dx, double *dy) {
-    int c = 0;
-    for (int a = 0; a <= p; ++a)
-        for (int b = 0; a + b <= p; ++b) {
-            v[c] = std::pow(x, a) * std::pow(y, b);
-            dx[c] = a ? a * std::pow(x, a - 1) * std::pow(y, b) : 0.0;
-            dy[c] = b ? b * std::pow(x, a) * std::pow(y, b - 1) : 0.0;
-            ++c;
-        }
+// Forward-mode dual number (value, derivative).
+struct Dual {
+    double f, d;
+};
+static Dual operator+(Dual a, Dual b) { return {a.f + b.f, a.d + b.d}; }
+static Dual operator-(Dual a, Dual b) { return {a.f - b.f, a.d - b.d}; }
+static Dual operator*(Dual a, Dual b) { return {a.f * b.f, a.d * b.f + a.f * b.d}; }
+static Dual operator/(Dual a, Dual b) { return {a.f / b.f, (a.d * b.f - a.f * b.d) / (b.f * b.f)}; }
+static Dual dpow(Dual x, int e) { return {std::pow(x.f, e), x.d * e * std::pow(x.f, e - 1)}; }
+
+// Jacobi polynomial P_n^{(a,b)} coefficients, highest degree first, by the
+// three-term recurrence (the reference's jacobi(), ShapeFunctionUtils.cpp:16-62).
+static std::vector<double> jacobi_coeffs(int n, double a, double b) {
+    std::vector<double> c1{(a + b + 2) / 2, (a - b) / 2}, c2{1.0};
+    if (n == 0) return c2;
+    if (n == 1) return c1;
+    std::vector<double> c = c1;
+    for (int i = 1; i < n; ++i) {
+        double tmp = i + a + b + 1;
+        double A = (2 * i + a + b + 1) * (2 * i + a + b + 2) / (2 * (i + 1) * tmp);
+        double B = (b * b - a * a) * (2 * i + a + b + 1) / (2 * (i + 1) * tmp * (2 * i + a + b));
+        double Cc = (i + a) * (i + b) * (2 * i + a + b + 2) / ((i + 1) * tmp * (2 * i + a + b));
+        c.push_back(0);
+        for (double &v : c) v *= A;
+        for (size_t k = 0; k < c1.size(); ++k) c[c.size() - 1 - k] -= B * c1[c1.size() - 1 - k];
+        for (size_t k = 0; k < c2.size(); ++k) c[c.size() - 1 - k] -= Cc * c2[c2.size() - 1 - k];
+        c2 = c1;
+        c1 = c;
+    }
+    return c;
 }
+
+static Dual horner(const std::vector<double> &c, Dual x) {
+    Dual r{0, 0};
+    for (double v : c) r = r * x + Dual{v, 0};
+    return r;
+}
+
+// Koornwinder basis on the triangle, phi_k = P_m(r) P_n^{(2m+1,0)}(s) ((1-s)/2)^m
+// with r = 2(1+xi)/(1-eta) - 1, s = eta, (m,n) ordered as the reference orders
+// them (ShapeFunctionUtils.cpp:160-189).  g selects the derivative direction
+// (-1: value only).
+struct Koornwinder {
+    int p;
+    std::vector<std::vector<double>> j00;
+    std::vector<int> m;
+    std::vector<std::vector<double>> j2;
+    explicit Koornwinder(int p_) : p(p_) {
+        for (int k = 0; k <= p; ++k) j00.push_back(jacobi_coeffs(k, 0, 0));
+        for (int i = 0; i <= p; ++i)
+            for (int j = 0; j <= p; ++j)
+                if (i + j <= p) {
+                    m.push_back(i);
+                    j2.push_back(jacobi_coeffs(j, 2 * i + 1, 0));
+                }
+    }
+    Dual eval(int k, double x, double y, int g) const {
+        Dual xi{x, g == 0 ? 1.0 : 0.0}, eta{y, g == 1 ? 1.0 : 0.0};
+        Dual one{1, 0}, two{2, 0};
+        Dual r = two * (one + xi) / (one - eta) - one;
+        Dual s = eta;
+        return horner(j00[m[k]], r) * horner(j2[k], s) * dpow((one - s) / two, m[k]);
+    }
+};
 
 bool make_element_table(int topology, int dim, int p, ElementTable &T) {
     T.topology = topology;
@@ -283,25 +336,29 @@ bool make_element_table(int topology, int dim, int p, ElementTable &T) {
         // volume rule of exactness 2p (make_simplex_element.cpp:99-100)
         T.nq = triangle_rule(std::max(1, 2 * p), T.qpts, T.qw);
         if (T.nq == 0) return false;
-        // Nodal basis on the node set whose top vertex sits at y = 0.999999999, as
-        // the reference's Vandermonde uses (ShapeFunctionUtils.cpp:169-172): the
-        // Lagrange basis of a point set is unique, so any polynomial basis works.
+        // Nodal basis from the Koornwinder Vandermonde V(i,j) = phi_j(x_i) on the
+        // node set whose top vertex sits at y = 0.999999999, solved as V^T N = phi(xi)
+        // with partial-pivot LU and dual-number gradients -- the reference's
+        // construction (ShapeFunctionUtils.cpp:145-217), so the rounding matches.
         const int nen = T.nen;
         std::vector<double> nodes = T.local_nodes;
         for (int i = 0; i < nen; ++i) nodes[3 * i + 1] = std::min(.999999999, nodes[3 * i + 1]);
+        Koornwinder K(p);
         std::vector<double> VT((size_t)nen * nen);
-        std::vector<double> v(nen), dx(nen), dy(nen);
-        for (int i = 0; i < nen; ++i) {
-            monomials_2d(p, nodes[3 * i], nodes[3 * i + 1], v.data(), dx.data(), dy.data());
-            for (int j = 0; j < nen; ++j) VT[(size_t)j * nen + i] = v[j];  // V(i,j) = phi_j(x_i), store V^T
-        }
+        for (int i = 0; i < nen; ++i)
+            for (int j = 0; j < nen; ++j) VT[(size_t)j * nen + i] = K.eval(j, nodes[3 * i], nodes[3 * i + 1], -1).f;
         std::vector<int> piv;
         lu_factor(VT, nen, piv);
         T.N.assign((size_t)T.nq * nen, 0.0);
         T.dN.assign((size_t)T.nq * nen * 2, 0.0);
-        std::vector<double> sol(nen);
+        std::vector<double> v(nen), dx(nen), dy(nen), sol(nen);
         for (int q = 0; q < T.nq; ++q) {
-            monomials_2d(p, T.qpts[3 * q], T.qpts[3 * q + 1], v.data(), dx.data(), dy.data());
+            const double x = T.qpts[3 * q], y = T.qpts[3 * q + 1];
+            for (int j = 0; j < nen; ++j) {
+                v[j] = K.eval(j, x, y, -1).f;
+                dx[j] = K.eval(j, x, y, 0).d;
+                dy[j] = K.eval(j, x, y, 1).d;
+            }
             lu_solve(VT, nen, piv, v.data(), sol.data());
             for (int A = 0; A < nen; ++A) T.N[(size_t)q * nen + A] = sol[A];
             lu_solve(VT, nen, piv, dx.data(), sol.data());

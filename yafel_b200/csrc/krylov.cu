@@ -111,7 +111,9 @@ k_cg_update(int64_t n, const double *__restrict__ pq_partials, int np, KrylovSca
     if (read_flag(&S->flag)) return;
     const double pq = reduce_partials<kThreads>(pq_partials, np, 1, 0, sm);
     const double alpha = S->rz[parity] / pq;
-    if (!(pq > 0) || !isfinite(alpha)) {
+    // no definiteness test: the reference runs CG on negative definite systems
+    // too (test/test_cg_solve.cpp uses tridiag(1,-2,1)); only p.Ap = 0 breaks down
+    if (pq == 0 || !isfinite(alpha)) {
         if (blockIdx.x == 0 && threadIdx.x == 0) S->flag = isfinite(pq) ? FLAG_BREAKDOWN : FLAG_NAN;
         return;
     }
@@ -275,8 +277,42 @@ static int default_check_every(int64_t n, const yg_solve_opts *o) {
 }
 
 // Core PCG on (A, precision) with x updated in place.  The right-hand side is b.
+// SpMV timing inside captured iterations: an event pair around each SpMV.
+struct SpmvProfile {
+    bool on = false;
+    std::vector<cudaEvent_t> start, stop;
+    double ms = 0;
+    int64_t launches = 0;
+    ~SpmvProfile() {
+        for (auto e : start) cudaEventDestroy(e);
+        for (auto e : stop) cudaEventDestroy(e);
+    }
+    yg_status init(int m) {
+        if (!on) return YG_OK;
+        start.resize(m);
+        stop.resize(m);
+        for (int i = 0; i < m; ++i) {
+            YG_CUDA(cudaEventCreate(&start[i]));
+            YG_CUDA(cudaEventCreate(&stop[i]));
+        }
+        return YG_OK;
+    }
+    // add the first `done` pairs of the last replay (later ones were no-ops)
+    yg_status collect(int64_t done) {
+        if (!on) return YG_OK;
+        for (int64_t i = 0; i < done && i < (int64_t)start.size(); ++i) {
+            float t = 0;
+            YG_CUDA(cudaEventElapsedTime(&t, start[i], stop[i]));
+            ms += t;
+            ++launches;
+        }
+        return YG_OK;
+    }
+};
+
 static yg_status pcg_core(yg_matrix A, yg_precond M, const double *b, double *x, int precision, int criterion,
-                          double tol, int64_t maxiter, int check_every, Work &w, int64_t *iters, int *flag_out) {
+                          double tol, int64_t maxiter, int check_every, Work &w, int64_t *iters, int *flag_out,
+                          SpmvProfile *prof = nullptr) {
     yg_context ctx = A->ctx;
     const int64_t n = A->rows();
     const bool fused = !M || precond_fusable(M);
@@ -307,8 +343,12 @@ static yg_status pcg_core(yg_matrix A, yg_precond M, const double *b, double *x,
     YG_LAUNCHED(ctx);
     YG_CUDA(cudaGetLastError());
 
+    int slot = 0;
     auto one = [&](int parity) -> yg_status {
+        if (prof && prof->on) YG_CUDA(cudaEventRecordWithFlags(prof->start[slot], st, cudaEventRecordExternal));
         YG_TRY(spmv_launch(A, w.p, w.q, precision, P, &S->flag, spmv_grid));
+        if (prof && prof->on) YG_CUDA(cudaEventRecordWithFlags(prof->stop[slot], st, cudaEventRecordExternal));
+        ++slot;
         if (fused) {
             k_cg_update<true><<<G, kThreads, 0, st>>>(n, P, spmv_grid, S, parity, x, w.r, w.p, w.q, dinv, P + 2 * G);
             YG_LAUNCHED(ctx);
@@ -329,11 +369,14 @@ static yg_status pcg_core(yg_matrix A, yg_precond M, const double *b, double *x,
     YG_TRY(read_scalars(ctx, &hs));
     if (hs.flag == FLAG_RUN) {
         IterGraph g;
+        if (prof && prof->on && prof->start.empty()) YG_TRY(prof->init(check_every));
         YG_TRY(capture(ctx, check_every, one, g));
         for (;;) {
+            int64_t before = hs.iter;
             YG_CUDA(cudaGraphLaunch(g.exec, st));
             ctx->launches += g.kernels;
             YG_TRY(read_scalars(ctx, &hs));
+            if (prof) YG_TRY(prof->collect(hs.iter - before));
             if (hs.flag != FLAG_RUN) break;
         }
     }
@@ -363,8 +406,10 @@ yg_status solve_cg(yg_matrix A, yg_precond M, yg_vector bv, yg_vector xv, const 
     yg_solve_stats st{};
     int flag = FLAG_RUN;
     int64_t its = 0;
+    SpmvProfile prof;
+    prof.on = o.profile != 0;
     if (o.precision == YG_PREC_FP64) {
-        YG_TRY(pcg_core(A, M, bv->d, xv->d, YG_PREC_FP64, o.criterion, o.tol, maxiter, m, w, &its, &flag));
+        YG_TRY(pcg_core(A, M, bv->d, xv->d, YG_PREC_FP64, o.criterion, o.tol, maxiter, m, w, &its, &flag, &prof));
         st.iterations = its;
         // RELRES: the recursive residual triggered the stop; confirm with the true
         // residual and continue from it (at most a few restarts) if it drifted.
@@ -374,7 +419,7 @@ yg_status solve_cg(yg_matrix A, yg_precond M, yg_vector bv, yg_vector xv, const 
                 YG_TRY(true_relres(A, bv->d, xv->d, w.q, &rel));
                 if (rel <= o.tol) break;
                 int64_t more = 0;
-                YG_TRY(pcg_core(A, M, bv->d, xv->d, YG_PREC_FP64, o.criterion, o.tol, maxiter - st.iterations, m, w, &more, &flag));
+                YG_TRY(pcg_core(A, M, bv->d, xv->d, YG_PREC_FP64, o.criterion, o.tol, maxiter - st.iterations, m, w, &more, &flag, &prof));
                 st.iterations += more;
             }
         }
@@ -407,7 +452,7 @@ yg_status solve_cg(yg_matrix A, yg_precond M, yg_vector bv, yg_vector xv, const 
             YG_CUDA(cudaMemsetAsync(w.d, 0, sizeof(double) * n, ctx->stream));
             int iflag = 0;
             int64_t iits = 0;
-            YG_TRY(pcg_core(A, M, w.t, w.d, YG_PREC_MIXED, YG_CRIT_RELRES, eta, maxiter - st.iterations, m, w, &iits, &iflag));
+            YG_TRY(pcg_core(A, M, w.t, w.d, YG_PREC_MIXED, YG_CRIT_RELRES, eta, maxiter - st.iterations, m, w, &iits, &iflag, &prof));
             st.iterations += iits;
             st.refinements += 1;
             k_add<<<stream_grid(ctx, n), kThreads, 0, ctx->stream>>>(n, xv->d, w.d);
@@ -425,6 +470,8 @@ yg_status solve_cg(yg_matrix A, yg_precond M, yg_vector bv, yg_vector xv, const 
     cudaEventDestroy(e1);
     st.rel_residual = rel;
     st.device_ms = ms;
+    st.spmv_ms = prof.ms;
+    st.spmv_launches = prof.launches;
     yg_status s = flag_to_status(flag);
     if (o.criterion == YG_CRIT_RELRES && s == YG_OK && !(rel <= o.tol)) s = YG_NOT_CONVERGED;
     st.status = s;
