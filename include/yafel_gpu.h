@@ -176,6 +176,19 @@ enum { YG_PREC_FP64 = 0, YG_PREC_MIXED = 1 };
 YG_API yg_status yg_spmv(yg_matrix A, yg_vector x, yg_vector y);
 YG_API yg_status yg_spmv_ex(yg_matrix A, yg_vector x, yg_vector y, int32_t precision);
 
+/* SpMV kernel choice (no reference counterpart; the reference has one loop).
+ * variant 0: flat, `lanes` lanes per block row read the value stream coalesced;
+ * variant 1: each warp stages its rows' values in shared memory with cp.async
+ * (2x2 and 3x3 blocks).  variant -1 re-runs the device autotuner, which times
+ * the candidates on this matrix and keeps the fastest (it also runs on the
+ * first SpMV or solve of a matrix). */
+YG_API yg_status yg_matrix_set_spmv(yg_matrix A, int32_t variant, int32_t lanes);
+YG_API yg_status yg_matrix_get_spmv(yg_matrix A, int32_t *variant, int32_t *lanes);
+/* Average device time of `reps` back-to-back SpMVs (CUDA events on the
+ * context's stream), for roofline measurements. */
+YG_API yg_status yg_spmv_bench(yg_matrix A, yg_vector x, yg_vector y, int32_t precision, int32_t reps,
+                               double *ms_per_launch);
+
 /* ------------------------------------------------------------------ preconditioners */
 
 /* IdentityPreconditioner (IdentityPreconditioner.hpp:20-29), JacobiPreconditioner

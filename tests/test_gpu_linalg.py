@@ -45,12 +45,19 @@ def test_spmv_matches_oracle(ctx, B, per_row):
     A = yb.sparse_bcsr.from_bcsr(B, rp, col, val) if B > 1 else yb.sparse_csr.from_csr(rp, col, val)
     Ao = bcsr_to_oracle_csr(rp, col, val, B)
     x = np.random.Generator(np.random.PCG64(7)).standard_normal(A.cols())
-    y = A * x
     yo = Ao.spmv(x)
     scale = np.abs(val).max() * np.abs(x).max() * (per_row + 1) * B
-    assert np.abs(y - yo).max() <= 1e-14 * scale
-    # determinism: same bits twice
-    assert np.array_equal(y, A * x)
+    variants = [(0, 4), (0, 32)] + ([(1, 32)] if B in (2, 3) else []) + [(-1, 32)]
+    for v, L in variants:
+        A.set_spmv(v, L)
+        y = A * x
+        assert np.abs(y - yo).max() <= 1e-14 * scale, (v, L)
+        # determinism: same bits twice
+        assert np.array_equal(y, A * x)
+        if B in (2, 3):
+            y32 = A.spmv(x, precision=yb.PREC_MIXED).numpy()
+            yo32 = bcsr_to_oracle_csr(rp, col, val.astype(np.float32).astype(np.float64), B).spmv(x)
+            assert np.abs(y32 - yo32).max() <= 1e-13 * np.abs(yo32).max(), (v, L)
 
 
 @pytest.mark.parametrize("B", [1, 3])

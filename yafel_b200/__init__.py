@@ -344,6 +344,23 @@ class _Matrix:
     def make_fp32(self):
         check(lib().yg_matrix_make_fp32(self.h))
 
+    def set_spmv(self, variant, lanes=32):
+        """variant 0 flat (lanes per row), 1 shared-memory staged, -1 autotune."""
+        check(lib().yg_matrix_set_spmv(self.h, int(variant), int(lanes)))
+
+    def get_spmv(self):
+        v, l = C.c_int32(), C.c_int32()
+        check(lib().yg_matrix_get_spmv(self.h, C.byref(v), C.byref(l)))
+        return v.value, l.value
+
+    def spmv_bench(self, reps=10, precision=PREC_FP64, x=None):
+        """Average device milliseconds of one SpMV (CUDA events)."""
+        xd = x if x is not None else DeviceVector(np.ones(self._cols), self.ctx)
+        yd = DeviceVector(self._rows, self.ctx)
+        ms = C.c_double()
+        check(lib().yg_spmv_bench(self.h, xd.h, yd.h, precision, int(reps), C.byref(ms)))
+        return ms.value
+
     def spmv(self, x, y=None, precision=PREC_FP64):
         xd, _ = _as_device(x, self.ctx)
         yd = y if y is not None else DeviceVector(self._rows, self.ctx)

@@ -16,6 +16,7 @@
 #include "internal.h"
 #include "device_common.cuh"
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 
@@ -137,7 +138,8 @@ k_bicg_s(int64_t n, const double *__restrict__ partials, int np, KrylovScalars *
 __global__ void __launch_bounds__(kThreads)
 k_bicg_x(int64_t n, const double *__restrict__ partials, int np, KrylovScalars *S, double *__restrict__ x,
          double *__restrict__ r, const double *__restrict__ rhat, const double *__restrict__ ph,
-         const double *__restrict__ s, const double *__restrict__ t, double *__restrict__ partials_out) {
+         const double *__restrict__ sh, const double *__restrict__ s, const double *__restrict__ t,
+         double *__restrict__ partials_out) {
     __shared__ double sm[kThreads / 32 + 1];
     if (read_flag(&S->flag)) return;
     const double ts = reduce_partials<kThreads>(partials, np, 2, 0, sm);
@@ -148,7 +150,7 @@ k_bicg_x(int64_t n, const double *__restrict__ partials, int np, KrylovScalars *
     block_chunk(n, lo, hi);
     double s0 = 0, s1 = 0;
     for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
-        x[i] += ph[i] * alpha + s[i] * omega;
+        x[i] += ph[i] * alpha + sh[i] * omega;  // M^-1 p and M^-1 s (p and s without M)
         double ri = s[i] - t[i] * omega;
         r[i] = ri;
         s0 += rhat[i] * ri;
@@ -204,6 +206,7 @@ yg_status solve_bicgstab(yg_matrix A, yg_precond M, yg_vector bv, yg_vector xv, 
     const double *dinv = precond_dinv(M);
     const int64_t maxiter = o.maxiter > 0 ? o.maxiter : 100 * n + 1000;
     const int G = ctx->reduce_blocks;
+    const int SG = std::min(spmv_default_grid(A), G);  // SpMV grid = partials count
     cudaStream_t st = ctx->stream;
     double *P = ctx->d_partials;
     KrylovScalars *S = ctx->d_scalars;
@@ -243,11 +246,11 @@ yg_status solve_bicgstab(yg_matrix A, yg_precond M, yg_vector bv, yg_vector xv, 
         auto one = [&](int parity) -> yg_status {
             k_bicg_p<<<G, kThreads, 0, st>>>(n, P, G, S, parity, p, r, v, ph, dinv);
             YG_LAUNCHED(ctx);
-            YG_TRY(spmv_launch_ex(A, pin, v, YG_PREC_FP64, rhat, P + 2 * G, 1, &S->flag, G));
-            k_bicg_s<<<G, kThreads, 0, st>>>(n, P + 2 * G, G, S, parity, r, v, s, sh, dinv);
+            YG_TRY(spmv_launch_ex(A, pin, v, YG_PREC_FP64, rhat, P + 2 * G, 1, &S->flag, SG));
+            k_bicg_s<<<G, kThreads, 0, st>>>(n, P + 2 * G, SG, S, parity, r, v, s, sh, dinv);
             YG_LAUNCHED(ctx);
-            YG_TRY(spmv_launch_ex(A, sin, t, YG_PREC_FP64, s, P + 4 * G, 2, &S->flag, G));
-            k_bicg_x<<<G, kThreads, 0, st>>>(n, P + 4 * G, G, S, xv->d, r, rhat, pin, s, t, P);
+            YG_TRY(spmv_launch_ex(A, sin, t, YG_PREC_FP64, s, P + 4 * G, 2, &S->flag, SG));
+            k_bicg_x<<<G, kThreads, 0, st>>>(n, P + 4 * G, SG, S, xv->d, r, rhat, pin, sin, s, t, P);
             YG_LAUNCHED(ctx);
             return YG_OK;
         };
@@ -391,6 +394,7 @@ extern "C" yg_status yg_bicgstab(yg_matrix A, yg_precond M, yg_vector b, yg_vect
     if (!A || !b || !x) return fail(YG_BAD_ARG, "yg_bicgstab: NULL argument");
     if (A->rows() != A->cols() || b->n != A->rows() || x->n != A->rows())
         return fail(YG_BAD_ARG, "yg_bicgstab: dimension mismatch");
+    YG_TRY(spmv_autotune_device(A));
     yg_status s = solve_bicgstab(A, M, b, x, opts, stats);
     if (s != YG_OK && s != YG_UNSUPPORTED && s < YG_TIMEOUT) set_error("yg_bicgstab: %s", yg_status_string(s));
     return s;

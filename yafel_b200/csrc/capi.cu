@@ -452,7 +452,52 @@ extern "C" yg_status yg_spmv_ex(yg_matrix A, yg_vector x, yg_vector y, int32_t p
         return fail(YG_BAD_ARG, "yg_spmv: dimension mismatch (A %lldx%lld, x %lld, y %lld)", (long long)A->rows(),
                     (long long)A->cols(), (long long)x->n, (long long)y->n);
     if (precision == YG_PREC_MIXED && !A->d_val32) YG_TRY(yg_matrix_make_fp32(A));
+    YG_TRY(spmv_autotune_device(A));
     return spmv_launch(A, x->d, y->d, precision, nullptr, nullptr, spmv_default_grid(A));
 }
 
 extern "C" yg_status yg_spmv(yg_matrix A, yg_vector x, yg_vector y) { return yg_spmv_ex(A, x, y, YG_PREC_FP64); }
+
+extern "C" yg_status yg_matrix_set_spmv(yg_matrix A, int32_t variant, int32_t lanes) {
+    if (!A || variant < -1 || variant > 1 || (lanes != 2 && lanes != 4 && lanes != 8 && lanes != 16 && lanes != 32))
+        return fail(YG_BAD_ARG, "yg_matrix_set_spmv: bad variant/lanes");
+    if (variant == 1 && A->block != 2 && A->block != 3) return fail(YG_UNSUPPORTED, "staged SpMV needs 2x2 or 3x3 blocks");
+    if (variant < 0) {  // re-run the device autotuner
+        A->tuned = false;
+        return spmv_autotune_device(A);
+    }
+    A->variant = variant;
+    A->lanes = lanes;
+    A->tuned = true;
+    return YG_OK;
+}
+
+extern "C" yg_status yg_matrix_get_spmv(yg_matrix A, int32_t *variant, int32_t *lanes) {
+    if (!A) return fail(YG_BAD_ARG, "NULL matrix");
+    if (variant) *variant = A->variant;
+    if (lanes) *lanes = A->lanes;
+    return YG_OK;
+}
+
+extern "C" yg_status yg_spmv_bench(yg_matrix A, yg_vector x, yg_vector y, int32_t precision, int32_t reps,
+                                   double *ms_per_launch) {
+    if (!A || !x || !y || reps < 1 || !ms_per_launch) return fail(YG_BAD_ARG, "yg_spmv_bench: bad argument");
+    if (x->n != A->cols() || y->n != A->rows()) return fail(YG_BAD_ARG, "yg_spmv_bench: dimension mismatch");
+    if (precision == YG_PREC_MIXED && !A->d_val32) YG_TRY(yg_matrix_make_fp32(A));
+    yg_context ctx = A->ctx;
+    int grid = spmv_default_grid(A);
+    YG_TRY(spmv_launch(A, x->d, y->d, precision, nullptr, nullptr, grid));
+    cudaEvent_t e0, e1;
+    YG_CUDA(cudaEventCreate(&e0));
+    YG_CUDA(cudaEventCreate(&e1));
+    cudaEventRecord(e0, ctx->stream);
+    for (int r = 0; r < reps; ++r) YG_TRY(spmv_launch(A, x->d, y->d, precision, nullptr, nullptr, grid));
+    cudaEventRecord(e1, ctx->stream);
+    YG_CUDA(cudaEventSynchronize(e1));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *ms_per_launch = ms / reps;
+    return YG_OK;
+}

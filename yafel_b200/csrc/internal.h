@@ -88,7 +88,9 @@ struct yg_matrix_t {
     double *d_val = nullptr;      // nnzb*block*block (row-major blocks)
     float *d_val32 = nullptr;     // optional FP32 copy
     int32_t *d_diag = nullptr;    // position of the diagonal block in each block row, -1 if absent
-    int lanes = 32;               // SpMV lanes per block row (autotuned)
+    int lanes = 32;               // SpMV lanes per block row (flat variant)
+    int variant = 0;              // SpMV variant: 0 flat lane-strided, 1 shared-memory staged (B = 2, 3)
+    bool tuned = false;
     const void *owner = nullptr;  // dofmap whose pattern this is (assembly re-use)
     int32_t owner_format = -1;
     int64_t rows() const { return nbrows * block; }
@@ -125,6 +127,7 @@ yg_status spmv_launch_ex(yg_matrix A, const double *x, double *y, int precision,
                          int dot_mode, const int32_t *flag, int grid);
 int spmv_default_grid(yg_matrix A);
 void spmv_autotune(yg_matrix A);
+yg_status spmv_autotune_device(yg_matrix A);
 yg_status vector_dot(yg_context ctx, const double *a, const double *b, int64_t n, double *out);
 yg_status matrix_build_diag(yg_matrix A);
 yg_status matrix_from_device_pattern(yg_matrix A);

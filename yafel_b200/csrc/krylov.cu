@@ -19,6 +19,7 @@
 #include "internal.h"
 #include "device_common.cuh"
 
+#include <algorithm>
 #include <cmath>
 #include <chrono>
 
@@ -318,7 +319,7 @@ static yg_status pcg_core(yg_matrix A, yg_precond M, const double *b, double *x,
     const bool fused = !M || precond_fusable(M);
     const double *dinv = M ? precond_dinv(M) : nullptr;
     const int G = ctx->reduce_blocks;
-    const int spmv_grid = G;
+    const int spmv_grid = std::min(spmv_default_grid(A), kMaxReduceBlocks);
     double *P = ctx->d_partials;  // [0,G): p.q ; [2G,4G): r.z/r.r pairs ; [4G, 7G): init triples
     KrylovScalars *S = ctx->d_scalars;
     cudaStream_t st = ctx->stream;
@@ -489,6 +490,7 @@ extern "C" yg_status yg_cg(yg_matrix A, yg_precond M, yg_vector b, yg_vector x, 
     if (A->rows() != A->cols() || b->n != A->rows() || x->n != A->rows())
         return fail(YG_BAD_ARG, "yg_cg: dimension mismatch");
     if (M && M->A->rows() != A->rows()) return fail(YG_BAD_ARG, "yg_cg: preconditioner size mismatch");
+    YG_TRY(spmv_autotune_device(A));
     yg_status s = solve_cg(A, M, b, x, opts, stats);
     if (s != YG_OK && s != YG_NOT_CONVERGED && s != YG_BREAKDOWN && s != YG_NAN) return s;
     if (s != YG_OK) set_error("yg_cg: %s", yg_status_string(s));
