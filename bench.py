@@ -128,15 +128,27 @@ def run_gpu(args):
         bcs.append(bc)
     trac_dev = yb.DeviceVector(traction, ctx)
 
-    def step(precision, profile=False):
+    phases = {"assemble": [], "bc": [], "solve": []}
+
+    def step(precision, profile=False, record=False):
+        t0 = time.perf_counter()
         fe = yb.FESystem(dm, 3, format=yb.BCSR)
         yb.CGAssembly(phys, fe)
         K, F = fe.getGlobalTangent(), fe.getGlobalResidual()
         F.axpy(1.0, trac_dev)
+        ctx.synchronize()
+        t1 = time.perf_counter()
         for bc in bcs:
             bc.apply(K, F)
         M = yb.JacobiPreconditioner(K)
+        ctx.synchronize()
+        t2 = time.perf_counter()
         x, st = yb.solve(K, F, M=M, tol=TOL, precision=precision, profile=profile)
+        t3 = time.perf_counter()
+        if record:
+            phases["assemble"].append(t1 - t0)
+            phases["bc"].append(t2 - t1)
+            phases["solve"].append(t3 - t2)
         return K, x, st
 
     def timed(precision, steps, warmup, profile=False):
@@ -150,7 +162,7 @@ def run_gpu(args):
         t0 = time.perf_counter()
         stats = []
         for _ in range(steps):
-            K, x, st = step(precision, profile)
+            K, x, st = step(precision, profile, record=(precision == 0))
             stats.append(st)
         ctx.synchronize()
         wall = time.perf_counter() - t0
@@ -162,7 +174,8 @@ def run_gpu(args):
     clocks.start()
     wall64, st64, launches, K, x = timed(0, args.steps, args.warmup, profile=True)
     clk = clocks.stop()
-    wallmx, stmx, _, _, _ = timed(1, args.steps, max(1, args.warmup // 3))
+    wallmx, stmx, _, Kmx, _ = timed(1, args.steps, max(1, args.warmup // 3), profile=True)
+    wallir, stir, _, _, _ = timed(2, 1, 0)
     step_s = wall64 / args.steps
     if torch_dist:
         import torch
@@ -197,6 +210,10 @@ def run_gpu(args):
     nnzb = K.nnz() // 9
     spmv_bytes = bcsr3_spmv_bytes(nnzb, ndofs)
     spmv_ms = sum(s.spmv_ms for s in st64) / max(1, sum(s.spmv_launches for s in st64))
+    spmv32_ms = sum(s.spmv_ms for s in stmx) / max(1, sum(s.spmv_launches for s in stmx))
+    spmv32_bytes = nnzb * (4 * 9 + 4) + 4 * (ndofs // 3 + 1) + 16 * ndofs
+    variant, lanes = K.get_spmv()
+    kname = ("k_bcsr_spmv_staged<3,double,1>" if variant == 1 else "k_bcsr_spmv<3,%d,double,1>" % lanes)
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -222,14 +239,18 @@ def run_gpu(args):
         "gpu_launches": int(launches),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None, "traffic": None,
-                     "kernel": "k_bcsr_spmv<3,32,double,1>", "bytes_per_launch": spmv_bytes,
-                     "ms_per_launch": spmv_ms, "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback"},
+                     "kernel": kname, "bytes_per_launch": spmv_bytes,
+                     "ms_per_launch": spmv_ms, "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback",
+                     "fp32_values_kernel_GBs": spmv32_bytes / (spmv32_ms * 1e-3) / 1e9 if spmv32_ms > 0 else None},
         "solver": {"fp64_iterations": iters64, "fp64_relres": max(s.rel_residual for s in st64),
                    "mixed_iterations": itersmx, "mixed_relres": max(s.rel_residual for s in stmx),
                    "mixed_refinements": statistics.mean(s.refinements for s in stmx),
                    "fp64_step_ms": step_s * 1e3, "mixed_step_ms": mixed_step * 1e3,
                    "mixed_dofs_per_s": ws * ndofs / mixed_step, "mixed_speedup": step_s / mixed_step,
-                   "solve_ms": statistics.mean(s.device_ms for s in st64)},
+                   "solve_ms": statistics.mean(s.device_ms for s in st64),
+                   "mixed_ir_iterations": stir[0].iterations, "mixed_ir_step_ms": wallir * 1e3,
+                   "mixed_ir_relres": stir[0].rel_residual},
+        "phases_ms": {k: 1e3 * statistics.mean(v) for k, v in phases.items() if v},
         "setup": {"dof_numbering_s": t_dof},
         "clocks": clk,
     }

@@ -172,7 +172,7 @@ YG_API yg_status yg_matrix_make_fp32(yg_matrix A);
 /* y = A*x: csr_spmv / bcsr_spmv via operator* (include/old_handmade_linalg/csr_spmv.hpp:25-56,
  * bcsr_spmv.hpp:23-62, operators.hpp:117-131).  precision: YG_PREC_FP64 or
  * YG_PREC_MIXED (FP32 values, FP64 vectors and accumulation). */
-enum { YG_PREC_FP64 = 0, YG_PREC_MIXED = 1 };
+enum { YG_PREC_FP64 = 0, YG_PREC_MIXED = 1, YG_PREC_MIXED_IR = 2 };
 YG_API yg_status yg_spmv(yg_matrix A, yg_vector x, yg_vector y);
 YG_API yg_status yg_spmv_ex(yg_matrix A, yg_vector x, yg_vector y, int32_t precision);
 
@@ -216,7 +216,11 @@ YG_API int64_t yg_precond_zero_pivots(yg_precond M);
 enum { YG_CRIT_REFERENCE = 0, YG_CRIT_RELRES = 1 };
 typedef struct yg_solve_opts {
     int32_t criterion;  /* YG_CRIT_* */
-    int32_t precision;  /* YG_PREC_FP64, or YG_PREC_MIXED: FP32 matrix inside FP64 iterative refinement */
+    int32_t precision;  /* YG_PREC_FP64; YG_PREC_MIXED: the iteration's SpMV reads FP32 values (FP64
+                           vectors, accumulation and dots) and the residual is replaced by the FP64
+                           true residual b - A x whenever it fell 10x -- each replacement is an FP64
+                           refinement step; YG_PREC_MIXED_IR: restarted FP64 iterative refinement
+                           around FP32-SpMV PCG inner solves */
     double tol;         /* see criterion */
     int64_t maxiter;    /* 0 = the reference's default (N for CG) */
     int32_t check_every;/* iterations between host convergence checks (0 = automatic) */
@@ -226,7 +230,7 @@ typedef struct yg_solve_stats {
     int64_t iterations;       /* Krylov iterations (inner iterations summed for MIXED) */
     double rel_residual;      /* ||b - A x|| / ||b|| recomputed in FP64 */
     int32_t status;           /* yg_status of the solve */
-    int32_t refinements;      /* outer FP64 refinement steps (MIXED) */
+    int32_t refinements;      /* FP64 residual replacements / refinement steps */
     double device_ms;         /* device time of the solve (CUDA events) */
     double spmv_ms;           /* with opts.profile: summed device time of the iteration SpMVs */
     int64_t spmv_launches;    /* with opts.profile: number of SpMVs timed */

@@ -27,7 +27,7 @@ __all__ = ["Context", "default_context", "Mesh", "DoFManager", "FESystem", "CGAs
 CG_SOLVER_TOL = 1.0e-14
 
 CSR, BCSR = 0, 1
-PREC_FP64, PREC_MIXED = 0, 1
+PREC_FP64, PREC_MIXED, PREC_MIXED_IR = 0, 1, 2
 CRIT_REFERENCE, CRIT_RELRES = 0, 1
 POISSON, ELASTICITY, SUPG = 0, 1, 2
 

@@ -101,6 +101,21 @@ k_cg_scalars_init(KrylovScalars *S, const double *__restrict__ partials, int np,
     }
 }
 
+// After a residual replacement: r.z and r.r of the true FP64 residual into both
+// parity slots.
+__global__ void __launch_bounds__(kThreads)
+k_cg_scalars_replace(KrylovScalars *S, const double *__restrict__ partials, int np, int stride, int clear_flag) {
+    __shared__ double sm[kThreads / 32 + 1];
+    double rz = reduce_partials<kThreads>(partials, np, stride, 0, sm);
+    double rr = reduce_partials<kThreads>(partials, np, stride, 1, sm);
+    if (threadIdx.x == 0) {
+        S->rz[0] = rz;
+        S->rz[1] = rz;
+        S->rr = rr;
+        if (clear_flag) S->flag = 0;
+    }
+}
+
 // Kernel 2 of the iteration.  JAC: z = dinv*r computed in registers (M is
 // Jacobi or identity); otherwise only r.r partials (z comes from M later).
 template <bool FUSED>
@@ -313,7 +328,7 @@ struct SpmvProfile {
 
 static yg_status pcg_core(yg_matrix A, yg_precond M, const double *b, double *x, int precision, int criterion,
                           double tol, int64_t maxiter, int check_every, Work &w, int64_t *iters, int *flag_out,
-                          SpmvProfile *prof = nullptr) {
+                          SpmvProfile *prof = nullptr, int64_t *replacements = nullptr) {
     yg_context ctx = A->ctx;
     const int64_t n = A->rows();
     const bool fused = !M || precond_fusable(M);
@@ -366,19 +381,71 @@ static yg_status pcg_core(yg_matrix A, yg_precond M, const double *b, double *x,
         }
         return YG_OK;
     };
+    // Residual replacement: r = b - A x with the FP64 matrix, r.z and r.r of it into
+    // the scalars (z stays implicit in the fused path).  It is the FP64
+    // iterative-refinement step of the mixed-precision solve, and the final check
+    // of every RELRES solve.
+    auto replace = [&](int clear_flag) -> yg_status {
+        YG_TRY(spmv_launch(A, x, w.q, YG_PREC_FP64, nullptr, nullptr, spmv_default_grid(A)));
+        if (fused) {
+            k_residual_init<<<G, kThreads, 0, st>>>(n, b, w.q, w.r, nullptr, dinv, P + 4 * G);
+            YG_LAUNCHED(ctx);
+        } else {
+            k_residual_init<<<G, kThreads, 0, st>>>(n, b, w.q, w.r, nullptr, nullptr, P + 4 * G);
+            YG_LAUNCHED(ctx);
+            YG_TRY(precond_apply_dev(M, w.r, w.z));
+            k_dot2_partials<<<G, kThreads, 0, st>>>(n, w.r, w.z, P + 4 * G, nullptr, 0, 3);
+            YG_LAUNCHED(ctx);
+        }
+        k_cg_scalars_replace<<<1, kThreads, 0, st>>>(S, P + 4 * G, G, 3, clear_flag);
+        YG_LAUNCHED(ctx);
+        if (replacements) ++*replacements;
+        return YG_OK;
+    };
+    const bool reliable = (precision == YG_PREC_MIXED);
     KrylovScalars hs;
     YG_TRY(read_scalars(ctx, &hs));
-    if (hs.flag == FLAG_RUN) {
+    if (hs.flag == FLAG_RUN || (hs.flag == FLAG_CONVERGED && criterion == YG_CRIT_RELRES && hs.iter > 0)) {
         IterGraph g;
         if (prof && prof->on && prof->start.empty()) YG_TRY(prof->init(check_every));
         YG_TRY(capture(ctx, check_every, one, g));
+        double rr_last = hs.rr;  // r.r at the last replacement
+        int false_stops = 0;
         for (;;) {
             int64_t before = hs.iter;
             YG_CUDA(cudaGraphLaunch(g.exec, st));
             ctx->launches += g.kernels;
             YG_TRY(read_scalars(ctx, &hs));
             if (prof) YG_TRY(prof->collect(hs.iter - before));
-            if (hs.flag != FLAG_RUN) break;
+            if (hs.flag == FLAG_RUN) {
+                // replace once the recursive residual fell 10x since the last time
+                if (reliable && hs.rr < 1e-2 * rr_last) {
+                    YG_TRY(replace(0));
+                    YG_TRY(read_scalars(ctx, &hs));
+                    rr_last = hs.rr;
+                }
+                continue;
+            }
+            if (hs.flag == FLAG_CONVERGED && criterion == YG_CRIT_RELRES) {
+                // the recursive residual triggered the stop; the FP64 residual decides
+                YG_TRY(replace(1));
+                YG_TRY(read_scalars(ctx, &hs));
+                rr_last = hs.rr;
+                if (sqrt(hs.rr) <= tol * sqrt(hs.bb) || hs.iter >= maxiter || ++false_stops > 20) {
+                    hs.flag = (sqrt(hs.rr) <= tol * sqrt(hs.bb)) ? FLAG_CONVERGED
+                                                                  : (hs.iter >= maxiter ? FLAG_MAXITER : FLAG_CONVERGED);
+                    break;
+                }
+                // continue from the true residual with a fresh direction p = M^-1 r
+                if (fused) {
+                    k_p_init<<<stream_grid(ctx, n), kThreads, 0, st>>>(n, w.p, w.r, nullptr, dinv);
+                } else {
+                    k_p_init<<<stream_grid(ctx, n), kThreads, 0, st>>>(n, w.p, w.r, w.z, nullptr);
+                }
+                YG_LAUNCHED(ctx);
+                continue;
+            }
+            break;
         }
     }
     *iters = hs.iter;
@@ -409,25 +476,19 @@ yg_status solve_cg(yg_matrix A, yg_precond M, yg_vector bv, yg_vector xv, const 
     int64_t its = 0;
     SpmvProfile prof;
     prof.on = o.profile != 0;
-    if (o.precision == YG_PREC_FP64) {
-        YG_TRY(pcg_core(A, M, bv->d, xv->d, YG_PREC_FP64, o.criterion, o.tol, maxiter, m, w, &its, &flag, &prof));
+    if (o.precision == YG_PREC_FP64 || o.precision == YG_PREC_MIXED) {
+        // FP64, or FP32 matrix values in the iteration with the residual replaced
+        // by the FP64 true residual each time it fell 10x (refinement steps).
+        if (o.precision == YG_PREC_MIXED && !A->d_val32) YG_TRY(yg_matrix_make_fp32(A));
+        int64_t repl = 0;
+        YG_TRY(pcg_core(A, M, bv->d, xv->d, o.precision, o.criterion, o.tol, maxiter, m, w, &its, &flag, &prof,
+                        &repl));
         st.iterations = its;
-        // RELRES: the recursive residual triggered the stop; confirm with the true
-        // residual and continue from it (at most a few restarts) if it drifted.
-        if (o.criterion == YG_CRIT_RELRES) {
-            for (int restart = 0; restart < 4 && flag == FLAG_CONVERGED; ++restart) {
-                double rel = 0;
-                YG_TRY(true_relres(A, bv->d, xv->d, w.q, &rel));
-                if (rel <= o.tol) break;
-                int64_t more = 0;
-                YG_TRY(pcg_core(A, M, bv->d, xv->d, YG_PREC_FP64, o.criterion, o.tol, maxiter - st.iterations, m, w, &more, &flag, &prof));
-                st.iterations += more;
-            }
-        }
+        st.refinements = (int32_t)repl;
     } else {
-        // Mixed precision: FP64 iterative refinement around a PCG whose SpMV reads
-        // FP32 values (FP64 vectors and accumulation).  Outer residuals and the
-        // final check are FP64.
+        // YG_PREC_MIXED_IR: restarted FP64 iterative refinement around a PCG whose
+        // SpMV reads FP32 values (FP64 vectors and accumulation).  Outer residuals
+        // and the final check are FP64.
         if (!A->d_val32) YG_TRY(yg_matrix_make_fp32(A));
         YG_TRY(alloc_vec(ctx, &w.d, n));
         YG_TRY(alloc_vec(ctx, &w.t, n));
@@ -453,7 +514,7 @@ yg_status solve_cg(yg_matrix A, yg_precond M, yg_vector bv, yg_vector xv, const 
             YG_CUDA(cudaMemsetAsync(w.d, 0, sizeof(double) * n, ctx->stream));
             int iflag = 0;
             int64_t iits = 0;
-            YG_TRY(pcg_core(A, M, w.t, w.d, YG_PREC_MIXED, YG_CRIT_RELRES, eta, maxiter - st.iterations, m, w, &iits, &iflag, &prof));
+            YG_TRY(pcg_core(A, M, w.t, w.d, YG_PREC_MIXED_IR, YG_CRIT_RELRES, eta, maxiter - st.iterations, m, w, &iits, &iflag, &prof));
             st.iterations += iits;
             st.refinements += 1;
             k_add<<<stream_grid(ctx, n), kThreads, 0, ctx->stream>>>(n, xv->d, w.d);

@@ -88,21 +88,24 @@ k_bcsr_spmv(int64_t nbrows, const int32_t *__restrict__ rowptr, const int32_t *_
 }
 
 // ---------------------------------------------------------------------------
-// Staged variant for B = 2, 3.  Each warp owns a sequence of block rows; the
-// row's value bytes are copied into a per-warp shared-memory stage with 16-byte
-// cp.async copies (L2 evict-first), double-buffered so the next chunk is in
-// flight while the current one is consumed.  Then lane l owns whole blocks
-// l, l+32, ... of the chunk: it reads the block's B*B values from shared memory,
-// one column index and B entries of x, so each value costs one shared load and
-// one FMA.  A chunk holds up to CH blocks; longer rows are processed in chunks.
-// Copies start at the 16-byte boundary below the chunk and end at the one above
-// it (allocations carry 16 bytes of padding), and the consumer skips the lead.
+// Staged variant for B = 2, 3.  Each warp owns a sequence of block rows (grid
+// stride) cut into chunks of at most CH blocks.  A chunk's value bytes and its
+// block-column indices are copied into a per-warp shared-memory stage with
+// 16-byte cp.async copies (L2 evict-first); NST stages form a ring, so NST-1
+// chunks are in flight while one is consumed.  Consuming, lane l owns whole
+// blocks l, l+32, ... of the chunk: B*B shared loads of values, one shared load
+// of the column, B loads of x from L2, B*B FMAs.  Copies start at the 16-byte
+// boundary at or below the data and end at the one at or above it (device
+// allocations carry 16 bytes of padding); the consumer skips the lead bytes.
 template <int B, typename VT>
 struct Staged {
-    static constexpr int CH = 64;                                     // blocks per chunk
-    static constexpr int STAGE = CH * B * B * (int)sizeof(VT) + 32;   // bytes per stage
-    static constexpr int WARPS = 8;
-    static constexpr int SMEM = WARPS * 2 * STAGE;
+    static constexpr int CH = 64;                                      // blocks per chunk
+    static constexpr int VBYTES = CH * B * B * (int)sizeof(VT) + 32;   // value bytes per stage
+    static constexpr int CBYTES = CH * 4 + 32;                         // column bytes per stage
+    static constexpr int STAGE = VBYTES + CBYTES;
+    static constexpr int NST = 3;                                      // ring depth
+    static constexpr int WARPS = 4;
+    static constexpr int SMEM = WARPS * NST * STAGE;
 };
 
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem, uint64_t pol) {
@@ -110,7 +113,26 @@ __device__ __forceinline__ void cp_async16(void *smem, const void *gmem, uint64_
     asm volatile("cp.async.cg.shared.global.L2::cache_hint [%0], [%1], 16, %2;" ::"r"(s), "l"(gmem), "l"(pol));
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;"); }
-__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+// Chunk cursor of one warp: row r (grid stride `stride`), block offset b0.
+struct ChunkCursor {
+    int64_t r;
+    int b0, rs, re;
+    __device__ void load(const int32_t *__restrict__ rowptr, int64_t nbrows) {
+        rs = re = 0;
+        if (r < nbrows) { rs = __ldg(rowptr + r); re = __ldg(rowptr + r + 1); }
+    }
+    __device__ void advance(const int32_t *__restrict__ rowptr, int64_t nbrows, int64_t stride, int ch) {
+        b0 += ch;
+        if (b0 >= re - rs) {
+            r += stride;
+            b0 = 0;
+            load(rowptr, nbrows);
+        }
+    }
+};
 
 template <int B, typename VT, int DOT>
 __global__ void __launch_bounds__(Staged<B, VT>::WARPS * 32)
@@ -119,61 +141,60 @@ k_bcsr_spmv_staged(int64_t nbrows, const int32_t *__restrict__ rowptr, const int
                    const double *__restrict__ w, double *__restrict__ partials, const int32_t *__restrict__ flag) {
     using S = Staged<B, VT>;
     constexpr int B2 = B * B;
-    constexpr int BB = B2 * (int)sizeof(VT);  // bytes per block
+    constexpr int BB = B2 * (int)sizeof(VT);  // value bytes per block
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ double red[S::WARPS + 1];
+    __shared__ int leads[S::WARPS][S::NST][2];
     if (flag && read_flag(flag)) return;
     const uint64_t pol = evict_first_policy();
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    unsigned char *stage0 = smem_raw + (size_t)wib * 2 * S::STAGE;
-    const int64_t warp = (int64_t)blockIdx.x * S::WARPS + wib;
-    const int64_t nwarps = (int64_t)gridDim.x * S::WARPS;
+    unsigned char *ring = smem_raw + (size_t)wib * S::NST * S::STAGE;
+    const int64_t stride = (int64_t)gridDim.x * S::WARPS;
     const char *vbytes = reinterpret_cast<const char *>(val);
+    const char *cbytes = reinterpret_cast<const char *>(col);
 
-    // chunk cursor: row r, block offset b0 within the row
-    int64_t r = warp;
-    int b0 = 0;
-    int rs = 0, re = 0;
-    if (r < nbrows) { rs = __ldg(rowptr + r); re = __ldg(rowptr + r + 1); }
-    // issue the copy of chunk (r, b0) into stage st; returns the lead bytes
-    auto issue = [&](int64_t rr, int bb0, int rrs, int rre, int st) -> int {
-        int lead = 0;
-        if (rr < nbrows && rre > rrs) {
-            const int nb = min(S::CH, rre - rrs - bb0);
-            const int64_t start = (int64_t)(rrs + bb0) * BB;
-            const int64_t a0 = start & ~(int64_t)15;
-            const int64_t a1 = (start + (int64_t)nb * BB + 15) & ~(int64_t)15;
-            lead = (int)(start - a0);
-            unsigned char *dst = stage0 + st * S::STAGE;
-            for (int64_t off = (int64_t)lane * 16; off < a1 - a0; off += 32 * 16) cp_async16(dst + off, vbytes + a0 + off, pol);
+    auto issue = [&](const ChunkCursor &c, int st) {
+        int lv = 0, lc = 0;
+        if (c.r < nbrows && c.re > c.rs) {
+            const int nb = min(S::CH, c.re - c.rs - c.b0);
+            const int64_t first = (int64_t)(c.rs + c.b0);
+            const int64_t vs = first * BB, va = vs & ~(int64_t)15, ve = (vs + (int64_t)nb * BB + 15) & ~(int64_t)15;
+            const int64_t cs = first * 4, ca = cs & ~(int64_t)15, ce = (cs + (int64_t)nb * 4 + 15) & ~(int64_t)15;
+            lv = (int)(vs - va);
+            lc = (int)(cs - ca);
+            unsigned char *dst = ring + st * S::STAGE;
+            for (int64_t off = (int64_t)lane * 16; off < ve - va; off += 32 * 16) cp_async16(dst + off, vbytes + va + off, pol);
+            for (int64_t off = (int64_t)lane * 16; off < ce - ca; off += 32 * 16)
+                cp_async16(dst + S::VBYTES + off, cbytes + ca + off, pol);
         }
+        if (lane == 0) { leads[wib][st][0] = lv; leads[wib][st][1] = lc; }
         cp_async_commit();
-        return lead;
     };
+
+    ChunkCursor ci{(int64_t)blockIdx.x * S::WARPS + wib, 0, 0, 0};
+    ci.load(rowptr, nbrows);
+    ChunkCursor cc = ci;
+#pragma unroll
+    for (int k = 0; k < S::NST - 1; ++k) {
+        issue(ci, k);
+        if (ci.r < nbrows) ci.advance(rowptr, nbrows, stride, S::CH);
+    }
     double dot = 0, yy = 0;
     double acc[B];
 #pragma unroll
     for (int i = 0; i < B; ++i) acc[i] = 0;
     int st = 0;
-    int lead_cur = issue(r, b0, rs, re, 0);
-    while (r < nbrows) {
-        // next chunk cursor
-        int64_t rn = r;
-        int bn = b0 + S::CH, rsn = rs, ren = re;
-        if (bn >= re - rs) {
-            rn = r + nwarps;
-            bn = 0;
-            rsn = ren = 0;
-            if (rn < nbrows) { rsn = __ldg(rowptr + rn); ren = __ldg(rowptr + rn + 1); }
-        }
-        const int lead_next = issue(rn, bn, rsn, ren, st ^ 1);
-        cp_async_wait1();
+    while (cc.r < nbrows) {
+        issue(ci, (st + S::NST - 1) % S::NST);
+        if (ci.r < nbrows) ci.advance(rowptr, nbrows, stride, S::CH);
+        cp_async_wait<S::NST - 1>();
         __syncwarp();
-        // consume chunk (r, b0) from stage st
-        const int nb = max(0, min(S::CH, re - rs - b0));
-        const VT *blk = reinterpret_cast<const VT *>(stage0 + st * S::STAGE + lead_cur);
+        const int nb = max(0, min(S::CH, cc.re - cc.rs - cc.b0));
+        const unsigned char *stg = ring + st * S::STAGE;
+        const VT *blk = reinterpret_cast<const VT *>(stg + leads[wib][st][0]);
+        const int32_t *cix = reinterpret_cast<const int32_t *>(stg + S::VBYTES + leads[wib][st][1]);
         for (int j = lane; j < nb; j += 32) {
-            const int c = __ldg(col + rs + b0 + j);
+            const int c = cix[j];
             double xv[B];
 #pragma unroll
             for (int k = 0; k < B; ++k) xv[k] = __ldg(x + (int64_t)B * c + k);
@@ -183,7 +204,7 @@ k_bcsr_spmv_staged(int64_t nbrows, const int32_t *__restrict__ rowptr, const int
                 for (int k = 0; k < B; ++k) acc[i] = fma((double)blk[j * B2 + i * B + k], xv[k], acc[i]);
         }
         __syncwarp();
-        if (b0 + S::CH >= re - rs) {  // row complete
+        if (cc.b0 + S::CH >= cc.re - cc.rs) {  // row complete
 #pragma unroll
             for (int i = 0; i < B; ++i) {
 #pragma unroll
@@ -192,20 +213,16 @@ k_bcsr_spmv_staged(int64_t nbrows, const int32_t *__restrict__ rowptr, const int
             if (lane == 0) {
 #pragma unroll
                 for (int i = 0; i < B; ++i) {
-                    y[B * r + i] = acc[i];
-                    if (DOT >= 1) dot = fma(acc[i], w[B * r + i], dot);
+                    y[B * cc.r + i] = acc[i];
+                    if (DOT >= 1) dot = fma(acc[i], w[B * cc.r + i], dot);
                     if (DOT == 2) yy = fma(acc[i], acc[i], yy);
                 }
             }
 #pragma unroll
             for (int i = 0; i < B; ++i) acc[i] = 0;
         }
-        r = rn;
-        b0 = bn;
-        rs = rsn;
-        re = ren;
-        lead_cur = lead_next;
-        st ^= 1;
+        cc.advance(rowptr, nbrows, stride, S::CH);
+        st = (st + 1) % S::NST;
     }
     asm volatile("cp.async.wait_all;" ::: "memory");
     if (DOT) {
@@ -213,19 +230,19 @@ k_bcsr_spmv_staged(int64_t nbrows, const int32_t *__restrict__ rowptr, const int
         if (lane == 0) red[wib] = dot;
         __syncthreads();
         if (threadIdx.x == 0) {
-            double s = 0;
-            for (int i = 0; i < S::WARPS; ++i) s += red[i];
-            if (DOT == 1) partials[blockIdx.x] = s;
-            else partials[2 * blockIdx.x] = s;
+            double sum = 0;
+            for (int i = 0; i < S::WARPS; ++i) sum += red[i];
+            if (DOT == 1) partials[blockIdx.x] = sum;
+            else partials[2 * blockIdx.x] = sum;
         }
         if (DOT == 2) {
             __syncthreads();
             if (lane == 0) red[wib] = yy;
             __syncthreads();
             if (threadIdx.x == 0) {
-                double s = 0;
-                for (int i = 0; i < S::WARPS; ++i) s += red[i];
-                partials[2 * blockIdx.x + 1] = s;
+                double sum = 0;
+                for (int i = 0; i < S::WARPS; ++i) sum += red[i];
+                partials[2 * blockIdx.x + 1] = sum;
             }
         }
     }
@@ -291,7 +308,7 @@ yg_status spmv_launch_ex(yg_matrix A, const double *x, double *y, int precision,
     if (!partials) dot_mode = 0;
     if (!w) w = x;
     yg_status s;
-    if (precision == YG_PREC_MIXED) {
+    if (precision == YG_PREC_MIXED || precision == YG_PREC_MIXED_IR) {
         if (!A->d_val32) return fail(YG_BAD_ARG, "mixed-precision SpMV without FP32 values");
         s = launch_v<float>(A, A->d_val32, x, y, w, partials, dot_mode, flag, grid, st);
     } else {
@@ -308,9 +325,9 @@ yg_status spmv_launch(yg_matrix A, const double *x, double *y, int precision, do
 }
 
 int spmv_default_grid(yg_matrix A) {
-    if (A->variant == 1) {  // staged: 2 blocks of 8 warps per SM, a warp per row
-        int64_t need = (A->nbrows + 7) / 8;
-        int64_t g = (int64_t)A->ctx->num_sms * 2;
+    if (A->variant == 1) {  // staged: 3 blocks of 4 warps per SM, a warp per row
+        int64_t need = (A->nbrows + 3) / 4;
+        int64_t g = (int64_t)A->ctx->num_sms * 3;
         if (need < g) g = need;
         return (int)(g < 1 ? 1 : g);
     }
