@@ -109,6 +109,18 @@ __global__ void k_to_fp32(const double *__restrict__ v, float *__restrict__ o, i
         o[i] = (float)v[i];
 }
 
+// A kernel whose bounded wait expired leaves YG_TIMEOUT in the context's error
+// word; report it (once) and clear it.
+yg_status check_device_error(yg_context ctx) {
+    int32_t e = 0;
+    YG_CUDA(cudaMemcpy(&e, ctx->d_err, sizeof(int32_t), cudaMemcpyDeviceToHost));
+    if (e != 0) {
+        cudaMemset(ctx->d_err, 0, sizeof(int32_t));
+        return fail((yg_status)e, "a device wait expired (status %d); results of that launch are invalid", e);
+    }
+    return YG_OK;
+}
+
 int stream_grid(yg_context ctx, int64_t n) {
     int64_t g = (n + kThreads - 1) / kThreads;
     int64_t cap = (int64_t)ctx->num_sms * 8;
@@ -202,10 +214,11 @@ extern "C" yg_status yg_context_create(int32_t device, uint64_t hbm_budget_bytes
     YG_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
     yg_status s;
     if ((s = dev_alloc_t(ctx, &ctx->d_partials, 8 * kMaxReduceBlocks)) != YG_OK ||
-        (s = dev_alloc_t(ctx, &ctx->d_scalars, 4)) != YG_OK) {
+        (s = dev_alloc_t(ctx, &ctx->d_scalars, 4)) != YG_OK || (s = dev_alloc_t(ctx, &ctx->d_err, 4)) != YG_OK) {
         yg_context_destroy(ctx);
         return s;
     }
+    cudaMemset(ctx->d_err, 0, sizeof(int32_t));
     e = cudaMallocHost(&ctx->h_pinned, 64 * sizeof(double));
     if (e != cudaSuccess) {
         yg_context_destroy(ctx);
@@ -230,7 +243,7 @@ extern "C" yg_status yg_context_destroy(yg_context ctx) {
 extern "C" yg_status yg_context_synchronize(yg_context ctx) {
     if (!ctx) return fail(YG_BAD_ARG, "NULL context");
     YG_CUDA(cudaStreamSynchronize(ctx->stream));
-    return YG_OK;
+    return check_device_error(ctx);
 }
 
 extern "C" yg_status yg_context_memory(yg_context ctx, uint64_t *in_use, uint64_t *budget) {
@@ -453,15 +466,19 @@ extern "C" yg_status yg_spmv_ex(yg_matrix A, yg_vector x, yg_vector y, int32_t p
                     (long long)A->cols(), (long long)x->n, (long long)y->n);
     if (precision == YG_PREC_MIXED && !A->d_val32) YG_TRY(yg_matrix_make_fp32(A));
     YG_TRY(spmv_autotune_device(A));
-    return spmv_launch(A, x->d, y->d, precision, nullptr, nullptr, spmv_default_grid(A));
+    YG_TRY(spmv_launch(A, x->d, y->d, precision, nullptr, nullptr, spmv_default_grid(A)));
+    YG_CUDA(cudaStreamSynchronize(A->ctx->stream));
+    return check_device_error(A->ctx);
 }
 
 extern "C" yg_status yg_spmv(yg_matrix A, yg_vector x, yg_vector y) { return yg_spmv_ex(A, x, y, YG_PREC_FP64); }
 
 extern "C" yg_status yg_matrix_set_spmv(yg_matrix A, int32_t variant, int32_t lanes) {
-    if (!A || variant < -1 || variant > 1 || (lanes != 2 && lanes != 4 && lanes != 8 && lanes != 16 && lanes != 32))
+    if (!A || variant < -1 || variant > 2 ||
+        (lanes != 1 && lanes != 2 && lanes != 4 && lanes != 8 && lanes != 16 && lanes != 32))
         return fail(YG_BAD_ARG, "yg_matrix_set_spmv: bad variant/lanes");
-    if (variant == 1 && A->block != 2 && A->block != 3) return fail(YG_UNSUPPORTED, "staged SpMV needs 2x2 or 3x3 blocks");
+    if (variant >= 1 && A->block != 2 && A->block != 3) return fail(YG_UNSUPPORTED, "staged SpMV needs 2x2 or 3x3 blocks");
+    if (variant == 0 && lanes == 1) return fail(YG_BAD_ARG, "flat SpMV needs 2..32 lanes");
     if (variant < 0) {  // re-run the device autotuner
         A->tuned = false;
         return spmv_autotune_device(A);
@@ -499,5 +516,5 @@ extern "C" yg_status yg_spmv_bench(yg_matrix A, yg_vector x, yg_vector y, int32_
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     *ms_per_launch = ms / reps;
-    return YG_OK;
+    return check_device_error(ctx);
 }

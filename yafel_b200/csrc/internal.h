@@ -68,6 +68,7 @@ struct yg_context_t {
     double *d_partials = nullptr;   // 8 * kMaxReduceBlocks doubles
     double *h_pinned = nullptr;     // 64 doubles of pinned host memory
     KrylovScalars *d_scalars = nullptr;
+    int32_t *d_err = nullptr;       // device-side error word (bounded waits that expired)
     int reduce_blocks = 592;        // persistent grid for fused Krylov kernels
 };
 
@@ -89,7 +90,7 @@ struct yg_matrix_t {
     float *d_val32 = nullptr;     // optional FP32 copy
     int32_t *d_diag = nullptr;    // position of the diagonal block in each block row, -1 if absent
     int lanes = 32;               // SpMV lanes per block row (flat variant)
-    int variant = 0;              // SpMV variant: 0 flat lane-strided, 1 shared-memory staged (B = 2, 3)
+    int variant = 0;              // SpMV variant: 0 flat lane-strided, 1 cp.async staged, 2 TMA bulk staged (B = 2, 3)
     bool tuned = false;
     const void *owner = nullptr;  // dofmap whose pattern this is (assembly re-use)
     int32_t owner_format = -1;
@@ -129,6 +130,7 @@ int spmv_default_grid(yg_matrix A);
 void spmv_autotune(yg_matrix A);
 yg_status spmv_autotune_device(yg_matrix A);
 yg_status vector_dot(yg_context ctx, const double *a, const double *b, int64_t n, double *out);
+yg_status check_device_error(yg_context ctx);
 yg_status matrix_build_diag(yg_matrix A);
 yg_status matrix_from_device_pattern(yg_matrix A);
 

@@ -248,6 +248,266 @@ k_bcsr_spmv_staged(int64_t nbrows, const int32_t *__restrict__ rowptr, const int
     }
 }
 
+// ---------------------------------------------------------------------------
+// TMA variant for B = 2, 3 (variant 2).  Same chunking and lane-per-block
+// consumption as the staged variant, but each chunk is fetched by one lane with
+// two bulk asynchronous copies (cp.async.bulk: values, then block columns) that
+// complete on a per-stage mbarrier, so the copy costs two instructions instead
+// of one 16-byte cp.async per lane and line.  Lanes take two blocks at a time
+// with independent accumulators.  Waits on an mbarrier are bounded: after
+// kSpinLimit polls the kernel records YG_TIMEOUT in `err` and stops.
+constexpr long long kSpinLimit = 1ll << 26;
+
+template <int B, typename VT, int CH_, int NST_, int WARPS_>
+struct TmaCfg {
+    static constexpr int CH = CH_, NST = NST_, WARPS = WARPS_;
+    static constexpr int VBYTES = CH * B * B * (int)sizeof(VT) + 32;
+    static constexpr int CBYTES = CH * 4 + 32;
+    static constexpr int STAGE = VBYTES + CBYTES;
+    static constexpr int SMEM = WARPS * NST * STAGE + WARPS * NST * 8;  // stages + mbarriers
+};
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
+    unsigned a = (unsigned)__cvta_generic_to_shared(bar);
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(a), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes) {
+    unsigned a = (unsigned)__cvta_generic_to_shared(bar);
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(a), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity) {
+    unsigned a = (unsigned)__cvta_generic_to_shared(bar);
+    unsigned ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(a), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes, uint64_t *bar, uint64_t pol) {
+    unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    unsigned b = (unsigned)__cvta_generic_to_shared(bar);
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;" ::"r"(d),
+        "l"(src), "r"(bytes), "r"(b), "l"(pol)
+        : "memory");
+}
+
+template <int B, typename VT, int DOT, typename C>
+__global__ void __launch_bounds__(C::WARPS * 32)
+k_bcsr_spmv_tma(int64_t nbrows, const int32_t *__restrict__ rowptr, const int32_t *__restrict__ col,
+                const VT *__restrict__ val, const double *__restrict__ x, double *__restrict__ y,
+                const double *__restrict__ w, double *__restrict__ partials, const int32_t *__restrict__ flag,
+                int32_t *__restrict__ err) {
+    constexpr int B2 = B * B;
+    constexpr int BB = B2 * (int)sizeof(VT);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ double red[C::WARPS + 1];
+    __shared__ int leads[C::WARPS][C::NST][2];
+    if (flag && read_flag(flag)) return;
+    const uint64_t pol = evict_first_policy();
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    unsigned char *ring = smem_raw + (size_t)wib * C::NST * C::STAGE;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw + (size_t)C::WARPS * C::NST * C::STAGE) + wib * C::NST;
+    if (lane == 0)
+        for (int k = 0; k < C::NST; ++k) mbar_init(&bars[k], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    __syncwarp();
+    const int64_t stride = (int64_t)gridDim.x * C::WARPS;
+    const char *vbytes = reinterpret_cast<const char *>(val);
+    const char *cbytes = reinterpret_cast<const char *>(col);
+
+    // lane 0 issues both copies of chunk c into stage st
+    auto issue = [&](const ChunkCursor &c, int st) {
+        if (lane == 0) {
+            int lv = 0, lc = 0;
+            if (c.r < nbrows && c.re > c.rs) {
+                const int nb = min(C::CH, c.re - c.rs - c.b0);
+                const int64_t first = (int64_t)(c.rs + c.b0);
+                const int64_t vs = first * BB, va = vs & ~(int64_t)15, ve = (vs + (int64_t)nb * BB + 15) & ~(int64_t)15;
+                const int64_t cs = first * 4, ca = cs & ~(int64_t)15, ce = (cs + (int64_t)nb * 4 + 15) & ~(int64_t)15;
+                lv = (int)(vs - va);
+                lc = (int)(cs - ca);
+                unsigned char *dst = ring + st * C::STAGE;
+                mbar_expect_tx(&bars[st], (unsigned)((ve - va) + (ce - ca)));
+                bulk_g2s(dst, vbytes + va, (unsigned)(ve - va), &bars[st], pol);
+                bulk_g2s(dst + C::VBYTES, cbytes + ca, (unsigned)(ce - ca), &bars[st], pol);
+            } else {
+                mbar_expect_tx(&bars[st], 0);  // completes the phase with no transfer
+            }
+            leads[wib][st][0] = lv;
+            leads[wib][st][1] = lc;
+        }
+    };
+
+    ChunkCursor ci{(int64_t)blockIdx.x * C::WARPS + wib, 0, 0, 0};
+    ci.load(rowptr, nbrows);
+    ChunkCursor cc = ci;
+#pragma unroll
+    for (int k = 0; k < C::NST - 1; ++k) {
+        issue(ci, k);
+        if (ci.r < nbrows) ci.advance(rowptr, nbrows, stride, C::CH);
+    }
+    double dot = 0, yy = 0;
+    double acc[B], acc2[B];
+#pragma unroll
+    for (int i = 0; i < B; ++i) acc[i] = acc2[i] = 0;
+    int st = 0;
+    unsigned phase = 0;  // bit k: parity of stage k's next completion
+    bool timed_out = false;
+    while (cc.r < nbrows) {
+        issue(ci, (st + C::NST - 1) % C::NST);
+        if (ci.r < nbrows) ci.advance(rowptr, nbrows, stride, C::CH);
+        // bounded wait for stage st: lane 0 polls, the verdict is broadcast so the
+        // warp leaves together; the other lanes then observe the completed phase
+        // themselves (acquire) before reading the stage
+        int ok = 1;
+        if (lane == 0) {
+            long long spins = 0;
+            while (!mbar_try_wait(&bars[st], (phase >> st) & 1u))
+                if (++spins > kSpinLimit) { ok = 0; break; }
+        }
+        ok = __shfl_sync(0xffffffffu, ok, 0);
+        if (!ok) { timed_out = true; break; }
+        if (lane != 0) mbar_try_wait(&bars[st], (phase >> st) & 1u);
+        phase ^= (1u << st);
+        __syncwarp();
+        const int nb = max(0, min(C::CH, cc.re - cc.rs - cc.b0));
+        const unsigned char *stg = ring + st * C::STAGE;
+        const VT *blk = reinterpret_cast<const VT *>(stg + leads[wib][st][0]);
+        const int32_t *cix = reinterpret_cast<const int32_t *>(stg + C::VBYTES + leads[wib][st][1]);
+        int j = lane;
+        for (; j + 32 < nb; j += 64) {
+            const int c0 = cix[j], c1 = cix[j + 32];
+            double x0[B], x1[B];
+#pragma unroll
+            for (int k = 0; k < B; ++k) {
+                x0[k] = __ldg(x + (int64_t)B * c0 + k);
+                x1[k] = __ldg(x + (int64_t)B * c1 + k);
+            }
+#pragma unroll
+            for (int i = 0; i < B; ++i)
+#pragma unroll
+                for (int k = 0; k < B; ++k) {
+                    acc[i] = fma((double)blk[j * B2 + i * B + k], x0[k], acc[i]);
+                    acc2[i] = fma((double)blk[(j + 32) * B2 + i * B + k], x1[k], acc2[i]);
+                }
+        }
+        if (j < nb) {
+            const int c0 = cix[j];
+            double x0[B];
+#pragma unroll
+            for (int k = 0; k < B; ++k) x0[k] = __ldg(x + (int64_t)B * c0 + k);
+#pragma unroll
+            for (int i = 0; i < B; ++i)
+#pragma unroll
+                for (int k = 0; k < B; ++k) acc[i] = fma((double)blk[j * B2 + i * B + k], x0[k], acc[i]);
+        }
+        __syncwarp();
+        if (cc.b0 + C::CH >= cc.re - cc.rs) {  // row complete
+#pragma unroll
+            for (int i = 0; i < B; ++i) {
+                acc[i] += acc2[i];
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) acc[i] += __shfl_xor_sync(0xffffffffu, acc[i], o);
+            }
+            if (lane == 0) {
+#pragma unroll
+                for (int i = 0; i < B; ++i) {
+                    y[B * cc.r + i] = acc[i];
+                    if (DOT >= 1) dot = fma(acc[i], w[B * cc.r + i], dot);
+                    if (DOT == 2) yy = fma(acc[i], acc[i], yy);
+                }
+            }
+#pragma unroll
+            for (int i = 0; i < B; ++i) acc[i] = acc2[i] = 0;
+        }
+        cc.advance(rowptr, nbrows, stride, C::CH);
+        st = (st + 1) % C::NST;
+    }
+    if (timed_out && lane == 0 && err) atomicExch(err, (int32_t)YG_TIMEOUT);
+    // drain the copies still in flight into this warp's stages before the CTA
+    // exits (also after a timeout, again with a bound)
+    if (lane == 0) {
+        for (int k = 0; k < C::NST - 1; ++k) {
+            const int s2 = (st + k) % C::NST;
+            long long spins = 0;
+            while (!mbar_try_wait(&bars[s2], (phase >> s2) & 1u) && ++spins <= kSpinLimit) {
+            }
+            phase ^= (1u << s2);
+        }
+    }
+    __syncwarp();
+    if (DOT) {
+        if (lane == 0) red[wib] = dot;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double sum = 0;
+            for (int i = 0; i < C::WARPS; ++i) sum += red[i];
+            if (DOT == 1) partials[blockIdx.x] = sum;
+            else partials[2 * blockIdx.x] = sum;
+        }
+        if (DOT == 2) {
+            __syncthreads();
+            if (lane == 0) red[wib] = yy;
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                double sum = 0;
+                for (int i = 0; i < C::WARPS; ++i) sum += red[i];
+                partials[2 * blockIdx.x + 1] = sum;
+            }
+        }
+    }
+}
+
+template <int B, typename VT, int DOT, typename C>
+static yg_status launch_tma_cfg(yg_matrix A, const VT *val, const double *x, double *y, const double *w,
+                                double *partials, const int32_t *flag, int grid, cudaStream_t st) {
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_bcsr_spmv_tma<B, VT, DOT, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM);
+        attr = true;
+    }
+    k_bcsr_spmv_tma<B, VT, DOT, C><<<grid, C::WARPS * 32, C::SMEM, st>>>(A->nbrows, A->d_rowptr, A->d_col, val, x, y, w,
+                                                                        partials, flag, A->ctx->d_err);
+    YG_LAUNCHED(A->ctx);
+    return YG_OK;
+}
+
+// TMA configurations (chunk blocks, ring depth, warps per CTA) the autotuner tries.
+template <int B, typename VT>
+using TmaA = TmaCfg<B, VT, 64, 3, 4>;
+template <int B, typename VT>
+using TmaB = TmaCfg<B, VT, 32, 4, 8>;
+
+template <int B, typename VT, int DOT>
+static yg_status launch_tma(yg_matrix A, const VT *val, const double *x, double *y, const double *w, double *partials,
+                            const int32_t *flag, int grid, cudaStream_t st) {
+    if (A->lanes == 1) return launch_tma_cfg<B, VT, DOT, TmaB<B, VT>>(A, val, x, y, w, partials, flag, grid, st);
+    return launch_tma_cfg<B, VT, DOT, TmaA<B, VT>>(A, val, x, y, w, partials, flag, grid, st);
+}
+
+// CTAs per SM and warps per CTA of a TMA configuration (for the grid size).
+static void tma_shape(yg_matrix A, int *ctas_per_sm, int *warps) {
+    int smem, wp;
+    const bool f32 = false;
+    (void)f32;
+    if (A->block == 3) {
+        smem = A->lanes == 1 ? TmaB<3, double>::SMEM : TmaA<3, double>::SMEM;
+        wp = A->lanes == 1 ? TmaB<3, double>::WARPS : TmaA<3, double>::WARPS;
+    } else {
+        smem = A->lanes == 1 ? TmaB<2, double>::SMEM : TmaA<2, double>::SMEM;
+        wp = A->lanes == 1 ? TmaB<2, double>::WARPS : TmaA<2, double>::WARPS;
+    }
+    int per = (220 * 1024) / (smem + 1024);
+    if (per > 32 / wp * 2) per = 64 / wp;
+    *ctas_per_sm = per < 1 ? 1 : per;
+    *warps = wp;
+}
+
 template <int B, typename VT, int DOT>
 static yg_status launch_staged(yg_matrix A, const VT *val, const double *x, double *y, const double *w,
                                double *partials, const int32_t *flag, int grid, cudaStream_t st) {
@@ -280,6 +540,8 @@ static yg_status launch_l(yg_matrix A, const VT *val, const double *x, double *y
 template <typename VT, int DOT>
 static yg_status launch_b(yg_matrix A, const VT *val, const double *x, double *y, const double *w, double *partials,
                           const int32_t *flag, int grid, cudaStream_t st) {
+    if (A->variant == 2 && A->block == 3) return launch_tma<3, VT, DOT>(A, val, x, y, w, partials, flag, grid, st);
+    if (A->variant == 2 && A->block == 2) return launch_tma<2, VT, DOT>(A, val, x, y, w, partials, flag, grid, st);
     if (A->variant == 1 && A->block == 3) return launch_staged<3, VT, DOT>(A, val, x, y, w, partials, flag, grid, st);
     if (A->variant == 1 && A->block == 2) return launch_staged<2, VT, DOT>(A, val, x, y, w, partials, flag, grid, st);
     switch (A->block) {
@@ -325,6 +587,14 @@ yg_status spmv_launch(yg_matrix A, const double *x, double *y, int precision, do
 }
 
 int spmv_default_grid(yg_matrix A) {
+    if (A->variant == 2) {  // TMA: as many CTAs as fit, a warp per row
+        int per, wp;
+        tma_shape(A, &per, &wp);
+        int64_t need = (A->nbrows + wp - 1) / wp;
+        int64_t g = (int64_t)A->ctx->num_sms * per;
+        if (need < g) g = need;
+        return (int)(g < 1 ? 1 : g);
+    }
     if (A->variant == 1) {  // staged: 3 blocks of 4 warps per SM, a warp per row
         int64_t need = (A->nbrows + 3) / 4;
         int64_t g = (int64_t)A->ctx->num_sms * 3;
@@ -390,7 +660,11 @@ yg_status spmv_autotune_device(yg_matrix A) {
     double per_row = A->nbrows ? (double)A->nnzb * A->block * A->block / (double)A->nbrows : 1.0;
     for (int L : {2, 4, 8, 16, 32})
         if (L <= 4 * per_row + 4) cands.push_back({0, L});
-    if (A->block == 2 || A->block == 3) cands.push_back({1, 32});
+    if (A->block == 2 || A->block == 3) {
+        cands.push_back({1, 32});
+        cands.push_back({2, 32});  // TMA, 64-block chunks, 3 stages, 4 warps
+        cands.push_back({2, 1});   // TMA, 32-block chunks, 4 stages, 8 warps
+    }
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
