@@ -99,6 +99,36 @@ def bcsr3_spmv_bytes(nnzb, n):
     return nnzb * (8 * 9 + 4) + 4 * (nbrows + 1) + 8 * n + 8 * n
 
 
+def spmv_kernel_name(K, dot=1, vt="double"):
+    variant, lanes = K.get_spmv()
+    if variant == 2:
+        cfg = "64,3,4" if lanes != 1 else "32,4,8"
+        return "k_bcsr_spmv_tma<3,%s,%d,TmaCfg<3,%s,%s>>" % (vt, dot, vt, cfg)
+    if variant == 1:
+        return "k_bcsr_spmv_staged<3,%s,%d>" % (vt, dot)
+    return "k_bcsr_spmv<3,%d,%s,%d>" % (lanes, vt, dot)
+
+
+def run_spmv_profile(args):
+    """SpMV alone on the nx^3 Q2 elasticity matrix (GPU-assembled), for
+    roofline and ncu captures: FP64 then FP32 values, `--reps` launches each."""
+    import yafel_b200 as yb
+    dm = yb.DoFManager(problem(args.nx), 2, 3)
+    fe = yb.FESystem(dm, 3)
+    yb.CGAssembly(yb.LinearElasticity(3, E=E, nu=NU), fe, [yb.AssemblyRequirement.Tangent])
+    K = fe.getGlobalTangent()
+    if args.variant is not None:
+        K.set_spmv(args.variant, args.lanes)
+    n, nnzb = K.rows(), K.nnz() // 9
+    x = yb.DeviceVector(np.random.default_rng(0).standard_normal(n), dm.ctx)
+    out = {"mesh": "%d^3 Q2 hex" % args.nx, "dofs": n, "blocks": nnzb, "kernel": spmv_kernel_name(K, 0)}
+    for prec, name, nbytes in ((0, "fp64", bcsr3_spmv_bytes(nnzb, n)),
+                               (1, "fp32_values", nnzb * 40 + 4 * (n // 3 + 1) + 16 * n)):
+        ms = K.spmv_bench(reps=args.reps, precision=prec, x=x)
+        out[name] = {"ms": ms, "bytes": nbytes, "GB_s": nbytes / ms / 1e6}
+    print(json.dumps(out), flush=True)
+
+
 def run_gpu(args):
     import yafel_b200 as yb
     from yafel_b200 import loads
@@ -212,8 +242,7 @@ def run_gpu(args):
     spmv_ms = sum(s.spmv_ms for s in st64) / max(1, sum(s.spmv_launches for s in st64))
     spmv32_ms = sum(s.spmv_ms for s in stmx) / max(1, sum(s.spmv_launches for s in stmx))
     spmv32_bytes = nnzb * (4 * 9 + 4) + 4 * (ndofs // 3 + 1) + 16 * ndofs
-    variant, lanes = K.get_spmv()
-    kname = ("k_bcsr_spmv_staged<3,double,1>" if variant == 1 else "k_bcsr_spmv<3,%d,double,1>" % lanes)
+    kname = spmv_kernel_name(K)
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -345,8 +374,14 @@ def main():
     ap.add_argument("--nx", type=int, default=NX)
     ap.add_argument("--cpu-nx", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--spmv-profile", action="store_true", help="time the SpMV kernel alone (roofline/ncu)")
+    ap.add_argument("--variant", type=int, default=None, help="SpMV variant for --spmv-profile (0 flat, 1 staged, 2 TMA)")
+    ap.add_argument("--lanes", type=int, default=32, help="SpMV lanes / TMA configuration for --spmv-profile")
+    ap.add_argument("--reps", type=int, default=10)
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.spmv_profile:
+        run_spmv_profile(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_gpu(args)
