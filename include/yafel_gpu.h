@@ -246,6 +246,33 @@ YG_API yg_status yg_cg(yg_matrix A, yg_precond M, yg_vector b, yg_vector x, cons
 YG_API yg_status yg_bicgstab(yg_matrix A, yg_precond M, yg_vector b, yg_vector x,
                       const yg_solve_opts *opts, yg_solve_stats *stats);
 
+/* ------------------------------------------------------------------ batched and served solves */
+
+/* Many independent systems advanced together by shared persistent-grid kernels
+ * (Jacobi-PCG, relative-residual criterion).  No reference counterpart: the
+ * reference solves one system per pcg_solve call.  Each system keeps its own
+ * matrix (CSR or 2x2/3x3 BCSR), right-hand side and iterate, which must stay
+ * alive while it is in the batch; x holds x0 when added and the solution when
+ * finished.  Systems may be added and removed between calls of yg_batch_run
+ * (continuous batching); work advances in blocks of iterations captured in one
+ * CUDA graph followed by an FP64 verification pass (true residual b - A x for
+ * converged systems, and the residual replacement of YG_PREC_MIXED). */
+typedef struct yg_batch_t *yg_batch;
+YG_API yg_status yg_batch_create(yg_context ctx, int32_t capacity, yg_batch *out);
+YG_API yg_status yg_batch_destroy(yg_batch B);
+/* opts: criterion must be YG_CRIT_RELRES; precision YG_PREC_FP64 or YG_PREC_MIXED. */
+YG_API yg_status yg_batch_add(yg_batch B, yg_matrix A, yg_vector b, yg_vector x, const yg_solve_opts *opts,
+                              int32_t *slot);
+YG_API yg_status yg_batch_remove(yg_batch B, int32_t slot);
+/* Run at most max_blocks blocks of iterations (0 = until no system is active);
+ * *n_active receives the number of systems still iterating. */
+YG_API yg_status yg_batch_run(yg_batch B, int32_t max_blocks, int32_t *n_active);
+/* Status (YG_OK when converged and verified in FP64), iterations and FP64 relative
+ * residual of a slot. */
+YG_API yg_status yg_batch_stats(yg_batch B, int32_t slot, yg_solve_stats *stats);
+/* Autotune rows per work item and lanes per row for the systems present. */
+YG_API yg_status yg_batch_tune(yg_batch B);
+
 #ifdef __cplusplus
 }
 #endif

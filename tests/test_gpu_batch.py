@@ -1,0 +1,92 @@
+"""Batched and continuous-batching solves (yg_batch_*): every system converges to
+a 1e-10 relative residual (checked in FP64 against the oracle-assembled system),
+and a system's result is the same alone and in the mix."""
+import numpy as np
+import pytest
+
+import yafel_b200 as yb
+from oracle import oracle as O
+from yafel_b200 import workloads
+from yafel_b200._lib import check, lib
+
+pytestmark = pytest.mark.gpu
+
+
+def assemble_problem(spec, ctx):
+    mesh = workloads.build_mesh(spec)
+    dpn, dim = spec["dpn"], spec["dim"]
+    dm = yb.DoFManager(mesh, spec["order"], dpn, ctx=ctx)
+    fe = yb.FESystem(dm, dim, format=yb.CSR if dpn == 1 else yb.BCSR)
+    phys = yb.PoissonEquation(dim, f=0.0) if spec["kind"] == "poisson" else yb.LinearElasticity(dim, body=(0, 0, 0))
+    yb.CGAssembly(phys, fe, [yb.AssemblyRequirement.Tangent])
+    K = fe.getGlobalTangent()
+    b = yb.DeviceVector(workloads.rhs(spec, dm.ndofs), ctx)
+    dofs = workloads.clamp_dofs(dm.dof_nodes, dpn)
+    zeros = np.zeros(dofs.size)
+    check(lib().yg_dirichlet_apply(K.h, b.h, yb._ptr(dofs), yb._ptr(zeros), dofs.size))
+    return mesh, K, b, dofs
+
+
+def oracle_relres(spec, mesh, dofs, b_host, x):
+    odm = O.dofmanager(mesh, spec["order"])
+    kind = O.POISSON if spec["kind"] == "poisson" else O.ELASTICITY
+    params = [1.0, 0.0] if kind == O.POISSON else [1.0, 0.576923076923077, 0.3846153846153846, 0, 0, 0]
+    K, _ = O.assemble(odm, spec["dpn"], spec["dim"], kind, params)
+    mask = np.zeros(K.nrows, np.uint8)
+    mask[dofs] = 1
+    bb = workloads.rhs(spec, K.nrows)
+    O.dirichlet_apply(K, bb, mask, np.zeros(K.nrows))
+    assert np.allclose(bb, b_host, rtol=0, atol=1e-12 * np.abs(bb).max())
+    return O.true_relres(K, bb, x)
+
+
+SPECS = [dict(workloads.problem_spec(i, lo=1e3, hi=2e4)) for i in range(6)]
+
+
+@pytest.mark.parametrize("precision", [yb.PREC_FP64, yb.PREC_MIXED])
+def test_batch_converges_and_matches_single_solves(ctx, precision):
+    probs = [assemble_problem(s, ctx) for s in SPECS]
+    B = yb.Batch(len(probs), ctx)
+    slots = [B.add(K, b, precision=precision) for (_, K, b, _) in probs]
+    B.tune()
+    assert B.run() == 0
+    for spec, (mesh, K, b, dofs), s in zip(SPECS, probs, slots):
+        st = B.stats(s)
+        assert st.status == 0 and st.rel_residual <= 1e-10, (spec, st.status, st.rel_residual)
+        x = B.solution(s).numpy()
+        assert oracle_relres(spec, mesh, dofs, b.numpy(), x) <= 1e-10
+        xs, sts = yb.solve(K, b, M=yb.JacobiPreconditioner(K), tol=1e-10)
+        assert sts.status == 0
+        assert np.linalg.norm(x - xs.numpy()) <= 1e-6 * np.linalg.norm(xs.numpy())
+
+
+def test_continuous_batching_same_result_alone_and_in_mix(ctx):
+    probs = [assemble_problem(s, ctx) for s in SPECS]
+    # alone: each system in a batch of its own
+    alone = []
+    for (_, K, b, _) in probs:
+        B1 = yb.Batch(1, ctx)
+        s = B1.add(K, b)
+        B1.run()
+        alone.append(B1.solution(s).numpy())
+    # mixed, with arrivals and a departure while others iterate
+    B = yb.Batch(4, ctx)
+    live = {}
+    queue = list(range(len(probs)))
+    done = {}
+    for _ in range(200):
+        while queue and len(live) < 4:
+            i = queue.pop(0)
+            live[B.add(probs[i][1], probs[i][2])] = i
+        active = B.run(max_blocks=1)
+        for s, i in list(live.items()):
+            st = B.stats(s)
+            if st.status == 0:
+                done[i] = B.solution(s).numpy().copy()
+                B.remove(s)
+                del live[s]
+        if not queue and not live:
+            break
+    assert len(done) == len(probs)
+    for i in range(len(probs)):
+        assert np.array_equal(done[i], alone[i]), i

@@ -21,7 +21,7 @@ __all__ = ["Context", "default_context", "Mesh", "DoFManager", "FESystem", "CGAs
            "AssemblyRequirement", "PoissonEquation", "LinearElasticity", "AdvectionDiffusionSUPG",
            "DirichletBC", "DeviceVector", "sparse_csr", "sparse_bcsr", "JacobiPreconditioner",
            "ILUPreconditioner", "IdentityPreconditioner", "cg_solve", "pcg_solve",
-           "bicgstab_solve", "solve", "YafelError", "meshgen", "CG_SOLVER_TOL"]
+           "bicgstab_solve", "solve", "Batch", "YafelError", "meshgen", "CG_SOLVER_TOL"]
 
 # cg_solve.hpp:21, pcg_solve.hpp:21, bicgstab_solve.hpp:13
 CG_SOLVER_TOL = 1.0e-14
@@ -629,3 +629,52 @@ def bicgstab_solve(A, rhs, x0=None, TOL=CG_SOLVER_TOL):
     ||Ax-b||^2/||b||^2 < TOL every max(N/100,1) iterations."""
     x, _ = solve(A, rhs, x0, None, "bicgstab", CRIT_REFERENCE, TOL)
     return x.numpy()
+
+
+# ------------------------------------------------------------------ batched / served solves
+
+class Batch:
+    """Many systems advanced together (yg_batch_*): add (A, b, x0) triples, run
+    until all converge or step block by block while adding/removing systems."""
+
+    def __init__(self, capacity, ctx=None):
+        self.ctx = ctx or default_context()
+        h = C.c_void_p()
+        check(lib().yg_batch_create(self.ctx.h, int(capacity), C.byref(h)), "Batch")
+        self.h = h
+        self._keep = {}
+
+    def add(self, A, b, x0=None, tol=1e-10, precision=PREC_FP64, maxiter=0):
+        bd, _ = _as_device(b, self.ctx)
+        xd = x0 if isinstance(x0, DeviceVector) else DeviceVector(
+            np.zeros(A.rows()) if x0 is None else np.asarray(x0, dtype=np.float64), self.ctx)
+        opts = SolveOpts(CRIT_RELRES, precision, tol, maxiter, 0, 0)
+        slot = C.c_int32()
+        check(lib().yg_batch_add(self.h, A.h, bd.h, xd.h, C.byref(opts), C.byref(slot)), "Batch.add")
+        self._keep[slot.value] = (A, bd, xd)
+        return slot.value
+
+    def remove(self, slot):
+        check(lib().yg_batch_remove(self.h, int(slot)), "Batch.remove")
+        self._keep.pop(slot, None)
+
+    def run(self, max_blocks=0):
+        n = C.c_int32()
+        check(lib().yg_batch_run(self.h, int(max_blocks), C.byref(n)), "Batch.run")
+        return n.value
+
+    def tune(self):
+        check(lib().yg_batch_tune(self.h), "Batch.tune")
+
+    def stats(self, slot):
+        st = SolveStats()
+        check(lib().yg_batch_stats(self.h, int(slot), C.byref(st)), "Batch.stats")
+        return st
+
+    def solution(self, slot):
+        return self._keep[slot][2]
+
+    def __del__(self):
+        if getattr(self, "h", None) and _alive(getattr(self, "ctx", None)):
+            lib().yg_batch_destroy(self.h)
+        self.h = None

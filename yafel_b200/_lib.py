@@ -73,6 +73,13 @@ SIGNATURES = {
     "yg_precond_zero_pivots": (i64, [vp]),
     "yg_cg": (i32, [vp, vp, vp, vp, P(SolveOpts), P(SolveStats)]),
     "yg_bicgstab": (i32, [vp, vp, vp, vp, P(SolveOpts), P(SolveStats)]),
+    "yg_batch_create": (i32, [vp, i32, P(vp)]),
+    "yg_batch_destroy": (i32, [vp]),
+    "yg_batch_add": (i32, [vp, vp, vp, vp, P(SolveOpts), P(i32)]),
+    "yg_batch_remove": (i32, [vp, i32]),
+    "yg_batch_run": (i32, [vp, i32, P(i32)]),
+    "yg_batch_stats": (i32, [vp, i32, P(SolveStats)]),
+    "yg_batch_tune": (i32, [vp]),
 }
 
 

@@ -1,0 +1,51 @@
+"""Seeded synthetic problem sets for the batched and served forms.
+
+Every problem is a 2D (or 3D) Poisson or linear-elasticity system on a
+structured grid whose cells are quads or triangle pairs (seeded coin) with
+interior nodes jittered by U(-0.2, 0.2)*h, Dirichlet u = 0 on x = 0 and an
+i.i.d. N(0,1) right-hand side.  Problem i of a set uses the seed base + i
+(numpy PCG64), so a set is reproducible.
+"""
+import math
+
+import numpy as np
+
+from . import meshgen
+
+BASE_SEED = 20261203
+
+
+def grid_for_dofs(target_dofs, p, dpn, dim=2):
+    """Cells per side of a square (cube) grid whose order-p DoF count is close
+    to target_dofs: dofs = dpn * (p*n + 1)^dim."""
+    n = ((target_dofs / dpn) ** (1.0 / dim) - 1.0) / p
+    return max(1, int(round(n)))
+
+
+def problem_spec(i, base=BASE_SEED, lo=1e3, hi=2e5, orders=(1, 2, 3), kinds=("poisson", "elasticity"), dims=(2,)):
+    rng = np.random.Generator(np.random.PCG64(base + i))
+    target = math.exp(rng.uniform(math.log(lo), math.log(hi)))
+    p = int(rng.choice(orders))
+    kind = str(rng.choice(kinds))
+    dim = int(rng.choice(dims))
+    dpn = dim if kind == "elasticity" else 1
+    n = grid_for_dofs(target, p, dpn, dim)
+    return {"index": i, "seed": base + i, "target_dofs": target, "order": p, "kind": kind, "dim": dim, "dpn": dpn,
+            "n": n}
+
+
+def build_mesh(spec):
+    p, n = spec["order"], spec["n"]
+    if spec["dim"] == 2:
+        return meshgen.jittered_mixed(n, n, seed=spec["seed"], order=meshgen.corner_order(p))
+    return meshgen.structured_hex(n, n, n, order=meshgen.corner_order(p))
+
+
+def rhs(spec, ndofs):
+    rng = np.random.Generator(np.random.PCG64(spec["seed"] + 7919))
+    return rng.standard_normal(ndofs)
+
+
+def clamp_dofs(X, dpn):
+    nodes = np.nonzero(np.abs(X[:, 0]) < 1e-9)[0]
+    return (nodes[:, None] * dpn + np.arange(dpn)[None, :]).ravel().astype(np.int64)
