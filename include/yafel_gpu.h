@@ -273,6 +273,28 @@ YG_API yg_status yg_batch_stats(yg_batch B, int32_t slot, yg_solve_stats *stats)
 /* Autotune rows per work item and lanes per row for the systems present. */
 YG_API yg_status yg_batch_tune(yg_batch B);
 
+/* ------------------------------------------------------------------ allocation-free dot product */
+
+/* *out = sum_i x[i]*y[i], with x, y and out device pointers and stream a
+ * cudaStream_t (NULL: the default stream of the current device).  No
+ * counterpart in the reference, which has no device code.
+ *
+ * For callers that must not allocate device memory when they need a
+ * reduction: a host framework that has reserved the device's memory for its
+ * own pool (cudaMalloc would fail or grow past the budget it accounts for), or
+ * a latency-bound loop between solver steps (cudaMalloc and cudaFree
+ * synchronise the device).  It needs no yg_context, whose creation allocates.
+ * The call allocates nothing: its partial sums live in a fixed 64 KiB array of
+ * this library's device code, one per device; nothing in it has to start at
+ * zero.  Limits: n <= 67,108,864 (8192 partial sums of 8192 values each);
+ * larger n fails with YG_BAD_ARG and a message (use yg_vector_dot).  The first
+ * call on each device looks up the array's address (cudaGetSymbolAddress),
+ * which may load this library's device code: make that first call before any
+ * stream capture.  Calls that overlap on the same device (other streams or
+ * host threads) share the array and race; order them on one stream.  The
+ * launch is asynchronous: *out is ready when the stream reaches it. */
+YG_API yg_status yg_dot_static_scratch(const double *x, const double *y, int64_t n, double *out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

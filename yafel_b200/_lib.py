@@ -80,6 +80,7 @@ SIGNATURES = {
     "yg_batch_run": (i32, [vp, i32, P(i32)]),
     "yg_batch_stats": (i32, [vp, i32, P(SolveStats)]),
     "yg_batch_tune": (i32, [vp]),
+    "yg_dot_static_scratch": (i32, [vp, vp, i64, vp, vp]),
 }
 
 
