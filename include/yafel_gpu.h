@@ -264,6 +264,9 @@ YG_API yg_status yg_batch_destroy(yg_batch B);
 YG_API yg_status yg_batch_add(yg_batch B, yg_matrix A, yg_vector b, yg_vector x, const yg_solve_opts *opts,
                               int32_t *slot);
 YG_API yg_status yg_batch_remove(yg_batch B, int32_t slot);
+/* Solve a slot's system again from its current x (the caller may have changed
+ * x or b in place); slot -1 resets every system in the batch. */
+YG_API yg_status yg_batch_reset(yg_batch B, int32_t slot);
 /* Run at most max_blocks blocks of iterations (0 = until no system is active);
  * *n_active receives the number of systems still iterating. */
 YG_API yg_status yg_batch_run(yg_batch B, int32_t max_blocks, int32_t *n_active);

@@ -7,24 +7,12 @@ import pytest
 import yafel_b200 as yb
 from oracle import oracle as O
 from yafel_b200 import workloads
-from yafel_b200._lib import check, lib
 
 pytestmark = pytest.mark.gpu
 
 
 def assemble_problem(spec, ctx):
-    mesh = workloads.build_mesh(spec)
-    dpn, dim = spec["dpn"], spec["dim"]
-    dm = yb.DoFManager(mesh, spec["order"], dpn, ctx=ctx)
-    fe = yb.FESystem(dm, dim, format=yb.CSR if dpn == 1 else yb.BCSR)
-    phys = yb.PoissonEquation(dim, f=0.0) if spec["kind"] == "poisson" else yb.LinearElasticity(dim, body=(0, 0, 0))
-    yb.CGAssembly(phys, fe, [yb.AssemblyRequirement.Tangent])
-    K = fe.getGlobalTangent()
-    b = yb.DeviceVector(workloads.rhs(spec, dm.ndofs), ctx)
-    dofs = workloads.clamp_dofs(dm.dof_nodes, dpn)
-    zeros = np.zeros(dofs.size)
-    check(lib().yg_dirichlet_apply(K.h, b.h, yb._ptr(dofs), yb._ptr(zeros), dofs.size))
-    return mesh, K, b, dofs
+    return workloads.assemble(spec, ctx)
 
 
 def oracle_relres(spec, mesh, dofs, b_host, x):
@@ -90,3 +78,18 @@ def test_continuous_batching_same_result_alone_and_in_mix(ctx):
     assert len(done) == len(probs)
     for i in range(len(probs)):
         assert np.array_equal(done[i], alone[i]), i
+
+
+def test_reset_solves_again_to_the_same_bits(ctx):
+    probs = [assemble_problem(s, ctx) for s in SPECS[:3]]
+    B = yb.Batch(3, ctx)
+    slots = [B.add(K, b) for (_, K, b, _) in probs]
+    assert B.run() == 0
+    first = [B.solution(s).numpy().copy() for s in slots]
+    for s in slots:
+        B.solution(s).fill(0.0)
+    B.reset()
+    assert B.run() == 0
+    for s, f in zip(slots, first):
+        assert B.stats(s).status == 0
+        assert np.array_equal(B.solution(s).numpy(), f)

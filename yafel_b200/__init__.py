@@ -658,6 +658,10 @@ class Batch:
         check(lib().yg_batch_remove(self.h, int(slot)), "Batch.remove")
         self._keep.pop(slot, None)
 
+    def reset(self, slot=-1):
+        """Solve again from the current x of `slot` (every slot when -1)."""
+        check(lib().yg_batch_reset(self.h, int(slot)), "Batch.reset")
+
     def run(self, max_blocks=0):
         n = C.c_int32()
         check(lib().yg_batch_run(self.h, int(max_blocks), C.byref(n)), "Batch.run")

@@ -77,6 +77,7 @@ SIGNATURES = {
     "yg_batch_destroy": (i32, [vp]),
     "yg_batch_add": (i32, [vp, vp, vp, vp, P(SolveOpts), P(i32)]),
     "yg_batch_remove": (i32, [vp, i32]),
+    "yg_batch_reset": (i32, [vp, i32]),
     "yg_batch_run": (i32, [vp, i32, P(i32)]),
     "yg_batch_stats": (i32, [vp, i32, P(SolveStats)]),
     "yg_batch_tune": (i32, [vp]),

@@ -2,19 +2,27 @@
 //
 // No reference counterpart: the reference solves one system per call
 // (pcg_solve.hpp:126-178).  Each system keeps its own matrix (CSR or BCSR with
-// 2x2 / 3x3 blocks), right-hand side, iterate and work vectors; a device table
-// of system descriptors and a table of work items (row ranges of one system)
-// drive persistent-grid kernels that advance every active system by one Jacobi-
-// PCG iteration:
-//   SpMV (one launch per block size present) with per-item partials of p.Ap,
-//   update   : every CTA of a system reduces that system's items in a fixed order
-//              -> alpha_s; x, r update; Jacobi z; partials of r.z, r.r
-//   pupdate  : -> beta_s; p update; the CTA of the system's first item records
-//              the scalars and a stop reason.
-// Converged systems drop out of the iteration kernels at once.  A block of m
+// 2x2 / 3x3 blocks), right-hand side, iterate and work vectors.  A system's
+// block rows are cut into tiles of whole rows holding at most TileCfg<B>::BLOCKS
+// blocks, and runs of consecutive tiles form work items; a device table of
+// system descriptors and one of work items drive persistent-grid kernels that
+// advance every active system by one Jacobi-PCG iteration:
+//   SpMV (one launch per block size present): each CTA streams the tiles of its
+//        items through a shared-memory ring filled by bulk asynchronous copies
+//        (cp.async.bulk + mbarrier), q = A p, per-item partials of p.q; the CTA
+//        that finishes a system's last item sums its partials in item order
+//        -> alpha (and the breakdown test);
+//   update : x, r updates, Jacobi z, partials of r.z and r.r; the last CTA of a
+//        system -> beta, the stopping tests, the mixed-precision replacement test;
+//   pupdate: p = z + beta p.
+// Every decision about a system is taken once, by the CTA that completes it, so
+// every CTA of the next kernel sees the same state.  Sums run in a fixed order
+// over a fixed item decomposition: a system's result does not depend on which
+// other systems share the batch.  Converged systems drop out of the kernels at
+// once and out of the item table at the next compaction.  A block of m
 // iterations plus a verification pass is captured into one CUDA graph and
 // replayed; the verification pass recomputes b - A x in FP64 for systems whose
-// recursive residual converged (stop) or, in mixed precision, fell 10x since
+// recursive residual converged (stop) or, in mixed precision, fell 100x since
 // the last replacement (replace), and for newly added systems (init).  Systems
 // can be added and removed between replays (continuous batching): only the
 // descriptor and item tables change, and kernels read their item counts from
@@ -30,7 +38,6 @@
 
 namespace yg {
 int stream_grid(yg_context ctx, int64_t n);
-yg_status spmv_autotune_device(yg_matrix A);
 }
 
 enum BatchFlag : int32_t { BF_RUN = 0, BF_DONE = 1, BF_BREAK = 2, BF_NANF = 3, BF_MAXIT = 4, BF_INIT = 5, BF_EMPTY = 6 };
@@ -43,28 +50,32 @@ struct BatchSys {
     const float *val32;
     const double *b, *dinv;
     double *x, *r, *p, *q;
+    const int32_t *tiles;  // first block row of each tile, ntiles + 1 entries
     int32_t item_begin, item_end;
-    int32_t precision;  // YG_PREC_FP64 or YG_PREC_MIXED
-    int32_t pad;
+    int32_t precision;     // YG_PREC_FP64 or YG_PREC_MIXED
+    int32_t ntiles;
 };
 
 struct BatchScal {
     double rz[2];
     double bb, rr, rr_last, tol;
+    double alpha, beta;
     int64_t iter, maxiter;
     int32_t flag, stop, replace, restart;
+    int32_t ticket, pad;   // items of the running kernel finished (reset by the last)
     int64_t replacements;
-    double true_rr;  // r.r of the last FP64 true residual
+    double true_rr;        // r.r of the last FP64 true residual
 };
 
 struct BatchItem {
-    int32_t sys, brow_begin, brow_end, pad;
+    int32_t sys, tile_begin, tile_end, row_begin, row_end, pad;
 };
 
 struct yg_batch_t {
     yg_context ctx = nullptr;
     int32_t capacity = 0;
     std::vector<BatchSys> sys;          // host mirror
+    std::vector<std::vector<int32_t>> tiles;  // host copy of each system's tiles
     std::vector<int32_t> used;          // slot in use
     std::vector<yg_matrix> mats;
     std::vector<yg_solve_opts> opts;
@@ -75,9 +86,11 @@ struct yg_batch_t {
     double *d_part = nullptr;           // partials: 2 per item
     double *d_part2 = nullptr;
     int32_t max_items = 0, n_items = 0;
-    int32_t group_rows[4] = {0, 0, 0, 0};  // rows per item per block size
-    int32_t lanes[4] = {4, 4, 4, 4};
+    int32_t tiles_per_item[4] = {0, 8, 8, 8};
+    int32_t lanes[4] = {4, 4, 8, 16};
     unsigned groups_present = 0, graph_groups = 0;
+    bool dirty = false;                 // item table out of date (systems added, removed or reset)
+    int32_t live_items = 0;             // items of systems that may still iterate (host view)
     int m = 16;
     cudaGraphExec_t exec = nullptr;
     cudaGraph_t graph = nullptr;
@@ -87,12 +100,31 @@ struct yg_batch_t {
 
 namespace yg {
 
+// ---------------------------------------------------------------- tiles
+
+// Blocks per tile: the values and block columns of a full FP64 tile fill one
+// shared-memory stage of about 18 KB.
+template <int B> struct TileCfg;
+template <> struct TileCfg<1> { static constexpr int BLOCKS = 1536; };
+template <> struct TileCfg<2> { static constexpr int BLOCKS = 512; };
+template <> struct TileCfg<3> { static constexpr int BLOCKS = 224; };
+
+static int tile_blocks(int B) { return B == 1 ? TileCfg<1>::BLOCKS : (B == 2 ? TileCfg<2>::BLOCKS : TileCfg<3>::BLOCKS); }
+
+template <int B>
+struct Stage {
+    static constexpr int NST = 3;
+    static constexpr int VBYTES = TileCfg<B>::BLOCKS * B * B * 8 + 32;  // FP64 values + alignment slack
+    static constexpr int CBYTES = TileCfg<B>::BLOCKS * 4 + 32;
+    static constexpr int BYTES = VBYTES + CBYTES;
+    static constexpr int SMEM = NST * BYTES + NST * 8;  // stages + mbarriers
+};
+
 // ---------------------------------------------------------------- kernels
 
 // Whether system state `sc` takes part in a kernel of the given kind, decided
-// once per CTA: thread 0 reads the state (a peer CTA of the same system may
-// change `stop` during update/pupdate) and broadcasts it, so every thread of the
-// CTA takes the same branch around the block reductions.
+// once per CTA: thread 0 reads the state and broadcasts it, so every thread of
+// the CTA takes the same branch around the block reductions.
 enum { ACT_ITER = 0, ACT_VERIFY = 1, ACT_RESTART = 2 };
 __device__ __forceinline__ bool cta_active(const BatchScal *sc, int kind, int *flag_sm) {
     __syncthreads();
@@ -109,97 +141,236 @@ __device__ __forceinline__ bool cta_active(const BatchScal *sc, int kind, int *f
     return *flag_sm != 0;
 }
 
-// Reduce the partials of system s (items [ib, ie), stride 2, offset off).
-__device__ __forceinline__ double sys_reduce(const double *__restrict__ part, int ib, int ie, int off, double *sm) {
+// After thread 0 published this item's partials: count the item in the system's
+// ticket; returns (to every thread) whether this CTA finished the system's last
+// item, in which case the ticket is reset and all partials are visible.
+__device__ __forceinline__ bool last_of_system(BatchScal *sc, int n_items, int *flag_sm) {
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const int old = atomicAdd(&sc->ticket, 1);
+        const int last = (old == n_items - 1);
+        if (last) {
+            sc->ticket = 0;
+            __threadfence();
+        }
+        *flag_sm = last;
+    }
+    __syncthreads();
+    return *flag_sm != 0;
+}
+
+// Fixed-order sum of partials [ib, ie) (stride 2, offset off), result in every thread.
+__device__ __forceinline__ double sum_items(const double *part, int ib, int ie, int off, double *sm) {
     double v = 0;
-    for (int i = ib + threadIdx.x; i < ie; i += blockDim.x) v += part[2 * (int64_t)i + off];
+    for (int i = ib + threadIdx.x; i < ie; i += blockDim.x) v += __ldcg(part + 2 * (int64_t)i + off);
     return block_sum_all<kThreads>(v, sm);
 }
 
-// MODE 0: iteration, q = A p (FP32 or FP64 values), partials of p.q.
+// Rows [r0, r1) of one tile: L lanes per block row; vals / cols point at the
+// tile's first block (shared memory, or global memory for an oversized tile).
+template <int B, int L, int MODE, typename VT>
+__device__ __forceinline__ double tile_rows(const BatchSys &d, int r0, int r1, int b0, const VT *vals,
+                                           const int32_t *cols, const double *__restrict__ xin) {
+    constexpr int B2 = B * B;
+    constexpr int G = kThreads / L;
+    const int lane = threadIdx.x & 31, glane = lane % L, grp = threadIdx.x / L;
+    double dot = 0;
+    for (int rb = r0; rb < r1; rb += G) {
+        const int r = rb + grp;
+        double acc[B];
+#pragma unroll
+        for (int i = 0; i < B; ++i) acc[i] = 0;
+        if (r < r1) {
+            const int rs = d.rowptr[r] - b0, re = d.rowptr[r + 1] - b0;
+            int j = rs + glane;
+            for (; j + L < re; j += 2 * L) {
+                const int c0 = cols[j], c1 = cols[j + L];
+                double x0[B], x1[B];
+#pragma unroll
+                for (int k = 0; k < B; ++k) {
+                    x0[k] = __ldg(xin + (int64_t)B * c0 + k);
+                    x1[k] = __ldg(xin + (int64_t)B * c1 + k);
+                }
+#pragma unroll
+                for (int i = 0; i < B; ++i)
+#pragma unroll
+                    for (int k = 0; k < B; ++k) {
+                        acc[i] = fma((double)vals[j * B2 + i * B + k], x0[k], acc[i]);
+                        acc[i] = fma((double)vals[(j + L) * B2 + i * B + k], x1[k], acc[i]);
+                    }
+            }
+            if (j < re) {
+                const int c0 = cols[j];
+#pragma unroll
+                for (int i = 0; i < B; ++i)
+#pragma unroll
+                    for (int k = 0; k < B; ++k)
+                        acc[i] = fma((double)vals[j * B2 + i * B + k], __ldg(xin + (int64_t)B * c0 + k), acc[i]);
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < B; ++i)
+#pragma unroll
+            for (int o = L / 2; o > 0; o >>= 1) acc[i] += __shfl_xor_sync(0xffffffffu, acc[i], o);
+        if (r < r1 && glane == 0) {
+#pragma unroll
+            for (int i = 0; i < B; ++i) {
+                d.q[(int64_t)B * r + i] = acc[i];
+                if (MODE == 0) dot = fma(acc[i], xin[(int64_t)B * r + i], dot);
+            }
+        }
+    }
+    return dot;
+}
+
+// CTA-wide bounded wait on a stage: thread 0 polls, the verdict is broadcast;
+// the other threads then observe the completed phase themselves (acquire).
+__device__ __forceinline__ bool stage_wait(uint64_t *bar, unsigned parity, int *flag_sm) {
+    if (threadIdx.x == 0) {
+        long long spins = 0;
+        int ok = 1;
+        while (!mbar_try_wait(bar, parity))
+            if (++spins > kSpinLimit) { ok = 0; break; }
+        *flag_sm = ok;
+    }
+    __syncthreads();
+    const bool ok = *flag_sm != 0;
+    if (ok && threadIdx.x != 0) mbar_try_wait(bar, parity);
+    return ok;
+}
+
+// Thread 0 issues the bulk copies of tile t (values, then block columns) into
+// stage seq % NST; an empty or oversized tile completes its phase with no
+// transfer and is read from global memory instead.
+template <int B>
+__device__ __forceinline__ void issue_tile(unsigned char *smem_raw, uint64_t *bars, uint32_t seq,
+                                           const int32_t *__restrict__ rowptr, const int32_t *__restrict__ tiles, int t,
+                                           const char *vbase, int vsz, const int32_t *col, uint64_t pol) {
+    using S = Stage<B>;
+    constexpr int B2 = B * B;
+    if (threadIdx.x != 0) return;
+    const int st = seq % S::NST;
+    const int b0 = rowptr[tiles[t]], b1 = rowptr[tiles[t + 1]];
+    const int nb = b1 - b0;
+    if (nb > 0 && nb <= TileCfg<B>::BLOCKS) {
+        const int64_t vs = (int64_t)b0 * B2 * vsz, va = vs & ~(int64_t)15;
+        const int64_t ve = (vs + (int64_t)nb * B2 * vsz + 15) & ~(int64_t)15;
+        const int64_t cs = (int64_t)b0 * 4, ca = cs & ~(int64_t)15, ce = (cs + (int64_t)nb * 4 + 15) & ~(int64_t)15;
+        unsigned char *dst = smem_raw + (size_t)st * S::BYTES;
+        mbar_expect_tx(&bars[st], (unsigned)((ve - va) + (ce - ca)));
+        bulk_g2s(dst, vbase + va, (unsigned)(ve - va), &bars[st], pol);
+        bulk_g2s(dst + S::VBYTES, reinterpret_cast<const char *>(col) + ca, (unsigned)(ce - ca), &bars[st], pol);
+    } else {
+        mbar_expect_tx(&bars[st], 0);
+    }
+}
+
+// MODE 0: iteration, q = A p (FP32 values for mixed-precision systems), partials
+//         of p.q; the last CTA of a system computes alpha (commit != 0).
 // MODE 1: verification, q = A x with FP64 values for systems being initialised,
 //         stopped on a converged recursive residual, or due a replacement.
 template <int B, int L, int MODE>
 __global__ void __launch_bounds__(kThreads)
 k_batch_spmv(const BatchItem *__restrict__ items, const int32_t *__restrict__ ranges, const BatchSys *__restrict__ sys,
-             const BatchScal *__restrict__ scal, double *__restrict__ part) {
-    __shared__ double sm[kThreads / 32 + 1];
-    __shared__ int act;
+             BatchScal *__restrict__ scal, double *__restrict__ part, int parity, int commit, int32_t *__restrict__ err) {
+    using S = Stage<B>;
     constexpr int B2 = B * B;
-    constexpr int GPB = kThreads / L;  // row groups per CTA
+    constexpr int CAP = TileCfg<B>::BLOCKS;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ double sm[kThreads / 32 + 1];
+    __shared__ int flag_sm;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw + (size_t)S::NST * S::BYTES);
+    if (threadIdx.x == 0)
+        for (int k = 0; k < S::NST; ++k) mbar_init(&bars[k], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    __syncthreads();
+    const uint64_t pol = evict_first_policy();
+    uint32_t seq_issue = 0, seq_wait = 0;  // tiles issued / consumed by this CTA
+    bool timed_out = false;
     const int g0 = ranges[B - 1], g1 = ranges[B];
-    const int lane = threadIdx.x & 31, glane = lane % L;
-    const int grp = threadIdx.x / L;
-    for (int it = g0 + blockIdx.x; it < g1; it += gridDim.x) {
+    for (int it = g0 + blockIdx.x; it < g1 && !timed_out; it += gridDim.x) {
         const BatchItem item = items[it];
         const int s = item.sys;
-        if (!cta_active(&scal[s], MODE == 0 ? ACT_ITER : ACT_VERIFY, &act)) continue;
+        if (!cta_active(&scal[s], MODE == 0 ? ACT_ITER : ACT_VERIFY, &flag_sm)) continue;
         const BatchSys d = sys[s];
-        const double *xin = MODE == 0 ? d.p : d.x;
         const bool f32 = (MODE == 0 && d.precision == YG_PREC_MIXED);
+        const int vsz = f32 ? 4 : 8;
+        const char *vbase = f32 ? reinterpret_cast<const char *>(d.val32) : reinterpret_cast<const char *>(d.val);
+        const double *xin = MODE == 0 ? d.p : d.x;
+        int t_issue = item.tile_begin;
+        while (t_issue < item.tile_end && seq_issue - seq_wait < (uint32_t)(S::NST - 1))
+            issue_tile<B>(smem_raw, bars, seq_issue++, d.rowptr, d.tiles, t_issue++, vbase, vsz, d.col, pol);
         double dot = 0;
-        for (int rb = item.brow_begin; rb < item.brow_end; rb += GPB) {
-            const int r = rb + grp;
-            double acc[B];
-#pragma unroll
-            for (int i = 0; i < B; ++i) acc[i] = 0;
-            if (r < item.brow_end) {
-                const int rs = d.rowptr[r], re = d.rowptr[r + 1];
-                const int nv = (re - rs) * B2;
-                int j = glane / B2, e = glane % B2;
-                for (int k = glane; k < nv; k += L) {
-                    const double v = f32 ? (double)d.val32[(int64_t)rs * B2 + k] : d.val[(int64_t)rs * B2 + k];
-                    const int i = e / B, c = e - (e / B) * B;
-                    const double xv = xin[(int64_t)B * d.col[rs + j] + c];
-#pragma unroll
-                    for (int ii = 0; ii < B; ++ii) acc[ii] = (ii == i) ? fma(v, xv, acc[ii]) : acc[ii];
-                    e += L % B2;
-                    j += L / B2;
-                    if (e >= B2) { e -= B2; ++j; }
-                }
+        for (int t = item.tile_begin; t < item.tile_end; ++t) {
+            if (t_issue < item.tile_end && seq_issue - seq_wait < (uint32_t)S::NST)
+                issue_tile<B>(smem_raw, bars, seq_issue++, d.rowptr, d.tiles, t_issue++, vbase, vsz, d.col, pol);
+            const int st = seq_wait % S::NST;
+            if (!stage_wait(&bars[st], (seq_wait / S::NST) & 1u, &flag_sm)) {
+                timed_out = true;
+                break;
             }
-#pragma unroll
-            for (int i = 0; i < B; ++i) {
-#pragma unroll
-                for (int o = L / 2; o > 0; o >>= 1) acc[i] += __shfl_xor_sync(0xffffffffu, acc[i], o);
+            const int r0 = d.tiles[t], r1 = d.tiles[t + 1];
+            const int b0 = d.rowptr[r0], nb = d.rowptr[r1] - b0;
+            const unsigned char *stg = smem_raw + (size_t)st * S::BYTES;
+            const int lv = (int)(((int64_t)b0 * B2 * vsz) & 15), lc = (int)(((int64_t)b0 * 4) & 15);
+            const int32_t *cols = nb <= CAP ? reinterpret_cast<const int32_t *>(stg + S::VBYTES + lc) : d.col + b0;
+            if (f32) {
+                const float *v = nb <= CAP ? reinterpret_cast<const float *>(stg + lv) : d.val32 + (int64_t)b0 * B2;
+                dot += tile_rows<B, L, MODE, float>(d, r0, r1, b0, v, cols, xin);
+            } else {
+                const double *v = nb <= CAP ? reinterpret_cast<const double *>(stg + lv) : d.val + (int64_t)b0 * B2;
+                dot += tile_rows<B, L, MODE, double>(d, r0, r1, b0, v, cols, xin);
             }
-            if (r < item.brow_end && glane == 0) {
-#pragma unroll
-                for (int i = 0; i < B; ++i) {
-                    d.q[(int64_t)B * r + i] = acc[i];
-                    if (MODE == 0) dot = fma(acc[i], xin[(int64_t)B * r + i], dot);
-                }
-            }
+            ++seq_wait;
+            __syncthreads();  // the stage is free for the next issue
         }
-        if (MODE == 0) {
+        if (timed_out) break;
+        if (MODE == 0 && commit) {
             dot = block_sum<kThreads>(dot, sm);
             if (threadIdx.x == 0) part[2 * (int64_t)it] = dot;
+            const int n_items = d.item_end - d.item_begin;
+            if (last_of_system(&scal[s], n_items, &flag_sm)) {
+                const double pq = sum_items(part, d.item_begin, d.item_end, 0, sm);
+                if (threadIdx.x == 0) {
+                    BatchScal &sc = scal[s];
+                    const double alpha = sc.rz[parity] / pq;
+                    if (pq == 0 || !isfinite(alpha)) sc.stop = isfinite(pq) ? BS_BREAK : BS_NAN;
+                    else sc.alpha = alpha;
+                }
+            }
         }
     }
+    if (timed_out && threadIdx.x == 0 && err) atomicExch(err, (int32_t)YG_TIMEOUT);
+    // drain the copies still in flight before the CTA exits (bounded)
+    if (threadIdx.x == 0) {
+        while (seq_wait != seq_issue) {
+            const int st = seq_wait % S::NST;
+            long long spins = 0;
+            while (!mbar_try_wait(&bars[st], (seq_wait / S::NST) & 1u) && ++spins <= kSpinLimit) {
+            }
+            ++seq_wait;
+        }
+    }
+    __syncthreads();
 }
 
-// alpha, x and r updates, Jacobi z, partials of r.z and r.r
+// x and r updates, Jacobi z, partials of r.z and r.r; the last CTA of a system
+// takes its decisions: beta, convergence of the recursive residual, NaN,
+// iteration cap, and (mixed precision) a due residual replacement.
 __global__ void __launch_bounds__(kThreads)
 k_batch_update(const BatchItem *__restrict__ items, const int32_t *__restrict__ ranges, const BatchSys *__restrict__ sys,
-               BatchScal *__restrict__ scal, int parity, const double *__restrict__ part_in, double *__restrict__ part_out) {
+               BatchScal *__restrict__ scal, int parity, double *__restrict__ part) {
     __shared__ double sm[kThreads / 32 + 1];
-    __shared__ int act;
+    __shared__ int flag_sm;
     const int n_items = ranges[3];
     for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
         const BatchItem item = items[it];
         const int s = item.sys;
         BatchScal &sc = scal[s];
-        if (!cta_active(&sc, ACT_ITER, &act)) continue;
+        if (!cta_active(&sc, ACT_ITER, &flag_sm)) continue;
         const BatchSys d = sys[s];
-        const double pq = sys_reduce(part_in, d.item_begin, d.item_end, 0, sm);
-        const double alpha = sc.rz[parity] / pq;
-        if (pq == 0 || !isfinite(alpha)) {
-            if (it == d.item_begin && threadIdx.x == 0) sc.stop = isfinite(pq) ? BS_BREAK : BS_NAN;
-            continue;
-        }
-        // the iteration count changes here, not in pupdate, whose CTAs all read it
-        if (it == d.item_begin && threadIdx.x == 0) sc.iter += 1;
-        const int64_t lo = (int64_t)item.brow_begin * d.block, hi = (int64_t)item.brow_end * d.block;
+        const double alpha = __ldcg(&sc.alpha);
+        const int64_t lo = (int64_t)item.row_begin * d.block, hi = (int64_t)item.row_end * d.block;
         double srz = 0, srr = 0;
         for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
             d.x[i] += d.p[i] * alpha;
@@ -211,44 +382,41 @@ k_batch_update(const BatchItem *__restrict__ items, const int32_t *__restrict__ 
         srz = block_sum<kThreads>(srz, sm);
         srr = block_sum<kThreads>(srr, sm);
         if (threadIdx.x == 0) {
-            part_out[2 * (int64_t)it] = srz;
-            part_out[2 * (int64_t)it + 1] = srr;
+            part[2 * (int64_t)it] = srz;
+            part[2 * (int64_t)it + 1] = srr;
+        }
+        if (last_of_system(&sc, d.item_end - d.item_begin, &flag_sm)) {
+            const double rz_new = sum_items(part, d.item_begin, d.item_end, 0, sm);
+            const double rr = sum_items(part, d.item_begin, d.item_end, 1, sm);
+            if (threadIdx.x == 0) {
+                int stop = BS_NONE;
+                if (sqrt(rr) <= sc.tol * sqrt(sc.bb)) stop = BS_CONV;
+                else if (!isfinite(rz_new)) stop = BS_NAN;
+                else if (sc.iter + 1 >= sc.maxiter) stop = BS_MAXIT;
+                sc.beta = rz_new / sc.rz[parity];
+                sc.rz[parity ^ 1] = rz_new;
+                sc.rr = rr;
+                sc.iter += 1;
+                if (stop == BS_NONE && d.precision == YG_PREC_MIXED && rr < 1e-2 * sc.rr_last) sc.replace = 1;
+                sc.stop = stop;
+            }
         }
     }
 }
 
-// beta and p update; the first item's CTA records the scalars and stop reason
+// p = z + beta p for systems that go on iterating
 __global__ void __launch_bounds__(kThreads)
 k_batch_pupdate(const BatchItem *__restrict__ items, const int32_t *__restrict__ ranges, const BatchSys *__restrict__ sys,
-                BatchScal *__restrict__ scal, int parity, const double *__restrict__ part) {
-    __shared__ double sm[kThreads / 32 + 1];
-    __shared__ int act;
+                const BatchScal *__restrict__ scal) {
+    __shared__ int flag_sm;
     const int n_items = ranges[3];
     for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
         const BatchItem item = items[it];
         const int s = item.sys;
-        BatchScal &sc = scal[s];
-        // a peer CTA of this system may set `stop` during this kernel; it only
-        // does so when the decision below is also to stop, so skipping is consistent
-        if (!cta_active(&sc, ACT_ITER, &act)) continue;
+        if (!cta_active(&scal[s], ACT_ITER, &flag_sm)) continue;
         const BatchSys d = sys[s];
-        const double rz_new = sys_reduce(part, d.item_begin, d.item_end, 0, sm);
-        const double rr = sys_reduce(part, d.item_begin, d.item_end, 1, sm);
-        const double rz_old = sc.rz[parity];
-        int stop = BS_NONE;
-        if (sqrt(rr) <= sc.tol * sqrt(sc.bb)) stop = BS_CONV;
-        else if (!isfinite(rz_new)) stop = BS_NAN;
-        else if (sc.iter >= sc.maxiter) stop = BS_MAXIT;
-        const bool rep = (stop == BS_NONE && d.precision == YG_PREC_MIXED && rr < 1e-2 * sc.rr_last);
-        if (it == d.item_begin && threadIdx.x == 0) {
-            sc.rz[parity ^ 1] = rz_new;
-            sc.rr = rr;
-            if (stop != BS_NONE) sc.stop = stop;
-            if (rep) sc.replace = 1;
-        }
-        if (stop != BS_NONE) continue;
-        const double beta = rz_new / rz_old;
-        const int64_t lo = (int64_t)item.brow_begin * d.block, hi = (int64_t)item.brow_end * d.block;
+        const double beta = __ldcg(&scal[s].beta);
+        const int64_t lo = (int64_t)item.row_begin * d.block, hi = (int64_t)item.row_end * d.block;
         for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) d.p[i] = d.dinv[i] * d.r[i] + beta * d.p[i];
     }
 }
@@ -259,14 +427,14 @@ __global__ void __launch_bounds__(kThreads)
 k_batch_residual(const BatchItem *__restrict__ items, const int32_t *__restrict__ ranges, const BatchSys *__restrict__ sys,
                  const BatchScal *__restrict__ scal, double *__restrict__ part, double *__restrict__ part_bb) {
     __shared__ double sm[kThreads / 32 + 1];
-    __shared__ int act;
+    __shared__ int flag_sm;
     const int n_items = ranges[3];
     for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
         const BatchItem item = items[it];
         const int s = item.sys;
-        if (!cta_active(&scal[s], ACT_VERIFY, &act)) continue;
+        if (!cta_active(&scal[s], ACT_VERIFY, &flag_sm)) continue;
         const BatchSys d = sys[s];
-        const int64_t lo = (int64_t)item.brow_begin * d.block, hi = (int64_t)item.brow_end * d.block;
+        const int64_t lo = (int64_t)item.row_begin * d.block, hi = (int64_t)item.row_end * d.block;
         double srz = 0, srr = 0, sbb = 0;
         for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
             const double ri = d.b[i] - d.q[i];
@@ -293,6 +461,7 @@ __global__ void k_batch_decide(int cap, const BatchSys *__restrict__ sys, BatchS
     if (s >= cap) return;
     BatchScal &sc = scal[s];
     sc.restart = 0;
+    sc.ticket = 0;
     if (sc.flag == BF_RUN && (sc.stop == BS_BREAK || sc.stop == BS_NAN || sc.stop == BS_MAXIT)) {
         sc.flag = sc.stop == BS_BREAK ? BF_BREAK : (sc.stop == BS_NAN ? BF_NANF : BF_MAXIT);
         return;
@@ -334,14 +503,14 @@ __global__ void k_batch_decide(int cap, const BatchSys *__restrict__ sys, BatchS
 __global__ void __launch_bounds__(kThreads)
 k_batch_restart(const BatchItem *__restrict__ items, const int32_t *__restrict__ ranges, const BatchSys *__restrict__ sys,
                 const BatchScal *__restrict__ scal) {
-    __shared__ int act;
+    __shared__ int flag_sm;
     const int n_items = ranges[3];
     for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
         const BatchItem item = items[it];
         const int s = item.sys;
-        if (!cta_active(&scal[s], ACT_RESTART, &act)) continue;
+        if (!cta_active(&scal[s], ACT_RESTART, &flag_sm)) continue;
         const BatchSys d = sys[s];
-        const int64_t lo = (int64_t)item.brow_begin * d.block, hi = (int64_t)item.brow_end * d.block;
+        const int64_t lo = (int64_t)item.row_begin * d.block, hi = (int64_t)item.row_end * d.block;
         for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) d.p[i] = d.dinv[i] * d.r[i];
     }
 }
@@ -360,32 +529,61 @@ __global__ void k_batch_jacobi(int64_t nbrows, int B, const int32_t *__restrict_
 
 static int batch_grid(yg_context ctx) { return ctx->num_sms * 4; }
 
-template <int B, int MODE>
-static void launch_bspmv(yg_batch bt, int L) {
-    yg_context ctx = bt->ctx;
-    const int g = batch_grid(ctx);
-    switch (L) {
-    case 2: k_batch_spmv<B, 2, MODE><<<g, kThreads, 0, ctx->stream>>>(bt->d_items, bt->d_ranges, bt->d_sys, bt->d_scal, bt->d_part); break;
-    case 4: k_batch_spmv<B, 4, MODE><<<g, kThreads, 0, ctx->stream>>>(bt->d_items, bt->d_ranges, bt->d_sys, bt->d_scal, bt->d_part); break;
-    case 8: k_batch_spmv<B, 8, MODE><<<g, kThreads, 0, ctx->stream>>>(bt->d_items, bt->d_ranges, bt->d_sys, bt->d_scal, bt->d_part); break;
-    case 16: k_batch_spmv<B, 16, MODE><<<g, kThreads, 0, ctx->stream>>>(bt->d_items, bt->d_ranges, bt->d_sys, bt->d_scal, bt->d_part); break;
-    default: k_batch_spmv<B, 32, MODE><<<g, kThreads, 0, ctx->stream>>>(bt->d_items, bt->d_ranges, bt->d_sys, bt->d_scal, bt->d_part); break;
+// grid of the SpMV kernels: resident CTAs per SM (shared memory bound) x SMs
+template <int B, int L, int MODE>
+static int spmv_grid(yg_context ctx) {
+    static int per_sm = 0;
+    if (per_sm == 0) {
+        cudaFuncSetAttribute(k_batch_spmv<B, L, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, Stage<B>::SMEM);
+        int n = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_spmv<B, L, MODE>, kThreads, Stage<B>::SMEM) !=
+                cudaSuccess || n < 1)
+            n = 1;
+        per_sm = n;
     }
+    return per_sm * ctx->num_sms;
+}
+
+template <int B, int L, int MODE>
+static void launch_spmv_l(yg_batch bt, int parity, int commit) {
+    yg_context ctx = bt->ctx;
+    k_batch_spmv<B, L, MODE><<<spmv_grid<B, L, MODE>(ctx), kThreads, Stage<B>::SMEM, ctx->stream>>>(
+        bt->d_items, bt->d_ranges, bt->d_sys, bt->d_scal, bt->d_part, parity, commit, ctx->d_err);
     YG_LAUNCHED(ctx);
 }
 
+template <int B, int MODE>
+static void launch_bspmv(yg_batch bt, int L, int parity, int commit) {
+    switch (L) {
+    case 2: launch_spmv_l<B, 2, MODE>(bt, parity, commit); break;
+    case 4: launch_spmv_l<B, 4, MODE>(bt, parity, commit); break;
+    case 8: launch_spmv_l<B, 8, MODE>(bt, parity, commit); break;
+    case 16: launch_spmv_l<B, 16, MODE>(bt, parity, commit); break;
+    default: launch_spmv_l<B, 32, MODE>(bt, parity, commit); break;
+    }
+}
+
+// set the shared-memory attribute of every SpMV instantiation (outside capture)
+template <int B>
+static void prepare_spmv_b(yg_context ctx) {
+    spmv_grid<B, 2, 0>(ctx); spmv_grid<B, 4, 0>(ctx); spmv_grid<B, 8, 0>(ctx); spmv_grid<B, 16, 0>(ctx);
+    spmv_grid<B, 32, 0>(ctx);
+    spmv_grid<B, 2, 1>(ctx); spmv_grid<B, 4, 1>(ctx); spmv_grid<B, 8, 1>(ctx); spmv_grid<B, 16, 1>(ctx);
+    spmv_grid<B, 32, 1>(ctx);
+}
+
 template <int MODE>
-static void launch_bspmv_groups(yg_batch bt) {
-    if (bt->groups_present & 1) launch_bspmv<1, MODE>(bt, bt->lanes[1]);
-    if (bt->groups_present & 2) launch_bspmv<2, MODE>(bt, bt->lanes[2]);
-    if (bt->groups_present & 4) launch_bspmv<3, MODE>(bt, bt->lanes[3]);
+static void launch_bspmv_groups(yg_batch bt, int parity) {
+    if (bt->groups_present & 1) launch_bspmv<1, MODE>(bt, bt->lanes[1], parity, 1);
+    if (bt->groups_present & 2) launch_bspmv<2, MODE>(bt, bt->lanes[2], parity, 1);
+    if (bt->groups_present & 4) launch_bspmv<3, MODE>(bt, bt->lanes[3], parity, 1);
 }
 
 // the verification pass (also initialises newly added systems)
 static void launch_verify(yg_batch bt) {
     yg_context ctx = bt->ctx;
     const int g = batch_grid(ctx);
-    launch_bspmv_groups<1>(bt);
+    launch_bspmv_groups<1>(bt, 0);
     k_batch_residual<<<g, kThreads, 0, ctx->stream>>>(bt->d_items, bt->d_ranges, bt->d_sys, bt->d_scal, bt->d_part,
                                                      bt->d_part2);
     YG_LAUNCHED(ctx);
@@ -399,12 +597,11 @@ static void launch_verify(yg_batch bt) {
 static void launch_iteration(yg_batch bt, int parity) {
     yg_context ctx = bt->ctx;
     const int g = batch_grid(ctx);
-    launch_bspmv_groups<0>(bt);
-    k_batch_update<<<g, kThreads, 0, ctx->stream>>>(bt->d_items, bt->d_ranges, bt->d_sys, bt->d_scal, parity, bt->d_part,
+    launch_bspmv_groups<0>(bt, parity);
+    k_batch_update<<<g, kThreads, 0, ctx->stream>>>(bt->d_items, bt->d_ranges, bt->d_sys, bt->d_scal, parity,
                                                    bt->d_part2);
     YG_LAUNCHED(ctx);
-    k_batch_pupdate<<<g, kThreads, 0, ctx->stream>>>(bt->d_items, bt->d_ranges, bt->d_sys, bt->d_scal, parity,
-                                                    bt->d_part2);
+    k_batch_pupdate<<<g, kThreads, 0, ctx->stream>>>(bt->d_items, bt->d_ranges, bt->d_sys, bt->d_scal);
     YG_LAUNCHED(ctx);
 }
 
@@ -415,7 +612,19 @@ static void drop_graph(yg_batch bt) {
     bt->graph = nullptr;
 }
 
-// Rebuild the item table: systems grouped by block size, rows cut into items.
+// Whether system s may still iterate, as the host last saw its flag.
+static bool sys_live(yg_batch bt, int s) {
+    const int f = bt->h_scal[s].flag;
+    return bt->used[s] && (f == BF_RUN || f == BF_INIT);
+}
+
+// Rebuild the item table: systems grouped by block size, tiles grouped into
+// items.  Systems that finished are left out (their kernels' item loops stay
+// short); the block sizes present count every system in the batch, so
+// compaction never changes the set of SpMV launches that the captured graph
+// holds.  A system's tiles are always grouped the same way for a given tuning,
+// so its reductions add the same partials in the same order whatever else is in
+// the table.
 static yg_status rebuild_items(yg_batch bt) {
     yg_context ctx = bt->ctx;
     std::vector<BatchItem> items;
@@ -423,27 +632,28 @@ static yg_status rebuild_items(yg_batch bt) {
     unsigned present = 0;
     for (int B = 1; B <= 3; ++B) {
         ranges[B - 1] = (int32_t)items.size();
-        const int R = bt->group_rows[B];
+        const int T = std::max(1, bt->tiles_per_item[B]);
         for (int s = 0; s < bt->capacity; ++s) {
             if (!bt->used[s] || bt->sys[s].block != B) continue;
             present |= 1u << (B - 1);
-            bt->sys[s].item_begin = (int32_t)items.size();
-            for (int r0 = 0; r0 < bt->sys[s].nbrows; r0 += R)
-                items.push_back({s, r0, std::min(bt->sys[s].nbrows, r0 + R), 0});
-            if (bt->sys[s].nbrows == 0) items.push_back({s, 0, 0, 0});
-            bt->sys[s].item_end = (int32_t)items.size();
+            BatchSys &d = bt->sys[s];
+            d.item_begin = (int32_t)items.size();
+            if (!sys_live(bt, s)) {
+                d.item_end = d.item_begin;
+                continue;
+            }
+            const std::vector<int32_t> &tl = bt->tiles[s];
+            for (int t0 = 0; t0 < d.ntiles; t0 += T) {
+                const int t1 = std::min(d.ntiles, t0 + T);
+                items.push_back({s, t0, t1, tl[t0], tl[t1], 0});
+            }
+            if (d.ntiles == 0) items.push_back({s, 0, 0, 0, 0, 0});
+            d.item_end = (int32_t)items.size();
         }
     }
-    // items were appended by block size, so group b is [ranges[b-1], ranges[b])
-    {
-        int32_t cnt[4] = {0, 0, 0, 0};
-        for (auto &it : items) cnt[bt->sys[it.sys].block]++;
-        ranges[0] = 0;
-        ranges[1] = cnt[1];
-        ranges[2] = cnt[1] + cnt[2];
-        ranges[3] = cnt[1] + cnt[2] + cnt[3];
-    }
+    ranges[3] = (int32_t)items.size();
     if ((int32_t)items.size() > bt->max_items) {
+        YG_CUDA(cudaStreamSynchronize(ctx->stream));
         dev_free(ctx, bt->d_items);
         dev_free(ctx, bt->d_part);
         dev_free(ctx, bt->d_part2);
@@ -463,6 +673,8 @@ static yg_status rebuild_items(yg_batch bt) {
     YG_CUDA(cudaMemcpy(bt->d_ranges, ranges, sizeof(ranges), cudaMemcpyHostToDevice));
     YG_CUDA(cudaMemcpy(bt->d_sys, bt->sys.data(), sizeof(BatchSys) * bt->capacity, cudaMemcpyHostToDevice));
     bt->groups_present = present;
+    bt->live_items = bt->n_items;
+    bt->dirty = false;
     return YG_OK;
 }
 
@@ -487,10 +699,27 @@ static yg_status capture_graph(yg_batch bt) {
 static void release_slot(yg_batch bt, int s) {
     yg_context ctx = bt->ctx;
     BatchSys &d = bt->sys[s];
-    for (void *ptr : {(void *)d.r, (void *)d.p, (void *)d.q, (void *)d.dinv}) dev_free(ctx, ptr);
+    for (void *ptr : {(void *)d.r, (void *)d.p, (void *)d.q, (void *)d.dinv, (void *)d.tiles}) dev_free(ctx, ptr);
     d = BatchSys{};
+    bt->tiles[s].clear();
     bt->used[s] = 0;
     bt->mats[s] = nullptr;
+}
+
+// Cut block rows into tiles of whole rows with at most `cap` blocks each (a row
+// longer than cap forms a tile of its own, read from global memory).
+static void make_tiles(const std::vector<int32_t> &rp, int cap, std::vector<int32_t> &tiles) {
+    tiles.clear();
+    const int n = (int)rp.size() - 1;
+    tiles.push_back(0);
+    int start = 0;
+    for (int r = 0; r < n; ++r) {
+        if (r > start && rp[r + 1] - rp[start] > cap) {
+            tiles.push_back(r);
+            start = r;
+        }
+    }
+    if (n > 0) tiles.push_back(n);
 }
 
 }  // namespace yg
@@ -503,26 +732,25 @@ extern "C" yg_status yg_batch_create(yg_context ctx, int32_t capacity, yg_batch 
     bt->ctx = ctx;
     bt->capacity = capacity;
     bt->sys.assign(capacity, BatchSys{});
+    bt->tiles.assign(capacity, std::vector<int32_t>());
     bt->used.assign(capacity, 0);
     bt->mats.assign(capacity, nullptr);
     bt->opts.assign(capacity, yg_solve_opts{});
-    bt->h_scal.assign(capacity, BatchScal{});
-    bt->group_rows[1] = 1024;
-    bt->group_rows[2] = 512;
-    bt->group_rows[3] = 256;
-    bt->lanes[1] = 4;
-    bt->lanes[2] = 8;
-    bt->lanes[3] = 16;
     yg_status s;
     if ((s = dev_alloc_t(ctx, &bt->d_sys, capacity)) != YG_OK || (s = dev_alloc_t(ctx, &bt->d_scal, capacity)) != YG_OK ||
         (s = dev_alloc_t(ctx, &bt->d_ranges, 4)) != YG_OK) {
         yg_batch_destroy(bt);
         return s;
     }
+    prepare_spmv_b<1>(ctx);
+    prepare_spmv_b<2>(ctx);
+    prepare_spmv_b<3>(ctx);
     std::vector<BatchScal> init(capacity);
     for (auto &c : init) c.flag = BF_EMPTY;
+    bt->h_scal = init;
     cudaMemcpy(bt->d_scal, init.data(), sizeof(BatchScal) * capacity, cudaMemcpyHostToDevice);
     cudaMemset(bt->d_ranges, 0, sizeof(int32_t) * 4);
+    YG_CUDA(cudaGetLastError());
     *out = bt;
     return YG_OK;
 }
@@ -555,6 +783,12 @@ extern "C" yg_status yg_batch_add(yg_batch bt, yg_matrix A, yg_vector b, yg_vect
     if (s < 0) return fail(YG_OVER_BUDGET, "yg_batch_add: all %d slots in use", bt->capacity);
     yg_context ctx = bt->ctx;
     if (o.precision == YG_PREC_MIXED && !A->d_val32) YG_TRY(yg_matrix_make_fp32(A));
+    // tiles of whole rows, from the row pointer
+    std::vector<int32_t> rp(A->nbrows + 1);
+    YG_CUDA(cudaStreamSynchronize(ctx->stream));
+    YG_CUDA(cudaMemcpy(rp.data(), A->d_rowptr, sizeof(int32_t) * rp.size(), cudaMemcpyDeviceToHost));
+    std::vector<int32_t> tl;
+    make_tiles(rp, tile_blocks(A->block), tl);
     BatchSys d{};
     d.block = A->block;
     d.nbrows = (int32_t)A->nbrows;
@@ -565,15 +799,20 @@ extern "C" yg_status yg_batch_add(yg_batch bt, yg_matrix A, yg_vector b, yg_vect
     d.b = b->d;
     d.x = x->d;
     d.precision = o.precision;
+    d.ntiles = (int32_t)tl.size() - 1;
     const int64_t n = A->rows();
     double *dinv = nullptr;
+    int32_t *dtiles = nullptr;
     yg_status st;
     if ((st = dev_alloc_t(ctx, &d.r, n + 1)) != YG_OK || (st = dev_alloc_t(ctx, &d.p, n + 1)) != YG_OK ||
-        (st = dev_alloc_t(ctx, &d.q, n + 1)) != YG_OK || (st = dev_alloc_t(ctx, &dinv, n + 1)) != YG_OK) {
-        for (void *ptr : {(void *)d.r, (void *)d.p, (void *)d.q, (void *)dinv}) dev_free(ctx, ptr);
+        (st = dev_alloc_t(ctx, &d.q, n + 1)) != YG_OK || (st = dev_alloc_t(ctx, &dinv, n + 1)) != YG_OK ||
+        (st = dev_alloc_t(ctx, &dtiles, tl.size())) != YG_OK) {
+        for (void *ptr : {(void *)d.r, (void *)d.p, (void *)d.q, (void *)dinv, (void *)dtiles}) dev_free(ctx, ptr);
         return st;
     }
+    YG_CUDA(cudaMemcpy(dtiles, tl.data(), sizeof(int32_t) * tl.size(), cudaMemcpyHostToDevice));
     d.dinv = dinv;
+    d.tiles = dtiles;
     k_batch_jacobi<<<stream_grid(ctx, n), kThreads, 0, ctx->stream>>>(A->nbrows, A->block, A->d_diag, A->d_val, dinv);
     YG_LAUNCHED(ctx);
     BatchScal sc{};
@@ -581,12 +820,14 @@ extern "C" yg_status yg_batch_add(yg_batch bt, yg_matrix A, yg_vector b, yg_vect
     sc.tol = o.tol;
     sc.maxiter = o.maxiter > 0 ? o.maxiter : n;
     bt->sys[s] = d;
+    bt->tiles[s] = std::move(tl);
     bt->used[s] = 1;
     bt->mats[s] = A;
     bt->opts[s] = o;
     YG_CUDA(cudaStreamSynchronize(ctx->stream));
     YG_CUDA(cudaMemcpy(bt->d_scal + s, &sc, sizeof(BatchScal), cudaMemcpyHostToDevice));
-    YG_TRY(rebuild_items(bt));
+    bt->h_scal[s] = sc;
+    bt->dirty = true;
     *slot = s;
     return YG_OK;
 }
@@ -598,7 +839,28 @@ extern "C" yg_status yg_batch_remove(yg_batch bt, int32_t slot) {
     BatchScal sc{};
     sc.flag = BF_EMPTY;
     YG_CUDA(cudaMemcpy(bt->d_scal + slot, &sc, sizeof(BatchScal), cudaMemcpyHostToDevice));
-    return rebuild_items(bt);
+    bt->h_scal[slot] = sc;
+    bt->dirty = true;
+    return YG_OK;
+}
+
+extern "C" yg_status yg_batch_reset(yg_batch bt, int32_t slot) {
+    if (!bt || slot < -1 || slot >= bt->capacity || (slot >= 0 && !bt->used[slot]))
+        return fail(YG_BAD_ARG, "yg_batch_reset: bad slot");
+    YG_CUDA(cudaStreamSynchronize(bt->ctx->stream));
+    const int s0 = slot < 0 ? 0 : slot, s1 = slot < 0 ? bt->capacity : slot + 1;
+    for (int s = s0; s < s1; ++s) {
+        if (!bt->used[s]) continue;
+        const yg_solve_opts &o = bt->opts[s];
+        BatchScal sc{};
+        sc.flag = BF_INIT;
+        sc.tol = o.tol;
+        sc.maxiter = o.maxiter > 0 ? o.maxiter : (int64_t)bt->sys[s].nbrows * bt->sys[s].block;
+        bt->h_scal[s] = sc;
+    }
+    YG_CUDA(cudaMemcpy(bt->d_scal + s0, bt->h_scal.data() + s0, sizeof(BatchScal) * (s1 - s0), cudaMemcpyHostToDevice));
+    bt->dirty = true;
+    return YG_OK;
 }
 
 // Advance every active system by blocks of m iterations plus a verification
@@ -607,6 +869,7 @@ extern "C" yg_status yg_batch_remove(yg_batch bt, int32_t slot) {
 extern "C" yg_status yg_batch_run(yg_batch bt, int32_t max_blocks, int32_t *n_active) {
     if (!bt) return fail(YG_BAD_ARG, "yg_batch_run: NULL batch");
     yg_context ctx = bt->ctx;
+    if (bt->dirty) YG_TRY(rebuild_items(bt));
     if (!bt->exec || bt->graph_groups != bt->groups_present) YG_TRY(capture_graph(bt));
     launch_verify(bt);  // initialise systems added since the last run
     int active = 0;
@@ -616,10 +879,17 @@ extern "C" yg_status yg_batch_run(yg_batch bt, int32_t max_blocks, int32_t *n_ac
         YG_CUDA(cudaMemcpyAsync(bt->h_scal.data(), bt->d_scal, sizeof(BatchScal) * bt->capacity, cudaMemcpyDeviceToHost,
                                 ctx->stream));
         YG_CUDA(cudaStreamSynchronize(ctx->stream));
+        YG_TRY(check_device_error(ctx));
         active = 0;
+        int32_t live = 0;
         for (int s = 0; s < bt->capacity; ++s)
-            if (bt->used[s] && (bt->h_scal[s].flag == BF_RUN || bt->h_scal[s].flag == BF_INIT)) ++active;
+            if (sys_live(bt, s)) {
+                ++active;
+                live += bt->sys[s].item_end - bt->sys[s].item_begin;
+            }
         if (active == 0) break;
+        // drop finished systems from the item table once a quarter of it is idle
+        if (live < bt->live_items - bt->live_items / 4 && bt->live_items - live >= 64) YG_TRY(rebuild_items(bt));
     }
     if (n_active) *n_active = active;
     return check_device_error(ctx);
@@ -645,8 +915,9 @@ extern "C" yg_status yg_batch_stats(yg_batch bt, int32_t slot, yg_solve_stats *o
     return YG_OK;
 }
 
-// Choose rows per item and lanes per row for each block size from the systems
-// present, by timing the iteration SpMV of the whole batch (autotuned tiles).
+// Choose tiles per item and lanes per block row for each block size from the
+// systems present, by timing the iteration SpMV of the whole batch (without
+// committing its reductions).
 extern "C" yg_status yg_batch_tune(yg_batch bt) {
     if (!bt) return fail(YG_BAD_ARG, "yg_batch_tune: NULL batch");
     yg_context ctx = bt->ctx;
@@ -654,21 +925,22 @@ extern "C" yg_status yg_batch_tune(yg_batch bt) {
     YG_TRY(rebuild_items(bt));
     launch_verify(bt);
     YG_CUDA(cudaStreamSynchronize(ctx->stream));
+    YG_TRY(check_device_error(ctx));
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     for (int B = 1; B <= 3; ++B) {
         if (!(bt->groups_present & (1u << (B - 1)))) continue;
         float best = 1e30f;
-        int bestL = bt->lanes[B], bestR = bt->group_rows[B];
-        for (int R : {256, 1024, 4096}) {
-            bt->group_rows[B] = R;
+        int bestL = bt->lanes[B], bestT = bt->tiles_per_item[B];
+        for (int T : {2, 8, 32}) {
+            bt->tiles_per_item[B] = T;
             YG_TRY(rebuild_items(bt));
             for (int L : {2, 4, 8, 16, 32}) {
                 auto launch = [&]() {
-                    if (B == 1) launch_bspmv<1, 0>(bt, L);
-                    else if (B == 2) launch_bspmv<2, 0>(bt, L);
-                    else launch_bspmv<3, 0>(bt, L);
+                    if (B == 1) launch_bspmv<1, 0>(bt, L, 0, 0);
+                    else if (B == 2) launch_bspmv<2, 0>(bt, L, 0, 0);
+                    else launch_bspmv<3, 0>(bt, L, 0, 0);
                 };
                 launch();
                 cudaEventRecord(e0, ctx->stream);
@@ -677,16 +949,16 @@ extern "C" yg_status yg_batch_tune(yg_batch bt) {
                 cudaEventSynchronize(e1);
                 float ms = 0;
                 cudaEventElapsedTime(&ms, e0, e1);
-                if (ms < best) { best = ms; bestL = L; bestR = R; }
+                if (ms < best) { best = ms; bestL = L; bestT = T; }
             }
         }
         bt->lanes[B] = bestL;
-        bt->group_rows[B] = bestR;
+        bt->tiles_per_item[B] = bestT;
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     YG_TRY(rebuild_items(bt));
     drop_graph(bt);
     YG_CUDA(cudaGetLastError());
-    return YG_OK;
+    return check_device_error(ctx);
 }

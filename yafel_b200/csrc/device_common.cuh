@@ -76,3 +76,38 @@ __device__ __forceinline__ void block_chunk(int64_t n, int64_t &lo, int64_t &hi)
 __device__ __forceinline__ int read_flag(const int32_t *flag) {
     return *reinterpret_cast<const volatile int32_t *>(flag);
 }
+
+// ---- mbarrier + bulk asynchronous copy (cp.async.bulk) helpers
+
+// Bound on the polls of one mbarrier wait; a kernel that reaches it records
+// YG_TIMEOUT and stops instead of spinning on.
+constexpr long long kSpinLimit = 1ll << 26;
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
+    unsigned a = (unsigned)__cvta_generic_to_shared(bar);
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(a), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes) {
+    unsigned a = (unsigned)__cvta_generic_to_shared(bar);
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(a), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity) {
+    unsigned a = (unsigned)__cvta_generic_to_shared(bar);
+    unsigned ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(a), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes, uint64_t *bar, uint64_t pol) {
+    unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    unsigned b = (unsigned)__cvta_generic_to_shared(bar);
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;" ::"r"(d),
+        "l"(src), "r"(bytes), "r"(b), "l"(pol)
+        : "memory");
+}

@@ -256,7 +256,6 @@ k_bcsr_spmv_staged(int64_t nbrows, const int32_t *__restrict__ rowptr, const int
 // of one 16-byte cp.async per lane and line.  Lanes take two blocks at a time
 // with independent accumulators.  Waits on an mbarrier are bounded: after
 // kSpinLimit polls the kernel records YG_TIMEOUT in `err` and stops.
-constexpr long long kSpinLimit = 1ll << 26;
 
 template <int B, typename VT, int CH_, int NST_, int WARPS_>
 struct TmaCfg {
@@ -266,35 +265,6 @@ struct TmaCfg {
     static constexpr int STAGE = VBYTES + CBYTES;
     static constexpr int SMEM = WARPS * NST * STAGE + WARPS * NST * 8;  // stages + mbarriers
 };
-
-__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
-    unsigned a = (unsigned)__cvta_generic_to_shared(bar);
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(a), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes) {
-    unsigned a = (unsigned)__cvta_generic_to_shared(bar);
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(a), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity) {
-    unsigned a = (unsigned)__cvta_generic_to_shared(bar);
-    unsigned ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(a), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes, uint64_t *bar, uint64_t pol) {
-    unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-    unsigned b = (unsigned)__cvta_generic_to_shared(bar);
-    asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;" ::"r"(d),
-        "l"(src), "r"(bytes), "r"(b), "l"(pol)
-        : "memory");
-}
 
 template <int B, typename VT, int DOT, typename C>
 __global__ void __launch_bounds__(C::WARPS * 32)

@@ -49,3 +49,27 @@ def rhs(spec, ndofs):
 def clamp_dofs(X, dpn):
     nodes = np.nonzero(np.abs(X[:, 0]) < 1e-9)[0]
     return (nodes[:, None] * dpn + np.arange(dpn)[None, :]).ravel().astype(np.int64)
+
+
+def assemble(spec, ctx):
+    """Assemble problem `spec` on the device through the public API: DoF
+    numbering, tangent (CSR for Poisson, 2x2/3x3 BCSR for elasticity), the
+    N(0,1) right-hand side and u = 0 on x = 0.  Returns (mesh, K, b, clamp_dofs)."""
+    import yafel_b200 as yb
+    mesh = build_mesh(spec)
+    dpn, dim = spec["dpn"], spec["dim"]
+    dm = yb.DoFManager(mesh, spec["order"], dpn, ctx=ctx)
+    fe = yb.FESystem(dm, dim, format=yb.CSR if dpn == 1 else yb.BCSR)
+    if spec["kind"] == "poisson":
+        phys = yb.PoissonEquation(dim, f=0.0)
+    else:
+        phys = yb.LinearElasticity(dim, E=1.0, nu=0.3, body=(0.0, 0.0, 0.0))
+    yb.CGAssembly(phys, fe, [yb.AssemblyRequirement.Tangent])
+    K = fe.getGlobalTangent()
+    b = yb.DeviceVector(rhs(spec, dm.ndofs), ctx)
+    nodes = np.nonzero(np.abs(dm.dof_nodes[:, 0]) < 1e-9)[0].astype(np.int64)
+    for c in range(dpn):
+        bc = yb.DirichletBC(dm, 0.0, c)
+        bc.bc_nodes = nodes
+        bc.apply(K, b)
+    return mesh, K, b, clamp_dofs(dm.dof_nodes, dpn)
