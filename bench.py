@@ -283,6 +283,9 @@ def run_gpu(args):
         "setup": {"dof_numbering_s": t_dof},
         "clocks": clk,
     }
+    if ws == 1 and not args.no_extra:
+        out["small_poisson64"] = run_small_poisson(ctx)
+        out["q3_30cubed"] = run_q3(ctx)
     if rank == 0 and not args.no_cpu_baseline and ws == 1:
         out["cpu_baseline"] = cpu_baseline(args)
     if rank == 0:
@@ -290,6 +293,90 @@ def run_gpu(args):
     if torch_dist:
         torch_dist.barrier()
         torch_dist.destroy_process_group()
+
+
+def run_small_poisson(ctx, reps=30):
+    """64x64 Q1 Poisson on the unit square (4225 dofs, f=1, u=0 on the whole
+    boundary, 2x2 Gauss-Legendre, FP64 CSR, Jacobi-PCG to 1e-10).  The system
+    is L2-resident, so it reports latency and solves/s rather than a roofline:
+    one solve = assembly + Dirichlet + Jacobi + solve, the DoF numbering done
+    once.  Returns the summary dict."""
+    import yafel_b200 as yb
+    from yafel_b200 import meshgen
+    mesh = meshgen.structured_quad(64, 64, order=meshgen.corner_order(1))
+    dm = yb.DoFManager(mesh, 1, 1, ctx=ctx)
+    bc = yb.DirichletBC(dm, 0.0, 0)
+    bc.selectByFunction(lambda X: (X[:, 0] < 1e-9) | (X[:, 0] > 1 - 1e-9) | (X[:, 1] < 1e-9) | (X[:, 1] > 1 - 1e-9))
+    phys = yb.PoissonEquation(2, f=1.0)
+
+    def one():
+        fe = yb.FESystem(dm, 2, format=yb.CSR)
+        yb.CGAssembly(phys, fe)
+        K, F = fe.getGlobalTangent(), fe.getGlobalResidual()
+        bc.apply(K, F)
+        x, st = yb.solve(K, F, M=yb.JacobiPreconditioner(K), tol=TOL)
+        return K, x, st
+
+    for _ in range(3):
+        one()
+    lat, solve_ms = [], []
+    for _ in range(reps):
+        ctx.synchronize()
+        t0 = time.perf_counter()
+        K, x, st = one()
+        ctx.synchronize()
+        lat.append(time.perf_counter() - t0)
+        solve_ms.append(st.device_ms)
+    lat.sort()
+    return {"workload": "poisson_q1_quad_64x64_jacobi_pcg_1e-10", "dofs": dm.ndofs, "nnz": K.nnz(),
+            "iterations": st.iterations, "relres": st.rel_residual, "status": st.status,
+            "latency_ms_p50": 1e3 * lat[len(lat) // 2], "latency_ms_p99": 1e3 * lat[min(len(lat) - 1, int(0.99 * len(lat)))],
+            "solve_device_ms_p50": sorted(solve_ms)[len(solve_ms) // 2], "solves_per_s": len(lat) / sum(lat),
+            "l2": "L2-resident (%.2f MB): latency, not a roofline" % ((K.nnz() * 12 + dm.ndofs * 40) / 1e6)}
+
+
+def run_q3(ctx, nx=30, steps=2):
+    """3D elasticity, 30^3 Q3 hexes (2,260,713 dofs), clamp x=0, traction
+    (1,0,0) on x=1, BCSR3, Jacobi-PCG to 1e-10 in FP64 and in mixed precision
+    (FP32 matrix values, FP64 vectors, reductions and true-residual
+    replacement).  Reports dofs/s of assemble+solve for each and the relative
+    difference of the mixed solution from the FP64 one."""
+    import yafel_b200 as yb
+    from yafel_b200 import loads, meshgen
+    mesh = meshgen.structured_hex(nx, nx, nx, order=meshgen.corner_order(3))
+    dm = yb.DoFManager(mesh, 3, 3, ctx=ctx)
+    X = dm.dof_nodes
+    clamp = np.nonzero(np.abs(X[:, 0]) < 1e-9)[0].astype(np.int64)
+    trac = yb.DeviceVector(loads.hex_face_traction(dm, lambda Y: np.abs(Y[:, 0] - 1.0) < 1e-9, (1.0, 0.0, 0.0)), ctx)
+    phys = yb.LinearElasticity(3, E=E, nu=NU)
+    out = {"workload": "elasticity_q3_hex_%d^3_jacobi_pcg_1e-10" % nx, "dofs": dm.ndofs}
+    sol = {}
+    for name, prec in (("fp64", 0), ("mixed", 1)):
+        times, st = [], None
+        for k in range(steps + 1):
+            ctx.synchronize()
+            t0 = time.perf_counter()
+            fe = yb.FESystem(dm, 3, format=yb.BCSR)
+            yb.CGAssembly(phys, fe)
+            K, F = fe.getGlobalTangent(), fe.getGlobalResidual()
+            F.axpy(1.0, trac)
+            for c in range(3):
+                bc = yb.DirichletBC(dm, 0.0, c)
+                bc.bc_nodes = clamp
+                bc.apply(K, F)
+            x, st = yb.solve(K, F, M=yb.JacobiPreconditioner(K), tol=TOL, precision=prec)
+            ctx.synchronize()
+            if k > 0:
+                times.append(time.perf_counter() - t0)
+        sol[name] = x.numpy()
+        t = statistics.mean(times)
+        out[name] = {"s_per_solve": t, "dofs_per_s": dm.ndofs / t, "iterations": st.iterations,
+                     "relres": st.rel_residual, "status": st.status, "refinements": st.refinements}
+        out["blocks"] = K.nnz() // 9
+        del K, F, fe, x
+    out["mixed_speedup"] = out["fp64"]["s_per_solve"] / out["mixed"]["s_per_solve"]
+    out["mixed_rel_diff_vs_fp64"] = float(np.linalg.norm(sol["mixed"] - sol["fp64"]) / np.linalg.norm(sol["fp64"]))
+    return out
 
 
 BATCH_METRIC = "solves/sec to 1e-10 (batched 2D Poisson/elasticity, mixed precision)"
@@ -493,6 +580,7 @@ def main():
     ap.add_argument("--nx", type=int, default=NX)
     ap.add_argument("--cpu-nx", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extra", action="store_true", help="skip the 64x64 Poisson and 30^3 Q3 side measurements")
     ap.add_argument("--spmv-profile", action="store_true", help="time the SpMV kernel alone (roofline/ncu)")
     ap.add_argument("--variant", type=int, default=None, help="SpMV variant for --spmv-profile (0 flat, 1 staged, 2 TMA)")
     ap.add_argument("--lanes", type=int, default=32, help="SpMV lanes / TMA configuration for --spmv-profile")
