@@ -39,7 +39,8 @@ typedef enum yg_status {
     YG_BAD_ARG = 7,
     YG_CUDA_ERROR = 8,
     YG_UNSUPPORTED = 9,
-    YG_ZERO_PIVOT = 10    /* reported, not fatal: the reference warns and continues */
+    YG_ZERO_PIVOT = 10,   /* reported, not fatal: the reference warns and continues */
+    YG_RUNNING = 11       /* a batched or served solve still in progress */
 } yg_status;
 
 typedef struct yg_context_t *yg_context;
@@ -249,20 +250,29 @@ YG_API yg_status yg_bicgstab(yg_matrix A, yg_precond M, yg_vector b, yg_vector x
 /* ------------------------------------------------------------------ batched and served solves */
 
 /* Many independent systems advanced together by shared persistent-grid kernels
- * (Jacobi-PCG, relative-residual criterion).  No reference counterpart: the
- * reference solves one system per pcg_solve call.  Each system keeps its own
- * matrix (CSR or 2x2/3x3 BCSR), right-hand side and iterate, which must stay
- * alive while it is in the batch; x holds x0 when added and the solution when
- * finished.  Systems may be added and removed between calls of yg_batch_run
- * (continuous batching); work advances in blocks of iterations captured in one
- * CUDA graph followed by an FP64 verification pass (true residual b - A x for
- * converged systems, and the residual replacement of YG_PREC_MIXED). */
+ * (relative-residual criterion): symmetric positive definite systems by
+ * Jacobi-PCG, non-symmetric ones by BiCGSTAB with right Jacobi
+ * preconditioning, in the same launches.  No reference counterpart: the
+ * reference solves one system per pcg_solve / bicgstab_solve call.  Each system
+ * keeps its own matrix (CSR or 2x2/3x3 BCSR), right-hand side and iterate,
+ * which must stay alive while it is in the batch; x holds x0 when added and the
+ * solution when finished.  Systems may be added and removed between calls of
+ * yg_batch_run (continuous batching); work advances in blocks of iterations
+ * captured in one CUDA graph followed by an FP64 verification pass (true
+ * residual b - A x for converged systems, BiCGSTAB restarts after a breakdown,
+ * and the residual replacement of YG_PREC_MIXED).  A system's result does not
+ * depend on the other systems in the batch. */
 typedef struct yg_batch_t *yg_batch;
+enum { YG_METHOD_CG = 0, YG_METHOD_BICGSTAB = 1 };
 YG_API yg_status yg_batch_create(yg_context ctx, int32_t capacity, yg_batch *out);
 YG_API yg_status yg_batch_destroy(yg_batch B);
-/* opts: criterion must be YG_CRIT_RELRES; precision YG_PREC_FP64 or YG_PREC_MIXED. */
-YG_API yg_status yg_batch_add(yg_batch B, yg_matrix A, yg_vector b, yg_vector x, const yg_solve_opts *opts,
-                              int32_t *slot);
+/* method: YG_METHOD_CG (Jacobi-PCG) or YG_METHOD_BICGSTAB; opts: criterion must
+ * be YG_CRIT_RELRES, precision YG_PREC_FP64 or YG_PREC_MIXED. */
+YG_API yg_status yg_batch_add(yg_batch B, yg_matrix A, yg_vector b, yg_vector x, int32_t method,
+                              const yg_solve_opts *opts, int32_t *slot);
+/* Device bytes yg_batch_add allocates for a system of `rows` rows (work vectors
+ * and tile table), for admission against a memory budget. */
+YG_API int64_t yg_batch_work_bytes(int64_t rows, int32_t method);
 YG_API yg_status yg_batch_remove(yg_batch B, int32_t slot);
 /* Solve a slot's system again from its current x (the caller may have changed
  * x or b in place); slot -1 resets every system in the batch. */
@@ -270,10 +280,15 @@ YG_API yg_status yg_batch_reset(yg_batch B, int32_t slot);
 /* Run at most max_blocks blocks of iterations (0 = until no system is active);
  * *n_active receives the number of systems still iterating. */
 YG_API yg_status yg_batch_run(yg_batch B, int32_t max_blocks, int32_t *n_active);
-/* Status (YG_OK when converged and verified in FP64), iterations and FP64 relative
- * residual of a slot. */
+/* One block of iterations without waiting (the host may prepare new systems
+ * meanwhile), then yg_batch_wait for it; systems are added or removed only
+ * between a wait and the next launch. */
+YG_API yg_status yg_batch_launch(yg_batch B);
+YG_API yg_status yg_batch_wait(yg_batch B, int32_t *n_active);
+/* Status (YG_OK when converged and verified in FP64, YG_RUNNING while it
+ * iterates), iterations and FP64 relative residual of a slot. */
 YG_API yg_status yg_batch_stats(yg_batch B, int32_t slot, yg_solve_stats *stats);
-/* Autotune rows per work item and lanes per row for the systems present. */
+/* Autotune tiles per work item and lanes per block row for the systems present. */
 YG_API yg_status yg_batch_tune(yg_batch B);
 
 /* ------------------------------------------------------------------ allocation-free dot product */

@@ -17,8 +17,14 @@ def assemble_problem(spec, ctx):
 
 def oracle_relres(spec, mesh, dofs, b_host, x):
     odm = O.dofmanager(mesh, spec["order"])
-    kind = O.POISSON if spec["kind"] == "poisson" else O.ELASTICITY
-    params = [1.0, 0.0] if kind == O.POISSON else [1.0, 0.576923076923077, 0.3846153846153846, 0, 0, 0]
+    if spec["kind"] == "supg":
+        kind = O.SUPG
+        h = 1.0 / spec["n"]
+        params = [h / (2.0 * spec["peclet"]), h, 1.0, 0.0]
+    elif spec["kind"] == "poisson":
+        kind, params = O.POISSON, [1.0, 0.0]
+    else:
+        kind, params = O.ELASTICITY, [1.0, 0.576923076923077, 0.3846153846153846, 0, 0, 0]
     K, _ = O.assemble(odm, spec["dpn"], spec["dim"], kind, params)
     mask = np.zeros(K.nrows, np.uint8)
     mask[dofs] = 1
@@ -93,3 +99,44 @@ def test_reset_solves_again_to_the_same_bits(ctx):
     for s, f in zip(slots, first):
         assert B.stats(s).status == 0
         assert np.array_equal(B.solution(s).numpy(), f)
+
+
+MIXED_SPECS = [workloads.problem_spec(i, lo=1e3, hi=1e4, kinds=("supg", "poisson", "elasticity")) for i in range(8)]
+
+
+@pytest.mark.parametrize("precision", [yb.PREC_FP64, yb.PREC_MIXED])
+def test_batch_bicgstab_beside_pcg(ctx, precision):
+    """SUPG advection-diffusion systems (BiCGSTAB) and SPD systems (PCG) in one
+    batch: all reach 1e-10 (checked on the oracle-assembled system) and the
+    BiCGSTAB results agree with the single-system yg_bicgstab."""
+    assert any(s["kind"] == "supg" for s in MIXED_SPECS) and any(s["kind"] != "supg" for s in MIXED_SPECS)
+    probs = [assemble_problem(s, ctx) for s in MIXED_SPECS]
+    B = yb.Batch(len(probs), ctx)
+    slots = [B.add(K, b, precision=precision, method=workloads.method(s)) for s, (_, K, b, _) in zip(MIXED_SPECS, probs)]
+    B.tune()
+    assert B.run() == 0
+    for spec, (mesh, K, b, dofs), s in zip(MIXED_SPECS, probs, slots):
+        st = B.stats(s)
+        assert st.status == 0 and st.rel_residual <= 1e-10, (spec, st.status, st.rel_residual)
+        x = B.solution(s).numpy()
+        assert oracle_relres(spec, mesh, dofs, b.numpy(), x) <= 1e-10, spec
+        if spec["kind"] == "supg":
+            xs, sts = yb.solve(K, b, M=yb.JacobiPreconditioner(K), method="bicgstab", tol=1e-10)
+            assert sts.status == 0
+            assert np.linalg.norm(x - xs.numpy()) <= 1e-6 * np.linalg.norm(xs.numpy())
+
+
+def test_bicgstab_same_result_alone_and_in_mix(ctx):
+    probs = [assemble_problem(s, ctx) for s in MIXED_SPECS]
+    methods = [workloads.method(s) for s in MIXED_SPECS]
+    alone = []
+    for (_, K, b, _), m in zip(probs, methods):
+        B1 = yb.Batch(1, ctx)
+        s = B1.add(K, b, method=m)
+        assert B1.run() == 0
+        alone.append(B1.solution(s).numpy())
+    B = yb.Batch(len(probs), ctx)
+    slots = [B.add(K, b, method=m) for (_, K, b, _), m in zip(probs, methods)]
+    assert B.run() == 0
+    for i, s in enumerate(slots):
+        assert np.array_equal(B.solution(s).numpy(), alone[i]), i

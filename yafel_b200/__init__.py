@@ -28,6 +28,7 @@ CG_SOLVER_TOL = 1.0e-14
 
 CSR, BCSR = 0, 1
 PREC_FP64, PREC_MIXED, PREC_MIXED_IR = 0, 1, 2
+METHOD_CG, METHOD_BICGSTAB = 0, 1
 CRIT_REFERENCE, CRIT_RELRES = 0, 1
 POISSON, ELASTICITY, SUPG = 0, 1, 2
 
@@ -644,13 +645,16 @@ class Batch:
         self.h = h
         self._keep = {}
 
-    def add(self, A, b, x0=None, tol=1e-10, precision=PREC_FP64, maxiter=0):
+    def add(self, A, b, x0=None, tol=1e-10, precision=PREC_FP64, maxiter=0, method="cg"):
+        """Add A x = b (x0 default 0); method "cg" (Jacobi-PCG, SPD systems) or
+        "bicgstab" (right Jacobi-preconditioned BiCGSTAB).  Returns the slot."""
         bd, _ = _as_device(b, self.ctx)
         xd = x0 if isinstance(x0, DeviceVector) else DeviceVector(
             np.zeros(A.rows()) if x0 is None else np.asarray(x0, dtype=np.float64), self.ctx)
         opts = SolveOpts(CRIT_RELRES, precision, tol, maxiter, 0, 0)
         slot = C.c_int32()
-        check(lib().yg_batch_add(self.h, A.h, bd.h, xd.h, C.byref(opts), C.byref(slot)), "Batch.add")
+        m = {"cg": METHOD_CG, "bicgstab": METHOD_BICGSTAB}[method]
+        check(lib().yg_batch_add(self.h, A.h, bd.h, xd.h, m, C.byref(opts), C.byref(slot)), "Batch.add")
         self._keep[slot.value] = (A, bd, xd)
         return slot.value
 
@@ -669,6 +673,15 @@ class Batch:
 
     def tune(self):
         check(lib().yg_batch_tune(self.h), "Batch.tune")
+
+    def launch(self):
+        """One block of iterations without waiting; pair with wait()."""
+        check(lib().yg_batch_launch(self.h), "Batch.launch")
+
+    def wait(self):
+        n = C.c_int32()
+        check(lib().yg_batch_wait(self.h, C.byref(n)), "Batch.wait")
+        return n.value
 
     def stats(self, slot):
         st = SolveStats()

@@ -11,7 +11,7 @@ LIB_PATH = os.path.join(HERE, "libyafel_b200.so")
 _LIB = None
 
 YG_OK, YG_NOT_CONVERGED, YG_BREAKDOWN, YG_NAN, YG_TIMEOUT, YG_OUT_OF_MEMORY, YG_OVER_BUDGET, \
-    YG_BAD_ARG, YG_CUDA_ERROR, YG_UNSUPPORTED, YG_ZERO_PIVOT = range(11)
+    YG_BAD_ARG, YG_CUDA_ERROR, YG_UNSUPPORTED, YG_ZERO_PIVOT, YG_RUNNING = range(12)
 
 vp = C.c_void_p
 i32, i64, u32, u64, f64 = C.c_int32, C.c_int64, C.c_uint32, C.c_uint64, C.c_double
@@ -75,7 +75,10 @@ SIGNATURES = {
     "yg_bicgstab": (i32, [vp, vp, vp, vp, P(SolveOpts), P(SolveStats)]),
     "yg_batch_create": (i32, [vp, i32, P(vp)]),
     "yg_batch_destroy": (i32, [vp]),
-    "yg_batch_add": (i32, [vp, vp, vp, vp, P(SolveOpts), P(i32)]),
+    "yg_batch_add": (i32, [vp, vp, vp, vp, i32, P(SolveOpts), P(i32)]),
+    "yg_batch_work_bytes": (i64, [i64, i32]),
+    "yg_batch_launch": (i32, [vp]),
+    "yg_batch_wait": (i32, [vp, P(i32)]),
     "yg_batch_remove": (i32, [vp, i32]),
     "yg_batch_reset": (i32, [vp, i32]),
     "yg_batch_run": (i32, [vp, i32, P(i32)]),

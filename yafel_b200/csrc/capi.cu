@@ -270,6 +270,7 @@ extern "C" const char *yg_status_string(yg_status s) {
     case YG_CUDA_ERROR: return "CUDA error";
     case YG_UNSUPPORTED: return "unsupported";
     case YG_ZERO_PIVOT: return "zero pivot";
+    case YG_RUNNING: return "running";
     }
     return "unknown status";
 }

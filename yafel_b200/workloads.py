@@ -1,6 +1,7 @@
 """Seeded synthetic problem sets for the batched and served forms.
 
-Every problem is a 2D (or 3D) Poisson or linear-elasticity system on a
+Every problem is a 2D (or 3D) Poisson, linear-elasticity or SUPG
+advection-diffusion (element Peclet number log-uniform in [1, 100]) system on a
 structured grid whose cells are quads or triangle pairs (seeded coin) with
 interior nodes jittered by U(-0.2, 0.2)*h, Dirichlet u = 0 on x = 0 and an
 i.i.d. N(0,1) right-hand side.  Problem i of a set uses the seed base + i
@@ -30,8 +31,29 @@ def problem_spec(i, base=BASE_SEED, lo=1e3, hi=2e5, orders=(1, 2, 3), kinds=("po
     dim = int(rng.choice(dims))
     dpn = dim if kind == "elasticity" else 1
     n = grid_for_dofs(target, p, dpn, dim)
-    return {"index": i, "seed": base + i, "target_dofs": target, "order": p, "kind": kind, "dim": dim, "dpn": dpn,
+    spec = {"index": i, "seed": base + i, "target_dofs": target, "order": p, "kind": kind, "dim": dim, "dpn": dpn,
             "n": n}
+    if kind == "supg":
+        spec["peclet"] = math.exp(rng.uniform(math.log(1.0), math.log(100.0)))
+    return spec
+
+
+def method(spec):
+    """Krylov method of a problem: BiCGSTAB for the non-symmetric SUPG systems."""
+    return "bicgstab" if spec["kind"] == "supg" else "cg"
+
+
+def physics(spec):
+    """Device physics of a problem.  SUPG: U = (1,0,0), h = the cell size, and
+    k = U h / (2 Pe) for the drawn element Peclet number Pe."""
+    import yafel_b200 as yb
+    dim = spec["dim"]
+    if spec["kind"] == "poisson":
+        return yb.PoissonEquation(dim, f=0.0)
+    if spec["kind"] == "elasticity":
+        return yb.LinearElasticity(dim, E=1.0, nu=0.3, body=(0.0, 0.0, 0.0))
+    h = 1.0 / spec["n"]
+    return yb.AdvectionDiffusionSUPG(dim, k=h / (2.0 * spec["peclet"]), h=h, U0=1.0, Q=0.0)
 
 
 def build_mesh(spec):
@@ -60,11 +82,7 @@ def assemble(spec, ctx):
     dpn, dim = spec["dpn"], spec["dim"]
     dm = yb.DoFManager(mesh, spec["order"], dpn, ctx=ctx)
     fe = yb.FESystem(dm, dim, format=yb.CSR if dpn == 1 else yb.BCSR)
-    if spec["kind"] == "poisson":
-        phys = yb.PoissonEquation(dim, f=0.0)
-    else:
-        phys = yb.LinearElasticity(dim, E=1.0, nu=0.3, body=(0.0, 0.0, 0.0))
-    yb.CGAssembly(phys, fe, [yb.AssemblyRequirement.Tangent])
+    yb.CGAssembly(physics(spec), fe, [yb.AssemblyRequirement.Tangent])
     K = fe.getGlobalTangent()
     b = yb.DeviceVector(rhs(spec, dm.ndofs), ctx)
     nodes = np.nonzero(np.abs(dm.dof_nodes[:, 0]) < 1e-9)[0].astype(np.int64)
