@@ -498,6 +498,146 @@ def run_batch(args):
     print(json.dumps(out), flush=True)
 
 
+SERVE_METRIC = "served solves/sec to 1e-10 (continuous batching of Poisson arrivals), p50/p99 latency"
+
+
+def run_serve(args):
+    """Serving loop: `--requests` requests arrive as a Poisson process of rate
+    `--rate` per second (seeded): 2D/3D Poisson, elasticity and SUPG
+    advection-diffusion (BiCGSTAB), sizes log-uniform 1e3..1e6 dofs, orders 1-2.
+    Each request carries its mesh (built by the client beforehand); the server
+    side does the DoF numbering, device assembly, boundary conditions, the solve
+    to a 1e-10 relative residual and the download of the solution.  Requests are
+    admitted in arrival order under an HBM budget (`--budget-gb`) and solved
+    together in one batch (yg_server_*), in mixed precision (the value) and in
+    FP64; the same requests served one at a time by the plain FP64 single-system
+    solvers give the baseline.  Latency = arrival to solution on the host."""
+    import yafel_b200 as yb
+    from yafel_b200 import workloads
+    ctx = yb.Context(0)
+    N = args.requests
+    specs = workloads.serving_specs(N)
+    arr = workloads.arrivals(N, args.rate)
+    meshes = [workloads.build_mesh(s) for s in specs]
+    dofs = []
+    for s in specs:
+        dofs.append(s["dpn"] * (s["order"] * s["n"] + 1) ** s["dim"])
+    budget = int(args.budget_gb * 1e9)
+
+    def served(precision, idxs, clocks=None):
+        S = yb.Server(budget, max_active=args.max_active, ctx=ctx)
+        idx, pending = {}, []
+        lat, stats = {}, {}
+        state = {"nsub": 0}
+        n = len(idxs)
+        l0 = ctx.launches
+        ctx.synchronize()
+        t0 = time.perf_counter()
+
+        def take_arrivals():
+            t = time.perf_counter() - t0
+            while state["nsub"] < n and arr[idxs[state["nsub"]]] - arr[idxs[0]] <= t:
+                i = idxs[state["nsub"]]
+                idx[S.submit(workloads.est_bytes(specs[i]))] = i
+                state["nsub"] += 1
+
+        def admit_build():
+            while True:
+                r = S.admit()
+                if r is None:
+                    return
+                i = idx[r]
+                _, K, b, _ = workloads.assemble(specs[i], ctx, mesh=meshes[i])
+                x = yb.DeviceVector(K.rows(), ctx)
+                x.fill(0.0)
+                pending.append((r, K, b, x, i))
+
+        if clocks:
+            clocks.start()
+        while len(lat) < n:
+            take_arrivals()
+            admit_build()
+            for (r, K, b, x, i) in pending:
+                S.attach(r, K, b, x, method=workloads.method(specs[i]), precision=precision)
+            pending.clear()
+            if S.info()["active"] == 0:
+                if state["nsub"] < n:
+                    time.sleep(max(0.0, arr[idxs[state["nsub"]]] - arr[idxs[0]] - (time.perf_counter() - t0)))
+                continue
+            S.launch()
+            take_arrivals()
+            admit_build()
+            S.wait()
+            for r in S.finished():
+                i = idx[r]
+                stats[i] = S.poll(r)
+                S.solution(r).numpy()
+                lat[i] = time.perf_counter() - t0 - (arr[i] - arr[idxs[0]])
+                S.release(r)
+        total = time.perf_counter() - t0
+        clk = clocks.stop() if clocks else None
+        del S
+        return total, lat, stats, ctx.launches - l0, clk
+
+    def sequential(idxs):
+        lat, stats = {}, {}
+        ctx.synchronize()
+        t0 = time.perf_counter()
+        for i in idxs:
+            wait = arr[i] - arr[idxs[0]] - (time.perf_counter() - t0)
+            if wait > 0:
+                time.sleep(wait)
+            _, K, b, _ = workloads.assemble(specs[i], ctx, mesh=meshes[i])
+            x, st = yb.solve(K, b, M=yb.JacobiPreconditioner(K), method=workloads.method(specs[i]), tol=TOL)
+            x.numpy()
+            lat[i] = time.perf_counter() - t0 - (arr[i] - arr[idxs[0]])
+            stats[i] = st
+            del K, b, x
+        return time.perf_counter() - t0, lat, stats
+
+    def summary(total, lat, stats, idxs):
+        L = sorted(lat[i] for i in idxs)
+        d = sum(dofs[i] for i in idxs)
+        return {"s_total": total, "solves_per_s": len(idxs) / total, "dofs_per_s": d / total,
+                "latency_s_p50": L[len(L) // 2], "latency_s_p99": L[min(len(L) - 1, int(0.99 * len(L)))],
+                "latency_s_max": L[-1], "all_converged": all(stats[i].status == 0 for i in idxs),
+                "max_relres": max(stats[i].rel_residual for i in idxs),
+                "iterations_sum": int(sum(stats[i].iterations for i in idxs))}
+
+    # warm-up on the smallest requests (module loading, graph capture paths)
+    small = sorted(range(N), key=lambda i: dofs[i])[:max(3, args.warmup * 2)]
+    served(yb.PREC_MIXED, small)
+    served(yb.PREC_FP64, small)
+    everything = list(range(N))
+    clocks = Clocks(0)
+    tm, latm, stm, launches, clk = served(yb.PREC_MIXED, everything, clocks)
+    t64, lat64, st64, _, _ = served(yb.PREC_FP64, everything)
+    ts, lats, sts = sequential(everything)
+    mixed = summary(tm, latm, stm, everything)
+    h2d = sum(m["nodes"].nbytes + m["cell_nodes"].nbytes + m["offsets"].nbytes + m["cell_types"].nbytes for m in meshes) + \
+        8 * sum(dofs)
+    out = {"metric": SERVE_METRIC, "value": mixed["solves_per_s"], "unit": "solves/s", "n_gpus": 1, "steps": 1,
+           "warmup": 2, "ms_per_step": tm * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "f32 values, f64 vectors", "data": "synthetic, seeded (requests from seed %d)" %
+           (workloads.BASE_SEED + 1_000_000),
+           "config": {"workload": "serve_%d_requests_poisson_arrivals_%g_per_s" % (N, args.rate), "requests": N,
+                      "offered_rate_per_s": args.rate, "total_dofs": int(sum(dofs)), "min_dofs": int(min(dofs)),
+                      "max_dofs": int(max(dofs)), "budget_GB": args.budget_gb, "max_active": args.max_active,
+                      "kinds": {k: sum(1 for s in specs if s["kind"] == k) for k in ("poisson", "elasticity", "supg")},
+                      "dims": {str(d): sum(1 for s in specs if s["dim"] == d) for d in (2, 3)},
+                      "tolerance": "relative residual 1e-10 (FP64 true residual per request)",
+                      "l2": "requests together far larger than L2"},
+           "served_mixed": mixed, "served_fp64": summary(t64, lat64, st64, everything),
+           "sequential_fp64": summary(ts, lats, sts, everything),
+           "speedup_vs_sequential_fp64": {"served_mixed": ts / tm, "served_fp64": ts / t64},
+           "achieved_vs_offered": mixed["solves_per_s"] / args.rate,
+           "e2e": {"value": mixed["solves_per_s"], "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
+                   "d2h_bytes_per_step": int(8 * sum(dofs)),
+                   "includes": "DoF numbering, mesh upload, assembly, solve, solution download per request"},
+           "gpu_launches": int(launches), "clocks": clk}
+    print(json.dumps(out), flush=True)
+
+
 def cpu_sample(nx, threads):
     """The reference's CPU path on an nx^3 Q2 sample of the same problem:
     oracle assembly (restatement; the reference's own needs Eigen) + the
@@ -585,9 +725,13 @@ def main():
     ap.add_argument("--variant", type=int, default=None, help="SpMV variant for --spmv-profile (0 flat, 1 staged, 2 TMA)")
     ap.add_argument("--lanes", type=int, default=32, help="SpMV lanes / TMA configuration for --spmv-profile")
     ap.add_argument("--reps", type=int, default=10)
-    ap.add_argument("--workload", default="fem", choices=["fem", "batch"],
+    ap.add_argument("--workload", default="fem", choices=["fem", "batch", "serve"],
                     help="fem: 60^3 Q2 elasticity assemble+solve; batch: many 2D problems solved together")
     ap.add_argument("--problems", type=int, default=512, help="problems in the batched workload")
+    ap.add_argument("--requests", type=int, default=160, help="requests in the serving workload")
+    ap.add_argument("--rate", type=float, default=2000.0, help="arrival rate (req/s) of the serving workload")
+    ap.add_argument("--budget-gb", type=float, default=150.0, help="HBM budget of the serving workload")
+    ap.add_argument("--max-active", type=int, default=1024, help="systems solved together by the server")
     args = ap.parse_args()
     if args.spmv_profile:
         run_spmv_profile(args)
@@ -595,6 +739,8 @@ def main():
         run_reference(args)
     elif args.workload == "batch":
         run_batch(args)
+    elif args.workload == "serve":
+        run_serve(args)
     else:
         run_gpu(args)
 

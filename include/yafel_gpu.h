@@ -291,6 +291,34 @@ YG_API yg_status yg_batch_stats(yg_batch B, int32_t slot, yg_solve_stats *stats)
 /* Autotune tiles per work item and lanes per block row for the systems present. */
 YG_API yg_status yg_batch_tune(yg_batch B);
 
+/* A continuous-batching solve server on one context.  No reference
+ * counterpart.  A request is submitted with an estimate of the device bytes it
+ * needs; yg_server_admit hands out queued requests in arrival order while the
+ * admitted ones fit in the budget (the head of the queue waits for room); the
+ * caller builds an admitted request's system on the device and attaches it;
+ * attached systems advance together in one batch (PCG and BiCGSTAB).  Between
+ * yg_server_launch and yg_server_wait one block of iterations runs without
+ * blocking the host (build the next admitted systems meanwhile; attach only
+ * after the wait).  The wait retires finished requests: list them with
+ * yg_server_finished, read their stats with yg_server_poll and their solution
+ * from the x that was attached, then yg_server_release them, which returns
+ * their bytes to the budget. */
+typedef struct yg_server_t *yg_server;
+YG_API yg_status yg_server_create(yg_context ctx, uint64_t budget_bytes, int32_t max_active, yg_server *out);
+YG_API yg_status yg_server_destroy(yg_server S);
+YG_API yg_status yg_server_submit(yg_server S, uint64_t bytes, int64_t *id);
+/* *id = the next admitted request, or -1 when none fits now. */
+YG_API yg_status yg_server_admit(yg_server S, int64_t *id);
+YG_API yg_status yg_server_attach(yg_server S, int64_t id, yg_matrix A, yg_vector b, yg_vector x, int32_t method,
+                                  const yg_solve_opts *opts);
+YG_API yg_status yg_server_launch(yg_server S);
+YG_API yg_status yg_server_wait(yg_server S, int32_t *n_finished);
+YG_API yg_status yg_server_finished(yg_server S, int64_t *ids, int32_t cap, int32_t *n);
+/* stats->status is YG_RUNNING until the request finished. */
+YG_API yg_status yg_server_poll(yg_server S, int64_t id, yg_solve_stats *stats);
+YG_API yg_status yg_server_release(yg_server S, int64_t id);
+YG_API yg_status yg_server_info(yg_server S, int64_t *queued, int64_t *active, uint64_t *bytes_held);
+
 /* ------------------------------------------------------------------ allocation-free dot product */
 
 /* *out = sum_i x[i]*y[i], with x, y and out device pointers and stream a

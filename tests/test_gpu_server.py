@@ -1,0 +1,56 @@
+"""The continuous-batching solve server (yg_server_*): requests of every kind
+(2D/3D Poisson, elasticity, SUPG by BiCGSTAB) are admitted in arrival order
+under an HBM budget small enough to make the queue wait, every request reaches
+a 1e-10 relative residual, the held bytes never exceed the budget, and each
+result equals the one the system gets when solved alone in a batch."""
+import numpy as np
+import pytest
+
+import yafel_b200 as yb
+from yafel_b200 import workloads
+
+pytestmark = pytest.mark.gpu
+
+SPECS = workloads.serving_specs(12, lo=1e3, hi=2e4)
+
+
+def test_server_admits_by_budget_and_solves_everything(ctx):
+    assert {s["kind"] for s in SPECS} == {"poisson", "elasticity", "supg"}
+    assert {s["dim"] for s in SPECS} == {2, 3}
+    est = [workloads.est_bytes(s) for s in SPECS]
+    budget = 2 * max(est)
+    S = yb.Server(budget, max_active=8, ctx=ctx)
+    ids = {S.submit(e): i for i, e in enumerate(est)}
+    built, results, waited_for_room = {}, {}, False
+    while len(results) < len(SPECS):
+        while True:
+            rid = S.admit()
+            if rid is None:
+                break
+            spec = SPECS[ids[rid]]
+            mesh, K, b, _ = workloads.assemble(spec, ctx)
+            x = yb.DeviceVector(K.rows(), ctx)
+            x.fill(0.0)
+            S.attach(rid, K, b, x, method=workloads.method(spec))
+            built[rid] = (K, b)
+        info = S.info()
+        assert info["bytes_held"] <= budget
+        if info["queued"] > 0:
+            waited_for_room = True
+        S.launch()
+        S.wait()
+        for rid in S.finished():
+            st = S.poll(rid)
+            results[ids[rid]] = (st.status, st.rel_residual, S.solution(rid).numpy())
+            S.release(rid)
+            built.pop(rid)
+    assert waited_for_room
+    for i, (status, rel, x) in results.items():
+        assert status == 0 and rel <= 1e-10, (SPECS[i], status, rel)
+    # the same system solved alone
+    for i in (0, 5, 11):
+        mesh, K, b, _ = workloads.assemble(SPECS[i], ctx)
+        B = yb.Batch(1, ctx)
+        s = B.add(K, b, method=workloads.method(SPECS[i]))
+        assert B.run() == 0
+        assert np.array_equal(B.solution(s).numpy(), results[i][2]), i

@@ -695,3 +695,73 @@ class Batch:
         if getattr(self, "h", None) and _alive(getattr(self, "ctx", None)):
             lib().yg_batch_destroy(self.h)
         self.h = None
+
+
+class Server:
+    """Continuous-batching solve server (yg_server_*): requests are submitted
+    with a device-byte estimate, admitted in arrival order under an HBM budget,
+    built by the caller, attached, and advanced together in one batch."""
+
+    def __init__(self, budget_bytes, max_active=1024, ctx=None):
+        self.ctx = ctx or default_context()
+        h = C.c_void_p()
+        check(lib().yg_server_create(self.ctx.h, int(budget_bytes), int(max_active), C.byref(h)), "Server")
+        self.h = h
+        self._keep = {}
+
+    def submit(self, est_bytes):
+        r = C.c_int64()
+        check(lib().yg_server_submit(self.h, int(est_bytes), C.byref(r)), "Server.submit")
+        return r.value
+
+    def admit(self):
+        """Id of the next admitted request, or None."""
+        r = C.c_int64()
+        check(lib().yg_server_admit(self.h, C.byref(r)), "Server.admit")
+        return None if r.value < 0 else r.value
+
+    def attach(self, rid, A, b, x, method="cg", tol=1e-10, precision=PREC_FP64, maxiter=0):
+        opts = SolveOpts(CRIT_RELRES, precision, tol, maxiter, 0, 0)
+        m = {"cg": METHOD_CG, "bicgstab": METHOD_BICGSTAB}[method]
+        check(lib().yg_server_attach(self.h, int(rid), A.h, b.h, x.h, m, C.byref(opts)), "Server.attach")
+        self._keep[rid] = (A, b, x)
+
+    def launch(self):
+        check(lib().yg_server_launch(self.h), "Server.launch")
+
+    def wait(self):
+        n = C.c_int32()
+        check(lib().yg_server_wait(self.h, C.byref(n)), "Server.wait")
+        return n.value
+
+    def finished(self):
+        ids = (C.c_int64 * 4096)()
+        n = C.c_int32()
+        out = []
+        while True:
+            check(lib().yg_server_finished(self.h, ids, 4096, C.byref(n)), "Server.finished")
+            out.extend(ids[i] for i in range(n.value))
+            if n.value < 4096:
+                return out
+
+    def poll(self, rid):
+        st = SolveStats()
+        check(lib().yg_server_poll(self.h, int(rid), C.byref(st)), "Server.poll")
+        return st
+
+    def solution(self, rid):
+        return self._keep[rid][2]
+
+    def release(self, rid):
+        check(lib().yg_server_release(self.h, int(rid)), "Server.release")
+        self._keep.pop(rid, None)
+
+    def info(self):
+        q, a, b = C.c_int64(), C.c_int64(), C.c_uint64()
+        check(lib().yg_server_info(self.h, C.byref(q), C.byref(a), C.byref(b)), "Server.info")
+        return {"queued": q.value, "active": a.value, "bytes_held": b.value}
+
+    def __del__(self):
+        if getattr(self, "h", None) and _alive(getattr(self, "ctx", None)):
+            lib().yg_server_destroy(self.h)
+        self.h = None

@@ -1182,3 +1182,25 @@ extern "C" yg_status yg_batch_tune(yg_batch bt) {
     YG_CUDA(cudaGetLastError());
     return check_device_error(ctx);
 }
+
+namespace yg {
+// Host view of a slot after the last wait: whether it still iterates, and its
+// stats (from the state copied back at the end of the block).
+bool batch_slot_running(yg_batch bt, int32_t slot) { return sys_live(bt, slot); }
+
+void batch_slot_stats(yg_batch bt, int32_t slot, yg_solve_stats *out) {
+    const BatchScal &sc = bt->h_scal[slot];
+    yg_solve_stats st{};
+    st.iterations = sc.iter;
+    st.rel_residual = sc.bb > 0 ? std::sqrt(sc.true_rr / sc.bb) : std::sqrt(sc.true_rr);
+    st.refinements = (int32_t)sc.replacements;
+    switch (sc.flag) {
+    case BF_DONE: st.status = YG_OK; break;
+    case BF_BREAK: st.status = YG_BREAKDOWN; break;
+    case BF_NANF: st.status = YG_NAN; break;
+    case BF_RUN: case BF_INIT: st.status = YG_RUNNING; break;
+    default: st.status = YG_NOT_CONVERGED; break;
+    }
+    *out = st;
+}
+}  // namespace yg

@@ -132,6 +132,9 @@ yg_status spmv_autotune_device(yg_matrix A);
 yg_status vector_dot(yg_context ctx, const double *a, const double *b, int64_t n, double *out);
 yg_status check_device_error(yg_context ctx);
 yg_status matrix_build_diag(yg_matrix A);
+// batch engine, host side (batch.cu)
+bool batch_slot_running(yg_batch bt, int32_t slot);
+void batch_slot_stats(yg_batch bt, int32_t slot, yg_solve_stats *out);
 yg_status matrix_from_device_pattern(yg_matrix A);
 
 }  // namespace yg

@@ -73,12 +73,14 @@ def clamp_dofs(X, dpn):
     return (nodes[:, None] * dpn + np.arange(dpn)[None, :]).ravel().astype(np.int64)
 
 
-def assemble(spec, ctx):
+def assemble(spec, ctx, mesh=None):
     """Assemble problem `spec` on the device through the public API: DoF
-    numbering, tangent (CSR for Poisson, 2x2/3x3 BCSR for elasticity), the
-    N(0,1) right-hand side and u = 0 on x = 0.  Returns (mesh, K, b, clamp_dofs)."""
+    numbering, tangent (CSR for Poisson and SUPG, 2x2/3x3 BCSR for elasticity),
+    the N(0,1) right-hand side and u = 0 on x = 0.  `mesh` may be given when it
+    was built beforehand.  Returns (mesh, K, b, clamp_dofs)."""
     import yafel_b200 as yb
-    mesh = build_mesh(spec)
+    if mesh is None:
+        mesh = build_mesh(spec)
     dpn, dim = spec["dpn"], spec["dim"]
     dm = yb.DoFManager(mesh, spec["order"], dpn, ctx=ctx)
     fe = yb.FESystem(dm, dim, format=yb.CSR if dpn == 1 else yb.BCSR)
@@ -91,3 +93,28 @@ def assemble(spec, ctx):
         bc.bc_nodes = nodes
         bc.apply(K, b)
     return mesh, K, b, clamp_dofs(dm.dof_nodes, dpn)
+
+
+def est_bytes(spec):
+    """Upper estimate of the solver-resident device bytes of a problem, from its
+    size alone (before it is built): matrix values and columns with at most
+    dpn * (2p+1)^dim entries per row, the right-hand side, the iterate and the
+    Krylov work vectors (4 for PCG, 9 for BiCGSTAB), plus row data."""
+    p, dim, dpn, n = spec["order"], spec["dim"], spec["dpn"], spec["n"]
+    dofs = dpn * (p * n + 1) ** dim
+    nnz_row = dpn * (2 * p + 1) ** dim
+    vecs = (9 if spec["kind"] == "supg" else 4) + 2
+    return int(dofs * (12 * nnz_row + 8 * vecs + 16))
+
+
+def serving_specs(count, base=BASE_SEED + 1_000_000, lo=1e3, hi=1e6):
+    """Requests of the serving workload: sizes log-uniform in [lo, hi] dofs,
+    orders 1-2, 2D/3D Poisson, elasticity and SUPG advection-diffusion."""
+    return [problem_spec(i, base=base, lo=lo, hi=hi, orders=(1, 2), kinds=("poisson", "elasticity", "supg"),
+                         dims=(2, 3)) for i in range(count)]
+
+
+def arrivals(count, rate, seed=BASE_SEED + 2_000_000):
+    """Arrival times (s) of a Poisson process of the given rate (req/s)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    return np.cumsum(rng.exponential(1.0 / rate, count))
