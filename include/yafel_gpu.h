@@ -288,8 +288,13 @@ YG_API yg_status yg_batch_wait(yg_batch B, int32_t *n_active);
 /* Status (YG_OK when converged and verified in FP64, YG_RUNNING while it
  * iterates), iterations and FP64 relative residual of a slot. */
 YG_API yg_status yg_batch_stats(yg_batch B, int32_t slot, yg_solve_stats *stats);
-/* Autotune tiles per work item and lanes per block row for the systems present. */
+/* Autotune, per block size, the SpMV variant (0: tiles staged in shared memory
+ * by bulk asynchronous copies, 1: direct loads), tiles per work item and lanes
+ * per block row, for the systems present. */
 YG_API yg_status yg_batch_tune(yg_batch B);
+/* The tuning in use: out[3*(b-1) + {0,1,2}] = variant, lanes, tiles per item
+ * for block size b = 1, 2, 3. */
+YG_API yg_status yg_batch_get_tuning(yg_batch B, int32_t *out);
 
 /* A continuous-batching solve server on one context.  No reference
  * counterpart.  A request is submitted with an estimate of the device bytes it

@@ -674,6 +674,12 @@ class Batch:
     def tune(self):
         check(lib().yg_batch_tune(self.h), "Batch.tune")
 
+    def tuning(self):
+        """{block size: (variant, lanes, tiles per item)} in use."""
+        a = (C.c_int32 * 9)()
+        check(lib().yg_batch_get_tuning(self.h, a), "Batch.tuning")
+        return {b: (a[3 * (b - 1)], a[3 * (b - 1) + 1], a[3 * (b - 1) + 2]) for b in (1, 2, 3)}
+
     def launch(self):
         """One block of iterations without waiting; pair with wait()."""
         check(lib().yg_batch_launch(self.h), "Batch.launch")

@@ -5,10 +5,13 @@
 // matrix (CSR or BCSR with 2x2 / 3x3 blocks), right-hand side, iterate and work
 // vectors, and is solved either by Jacobi-PCG (symmetric positive definite
 // systems) or by BiCGSTAB with right Jacobi preconditioning (non-symmetric
-// ones).  A system's block rows are cut into tiles of whole rows holding at
-// most TileCfg<B>::BLOCKS blocks, and runs of consecutive tiles form work items,
-// grouped by (method, block size).  Persistent-grid kernels advance every
-// active system by one iteration in five steps:
+// ones).  Two work tables drive persistent-grid kernels over all systems:
+//   matrix items: a system's block rows cut into tiles of whole rows (at most
+//     WCfg<B>::CAP blocks each), runs of consecutive tiles forming an item that
+//     one warp streams through its own shared-memory ring (bulk asynchronous
+//     copies, cp.async.bulk + mbarrier) -- no CTA-wide barrier in the SpMV;
+//   vector items: row chunks of about 4096 entries, one CTA each.
+// Both are grouped by (method, block size).  One iteration is five steps:
 //   V1  BiCGSTAB: p = r + beta (p - omega v), ph = D^-1 p
 //   S1  SpMV: PCG q = A p (partials of p.q -> alpha); BiCGSTAB v = A ph
 //       (partials of r0.v -> alpha)
@@ -17,23 +20,21 @@
 //   S2  BiCGSTAB SpMV t = A sh (partials of t.s, t.t -> omega)
 //   V3  PCG: p = z + beta p; BiCGSTAB: x += alpha ph + omega sh, r = s - omega t,
 //       partials of r0.r, r.r -> beta and the stopping tests
-// (V1 and S2 are launched only when BiCGSTAB systems are present).  Each SpMV
-// CTA streams the tiles of its items through a shared-memory ring filled by
-// bulk asynchronous copies (cp.async.bulk + mbarrier).  Every decision about a
-// system is taken once, by the CTA that completes the system's last item of a
-// kernel (a per-system ticket), so every CTA of the next kernel sees the same
-// state.  Sums run in a fixed order over a fixed item decomposition: a system's
-// result does not depend on which other systems share the batch.  Converged
-// systems drop out of the kernels at once and out of the item table at the next
-// compaction.  A block of m iterations plus a verification pass is captured into
-// one CUDA graph and replayed; the verification pass recomputes b - A x in FP64
-// for systems whose recursive residual converged or broke down (stop), whose
-// mixed-precision residual fell 100x since the last replacement (replace), and
-// for newly added systems (init).  Systems can be added and removed between
-// replays (continuous batching): only the descriptor and item tables change,
-// and kernels read their item ranges from device memory, so the captured graph
-// stays valid while the set of (method, block size) groups present does not
-// change.
+// (V1 and S2 are launched only when BiCGSTAB systems are present).  Every
+// decision about a system is taken once, by the warp or CTA that completes the
+// system's last item of a kernel (a per-system ticket), so every CTA of the
+// next kernel sees the same state.  Sums run in a fixed order over a fixed item
+// decomposition: a system's result does not depend on which other systems
+// share the batch.  Converged systems drop out of the kernels at once and out
+// of the work tables at the next compaction.  A block of m iterations plus a
+// verification pass is captured into one CUDA graph and replayed; the
+// verification pass recomputes b - A x in FP64 for systems whose recursive
+// residual converged or broke down (stop), whose mixed-precision residual fell
+// 100x since the last replacement (replace), and for newly added systems
+// (init).  Systems can be added and removed between replays (continuous
+// batching): only the descriptor and work tables change, and kernels read their
+// ranges from device memory, so the captured graph stays valid while the set of
+// (method, block size) groups present does not change.
 #include "internal.h"
 #include "device_common.cuh"
 
@@ -60,7 +61,8 @@ struct BatchSys {
     double *x, *r, *p, *q;        // q: SpMV output of PCG and of the verification (BiCGSTAB: q is t)
     double *r0, *v, *s, *t, *ph, *sh;  // BiCGSTAB only
     const int32_t *tiles;         // first block row of each tile, ntiles + 1 entries
-    int32_t item_begin, item_end;
+    int32_t mitem_begin, mitem_end;  // matrix items (SpMV)
+    int32_t vitem_begin, vitem_end;  // vector items
     int32_t precision;            // YG_PREC_FP64 or YG_PREC_MIXED
     int32_t ntiles;
     int32_t method, pad;
@@ -78,11 +80,16 @@ struct BatchScal {
     double true_rr;               // r.r of the last FP64 true residual
 };
 
-struct BatchItem {
-    int32_t sys, tile_begin, tile_end, row_begin, row_end, pad;
+struct BatchMItem {
+    int32_t sys, tile_begin, tile_end, pad;
+};
+struct BatchVItem {
+    int32_t sys, row_begin, row_end, pad;  // block rows
 };
 
 constexpr int kGroups = 6;  // (method, block size): group = 3 * method + block - 1
+// d_ranges: [0, 8) first matrix item of each group then the end; [8, 16) the same for vector items
+constexpr int kVR = 8;
 
 struct yg_batch_t {
     yg_context ctx = nullptr;
@@ -94,16 +101,19 @@ struct yg_batch_t {
     std::vector<yg_solve_opts> opts;
     BatchSys *d_sys = nullptr;
     BatchScal *d_scal = nullptr;
-    BatchItem *d_items = nullptr;
-    int32_t *d_ranges = nullptr;        // [8]: first item of each group, then the end
-    double *d_part = nullptr;           // partials: 2 per item
-    double *d_part2 = nullptr;
-    int32_t max_items = 0, n_items = 0;
-    int32_t tiles_per_item[4] = {0, 8, 8, 8};
+    BatchMItem *d_mitems = nullptr;
+    BatchVItem *d_vitems = nullptr;
+    int32_t *d_ranges = nullptr;
+    double *d_mpart = nullptr;          // SpMV partials: 2 per matrix item
+    double *d_vpart = nullptr;          // vector partials: 2 per vector item
+    double *d_vpart2 = nullptr;         // b.b partials of the verification
+    int32_t max_mitems = 0, max_vitems = 0;
+    int32_t tiles_per_item[4] = {0, 4, 4, 4};
     int32_t lanes[4] = {4, 4, 8, 16};
+    int32_t variant[4] = {1, 1, 1, 0};   // SpMV variant per block size: 0 staged, 1 direct
     unsigned groups_present = 0, graph_groups = 0;
-    bool dirty = false;                 // item table out of date (systems added, removed or reset)
-    int32_t live_items = 0;             // items of systems that may still iterate (host view)
+    bool dirty = false;                 // work tables out of date (systems added, removed or reset)
+    int32_t live_items = 0;             // vector items of systems that may still iterate (host view)
     int m = 16;
     cudaGraphExec_t exec = nullptr;
     cudaGraph_t graph = nullptr;
@@ -113,46 +123,52 @@ struct yg_batch_t {
 
 namespace yg {
 
-// ---------------------------------------------------------------- tiles
+// ---------------------------------------------------------------- configuration
 
-// Blocks per tile: the values and block columns of a full FP64 tile fill one
-// shared-memory stage of about 18 KB.
-template <int B> struct TileCfg;
-template <> struct TileCfg<1> { static constexpr int BLOCKS = 1536; };
-template <> struct TileCfg<2> { static constexpr int BLOCKS = 512; };
-template <> struct TileCfg<3> { static constexpr int BLOCKS = 224; };
+// Per block size: blocks (and rows) per tile (CAP), stages of each warp's ring
+// (NST) and warps per CTA.  A stage holds one FP64 tile's values, block columns
+// and row pointers (4-10 KB).
+template <int B> struct WCfg;
+template <> struct WCfg<1> { static constexpr int CAP = 192, NST = 2, WARPS = 8; };
+template <> struct WCfg<2> { static constexpr int CAP = 72, NST = 2, WARPS = 8; };
+template <> struct WCfg<3> { static constexpr int CAP = 128, NST = 2, WARPS = 4; };
 
-static int tile_blocks(int B) { return B == 1 ? TileCfg<1>::BLOCKS : (B == 2 ? TileCfg<2>::BLOCKS : TileCfg<3>::BLOCKS); }
+static int tile_cap(int B) { return B == 1 ? WCfg<1>::CAP : (B == 2 ? WCfg<2>::CAP : WCfg<3>::CAP); }
 
 template <int B>
-struct Stage {
-    static constexpr int NST = 3;
-    static constexpr int VBYTES = TileCfg<B>::BLOCKS * B * B * 8 + 32;  // FP64 values + alignment slack
-    static constexpr int CBYTES = TileCfg<B>::BLOCKS * 4 + 32;
-    static constexpr int BYTES = VBYTES + CBYTES;
-    static constexpr int SMEM = NST * BYTES + NST * 8;  // stages + mbarriers
+struct WStage {
+    static constexpr int VB = WCfg<B>::CAP * B * B * 8 + 32;  // FP64 values + alignment slack
+    static constexpr int CB = WCfg<B>::CAP * 4 + 32;
+    static constexpr int RB = WCfg<B>::CAP * 4 + 48;  // row pointers of the tile's rows + 1
+    static constexpr int HB = 32;                      // tile header (TileHdr)
+    static constexpr int BYTES = VB + CB + RB + HB;
+    static constexpr int WARP_BYTES = WCfg<B>::NST * BYTES;
+    static constexpr int SMEM = WCfg<B>::WARPS * (WARP_BYTES + WCfg<B>::NST * 8);
 };
+
+// block rows per vector item: about 4096 entries
+static int vitem_rows(int B) { return 4096 / B; }
 
 // SpMV kinds
 enum { SP_CG = 0, SP_VERIFY = 1, SP_BICG_V = 2, SP_BICG_T = 3 };
 
-// ---------------------------------------------------------------- kernels
+// ---------------------------------------------------------------- device helpers
+
+enum { ACT_ITER = 0, ACT_VERIFY = 1, ACT_RESTART = 2 };
+__device__ __forceinline__ int activity(const BatchScal *sc, int kind) {
+    const volatile BatchScal *v = sc;
+    const int flag = v->flag, stop = v->stop, rep = v->replace, rst = v->restart;
+    if (kind == ACT_ITER) return flag == BF_RUN && stop == BS_NONE;
+    if (kind == ACT_VERIFY) return (flag == BF_INIT) || (flag == BF_RUN && (stop == BS_CONV || rep));
+    return rst != 0;
+}
 
 // Whether system state `sc` takes part in a kernel of the given kind, decided
 // once per CTA: thread 0 reads the state and broadcasts it, so every thread of
 // the CTA takes the same branch around the block reductions.
-enum { ACT_ITER = 0, ACT_VERIFY = 1, ACT_RESTART = 2 };
 __device__ __forceinline__ bool cta_active(const BatchScal *sc, int kind, int *flag_sm) {
     __syncthreads();
-    if (threadIdx.x == 0) {
-        const volatile BatchScal *v = sc;
-        const int flag = v->flag, stop = v->stop, rep = v->replace, rst = v->restart;
-        int a;
-        if (kind == ACT_ITER) a = (flag == BF_RUN && stop == BS_NONE);
-        else if (kind == ACT_VERIFY) a = (flag == BF_INIT) || (flag == BF_RUN && (stop == BS_CONV || rep));
-        else a = rst != 0;
-        *flag_sm = a;
-    }
+    if (threadIdx.x == 0) *flag_sm = activity(sc, kind);
     __syncthreads();
     return *flag_sm != 0;
 }
@@ -175,30 +191,57 @@ __device__ __forceinline__ bool last_of_system(BatchScal *sc, int n_items, int *
     return *flag_sm != 0;
 }
 
-// Fixed-order sum of partials [ib, ie) (stride 2, offset off), result in every thread.
+// The same for one warp (lane 0 publishes, the verdict is broadcast).
+__device__ __forceinline__ bool warp_last_of_system(BatchScal *sc, int n_items, int lane) {
+    int last = 0;
+    if (lane == 0) {
+        __threadfence();
+        const int old = atomicAdd(&sc->ticket, 1);
+        last = (old == n_items - 1);
+        if (last) {
+            sc->ticket = 0;
+            __threadfence();
+        }
+    }
+    return __shfl_sync(0xffffffffu, last, 0) != 0;
+}
+
+// Fixed-order sums of partials [ib, ie) (stride 2, offset off): by a CTA (result
+// in every thread) or by a warp (xor butterfly; result in every lane).
 __device__ __forceinline__ double sum_items(const double *part, int ib, int ie, int off, double *sm) {
     double v = 0;
     for (int i = ib + threadIdx.x; i < ie; i += blockDim.x) v += __ldcg(part + 2 * (int64_t)i + off);
     return block_sum_all<kThreads>(v, sm);
 }
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ double warp_sum_items(const double *part, int ib, int ie, int off, int lane) {
+    double v = 0;
+    for (int i = ib + lane; i < ie; i += 32) v += __ldcg(part + 2 * (int64_t)i + off);
+    return warp_sum(v);
+}
 
-// Rows [r0, r1) of one tile: L lanes per block row; vals / cols point at the
-// tile's first block (shared memory, or global memory for an oversized tile).
-// out = A xin on those rows; dot1 += out.w (iteration kinds), dot2 += out.out (SP_BICG_T).
+// Rows [r0, r1) of one tile, by one warp with L lanes per block row; vals / cols
+// point at the tile's first block and rowptr at row r0's pointer (shared
+// memory, or global memory for an oversized tile).  out = A xin on those rows; dot1 += out.w (iteration kinds),
+// dot2 += out.out (SP_BICG_T); the sums stay in the lanes that wrote the rows.
 template <int B, int L, int KIND, typename VT>
-__device__ __forceinline__ void tile_rows(const int32_t *__restrict__ rowptr, int r0, int r1, int b0, const VT *vals,
+__device__ __forceinline__ void tile_rows(const int32_t *rowptr, int r0, int r1, int b0, const VT *vals,
                                           const int32_t *cols, const double *__restrict__ xin, double *__restrict__ out,
-                                          const double *__restrict__ w, double &dot1, double &dot2) {
+                                          const double *__restrict__ w, double &dot1, double &dot2, int lane) {
     constexpr int B2 = B * B;
-    constexpr int G = kThreads / L;
-    const int lane = threadIdx.x & 31, glane = lane % L, grp = threadIdx.x / L;
+    constexpr int G = 32 / L;
+    const int glane = lane % L, grp = lane / L;
     for (int rb = r0; rb < r1; rb += G) {
         const int r = rb + grp;
         double acc[B];
 #pragma unroll
         for (int i = 0; i < B; ++i) acc[i] = 0;
         if (r < r1) {
-            const int rs = rowptr[r] - b0, re = rowptr[r + 1] - b0;
+            const int rs = rowptr[r - r0] - b0, re = rowptr[r - r0 + 1] - b0;
             int j = rs + glane;
             for (; j + L < re; j += 2 * L) {
                 const int c0 = cols[j], c1 = cols[j + L];
@@ -240,174 +283,422 @@ __device__ __forceinline__ void tile_rows(const int32_t *__restrict__ rowptr, in
     }
 }
 
-// CTA-wide bounded wait on a stage: thread 0 polls, the verdict is broadcast;
-// the other threads then observe the completed phase themselves (acquire).
-__device__ __forceinline__ bool stage_wait(uint64_t *bar, unsigned parity, int *flag_sm) {
-    if (threadIdx.x == 0) {
-        long long spins = 0;
-        int ok = 1;
-        while (!mbar_try_wait(bar, parity))
-            if (++spins > kSpinLimit) { ok = 0; break; }
-        *flag_sm = ok;
-    }
-    __syncthreads();
-    const bool ok = *flag_sm != 0;
-    if (ok && threadIdx.x != 0) mbar_try_wait(bar, parity);
-    return ok;
-}
+// Header of a staged tile, written by the issuing lane.
+struct TileHdr {
+    int32_t item, r0, r1, b0, nb, last, pad0, pad1;
+};
 
-// Thread 0 issues the bulk copies of tile t (values, then block columns) into
-// stage seq % NST; an empty or oversized tile completes its phase with no
-// transfer and is read from global memory instead.
+// Lane 0 issues the bulk copies of tile t of a system (values, block columns,
+// row pointers) into stage seq % NST of this warp's ring and writes the tile's
+// header; an empty or oversized tile completes its phase with no transfer and
+// is read from global memory instead.  t < 0 stands for an item without tiles.
 template <int B>
-__device__ __forceinline__ void issue_tile(unsigned char *smem_raw, uint64_t *bars, uint32_t seq,
+__device__ __forceinline__ void issue_tile(unsigned char *ring, uint64_t *bars, uint32_t seq, int item, int last,
                                            const int32_t *__restrict__ rowptr, const int32_t *__restrict__ tiles, int t,
-                                           const char *vbase, int vsz, const int32_t *col, uint64_t pol) {
-    using S = Stage<B>;
+                                           const char *vbase, int vsz, const int32_t *col, uint64_t pol, int lane) {
+    using S = WStage<B>;
     constexpr int B2 = B * B;
-    if (threadIdx.x != 0) return;
-    const int st = seq % S::NST;
-    const int b0 = rowptr[tiles[t]], b1 = rowptr[tiles[t + 1]];
-    const int nb = b1 - b0;
-    if (nb > 0 && nb <= TileCfg<B>::BLOCKS) {
+    if (lane != 0) return;
+    const int st = seq % WCfg<B>::NST;
+    unsigned char *dst = ring + (size_t)st * S::BYTES;
+    TileHdr *h = reinterpret_cast<TileHdr *>(dst + S::VB + S::CB + S::RB);
+    int r0 = 0, r1 = 0, b0 = 0, nb = 0;
+    if (t >= 0) {
+        r0 = tiles[t];
+        r1 = tiles[t + 1];
+        b0 = rowptr[r0];
+        nb = rowptr[r1] - b0;
+    }
+    h->item = item;
+    h->r0 = r0;
+    h->r1 = r1;
+    h->b0 = b0;
+    h->nb = nb;
+    h->last = last;
+    if (nb > 0 && nb <= WCfg<B>::CAP) {
         const int64_t vs = (int64_t)b0 * B2 * vsz, va = vs & ~(int64_t)15;
         const int64_t ve = (vs + (int64_t)nb * B2 * vsz + 15) & ~(int64_t)15;
         const int64_t cs = (int64_t)b0 * 4, ca = cs & ~(int64_t)15, ce = (cs + (int64_t)nb * 4 + 15) & ~(int64_t)15;
-        unsigned char *dst = smem_raw + (size_t)st * S::BYTES;
-        mbar_expect_tx(&bars[st], (unsigned)((ve - va) + (ce - ca)));
+        const int64_t ps = (int64_t)r0 * 4, pa = ps & ~(int64_t)15, pe = ((int64_t)r1 * 4 + 4 + 15) & ~(int64_t)15;
+        mbar_expect_tx(&bars[st], (unsigned)((ve - va) + (ce - ca) + (pe - pa)));
         bulk_g2s(dst, vbase + va, (unsigned)(ve - va), &bars[st], pol);
-        bulk_g2s(dst + S::VBYTES, reinterpret_cast<const char *>(col) + ca, (unsigned)(ce - ca), &bars[st], pol);
+        bulk_g2s(dst + S::VB, reinterpret_cast<const char *>(col) + ca, (unsigned)(ce - ca), &bars[st], pol);
+        bulk_g2s(dst + S::VB + S::CB, reinterpret_cast<const char *>(rowptr) + pa, (unsigned)(pe - pa), &bars[st], pol);
     } else {
         mbar_expect_tx(&bars[st], 0);
     }
 }
 
-// The SpMV of one group of items (ranges[g], ranges[g + 1]):
-//   SP_CG      q = A p, partials of p.q; last CTA: alpha = r.z / p.q
-//   SP_VERIFY  q = A x with FP64 values (systems under verification)
-//   SP_BICG_V  v = A ph, partials of r0.v; last CTA: alpha = rho / r0.v
-//   SP_BICG_T  t = A sh, partials of t.s and t.t; last CTA: omega = t.s / t.t
-// The iteration kinds read FP32 values for mixed-precision systems.  With
-// commit == 0 (autotuning) the reductions are not taken.
-template <int B, int L, int KIND>
-__global__ void __launch_bounds__(kThreads)
-k_batch_spmv(const BatchItem *__restrict__ items, const int32_t *__restrict__ ranges, int g,
-             const BatchSys *__restrict__ sys, BatchScal *__restrict__ scal, double *__restrict__ part, int parity,
-             int commit, int32_t *__restrict__ err) {
-    using S = Stage<B>;
+// Loads of one block's values (streamed: L1 no-allocate, L2 evict-first) and of
+// the B entries of x it multiplies, with vector loads where the layout allows.
+__device__ __forceinline__ double2 ld_stream2(const double *p, uint64_t pol) {
+    double2 v;
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;"
+        : "=d"(v.x), "=d"(v.y) : "l"(p), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ float ld_stream_f(const float *p, uint64_t pol) {
+    float v;
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ float4 ld_stream_f4(const float *p, uint64_t pol) {
+    float4 v;
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
+        : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "l"(p), "l"(pol));
+    return v;
+}
+template <int B2>
+__device__ __forceinline__ void load_block(const double *p, double *v, uint64_t pol) {
+    if (B2 == 4) {  // 32-byte blocks: 16-byte aligned
+        const double2 a = ld_stream2(p, pol), b = ld_stream2(p + 2, pol);
+        v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+    } else {
+#pragma unroll
+        for (int k = 0; k < B2; ++k) v[k] = ld_stream(p + k, pol);
+    }
+}
+template <int B2>
+__device__ __forceinline__ void load_block(const float *p, double *v, uint64_t pol) {
+    if (B2 == 4) {  // 16-byte blocks: 16-byte aligned
+        const float4 a = ld_stream_f4(p, pol);
+        v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+    } else {
+#pragma unroll
+        for (int k = 0; k < B2; ++k) v[k] = ld_stream_f(p + k, pol);
+    }
+}
+template <int B>
+__device__ __forceinline__ void load_x(const double *p, double *x) {
+    if (B == 2) {  // 16-byte aligned pairs
+        const double2 a = __ldg(reinterpret_cast<const double2 *>(p));
+        x[0] = a.x; x[1] = a.y;
+    } else {
+#pragma unroll
+        for (int k = 0; k < B; ++k) x[k] = __ldg(p + k);
+    }
+}
+
+// Warp-wide bounded wait on a stage: lane 0 polls, the verdict is broadcast; the
+// other lanes then observe the completed phase themselves (acquire).
+__device__ __forceinline__ bool warp_stage_wait(uint64_t *bar, unsigned parity, int lane) {
+    int ok = 1;
+    if (lane == 0) {
+        long long spins = 0;
+        while (!mbar_try_wait(bar, parity))
+            if (++spins > kSpinLimit) { ok = 0; break; }
+    }
+    ok = __shfl_sync(0xffffffffu, ok, 0);
+    if (ok && lane != 0) mbar_try_wait(bar, parity);
+    return ok != 0;
+}
+
+// ---------------------------------------------------------------- kernels
+
+// End of a matrix item in a warp: publish its partials; the warp that
+// completes the system's last item takes the reduction and the decision.
+template <int KIND>
+__device__ __forceinline__ void finish_item(const BatchSys *__restrict__ sys, BatchScal *__restrict__ scal,
+                                            double *__restrict__ part, int it, int s, int parity, double dot1,
+                                            double dot2, int lane) {
+    dot1 = warp_sum(dot1);
+    if (KIND == SP_BICG_T) dot2 = warp_sum(dot2);
+    if (lane == 0) {
+        part[2 * (int64_t)it] = dot1;
+        if (KIND == SP_BICG_T) part[2 * (int64_t)it + 1] = dot2;
+    }
+    const int ib = sys[s].mitem_begin, ie = sys[s].mitem_end;
+    if (!warp_last_of_system(&scal[s], ie - ib, lane)) return;
+    const double a = warp_sum_items(part, ib, ie, 0, lane);
+    const double tt = KIND == SP_BICG_T ? warp_sum_items(part, ib, ie, 1, lane) : 0.0;
+    if (lane != 0) return;
+    BatchScal &sc = scal[s];
+    if (KIND == SP_CG) {
+        const double alpha = sc.rz[parity] / a;
+        if (a == 0 || !isfinite(alpha)) sc.stop = isfinite(a) ? BS_BREAK : BS_NAN;
+        else sc.alpha = alpha;
+    } else if (KIND == SP_BICG_V) {
+        const double alpha = sc.rho / a;
+        sc.fresh = 0;
+        if (a == 0 || !isfinite(alpha)) sc.stop = isfinite(a) ? BS_CONV : BS_NAN;  // restart via verify
+        else sc.alpha = alpha;
+    } else {
+        sc.omega = tt > 0 ? a / tt : 0.0;
+    }
+}
+
+// Direct-load SpMV of one group (no staging): each warp takes whole items; L
+// lanes per block row, each lane loading up to four whole blocks (values with
+// vector loads and an L2 evict-first hint, columns, gathered x) before using
+// them.  Same operations and reductions as k_batch_spmv.
+template <int B, int L, int KIND, typename VT>
+__device__ __forceinline__ void direct_rows(const int32_t *__restrict__ rowptr, int r0, int r1,
+                                            const VT *__restrict__ val, const int32_t *__restrict__ col,
+                                            const double *__restrict__ xin, double *__restrict__ out,
+                                            const double *__restrict__ w, double &dot1, double &dot2, int lane,
+                                            uint64_t pol) {
     constexpr int B2 = B * B;
-    constexpr int CAP = TileCfg<B>::BLOCKS;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ double sm[kThreads / 32 + 1];
-    __shared__ int flag_sm;
-    uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw + (size_t)S::NST * S::BYTES);
-    if (threadIdx.x == 0)
-        for (int k = 0; k < S::NST; ++k) mbar_init(&bars[k], 1);
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    __syncthreads();
-    const uint64_t pol = evict_first_policy();
-    uint32_t seq_issue = 0, seq_wait = 0;  // tiles issued / consumed by this CTA
-    bool timed_out = false;
-    const int g0 = ranges[g], g1 = ranges[g + 1];
-    for (int it = g0 + blockIdx.x; it < g1 && !timed_out; it += gridDim.x) {
-        const BatchItem item = items[it];
-        const int s = item.sys;
-        if (!cta_active(&scal[s], KIND == SP_VERIFY ? ACT_VERIFY : ACT_ITER, &flag_sm)) continue;
-        const BatchSys d = sys[s];
-        const bool f32 = (KIND != SP_VERIFY && d.precision == YG_PREC_MIXED);
-        const int vsz = f32 ? 4 : 8;
-        const char *vbase = f32 ? reinterpret_cast<const char *>(d.val32) : reinterpret_cast<const char *>(d.val);
-        const double *xin = KIND == SP_CG ? d.p : KIND == SP_VERIFY ? d.x : KIND == SP_BICG_V ? d.ph : d.sh;
-        double *out = (KIND == SP_CG || KIND == SP_VERIFY) ? d.q : KIND == SP_BICG_V ? d.v : d.t;
-        const double *w = KIND == SP_CG ? d.p : KIND == SP_BICG_V ? d.r0 : d.s;
-        int t_issue = item.tile_begin;
-        while (t_issue < item.tile_end && seq_issue - seq_wait < (uint32_t)(S::NST - 1))
-            issue_tile<B>(smem_raw, bars, seq_issue++, d.rowptr, d.tiles, t_issue++, vbase, vsz, d.col, pol);
-        double dot1 = 0, dot2 = 0;
-        for (int t = item.tile_begin; t < item.tile_end; ++t) {
-            if (t_issue < item.tile_end && seq_issue - seq_wait < (uint32_t)S::NST)
-                issue_tile<B>(smem_raw, bars, seq_issue++, d.rowptr, d.tiles, t_issue++, vbase, vsz, d.col, pol);
-            const int st = seq_wait % S::NST;
-            if (!stage_wait(&bars[st], (seq_wait / S::NST) & 1u, &flag_sm)) {
-                timed_out = true;
-                break;
-            }
-            const int r0 = d.tiles[t], r1 = d.tiles[t + 1];
-            const int b0 = d.rowptr[r0], nb = d.rowptr[r1] - b0;
-            const unsigned char *stg = smem_raw + (size_t)st * S::BYTES;
-            const int lv = (int)(((int64_t)b0 * B2 * vsz) & 15), lc = (int)(((int64_t)b0 * 4) & 15);
-            const int32_t *cols = nb <= CAP ? reinterpret_cast<const int32_t *>(stg + S::VBYTES + lc) : d.col + b0;
-            if (f32) {
-                const float *v = nb <= CAP ? reinterpret_cast<const float *>(stg + lv) : d.val32 + (int64_t)b0 * B2;
-                tile_rows<B, L, KIND, float>(d.rowptr, r0, r1, b0, v, cols, xin, out, w, dot1, dot2);
-            } else {
-                const double *v = nb <= CAP ? reinterpret_cast<const double *>(stg + lv) : d.val + (int64_t)b0 * B2;
-                tile_rows<B, L, KIND, double>(d.rowptr, r0, r1, b0, v, cols, xin, out, w, dot1, dot2);
-            }
-            ++seq_wait;
-            __syncthreads();  // the stage is free for the next issue
-        }
-        if (timed_out) break;
-        if (KIND != SP_VERIFY && commit) {
-            dot1 = block_sum<kThreads>(dot1, sm);
-            if (KIND == SP_BICG_T) dot2 = block_sum<kThreads>(dot2, sm);
-            if (threadIdx.x == 0) {
-                part[2 * (int64_t)it] = dot1;
-                if (KIND == SP_BICG_T) part[2 * (int64_t)it + 1] = dot2;
-            }
-            if (last_of_system(&scal[s], d.item_end - d.item_begin, &flag_sm)) {
-                const double a = sum_items(part, d.item_begin, d.item_end, 0, sm);
-                const double tt = KIND == SP_BICG_T ? sum_items(part, d.item_begin, d.item_end, 1, sm) : 0.0;
-                if (threadIdx.x == 0) {
-                    BatchScal &sc = scal[s];
-                    if (KIND == SP_CG) {
-                        const double alpha = sc.rz[parity] / a;
-                        if (a == 0 || !isfinite(alpha)) sc.stop = isfinite(a) ? BS_BREAK : BS_NAN;
-                        else sc.alpha = alpha;
-                    } else if (KIND == SP_BICG_V) {
-                        const double alpha = sc.rho / a;
-                        sc.fresh = 0;
-                        if (a == 0 || !isfinite(alpha)) sc.stop = isfinite(a) ? BS_CONV : BS_NAN;  // restart via verify
-                        else sc.alpha = alpha;
-                    } else {
-                        sc.omega = tt > 0 ? a / tt : 0.0;
+    constexpr int G = 32 / L;
+    constexpr int U = 4;
+    const int glane = lane % L, grp = lane / L;
+    for (int rb = r0; rb < r1; rb += G) {
+        const int r = rb + grp;
+        double acc[B];
+#pragma unroll
+        for (int i = 0; i < B; ++i) acc[i] = 0;
+        if (r < r1) {
+            const int rs = rowptr[r], re = rowptr[r + 1];
+            for (int j0 = rs + glane; j0 < re; j0 += U * L) {
+                int c[U];
+                double v[U][B2], x[U][B];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int j = j0 + u * L;
+                    c[u] = j < re ? __ldg(col + j) : -1;
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int j = j0 + u * L;
+                    if (c[u] >= 0) {
+                        load_block<B2>(val + (int64_t)j * B2, v[u], pol);
+                        load_x<B>(xin + (int64_t)B * c[u], x[u]);
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    if (c[u] >= 0) {
+#pragma unroll
+                        for (int i = 0; i < B; ++i)
+#pragma unroll
+                            for (int k = 0; k < B; ++k) acc[i] = fma(v[u][i * B + k], x[u][k], acc[i]);
                     }
                 }
             }
         }
+#pragma unroll
+        for (int i = 0; i < B; ++i)
+#pragma unroll
+            for (int o = L / 2; o > 0; o >>= 1) acc[i] += __shfl_xor_sync(0xffffffffu, acc[i], o);
+        if (r < r1 && glane == 0) {
+#pragma unroll
+            for (int i = 0; i < B; ++i) {
+                out[(int64_t)B * r + i] = acc[i];
+                if (KIND != SP_VERIFY) dot1 = fma(acc[i], w[(int64_t)B * r + i], dot1);
+                if (KIND == SP_BICG_T) dot2 = fma(acc[i], acc[i], dot2);
+            }
+        }
     }
-    if (timed_out && threadIdx.x == 0 && err) atomicExch(err, (int32_t)YG_TIMEOUT);
-    // drain the copies still in flight before the CTA exits (bounded)
-    if (threadIdx.x == 0) {
+}
+
+template <int B, int L, int KIND>
+__global__ void __launch_bounds__(256)
+k_batch_spmv_direct(const BatchMItem *__restrict__ items, const int32_t *__restrict__ ranges, int g,
+                    const BatchSys *__restrict__ sys, BatchScal *__restrict__ scal, double *__restrict__ part,
+                    int parity, int commit) {
+    const int lane = threadIdx.x & 31;
+    const int W = gridDim.x * (blockDim.x >> 5);
+    const int g1 = ranges[g + 1];
+    const uint64_t pol = evict_first_policy();
+    for (int it = ranges[g] + blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); it < g1; it += W) {
+        const BatchMItem item = items[it];
+        const int s = item.sys;
+        int act = lane == 0 ? activity(&scal[s], KIND == SP_VERIFY ? ACT_VERIFY : ACT_ITER) : 0;
+        if (!__shfl_sync(0xffffffffu, act, 0)) continue;
+        const BatchSys &d = sys[s];
+        const double *xin = KIND == SP_CG ? d.p : KIND == SP_VERIFY ? d.x : KIND == SP_BICG_V ? d.ph : d.sh;
+        double *out = (KIND == SP_CG || KIND == SP_VERIFY) ? d.q : KIND == SP_BICG_V ? d.v : d.t;
+        const double *w = KIND == SP_CG ? d.p : KIND == SP_BICG_V ? d.r0 : d.s;
+        const int r0 = item.tile_begin < item.tile_end ? d.tiles[item.tile_begin] : 0;
+        const int r1 = item.tile_begin < item.tile_end ? d.tiles[item.tile_end] : 0;
+        double dot1 = 0, dot2 = 0;
+        if (KIND != SP_VERIFY && d.precision == YG_PREC_MIXED)
+            direct_rows<B, L, KIND, float>(d.rowptr, r0, r1, d.val32, d.col, xin, out, w, dot1, dot2, lane, pol);
+        else
+            direct_rows<B, L, KIND, double>(d.rowptr, r0, r1, d.val, d.col, xin, out, w, dot1, dot2, lane, pol);
+        if (KIND != SP_VERIFY && commit) finish_item<KIND>(sys, scal, part, it, s, parity, dot1, dot2, lane);
+    }
+}
+
+// The SpMV of one group of matrix items (ranges[g], ranges[g + 1]); each warp
+// takes whole items (g0 + warp id, then every W-th) and streams their tiles
+// through its ring, the issuing lane running up to NST tiles ahead, across item
+// boundaries:
+//   SP_CG      q = A p, partials of p.q; last warp: alpha = r.z / p.q
+//   SP_VERIFY  q = A x with FP64 values (systems under verification)
+//   SP_BICG_V  v = A ph, partials of r0.v; last warp: alpha = rho / r0.v
+//   SP_BICG_T  t = A sh, partials of t.s and t.t; last warp: omega = t.s / t.t
+// The iteration kinds read FP32 values for mixed-precision systems.  With
+// commit == 0 (autotuning) the reductions are not taken.  A system's state
+// cannot change while one of its items is still to be processed (its reductions
+// wait for all of them), so the activity test of an item read ahead holds.
+template <int B, int L, int KIND>
+__global__ void __launch_bounds__(WCfg<B>::WARPS * 32)
+k_batch_spmv(const BatchMItem *__restrict__ items, const int32_t *__restrict__ ranges, int g,
+             const BatchSys *__restrict__ sys, BatchScal *__restrict__ scal, double *__restrict__ part, int parity,
+             int commit, int32_t *__restrict__ err) {
+    using S = WStage<B>;
+    constexpr int B2 = B * B;
+    constexpr int CAP = WCfg<B>::CAP, NST = WCfg<B>::NST, WARPS = WCfg<B>::WARPS;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    unsigned char *ring = smem_raw + (size_t)wib * S::WARP_BYTES;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw + (size_t)WARPS * S::WARP_BYTES) + wib * NST;
+    if (lane == 0)
+        for (int k = 0; k < NST; ++k) mbar_init(&bars[k], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    __syncwarp();
+    const uint64_t pol = evict_first_policy();
+    const int g1 = ranges[g + 1];
+    const int W = gridDim.x * WARPS;
+    const int act_kind = KIND == SP_VERIFY ? ACT_VERIFY : ACT_ITER;
+
+    // issue cursor (uniform in the warp): item ii, its next tile ti < te
+    int ii = ranges[g] + blockIdx.x * WARPS + wib - W;
+    int ti = 0, te = 0;
+    const int32_t *i_rowptr = nullptr, *i_tiles = nullptr, *i_col = nullptr;
+    const char *i_vbase = nullptr;
+    int i_vsz = 8;
+    bool issue_done = false;
+    auto next_item = [&]() {  // advance the issue cursor to the next active item
+        for (;;) {
+            ii += W;
+            if (ii >= g1) {
+                issue_done = true;
+                return;
+            }
+            const BatchMItem item = items[ii];
+            int act = lane == 0 ? activity(&scal[item.sys], act_kind) : 0;
+            if (!__shfl_sync(0xffffffffu, act, 0)) continue;
+            const BatchSys &d = sys[item.sys];
+            const bool f32 = (KIND != SP_VERIFY && d.precision == YG_PREC_MIXED);
+            i_rowptr = d.rowptr;
+            i_tiles = d.tiles;
+            i_col = d.col;
+            i_vsz = f32 ? 4 : 8;
+            i_vbase = f32 ? reinterpret_cast<const char *>(d.val32) : reinterpret_cast<const char *>(d.val);
+            ti = item.tile_begin;
+            te = item.tile_end;
+            return;
+        }
+    };
+    uint32_t seq_issue = 0, seq_wait = 0;  // tiles issued / consumed by this warp
+    auto issue_next = [&]() {
+        if (ti >= te) {  // an item without tiles: one empty tile closes it
+            issue_tile<B>(ring, bars, seq_issue++, ii, 1, i_rowptr, i_tiles, -1, i_vbase, i_vsz, i_col, pol, lane);
+            next_item();
+            return;
+        }
+        const int last = ti + 1 == te;
+        issue_tile<B>(ring, bars, seq_issue++, ii, last, i_rowptr, i_tiles, ti, i_vbase, i_vsz, i_col, pol, lane);
+        if (++ti == te) next_item();
+    };
+    next_item();
+
+    // consume cursor: the item of the last consumed tile and its operands
+    int ci = -1, cs = 0;
+    const double *xin = nullptr, *w = nullptr;
+    double *out = nullptr;
+    const int32_t *c_rowptr = nullptr, *c_col = nullptr;
+    const double *c_val = nullptr;
+    const float *c_val32 = nullptr;
+    bool c_f32 = false;
+    double dot1 = 0, dot2 = 0;
+    bool timed_out = false;
+    for (;;) {
+        while (!issue_done && seq_issue - seq_wait < (uint32_t)NST) issue_next();
+        if (seq_wait == seq_issue) break;
+        const int st = seq_wait % NST;
+        if (!warp_stage_wait(&bars[st], (seq_wait / NST) & 1u, lane)) {
+            timed_out = true;
+            break;
+        }
+        const unsigned char *stg = ring + (size_t)st * S::BYTES;
+        const TileHdr h = *reinterpret_cast<const TileHdr *>(stg + S::VB + S::CB + S::RB);
+        if (h.item != ci) {
+            ci = h.item;
+            cs = items[ci].sys;
+            const BatchSys &d = sys[cs];
+            c_f32 = (KIND != SP_VERIFY && d.precision == YG_PREC_MIXED);
+            c_rowptr = d.rowptr;
+            c_col = d.col;
+            c_val = d.val;
+            c_val32 = d.val32;
+            xin = KIND == SP_CG ? d.p : KIND == SP_VERIFY ? d.x : KIND == SP_BICG_V ? d.ph : d.sh;
+            out = (KIND == SP_CG || KIND == SP_VERIFY) ? d.q : KIND == SP_BICG_V ? d.v : d.t;
+            w = KIND == SP_CG ? d.p : KIND == SP_BICG_V ? d.r0 : d.s;
+        }
+        if (h.r1 > h.r0) {
+            const int vsz = c_f32 ? 4 : 8;
+            const int lv = (int)(((int64_t)h.b0 * B2 * vsz) & 15), lc = (int)(((int64_t)h.b0 * 4) & 15);
+            const bool staged = h.nb > 0 && h.nb <= CAP;
+            const int32_t *cols = staged ? reinterpret_cast<const int32_t *>(stg + S::VB + lc) : c_col + h.b0;
+            const int32_t *rows = staged ? reinterpret_cast<const int32_t *>(stg + S::VB + S::CB + ((h.r0 * 4) & 15))
+                                         : c_rowptr + h.r0;
+            if (c_f32) {
+                const float *v = staged ? reinterpret_cast<const float *>(stg + lv) : c_val32 + (int64_t)h.b0 * B2;
+                tile_rows<B, L, KIND, float>(rows, h.r0, h.r1, h.b0, v, cols, xin, out, w, dot1, dot2, lane);
+            } else {
+                const double *v = staged ? reinterpret_cast<const double *>(stg + lv) : c_val + (int64_t)h.b0 * B2;
+                tile_rows<B, L, KIND, double>(rows, h.r0, h.r1, h.b0, v, cols, xin, out, w, dot1, dot2, lane);
+            }
+        }
+        ++seq_wait;
+        __syncwarp();  // the stage is free for the next issue
+        if (h.last) {
+            if (KIND != SP_VERIFY && commit) finish_item<KIND>(sys, scal, part, ci, cs, parity, dot1, dot2, lane);
+            dot1 = dot2 = 0;
+        }
+    }
+    if (timed_out && lane == 0 && err) atomicExch(err, (int32_t)YG_TIMEOUT);
+    // drain the copies still in flight before the warp exits (bounded)
+    if (lane == 0) {
         while (seq_wait != seq_issue) {
-            const int st = seq_wait % S::NST;
+            const int st = seq_wait % NST;
             long long spins = 0;
-            while (!mbar_try_wait(&bars[st], (seq_wait / S::NST) & 1u) && ++spins <= kSpinLimit) {
+            while (!mbar_try_wait(&bars[st], (seq_wait / NST) & 1u) && ++spins <= kSpinLimit) {
             }
             ++seq_wait;
         }
     }
-    __syncthreads();
+    __syncwarp();
 }
 
-// V1 (BiCGSTAB items only): p = r + beta (p - omega v) (p = r after a restart), ph = D^-1 p
+// Vector kernels take kU elements per thread per step, loads first, so each
+// thread keeps kU independent loads of every operand in flight.
+constexpr int kU = 4;
+
+// V1 (BiCGSTAB vector items only): p = r + beta (p - omega v) (p = r after a restart), ph = D^-1 p
 __global__ void __launch_bounds__(kThreads)
-k_batch_v1(const BatchItem *__restrict__ items, const int32_t *__restrict__ ranges, const BatchSys *__restrict__ sys,
+k_batch_v1(const BatchVItem *__restrict__ items, const int32_t *__restrict__ ranges, const BatchSys *__restrict__ sys,
            const BatchScal *__restrict__ scal) {
     __shared__ int flag_sm;
-    const int i0 = ranges[3], i1 = ranges[kGroups];
+    const int i0 = ranges[kVR + 3], i1 = ranges[kVR + kGroups];
     for (int it = i0 + blockIdx.x; it < i1; it += gridDim.x) {
-        const BatchItem item = items[it];
+        const BatchVItem item = items[it];
         const int s = item.sys;
         if (!cta_active(&scal[s], ACT_ITER, &flag_sm)) continue;
         const BatchSys d = sys[s];
         const bool fresh = __ldcg(&scal[s].fresh) != 0;
         const double beta = __ldcg(&scal[s].beta), omega = __ldcg(&scal[s].omega);
         const int64_t lo = (int64_t)item.row_begin * d.block, hi = (int64_t)item.row_end * d.block;
-        for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
-            const double pi = fresh ? d.r[i] : d.r[i] + beta * (d.p[i] - omega * d.v[i]);
-            d.p[i] = pi;
-            d.ph[i] = d.dinv[i] * pi;
+        double *__restrict__ p = d.p, *__restrict__ ph = d.ph;
+        const double *__restrict__ r = d.r, *__restrict__ v = d.v, *__restrict__ dinv = d.dinv;
+        for (int64_t i0 = lo + threadIdx.x; i0 < hi; i0 += kU * kThreads) {
+            double pv[kU], rv[kU], vv[kU], dv[kU];
+#pragma unroll
+            for (int k = 0; k < kU; ++k) {
+                const int64_t i = i0 + k * kThreads;
+                if (i < hi) { rv[k] = r[i]; dv[k] = dinv[i]; pv[k] = fresh ? 0.0 : p[i]; vv[k] = fresh ? 0.0 : v[i]; }
+            }
+#pragma unroll
+            for (int k = 0; k < kU; ++k) {
+                const int64_t i = i0 + k * kThreads;
+                if (i < hi) {
+                    const double pi = fresh ? rv[k] : rv[k] + beta * (pv[k] - omega * vv[k]);
+                    p[i] = pi;
+                    ph[i] = dv[k] * pi;
+                }
+            }
         }
     }
 }
@@ -417,13 +708,13 @@ k_batch_v1(const BatchItem *__restrict__ items, const int32_t *__restrict__ rang
 // iteration cap, a due mixed-precision replacement); BiCGSTAB s = r - alpha v,
 // sh = D^-1 s.
 __global__ void __launch_bounds__(kThreads)
-k_batch_v2(const BatchItem *__restrict__ items, const int32_t *__restrict__ ranges, const BatchSys *__restrict__ sys,
+k_batch_v2(const BatchVItem *__restrict__ items, const int32_t *__restrict__ ranges, const BatchSys *__restrict__ sys,
            BatchScal *__restrict__ scal, int parity, double *__restrict__ part) {
     __shared__ double sm[kThreads / 32 + 1];
     __shared__ int flag_sm;
-    const int n_items = ranges[kGroups];
+    const int n_items = ranges[kVR + kGroups];
     for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
-        const BatchItem item = items[it];
+        const BatchVItem item = items[it];
         const int s = item.sys;
         BatchScal &sc = scal[s];
         if (!cta_active(&sc, ACT_ITER, &flag_sm)) continue;
@@ -431,20 +722,50 @@ k_batch_v2(const BatchItem *__restrict__ items, const int32_t *__restrict__ rang
         const double alpha = __ldcg(&sc.alpha);
         const int64_t lo = (int64_t)item.row_begin * d.block, hi = (int64_t)item.row_end * d.block;
         if (d.method == BM_BICG) {
-            for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
-                const double si = d.r[i] - alpha * d.v[i];
-                d.s[i] = si;
-                d.sh[i] = d.dinv[i] * si;
+            double *__restrict__ sv = d.s, *__restrict__ sh = d.sh;
+            const double *__restrict__ r = d.r, *__restrict__ v = d.v, *__restrict__ dinv = d.dinv;
+            for (int64_t i0 = lo + threadIdx.x; i0 < hi; i0 += kU * kThreads) {
+                double rv[kU], vv[kU], dv[kU];
+#pragma unroll
+                for (int k = 0; k < kU; ++k) {
+                    const int64_t i = i0 + k * kThreads;
+                    if (i < hi) { rv[k] = r[i]; vv[k] = v[i]; dv[k] = dinv[i]; }
+                }
+#pragma unroll
+                for (int k = 0; k < kU; ++k) {
+                    const int64_t i = i0 + k * kThreads;
+                    if (i < hi) {
+                        const double si = rv[k] - alpha * vv[k];
+                        sv[i] = si;
+                        sh[i] = dv[k] * si;
+                    }
+                }
             }
             continue;
         }
         double srz = 0, srr = 0;
-        for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
-            d.x[i] += d.p[i] * alpha;
-            const double ri = d.r[i] + (-alpha) * d.q[i];
-            d.r[i] = ri;
-            srz += ri * (d.dinv[i] * ri);
-            srr += ri * ri;
+        {
+            double *__restrict__ x = d.x, *__restrict__ r = d.r;
+            const double *__restrict__ p = d.p, *__restrict__ q = d.q, *__restrict__ dinv = d.dinv;
+            for (int64_t i0 = lo + threadIdx.x; i0 < hi; i0 += kU * kThreads) {
+                double pv[kU], qv[kU], rv[kU], xv[kU], dv[kU];
+#pragma unroll
+                for (int k = 0; k < kU; ++k) {
+                    const int64_t i = i0 + k * kThreads;
+                    if (i < hi) { pv[k] = p[i]; qv[k] = q[i]; rv[k] = r[i]; xv[k] = x[i]; dv[k] = dinv[i]; }
+                }
+#pragma unroll
+                for (int k = 0; k < kU; ++k) {
+                    const int64_t i = i0 + k * kThreads;
+                    if (i < hi) {
+                        x[i] = xv[k] + pv[k] * alpha;
+                        const double ri = rv[k] + (-alpha) * qv[k];
+                        r[i] = ri;
+                        srz += ri * (dv[k] * ri);
+                        srr += ri * ri;
+                    }
+                }
+            }
         }
         srz = block_sum<kThreads>(srz, sm);
         srr = block_sum<kThreads>(srr, sm);
@@ -452,9 +773,9 @@ k_batch_v2(const BatchItem *__restrict__ items, const int32_t *__restrict__ rang
             part[2 * (int64_t)it] = srz;
             part[2 * (int64_t)it + 1] = srr;
         }
-        if (last_of_system(&sc, d.item_end - d.item_begin, &flag_sm)) {
-            const double rz_new = sum_items(part, d.item_begin, d.item_end, 0, sm);
-            const double rr = sum_items(part, d.item_begin, d.item_end, 1, sm);
+        if (last_of_system(&sc, d.vitem_end - d.vitem_begin, &flag_sm)) {
+            const double rz_new = sum_items(part, d.vitem_begin, d.vitem_end, 0, sm);
+            const double rr = sum_items(part, d.vitem_begin, d.vitem_end, 1, sm);
             if (threadIdx.x == 0) {
                 int stop = BS_NONE;
                 if (sqrt(rr) <= sc.tol * sqrt(sc.bb)) stop = BS_CONV;
@@ -476,13 +797,13 @@ k_batch_v2(const BatchItem *__restrict__ items, const int32_t *__restrict__ rang
 // convergence, NaN, cap, replacement; a breakdown asks the verification pass
 // for a restart).
 __global__ void __launch_bounds__(kThreads)
-k_batch_v3(const BatchItem *__restrict__ items, const int32_t *__restrict__ ranges, const BatchSys *__restrict__ sys,
+k_batch_v3(const BatchVItem *__restrict__ items, const int32_t *__restrict__ ranges, const BatchSys *__restrict__ sys,
            BatchScal *__restrict__ scal, double *__restrict__ part) {
     __shared__ double sm[kThreads / 32 + 1];
     __shared__ int flag_sm;
-    const int n_items = ranges[kGroups];
+    const int n_items = ranges[kVR + kGroups];
     for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
-        const BatchItem item = items[it];
+        const BatchVItem item = items[it];
         const int s = item.sys;
         BatchScal &sc = scal[s];
         if (!cta_active(&sc, ACT_ITER, &flag_sm)) continue;
@@ -490,17 +811,48 @@ k_batch_v3(const BatchItem *__restrict__ items, const int32_t *__restrict__ rang
         const int64_t lo = (int64_t)item.row_begin * d.block, hi = (int64_t)item.row_end * d.block;
         if (d.method == BM_CG) {
             const double beta = __ldcg(&sc.beta);
-            for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) d.p[i] = d.dinv[i] * d.r[i] + beta * d.p[i];
+            double *__restrict__ p = d.p;
+            const double *__restrict__ r = d.r, *__restrict__ dinv = d.dinv;
+            for (int64_t i0 = lo + threadIdx.x; i0 < hi; i0 += kU * kThreads) {
+                double pv[kU], rv[kU], dv[kU];
+#pragma unroll
+                for (int k = 0; k < kU; ++k) {
+                    const int64_t i = i0 + k * kThreads;
+                    if (i < hi) { pv[k] = p[i]; rv[k] = r[i]; dv[k] = dinv[i]; }
+                }
+#pragma unroll
+                for (int k = 0; k < kU; ++k) {
+                    const int64_t i = i0 + k * kThreads;
+                    if (i < hi) p[i] = dv[k] * rv[k] + beta * pv[k];
+                }
+            }
             continue;
         }
         const double alpha = __ldcg(&sc.alpha), omega = __ldcg(&sc.omega);
         double srr0 = 0, srr = 0;
-        for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
-            d.x[i] += alpha * d.ph[i] + omega * d.sh[i];
-            const double ri = d.s[i] - omega * d.t[i];
-            d.r[i] = ri;
-            srr0 += d.r0[i] * ri;
-            srr += ri * ri;
+        {
+            double *__restrict__ x = d.x, *__restrict__ r = d.r;
+            const double *__restrict__ ph = d.ph, *__restrict__ sh = d.sh, *__restrict__ sv = d.s,
+                                      *__restrict__ tv = d.t, *__restrict__ r0 = d.r0;
+            for (int64_t i0 = lo + threadIdx.x; i0 < hi; i0 += kU * kThreads) {
+                double a[kU], b[kU], c[kU], e[kU], f[kU], g[kU];
+#pragma unroll
+                for (int k = 0; k < kU; ++k) {
+                    const int64_t i = i0 + k * kThreads;
+                    if (i < hi) { a[k] = x[i]; b[k] = ph[i]; c[k] = sh[i]; e[k] = sv[i]; f[k] = tv[i]; g[k] = r0[i]; }
+                }
+#pragma unroll
+                for (int k = 0; k < kU; ++k) {
+                    const int64_t i = i0 + k * kThreads;
+                    if (i < hi) {
+                        x[i] = a[k] + (alpha * b[k] + omega * c[k]);
+                        const double ri = e[k] - omega * f[k];
+                        r[i] = ri;
+                        srr0 += g[k] * ri;
+                        srr += ri * ri;
+                    }
+                }
+            }
         }
         srr0 = block_sum<kThreads>(srr0, sm);
         srr = block_sum<kThreads>(srr, sm);
@@ -508,9 +860,9 @@ k_batch_v3(const BatchItem *__restrict__ items, const int32_t *__restrict__ rang
             part[2 * (int64_t)it] = srr0;
             part[2 * (int64_t)it + 1] = srr;
         }
-        if (last_of_system(&sc, d.item_end - d.item_begin, &flag_sm)) {
-            const double rho_new = sum_items(part, d.item_begin, d.item_end, 0, sm);
-            const double rr = sum_items(part, d.item_begin, d.item_end, 1, sm);
+        if (last_of_system(&sc, d.vitem_end - d.vitem_begin, &flag_sm)) {
+            const double rho_new = sum_items(part, d.vitem_begin, d.vitem_end, 0, sm);
+            const double rr = sum_items(part, d.vitem_begin, d.vitem_end, 1, sm);
             if (threadIdx.x == 0) {
                 const double beta = (rho_new / sc.rho) * (alpha / omega);
                 int stop = BS_NONE;
@@ -533,13 +885,13 @@ k_batch_v3(const BatchItem *__restrict__ items, const int32_t *__restrict__ rang
 // of r.z (PCG) or r0.r (BiCGSTAB; r.r for a system being initialised), r.r and
 // b.b for the systems under verification
 __global__ void __launch_bounds__(kThreads)
-k_batch_residual(const BatchItem *__restrict__ items, const int32_t *__restrict__ ranges, const BatchSys *__restrict__ sys,
+k_batch_residual(const BatchVItem *__restrict__ items, const int32_t *__restrict__ ranges, const BatchSys *__restrict__ sys,
                  const BatchScal *__restrict__ scal, double *__restrict__ part, double *__restrict__ part_bb) {
     __shared__ double sm[kThreads / 32 + 1];
     __shared__ int flag_sm;
-    const int n_items = ranges[kGroups];
+    const int n_items = ranges[kVR + kGroups];
     for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
-        const BatchItem item = items[it];
+        const BatchVItem item = items[it];
         const int s = item.sys;
         if (!cta_active(&scal[s], ACT_VERIFY, &flag_sm)) continue;
         const BatchSys d = sys[s];
@@ -583,7 +935,7 @@ __global__ void k_batch_decide(int cap, const BatchSys *__restrict__ sys, BatchS
     const BatchSys d = sys[s];
     const bool bicg = d.method == BM_BICG;
     double s1 = 0, rr = 0, bb = 0;
-    for (int i = d.item_begin; i < d.item_end; ++i) {
+    for (int i = d.vitem_begin; i < d.vitem_end; ++i) {
         s1 += part[2 * (int64_t)i];
         rr += part[2 * (int64_t)i + 1];
         bb += part_bb[2 * (int64_t)i];
@@ -621,12 +973,12 @@ __global__ void k_batch_decide(int cap, const BatchSys *__restrict__ sys, BatchS
 
 // verification, step 4: PCG p = z, BiCGSTAB r0 = r for restarted systems
 __global__ void __launch_bounds__(kThreads)
-k_batch_restart(const BatchItem *__restrict__ items, const int32_t *__restrict__ ranges, const BatchSys *__restrict__ sys,
+k_batch_restart(const BatchVItem *__restrict__ items, const int32_t *__restrict__ ranges, const BatchSys *__restrict__ sys,
                 const BatchScal *__restrict__ scal) {
     __shared__ int flag_sm;
-    const int n_items = ranges[kGroups];
+    const int n_items = ranges[kVR + kGroups];
     for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
-        const BatchItem item = items[it];
+        const BatchVItem item = items[it];
         const int s = item.sys;
         if (!cta_active(&scal[s], ACT_RESTART, &flag_sm)) continue;
         const BatchSys d = sys[s];
@@ -657,10 +1009,10 @@ template <int B, int L, int KIND>
 static int spmv_grid(yg_context ctx) {
     static int per_sm = 0;
     if (per_sm == 0) {
-        cudaFuncSetAttribute(k_batch_spmv<B, L, KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize, Stage<B>::SMEM);
+        cudaFuncSetAttribute(k_batch_spmv<B, L, KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize, WStage<B>::SMEM);
         int n = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_spmv<B, L, KIND>, kThreads, Stage<B>::SMEM) !=
-                cudaSuccess || n < 1)
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_spmv<B, L, KIND>, WCfg<B>::WARPS * 32,
+                                                          WStage<B>::SMEM) != cudaSuccess || n < 1)
             n = 1;
         per_sm = n;
     }
@@ -668,40 +1020,60 @@ static int spmv_grid(yg_context ctx) {
 }
 
 template <int B, int L, int KIND>
-static void launch_spmv_l(yg_batch bt, int g, int parity, int commit) {
+static int direct_grid(yg_context ctx) {
+    static int per_sm = 0;
+    if (per_sm == 0) {
+        int n = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_spmv_direct<B, L, KIND>, 256, 0) != cudaSuccess ||
+            n < 1)
+            n = 1;
+        per_sm = n;
+    }
+    return per_sm * ctx->num_sms;
+}
+
+template <int B, int L, int KIND>
+static void launch_spmv_l(yg_batch bt, int variant, int g, int parity, int commit) {
     yg_context ctx = bt->ctx;
-    k_batch_spmv<B, L, KIND><<<spmv_grid<B, L, KIND>(ctx), kThreads, Stage<B>::SMEM, ctx->stream>>>(
-        bt->d_items, bt->d_ranges, g, bt->d_sys, bt->d_scal, bt->d_part, parity, commit, ctx->d_err);
+    if (variant == 1) {
+        k_batch_spmv_direct<B, L, KIND><<<direct_grid<B, L, KIND>(ctx), 256, 0, ctx->stream>>>(
+            bt->d_mitems, bt->d_ranges, g, bt->d_sys, bt->d_scal, bt->d_mpart, parity, commit);
+    } else {
+        k_batch_spmv<B, L, KIND><<<spmv_grid<B, L, KIND>(ctx), WCfg<B>::WARPS * 32, WStage<B>::SMEM, ctx->stream>>>(
+            bt->d_mitems, bt->d_ranges, g, bt->d_sys, bt->d_scal, bt->d_mpart, parity, commit, ctx->d_err);
+    }
     YG_LAUNCHED(ctx);
 }
 
 template <int B, int KIND>
-static void launch_spmv_b(yg_batch bt, int L, int g, int parity, int commit) {
+static void launch_spmv_b(yg_batch bt, int V, int L, int g, int parity, int commit) {
     switch (L) {
-    case 2: launch_spmv_l<B, 2, KIND>(bt, g, parity, commit); break;
-    case 4: launch_spmv_l<B, 4, KIND>(bt, g, parity, commit); break;
-    case 8: launch_spmv_l<B, 8, KIND>(bt, g, parity, commit); break;
-    case 16: launch_spmv_l<B, 16, KIND>(bt, g, parity, commit); break;
-    default: launch_spmv_l<B, 32, KIND>(bt, g, parity, commit); break;
+    case 2: launch_spmv_l<B, 2, KIND>(bt, V, g, parity, commit); break;
+    case 4: launch_spmv_l<B, 4, KIND>(bt, V, g, parity, commit); break;
+    case 8: launch_spmv_l<B, 8, KIND>(bt, V, g, parity, commit); break;
+    case 16: launch_spmv_l<B, 16, KIND>(bt, V, g, parity, commit); break;
+    default: launch_spmv_l<B, 32, KIND>(bt, V, g, parity, commit); break;
     }
 }
 
 template <int KIND>
-static void launch_spmv_kind(yg_batch bt, int B, int L, int g, int parity, int commit) {
-    if (B == 1) launch_spmv_b<1, KIND>(bt, L, g, parity, commit);
-    else if (B == 2) launch_spmv_b<2, KIND>(bt, L, g, parity, commit);
-    else launch_spmv_b<3, KIND>(bt, L, g, parity, commit);
+static void launch_spmv_kind(yg_batch bt, int B, int V, int L, int g, int parity, int commit) {
+    if (B == 1) launch_spmv_b<1, KIND>(bt, V, L, g, parity, commit);
+    else if (B == 2) launch_spmv_b<2, KIND>(bt, V, L, g, parity, commit);
+    else launch_spmv_b<3, KIND>(bt, V, L, g, parity, commit);
 }
 
-// one SpMV launch for group g (method, block size) of the given kind
-static void launch_spmv(yg_batch bt, int kind, int g, int parity, int commit, int L = 0) {
+// one SpMV launch for group g (method, block size) of the given kind; variant
+// 0 stages tiles in shared memory, 1 loads directly
+static void launch_spmv(yg_batch bt, int kind, int g, int parity, int commit, int L = 0, int V = -1) {
     const int B = g % 3 + 1;
     if (L == 0) L = bt->lanes[B];
+    if (V < 0) V = bt->variant[B];
     switch (kind) {
-    case SP_CG: launch_spmv_kind<SP_CG>(bt, B, L, g, parity, commit); break;
-    case SP_VERIFY: launch_spmv_kind<SP_VERIFY>(bt, B, L, g, parity, commit); break;
-    case SP_BICG_V: launch_spmv_kind<SP_BICG_V>(bt, B, L, g, parity, commit); break;
-    default: launch_spmv_kind<SP_BICG_T>(bt, B, L, g, parity, commit); break;
+    case SP_CG: launch_spmv_kind<SP_CG>(bt, B, V, L, g, parity, commit); break;
+    case SP_VERIFY: launch_spmv_kind<SP_VERIFY>(bt, B, V, L, g, parity, commit); break;
+    case SP_BICG_V: launch_spmv_kind<SP_BICG_V>(bt, B, V, L, g, parity, commit); break;
+    default: launch_spmv_kind<SP_BICG_T>(bt, B, V, L, g, parity, commit); break;
     }
 }
 
@@ -710,6 +1082,8 @@ template <int B, int KIND>
 static void prepare_spmv_bk(yg_context ctx) {
     spmv_grid<B, 2, KIND>(ctx); spmv_grid<B, 4, KIND>(ctx); spmv_grid<B, 8, KIND>(ctx);
     spmv_grid<B, 16, KIND>(ctx); spmv_grid<B, 32, KIND>(ctx);
+    direct_grid<B, 2, KIND>(ctx); direct_grid<B, 4, KIND>(ctx); direct_grid<B, 8, KIND>(ctx);
+    direct_grid<B, 16, KIND>(ctx); direct_grid<B, 32, KIND>(ctx);
 }
 template <int B>
 static void prepare_spmv_b(yg_context ctx) {
@@ -726,13 +1100,13 @@ static void launch_verify(yg_batch bt) {
     const int grid = batch_grid(ctx);
     for (int g = 0; g < kGroups; ++g)
         if (has(bt, g)) launch_spmv(bt, SP_VERIFY, g, 0, 1);
-    k_batch_residual<<<grid, kThreads, 0, ctx->stream>>>(bt->d_items, bt->d_ranges, bt->d_sys, bt->d_scal, bt->d_part,
-                                                        bt->d_part2);
+    k_batch_residual<<<grid, kThreads, 0, ctx->stream>>>(bt->d_vitems, bt->d_ranges, bt->d_sys, bt->d_scal, bt->d_vpart,
+                                                        bt->d_vpart2);
     YG_LAUNCHED(ctx);
-    k_batch_decide<<<(bt->capacity + 127) / 128, 128, 0, ctx->stream>>>(bt->capacity, bt->d_sys, bt->d_scal, bt->d_part,
-                                                                         bt->d_part2);
+    k_batch_decide<<<(bt->capacity + 127) / 128, 128, 0, ctx->stream>>>(bt->capacity, bt->d_sys, bt->d_scal, bt->d_vpart,
+                                                                         bt->d_vpart2);
     YG_LAUNCHED(ctx);
-    k_batch_restart<<<grid, kThreads, 0, ctx->stream>>>(bt->d_items, bt->d_ranges, bt->d_sys, bt->d_scal);
+    k_batch_restart<<<grid, kThreads, 0, ctx->stream>>>(bt->d_vitems, bt->d_ranges, bt->d_sys, bt->d_scal);
     YG_LAUNCHED(ctx);
 }
 
@@ -740,17 +1114,17 @@ static void launch_iteration(yg_batch bt, int parity) {
     yg_context ctx = bt->ctx;
     const int grid = batch_grid(ctx);
     if (has_bicg(bt)) {
-        k_batch_v1<<<grid, kThreads, 0, ctx->stream>>>(bt->d_items, bt->d_ranges, bt->d_sys, bt->d_scal);
+        k_batch_v1<<<grid, kThreads, 0, ctx->stream>>>(bt->d_vitems, bt->d_ranges, bt->d_sys, bt->d_scal);
         YG_LAUNCHED(ctx);
     }
     for (int g = 0; g < kGroups; ++g)
         if (has(bt, g)) launch_spmv(bt, g < 3 ? SP_CG : SP_BICG_V, g, parity, 1);
-    k_batch_v2<<<grid, kThreads, 0, ctx->stream>>>(bt->d_items, bt->d_ranges, bt->d_sys, bt->d_scal, parity,
-                                                  bt->d_part2);
+    k_batch_v2<<<grid, kThreads, 0, ctx->stream>>>(bt->d_vitems, bt->d_ranges, bt->d_sys, bt->d_scal, parity,
+                                                  bt->d_vpart);
     YG_LAUNCHED(ctx);
     for (int g = 3; g < kGroups; ++g)
         if (has(bt, g)) launch_spmv(bt, SP_BICG_T, g, parity, 1);
-    k_batch_v3<<<grid, kThreads, 0, ctx->stream>>>(bt->d_items, bt->d_ranges, bt->d_sys, bt->d_scal, bt->d_part2);
+    k_batch_v3<<<grid, kThreads, 0, ctx->stream>>>(bt->d_vitems, bt->d_ranges, bt->d_sys, bt->d_scal, bt->d_vpart);
     YG_LAUNCHED(ctx);
 }
 
@@ -767,64 +1141,73 @@ static bool sys_live(yg_batch bt, int s) {
     return bt->used[s] && (f == BF_RUN || f == BF_INIT);
 }
 
-// Rebuild the item table: systems grouped by (method, block size), tiles
-// grouped into items.  Systems that finished are left out (their kernels' item
-// loops stay short); the groups present count every system in the batch, so
-// compaction never changes the set of SpMV launches that the captured graph
-// holds.  A system's tiles are always grouped the same way for a given tuning,
-// so its reductions add the same partials in the same order whatever else is in
-// the table.
+template <typename T>
+static yg_status grow(yg_context ctx, T **p, int32_t *cap, size_t need, double **part, double **part2) {
+    if ((int64_t)need <= *cap) return YG_OK;
+    YG_CUDA(cudaStreamSynchronize(ctx->stream));
+    dev_free(ctx, *p);
+    dev_free(ctx, *part);
+    if (part2) dev_free(ctx, *part2);
+    *p = nullptr;
+    *part = nullptr;
+    if (part2) *part2 = nullptr;
+    const int32_t c = (int32_t)need * 2 + 64;
+    YG_TRY(dev_alloc_t(ctx, p, c));
+    YG_TRY(dev_alloc_t(ctx, part, 2 * (size_t)c));
+    if (part2) YG_TRY(dev_alloc_t(ctx, part2, 2 * (size_t)c));
+    *cap = c;
+    return YG_OK;
+}
+
+// Rebuild the work tables: systems grouped by (method, block size); matrix
+// items of tiles_per_item tiles, vector items of vitem_rows block rows.
+// Systems that finished are left out (their kernels' item loops stay short);
+// the groups present count every system in the batch, so compaction never
+// changes the set of SpMV launches that the captured graph holds.  A system's
+// items are always cut the same way for a given tuning, so its reductions add
+// the same partials in the same order whatever else is in the tables.
 static yg_status rebuild_items(yg_batch bt) {
     yg_context ctx = bt->ctx;
-    std::vector<BatchItem> items;
-    int32_t ranges[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    std::vector<BatchMItem> mitems;
+    std::vector<BatchVItem> vitems;
+    int32_t ranges[2 * kVR] = {0};
     unsigned present = 0;
     for (int g = 0; g < kGroups; ++g) {
         const int method = g / 3, B = g % 3 + 1;
-        ranges[g] = (int32_t)items.size();
-        const int T = std::max(1, bt->tiles_per_item[B]);
+        ranges[g] = (int32_t)mitems.size();
+        ranges[kVR + g] = (int32_t)vitems.size();
+        const int T = std::max(1, bt->tiles_per_item[B]), VR = vitem_rows(B);
         for (int s = 0; s < bt->capacity; ++s) {
             if (!bt->used[s] || bt->sys[s].block != B || bt->sys[s].method != method) continue;
             present |= 1u << g;
             BatchSys &d = bt->sys[s];
-            d.item_begin = (int32_t)items.size();
-            if (!sys_live(bt, s)) {
-                d.item_end = d.item_begin;
-                continue;
+            d.mitem_begin = (int32_t)mitems.size();
+            d.vitem_begin = (int32_t)vitems.size();
+            if (sys_live(bt, s)) {
+                for (int t0 = 0; t0 < d.ntiles; t0 += T) mitems.push_back({s, t0, std::min(d.ntiles, t0 + T), 0});
+                if (d.ntiles == 0) mitems.push_back({s, 0, 0, 0});
+                for (int r0 = 0; r0 < d.nbrows; r0 += VR) vitems.push_back({s, r0, std::min(d.nbrows, r0 + VR), 0});
+                if (d.nbrows == 0) vitems.push_back({s, 0, 0, 0});
             }
-            const std::vector<int32_t> &tl = bt->tiles[s];
-            for (int t0 = 0; t0 < d.ntiles; t0 += T) {
-                const int t1 = std::min(d.ntiles, t0 + T);
-                items.push_back({s, t0, t1, tl[t0], tl[t1], 0});
-            }
-            if (d.ntiles == 0) items.push_back({s, 0, 0, 0, 0, 0});
-            d.item_end = (int32_t)items.size();
+            d.mitem_end = (int32_t)mitems.size();
+            d.vitem_end = (int32_t)vitems.size();
         }
     }
-    ranges[kGroups] = (int32_t)items.size();
-    ranges[kGroups + 1] = (int32_t)items.size();
-    if ((int32_t)items.size() > bt->max_items) {
-        YG_CUDA(cudaStreamSynchronize(ctx->stream));
-        dev_free(ctx, bt->d_items);
-        dev_free(ctx, bt->d_part);
-        dev_free(ctx, bt->d_part2);
-        bt->d_items = nullptr;
-        bt->d_part = bt->d_part2 = nullptr;
-        int32_t cap = (int32_t)items.size() * 2 + 64;
-        YG_TRY(dev_alloc_t(ctx, &bt->d_items, cap));
-        YG_TRY(dev_alloc_t(ctx, &bt->d_part, 2 * (size_t)cap));
-        YG_TRY(dev_alloc_t(ctx, &bt->d_part2, 2 * (size_t)cap));
-        bt->max_items = cap;
-        drop_graph(bt);  // the graph captured the old pointers
-    }
-    bt->n_items = (int32_t)items.size();
+    ranges[kGroups] = ranges[kGroups + 1] = (int32_t)mitems.size();
+    ranges[kVR + kGroups] = ranges[kVR + kGroups + 1] = (int32_t)vitems.size();
+    const bool regrow = (int64_t)mitems.size() > bt->max_mitems || (int64_t)vitems.size() > bt->max_vitems;
+    YG_TRY(grow(ctx, &bt->d_mitems, &bt->max_mitems, mitems.size(), &bt->d_mpart, (double **)nullptr));
+    YG_TRY(grow(ctx, &bt->d_vitems, &bt->max_vitems, vitems.size(), &bt->d_vpart, &bt->d_vpart2));
+    if (regrow) drop_graph(bt);  // the graph captured the old pointers
     YG_CUDA(cudaStreamSynchronize(ctx->stream));
-    if (!items.empty())
-        YG_CUDA(cudaMemcpy(bt->d_items, items.data(), sizeof(BatchItem) * items.size(), cudaMemcpyHostToDevice));
+    if (!mitems.empty())
+        YG_CUDA(cudaMemcpy(bt->d_mitems, mitems.data(), sizeof(BatchMItem) * mitems.size(), cudaMemcpyHostToDevice));
+    if (!vitems.empty())
+        YG_CUDA(cudaMemcpy(bt->d_vitems, vitems.data(), sizeof(BatchVItem) * vitems.size(), cudaMemcpyHostToDevice));
     YG_CUDA(cudaMemcpy(bt->d_ranges, ranges, sizeof(ranges), cudaMemcpyHostToDevice));
     YG_CUDA(cudaMemcpy(bt->d_sys, bt->sys.data(), sizeof(BatchSys) * bt->capacity, cudaMemcpyHostToDevice));
     bt->groups_present = present;
-    bt->live_items = bt->n_items;
+    bt->live_items = (int32_t)vitems.size();
     bt->dirty = false;
     return YG_OK;
 }
@@ -860,21 +1243,43 @@ static void release_slot(yg_batch bt, int s) {
     bt->mats[s] = nullptr;
 }
 
-// Cut block rows into tiles of whole rows with at most `cap` blocks each (a row
-// longer than cap forms a tile of its own, read from global memory).
+// Cut block rows into tiles of whole rows with at most `cap` blocks and `cap`
+// rows each (a row longer than cap forms a tile of its own, read from global
+// memory).
 static void make_tiles(const std::vector<int32_t> &rp, int cap, std::vector<int32_t> &tiles) {
     tiles.clear();
     const int n = (int)rp.size() - 1;
     tiles.push_back(0);
     int start = 0;
     for (int r = 0; r < n; ++r) {
-        if (r > start && rp[r + 1] - rp[start] > cap) {
+        if (r > start && (rp[r + 1] - rp[start] > cap || r - start >= cap)) {
             tiles.push_back(r);
             start = r;
         }
     }
     if (n > 0) tiles.push_back(n);
 }
+
+// Host view of a slot after the last wait: whether it still iterates, and its
+// stats (from the state copied back at the end of the block).
+bool batch_slot_running(yg_batch bt, int32_t slot) { return sys_live(bt, slot); }
+
+static void stats_of(const BatchScal &sc, yg_solve_stats *out) {
+    yg_solve_stats st{};
+    st.iterations = sc.iter;
+    st.rel_residual = sc.bb > 0 ? std::sqrt(sc.true_rr / sc.bb) : std::sqrt(sc.true_rr);
+    st.refinements = (int32_t)sc.replacements;
+    switch (sc.flag) {
+    case BF_DONE: st.status = YG_OK; break;
+    case BF_BREAK: st.status = YG_BREAKDOWN; break;
+    case BF_NANF: st.status = YG_NAN; break;
+    case BF_RUN: case BF_INIT: st.status = YG_RUNNING; break;
+    default: st.status = YG_NOT_CONVERGED; break;
+    }
+    *out = st;
+}
+
+void batch_slot_stats(yg_batch bt, int32_t slot, yg_solve_stats *out) { stats_of(bt->h_scal[slot], out); }
 
 }  // namespace yg
 
@@ -892,7 +1297,7 @@ extern "C" yg_status yg_batch_create(yg_context ctx, int32_t capacity, yg_batch 
     bt->opts.assign(capacity, yg_solve_opts{});
     yg_status s;
     if ((s = dev_alloc_t(ctx, &bt->d_sys, capacity)) != YG_OK || (s = dev_alloc_t(ctx, &bt->d_scal, capacity)) != YG_OK ||
-        (s = dev_alloc_t(ctx, &bt->d_ranges, 8)) != YG_OK) {
+        (s = dev_alloc_t(ctx, &bt->d_ranges, 2 * kVR)) != YG_OK) {
         yg_batch_destroy(bt);
         return s;
     }
@@ -903,7 +1308,7 @@ extern "C" yg_status yg_batch_create(yg_context ctx, int32_t capacity, yg_batch 
     for (auto &c : init) c.flag = BF_EMPTY;
     bt->h_scal = init;
     cudaMemcpy(bt->d_scal, init.data(), sizeof(BatchScal) * capacity, cudaMemcpyHostToDevice);
-    cudaMemset(bt->d_ranges, 0, sizeof(int32_t) * 8);
+    cudaMemset(bt->d_ranges, 0, sizeof(int32_t) * 2 * kVR);
     YG_CUDA(cudaGetLastError());
     *out = bt;
     return YG_OK;
@@ -915,8 +1320,8 @@ extern "C" yg_status yg_batch_destroy(yg_batch bt) {
     drop_graph(bt);
     for (int s = 0; s < bt->capacity; ++s)
         if (bt->used[s]) release_slot(bt, s);
-    for (void *p : {(void *)bt->d_sys, (void *)bt->d_scal, (void *)bt->d_items, (void *)bt->d_ranges, (void *)bt->d_part,
-                    (void *)bt->d_part2})
+    for (void *p : {(void *)bt->d_sys, (void *)bt->d_scal, (void *)bt->d_mitems, (void *)bt->d_vitems, (void *)bt->d_ranges,
+                    (void *)bt->d_mpart, (void *)bt->d_vpart, (void *)bt->d_vpart2})
         dev_free(bt->ctx, p);
     delete bt;
     return YG_OK;
@@ -949,7 +1354,7 @@ extern "C" yg_status yg_batch_add(yg_batch bt, yg_matrix A, yg_vector b, yg_vect
     YG_CUDA(cudaStreamSynchronize(ctx->stream));
     YG_CUDA(cudaMemcpy(rp.data(), A->d_rowptr, sizeof(int32_t) * rp.size(), cudaMemcpyDeviceToHost));
     std::vector<int32_t> tl;
-    make_tiles(rp, tile_blocks(A->block), tl);
+    make_tiles(rp, tile_cap(A->block), tl);
     BatchSys d{};
     d.block = A->block;
     d.nbrows = (int32_t)A->nbrows;
@@ -1055,7 +1460,7 @@ static yg_status batch_launch(yg_batch bt) {
 }
 
 // Wait for the launched block, count the systems still running and compact the
-// item table once a quarter of it is idle.
+// work tables once a quarter of the vector items is idle.
 static yg_status batch_collect(yg_batch bt, int *active_out) {
     yg_context ctx = bt->ctx;
     YG_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -1065,9 +1470,9 @@ static yg_status batch_collect(yg_batch bt, int *active_out) {
     for (int s = 0; s < bt->capacity; ++s)
         if (sys_live(bt, s)) {
             ++active;
-            live += bt->sys[s].item_end - bt->sys[s].item_begin;
+            live += bt->sys[s].vitem_end - bt->sys[s].vitem_begin;
         }
-    if (active > 0 && live < bt->live_items - bt->live_items / 4 && bt->live_items - live >= 64)
+    if (active > 0 && live < bt->live_items - bt->live_items / 4 && bt->live_items - live >= 16)
         YG_TRY(rebuild_items(bt));
     *active_out = active;
     return YG_OK;
@@ -1116,23 +1521,12 @@ extern "C" yg_status yg_batch_stats(yg_batch bt, int32_t slot, yg_solve_stats *o
     YG_CUDA(cudaStreamSynchronize(bt->ctx->stream));
     BatchScal sc;
     YG_CUDA(cudaMemcpy(&sc, bt->d_scal + slot, sizeof(BatchScal), cudaMemcpyDeviceToHost));
-    yg_solve_stats st{};
-    st.iterations = sc.iter;
-    st.rel_residual = sc.bb > 0 ? std::sqrt(sc.true_rr / sc.bb) : std::sqrt(sc.true_rr);
-    st.refinements = (int32_t)sc.replacements;
-    switch (sc.flag) {
-    case BF_DONE: st.status = YG_OK; break;
-    case BF_BREAK: st.status = YG_BREAKDOWN; break;
-    case BF_NANF: st.status = YG_NAN; break;
-    case BF_RUN: case BF_INIT: st.status = YG_RUNNING; break;
-    default: st.status = YG_NOT_CONVERGED; break;
-    }
-    *out = st;
+    stats_of(sc, out);
     return YG_OK;
 }
 
-// Choose tiles per item and lanes per block row for each block size from the
-// systems present, by timing the iteration SpMV of the whole batch (without
+// Choose the SpMV variant, tiles per matrix item and lanes per block row for each block size from
+// the systems present, by timing the iteration SpMV of the whole batch (without
 // committing its reductions).
 extern "C" yg_status yg_batch_tune(yg_batch bt) {
     if (!bt) return fail(YG_BAD_ARG, "yg_batch_tune: NULL batch");
@@ -1141,7 +1535,7 @@ extern "C" yg_status yg_batch_tune(yg_batch bt) {
     YG_TRY(rebuild_items(bt));
     launch_verify(bt);
     if (has_bicg(bt)) {
-        k_batch_v1<<<batch_grid(ctx), kThreads, 0, ctx->stream>>>(bt->d_items, bt->d_ranges, bt->d_sys, bt->d_scal);
+        k_batch_v1<<<batch_grid(ctx), kThreads, 0, ctx->stream>>>(bt->d_vitems, bt->d_ranges, bt->d_sys, bt->d_scal);
         YG_LAUNCHED(ctx);
     }
     YG_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -1153,27 +1547,29 @@ extern "C" yg_status yg_batch_tune(yg_batch bt) {
         const bool cg = has(bt, B - 1), bi = has(bt, 3 + B - 1);
         if (!cg && !bi) continue;
         float best = 1e30f;
-        int bestL = bt->lanes[B], bestT = bt->tiles_per_item[B];
-        for (int T : {2, 8, 32}) {
+        int bestL = bt->lanes[B], bestT = bt->tiles_per_item[B], bestV = bt->variant[B];
+        for (int T : {1, 4, 16}) {
             bt->tiles_per_item[B] = T;
             YG_TRY(rebuild_items(bt));
-            for (int L : {2, 4, 8, 16, 32}) {
-                auto launch = [&]() {
-                    if (cg) launch_spmv(bt, SP_CG, B - 1, 0, 0, L);
-                    if (bi) launch_spmv(bt, SP_BICG_V, 3 + B - 1, 0, 0, L);
-                };
-                launch();
-                cudaEventRecord(e0, ctx->stream);
-                for (int r = 0; r < 3; ++r) launch();
-                cudaEventRecord(e1, ctx->stream);
-                cudaEventSynchronize(e1);
-                float ms = 0;
-                cudaEventElapsedTime(&ms, e0, e1);
-                if (ms < best) { best = ms; bestL = L; bestT = T; }
-            }
+            for (int V : {0, 1})
+                for (int L : {2, 4, 8, 16, 32}) {
+                    auto launch = [&]() {
+                        if (cg) launch_spmv(bt, SP_CG, B - 1, 0, 0, L, V);
+                        if (bi) launch_spmv(bt, SP_BICG_V, 3 + B - 1, 0, 0, L, V);
+                    };
+                    launch();
+                    cudaEventRecord(e0, ctx->stream);
+                    for (int r = 0; r < 3; ++r) launch();
+                    cudaEventRecord(e1, ctx->stream);
+                    cudaEventSynchronize(e1);
+                    float ms = 0;
+                    cudaEventElapsedTime(&ms, e0, e1);
+                    if (ms < best) { best = ms; bestL = L; bestT = T; bestV = V; }
+                }
         }
         bt->lanes[B] = bestL;
         bt->tiles_per_item[B] = bestT;
+        bt->variant[B] = bestV;
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
@@ -1183,24 +1579,12 @@ extern "C" yg_status yg_batch_tune(yg_batch bt) {
     return check_device_error(ctx);
 }
 
-namespace yg {
-// Host view of a slot after the last wait: whether it still iterates, and its
-// stats (from the state copied back at the end of the block).
-bool batch_slot_running(yg_batch bt, int32_t slot) { return sys_live(bt, slot); }
-
-void batch_slot_stats(yg_batch bt, int32_t slot, yg_solve_stats *out) {
-    const BatchScal &sc = bt->h_scal[slot];
-    yg_solve_stats st{};
-    st.iterations = sc.iter;
-    st.rel_residual = sc.bb > 0 ? std::sqrt(sc.true_rr / sc.bb) : std::sqrt(sc.true_rr);
-    st.refinements = (int32_t)sc.replacements;
-    switch (sc.flag) {
-    case BF_DONE: st.status = YG_OK; break;
-    case BF_BREAK: st.status = YG_BREAKDOWN; break;
-    case BF_NANF: st.status = YG_NAN; break;
-    case BF_RUN: case BF_INIT: st.status = YG_RUNNING; break;
-    default: st.status = YG_NOT_CONVERGED; break;
+extern "C" yg_status yg_batch_get_tuning(yg_batch bt, int32_t *out) {
+    if (!bt || !out) return fail(YG_BAD_ARG, "yg_batch_get_tuning: NULL argument");
+    for (int B = 1; B <= 3; ++B) {
+        out[3 * (B - 1)] = bt->variant[B];
+        out[3 * (B - 1) + 1] = bt->lanes[B];
+        out[3 * (B - 1) + 2] = bt->tiles_per_item[B];
     }
-    *out = st;
+    return YG_OK;
 }
-}  // namespace yg
