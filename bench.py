@@ -132,14 +132,9 @@ def run_spmv_profile(args):
 def run_gpu(args):
     import yafel_b200 as yb
     from yafel_b200 import loads
-    ws, rank, local = dist_env()
-    torch_dist = None
-    if ws > 1:
-        import torch
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=600))
-        torch_dist = dist
+    from yafel_b200.replicas import Replicas
+    rep = Replicas("nccl")
+    ws, rank, local = rep.ws, rep.rank, rep.local
     ctx = yb.Context(local if ws > 1 else 0)
     lib = yb.lib()
     mesh = problem(args.nx)
@@ -185,8 +180,7 @@ def run_gpu(args):
         for _ in range(warmup):
             step(precision)
         ctx.synchronize()
-        if torch_dist:
-            torch_dist.barrier()
+        rep.barrier()
         launches0 = ctx.launches
         ev = [C.c_void_p(), C.c_void_p()]
         t0 = time.perf_counter()
@@ -206,13 +200,8 @@ def run_gpu(args):
     clk = clocks.stop()
     wallmx, stmx, _, Kmx, _ = timed(1, args.steps, max(1, args.warmup // 3), profile=True)
     wallir, stir, _, _, _ = timed(2, 1, 0)
-    step_s = wall64 / args.steps
-    if torch_dist:
-        import torch
-        t = torch.tensor([step_s], device="cuda")
-        torch_dist.all_reduce(t, op=torch_dist.ReduceOp.MAX)
-        step_s = float(t.item())
-    value = ws * ndofs / step_s
+    step_s = rep.max(wall64 / args.steps)
+    value = rep.job_rate(ndofs, step_s)
     # e2e: through the public API from host buffers every step: DoF numbering +
     # upload, assembly, BCs, host load vector upload, solve, solution download.
     e2e_steps = max(1, min(args.steps, 2))
@@ -234,7 +223,7 @@ def run_gpu(args):
             mesh["cell_types"].nbytes + traction.nbytes + 3 * clamp.size * 16 + \
             X.nbytes + dme.elements.nbytes  # numbering and element lists uploaded by DoFManager
         d2h = sol.nbytes
-    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    e2e_s = rep.max((time.perf_counter() - t0) / e2e_steps)
     # roofline of the dominant kernel (BCSR3 SpMV inside the PCG iterations)
     rp, col, _ = None, None, None
     nnzb = K.nnz() // 9
@@ -290,9 +279,7 @@ def run_gpu(args):
         out["cpu_baseline"] = cpu_baseline(args)
     if rank == 0:
         print(json.dumps(out), flush=True)
-    if torch_dist:
-        torch_dist.barrier()
-        torch_dist.destroy_process_group()
+    rep.close()
 
 
 def run_small_poisson(ctx, reps=30):
