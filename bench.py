@@ -513,6 +513,7 @@ def run_serve(args):
 
     def served(precision, idxs, clocks=None):
         S = yb.Server(budget, max_active=args.max_active, ctx=ctx)
+        S.set_solo_rows(args.solo_rows)
         idx, pending = {}, []
         lat, stats = {}, {}
         state = {"nsub": 0}
@@ -528,8 +529,8 @@ def run_serve(args):
                 idx[S.submit(workloads.est_bytes(specs[i]))] = i
                 state["nsub"] += 1
 
-        def admit_build():
-            while True:
+        def admit_build(limit):
+            for _ in range(limit):
                 r = S.admit()
                 if r is None:
                     return
@@ -541,19 +542,25 @@ def run_serve(args):
 
         if clocks:
             clocks.start()
+        tuned = False
         while len(lat) < n:
             take_arrivals()
-            admit_build()
+            if S.info()["active"] == 0 and not pending:
+                admit_build(1)
             for (r, K, b, x, i) in pending:
                 S.attach(r, K, b, x, method=workloads.method(specs[i]), precision=precision)
             pending.clear()
-            if S.info()["active"] == 0:
+            info = S.info()
+            if info["active"] == 0:
                 if state["nsub"] < n:
                     time.sleep(max(0.0, arr[idxs[state["nsub"]]] - arr[idxs[0]] - (time.perf_counter() - t0)))
                 continue
+            if not tuned and (info["active"] >= 32 or (info["queued"] == 0 and state["nsub"] == n)):
+                S.tune()  # once, on the mix attached by then
+                tuned = True
             S.launch()
             take_arrivals()
-            admit_build()
+            admit_build(args.build_per_block)  # host work overlaps the block
             S.wait()
             for r in S.finished():
                 i = idx[r]
@@ -610,6 +617,7 @@ def run_serve(args):
            "config": {"workload": "serve_%d_requests_poisson_arrivals_%g_per_s" % (N, args.rate), "requests": N,
                       "offered_rate_per_s": args.rate, "total_dofs": int(sum(dofs)), "min_dofs": int(min(dofs)),
                       "max_dofs": int(max(dofs)), "budget_GB": args.budget_gb, "max_active": args.max_active,
+                      "solo_rows": args.solo_rows,
                       "kinds": {k: sum(1 for s in specs if s["kind"] == k) for k in ("poisson", "elasticity", "supg")},
                       "dims": {str(d): sum(1 for s in specs if s["dim"] == d) for d in (2, 3)},
                       "tolerance": "relative residual 1e-10 (FP64 true residual per request)",
@@ -719,6 +727,9 @@ def main():
     ap.add_argument("--rate", type=float, default=2000.0, help="arrival rate (req/s) of the serving workload")
     ap.add_argument("--budget-gb", type=float, default=150.0, help="HBM budget of the serving workload")
     ap.add_argument("--max-active", type=int, default=1024, help="systems solved together by the server")
+    ap.add_argument("--build-per-block", type=int, default=4, help="requests the serving loop builds per block")
+    ap.add_argument("--solo-rows", type=int, default=0,
+                    help="served systems of at least this many rows are solved alone (0: batch all)")
     args = ap.parse_args()
     if args.spmv_profile:
         run_spmv_profile(args)

@@ -323,6 +323,12 @@ YG_API yg_status yg_server_finished(yg_server S, int64_t *ids, int32_t cap, int3
 YG_API yg_status yg_server_poll(yg_server S, int64_t id, yg_solve_stats *stats);
 YG_API yg_status yg_server_release(yg_server S, int64_t id);
 YG_API yg_status yg_server_info(yg_server S, int64_t *queued, int64_t *active, uint64_t *bytes_held);
+/* Autotune the shared batch's SpMV on the systems attached now (between a wait
+ * and the next launch). */
+YG_API yg_status yg_server_tune(yg_server S);
+/* Systems of at least `rows` rows (0: none) skip the batch: each wait solves
+ * one of them alone, to completion, with yg_cg or yg_bicgstab (Jacobi). */
+YG_API yg_status yg_server_set_solo_rows(yg_server S, int64_t rows);
 
 /* ------------------------------------------------------------------ allocation-free dot product */
 

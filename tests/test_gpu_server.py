@@ -2,7 +2,8 @@
 (2D/3D Poisson, elasticity, SUPG by BiCGSTAB) are admitted in arrival order
 under an HBM budget small enough to make the queue wait, every request reaches
 a 1e-10 relative residual, the held bytes never exceed the budget, and each
-result equals the one the system gets when solved alone in a batch."""
+batched result equals the one the system gets when solved alone in a batch;
+with a solo threshold, the large systems are solved alone in between."""
 import numpy as np
 import pytest
 
@@ -14,14 +15,16 @@ pytestmark = pytest.mark.gpu
 SPECS = workloads.serving_specs(12, lo=1e3, hi=2e4)
 
 
-def test_server_admits_by_budget_and_solves_everything(ctx):
+@pytest.mark.parametrize("solo_rows", [0, 4000])
+def test_server_admits_by_budget_and_solves_everything(ctx, solo_rows):
     assert {s["kind"] for s in SPECS} == {"poisson", "elasticity", "supg"}
     assert {s["dim"] for s in SPECS} == {2, 3}
     est = [workloads.est_bytes(s) for s in SPECS]
     budget = 2 * max(est)
     S = yb.Server(budget, max_active=8, ctx=ctx)
+    S.set_solo_rows(solo_rows)
     ids = {S.submit(e): i for i, e in enumerate(est)}
-    built, results, waited_for_room = {}, {}, False
+    built, results, waited_for_room, rows = {}, {}, False, {}
     while len(results) < len(SPECS):
         while True:
             rid = S.admit()
@@ -33,6 +36,7 @@ def test_server_admits_by_budget_and_solves_everything(ctx):
             x.fill(0.0)
             S.attach(rid, K, b, x, method=workloads.method(spec))
             built[rid] = (K, b)
+            rows[ids[rid]] = K.rows()
         info = S.info()
         assert info["bytes_held"] <= budget
         if info["queued"] > 0:
@@ -47,8 +51,10 @@ def test_server_admits_by_budget_and_solves_everything(ctx):
     assert waited_for_room
     for i, (status, rel, x) in results.items():
         assert status == 0 and rel <= 1e-10, (SPECS[i], status, rel)
-    # the same system solved alone
-    for i in (0, 5, 11):
+    if solo_rows:
+        assert any(r >= solo_rows for r in rows.values()) and any(r < solo_rows for r in rows.values())
+    # a batched system's result equals the one it gets alone in a batch
+    for i in [k for k in (0, 5, 11) if not solo_rows or rows[k] < solo_rows]:
         mesh, K, b, _ = workloads.assemble(SPECS[i], ctx)
         B = yb.Batch(1, ctx)
         s = B.add(K, b, method=workloads.method(SPECS[i]))

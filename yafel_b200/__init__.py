@@ -762,6 +762,13 @@ class Server:
         check(lib().yg_server_release(self.h, int(rid)), "Server.release")
         self._keep.pop(rid, None)
 
+    def tune(self):
+        check(lib().yg_server_tune(self.h), "Server.tune")
+
+    def set_solo_rows(self, rows):
+        """Systems of at least `rows` rows are solved alone (0: batch everything)."""
+        check(lib().yg_server_set_solo_rows(self.h, int(rows)), "Server.set_solo_rows")
+
     def info(self):
         q, a, b = C.c_int64(), C.c_int64(), C.c_uint64()
         check(lib().yg_server_info(self.h, C.byref(q), C.byref(a), C.byref(b)), "Server.info")

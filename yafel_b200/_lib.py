@@ -91,6 +91,8 @@ SIGNATURES = {
     "yg_server_poll": (i32, [vp, i64, P(SolveStats)]),
     "yg_server_release": (i32, [vp, i64]),
     "yg_server_info": (i32, [vp, P(i64), P(i64), P(u64)]),
+    "yg_server_tune": (i32, [vp]),
+    "yg_server_set_solo_rows": (i32, [vp, i64]),
     "yg_batch_remove": (i32, [vp, i32]),
     "yg_batch_reset": (i32, [vp, i32]),
     "yg_batch_run": (i32, [vp, i32, P(i32)]),

@@ -10,6 +10,9 @@
 // A launch runs one block of iterations without blocking the host, which
 // builds the next admitted systems meanwhile; the following wait retires the
 // systems that finished, whose results the client then reads and releases.
+// Systems of at least `solo_rows` rows (when set) fill the GPU on their own:
+// they skip the batch and are solved one at a time, after a block, by the
+// single-system solvers (autotuned SpMV, fused iterations).
 #include "internal.h"
 
 #include <deque>
@@ -25,6 +28,11 @@ struct Request {
     int state = RQ_QUEUED;
     int32_t slot = -1;
     yg_solve_stats stats{};
+    // a system solved alone
+    yg_matrix A = nullptr;
+    yg_vector b = nullptr, x = nullptr;
+    int32_t method = 0;
+    yg_solve_opts opts{};
 };
 
 uint64_t matrix_bytes(yg_matrix A) {
@@ -47,6 +55,8 @@ struct yg_server_t {
     std::unordered_map<int64_t, Request> reqs;
     std::vector<int64_t> slot_req;   // request of each batch slot, -1 when free
     std::vector<int64_t> finished;   // retired since the last yg_server_finished
+    int64_t solo_rows = 0;           // 0: every system goes to the batch
+    std::deque<int64_t> solo;        // attached systems solved alone, in order
 };
 
 using namespace yg;
@@ -112,6 +122,22 @@ extern "C" yg_status yg_server_attach(yg_server S, int64_t id, yg_matrix A, yg_v
     if (it == S->reqs.end() || it->second.state != RQ_ADMITTED)
         return fail(YG_BAD_ARG, "yg_server_attach: request %lld is not admitted", (long long)id);
     if (S->in_flight) return fail(YG_BAD_ARG, "yg_server_attach: a block is in flight; attach after yg_server_wait");
+    if (S->solo_rows > 0 && A->rows() >= S->solo_rows) {
+        Request &q = it->second;
+        const uint64_t actual = matrix_bytes(A) + 16 * (uint64_t)A->rows() + (uint64_t)yg_batch_work_bytes(A->rows(), method);
+        S->held = S->held - q.bytes + actual;
+        q.bytes = actual;
+        q.state = RQ_RUNNING;
+        q.A = A;
+        q.b = b;
+        q.x = x;
+        q.method = method;
+        q.opts = opts ? *opts : yg_solve_opts{YG_CRIT_RELRES, YG_PREC_FP64, 1e-10, 0, 0, 0};
+        q.opts.criterion = YG_CRIT_RELRES;
+        if (method == YG_METHOD_BICGSTAB) q.opts.precision = YG_PREC_FP64;  // the single-system BiCGSTAB is FP64
+        S->solo.push_back(id);
+        return YG_OK;
+    }
     int32_t slot = -1;
     YG_TRY(yg_batch_add(S->batch, A, b, x, method, opts, &slot));
     Request &q = it->second;
@@ -155,7 +181,32 @@ extern "C" yg_status yg_server_wait(yg_server S, int32_t *n_finished) {
             ++done;
         }
     }
+    // one system solved alone per wait
+    if (!S->solo.empty()) {
+        const int64_t r = S->solo.front();
+        S->solo.pop_front();
+        Request &q = S->reqs[r];
+        yg_precond M = nullptr;
+        YG_TRY(yg_precond_create(q.A, YG_PRECOND_JACOBI, &M));
+        yg_solve_stats st{};
+        yg_status e = q.method == YG_METHOD_BICGSTAB ? yg_bicgstab(q.A, M, q.b, q.x, &q.opts, &st)
+                                                      : yg_cg(q.A, M, q.b, q.x, &q.opts, &st);
+        yg_precond_destroy(M);
+        if (e != YG_OK && e != YG_NOT_CONVERGED && e != YG_BREAKDOWN && e != YG_NAN) return e;
+        q.stats = st;
+        q.state = RQ_DONE;
+        q.A = nullptr;
+        q.b = q.x = nullptr;
+        S->finished.push_back(r);
+        ++done;
+    }
     if (n_finished) *n_finished = done;
+    return YG_OK;
+}
+
+extern "C" yg_status yg_server_set_solo_rows(yg_server S, int64_t rows) {
+    if (!S || rows < 0) return fail(YG_BAD_ARG, "yg_server_set_solo_rows: bad argument");
+    S->solo_rows = rows;
     return YG_OK;
 }
 
@@ -194,7 +245,14 @@ extern "C" yg_status yg_server_release(yg_server S, int64_t id) {
 extern "C" yg_status yg_server_info(yg_server S, int64_t *queued, int64_t *active, uint64_t *bytes_held) {
     if (!S) return fail(YG_BAD_ARG, "yg_server_info: NULL server");
     if (queued) *queued = (int64_t)S->queue.size();
-    if (active) *active = S->attached;
+    if (active) *active = S->attached + (int64_t)S->solo.size();
     if (bytes_held) *bytes_held = S->held;
     return YG_OK;
+}
+
+extern "C" yg_status yg_server_tune(yg_server S) {
+    if (!S) return fail(YG_BAD_ARG, "yg_server_tune: NULL server");
+    if (S->in_flight) return fail(YG_BAD_ARG, "yg_server_tune: a block is in flight; tune after yg_server_wait");
+    if (S->attached == 0) return YG_OK;
+    return yg_batch_tune(S->batch);
 }
