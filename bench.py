@@ -99,10 +99,13 @@ def bcsr3_spmv_bytes(nnzb, n):
     return nnzb * (8 * 9 + 4) + 4 * (nbrows + 1) + 8 * n + 8 * n
 
 
+TMA_CFG = {32: "64,3,4", 1: "32,4,8", 2: "32,3,8", 4: "32,2,8", 8: "32,3,12", 16: "48,3,8"}
+
+
 def spmv_kernel_name(K, dot=1, vt="double"):
     variant, lanes = K.get_spmv()
     if variant == 2:
-        cfg = "64,3,4" if lanes != 1 else "32,4,8"
+        cfg = TMA_CFG.get(lanes, "64,3,4")
         return "k_bcsr_spmv_tma<3,%s,%d,TmaCfg<3,%s,%s>>" % (vt, dot, vt, cfg)
     if variant == 1:
         return "k_bcsr_spmv_staged<3,%s,%d>" % (vt, dot)

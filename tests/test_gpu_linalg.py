@@ -47,7 +47,8 @@ def test_spmv_matches_oracle(ctx, B, per_row):
     x = np.random.Generator(np.random.PCG64(7)).standard_normal(A.cols())
     yo = Ao.spmv(x)
     scale = np.abs(val).max() * np.abs(x).max() * (per_row + 1) * B
-    variants = [(0, 4), (0, 32)] + ([(1, 32), (2, 32), (2, 1)] if B in (2, 3) else []) + [(-1, 32)]
+    tma = [(2, L) for L in (32, 1, 2, 4, 8, 16)]
+    variants = [(0, 4), (0, 32)] + ([(1, 32)] + tma if B in (2, 3) else []) + [(-1, 32)]
     for v, L in variants:
         A.set_spmv(v, L)
         y = A * x

@@ -482,11 +482,15 @@ extern "C" yg_status yg_matrix_set_spmv(yg_matrix A, int32_t variant, int32_t la
     if (variant == 0 && lanes == 1) return fail(YG_BAD_ARG, "flat SpMV needs 2..32 lanes");
     if (variant < 0) {  // re-run the device autotuner
         A->tuned = false;
+        A->tuned32 = false;
         return spmv_autotune_device(A);
     }
     A->variant = variant;
     A->lanes = lanes;
     A->tuned = true;
+    A->variant32 = variant;  // the same kernel for FP32 values
+    A->lanes32 = lanes;
+    A->tuned32 = true;
     return YG_OK;
 }
 
@@ -503,7 +507,7 @@ extern "C" yg_status yg_spmv_bench(yg_matrix A, yg_vector x, yg_vector y, int32_
     if (x->n != A->cols() || y->n != A->rows()) return fail(YG_BAD_ARG, "yg_spmv_bench: dimension mismatch");
     if (precision == YG_PREC_MIXED && !A->d_val32) YG_TRY(yg_matrix_make_fp32(A));
     yg_context ctx = A->ctx;
-    int grid = spmv_default_grid(A);
+    int grid = spmv_grid_for(A, precision);
     YG_TRY(spmv_launch(A, x->d, y->d, precision, nullptr, nullptr, grid));
     cudaEvent_t e0, e1;
     YG_CUDA(cudaEventCreate(&e0));

@@ -91,6 +91,8 @@ struct yg_matrix_t {
     int32_t *d_diag = nullptr;    // position of the diagonal block in each block row, -1 if absent
     int lanes = 32;               // SpMV lanes per block row (flat variant)
     int variant = 0;              // SpMV variant: 0 flat lane-strided, 1 cp.async staged, 2 TMA bulk staged (B = 2, 3)
+    int variant32 = -1, lanes32 = 32;  // choice for FP32 values (-1: as for FP64)
+    bool tuned32 = false;
     bool tuned = false;
     const void *owner = nullptr;  // dofmap whose pattern this is (assembly re-use)
     int32_t owner_format = -1;
@@ -127,6 +129,7 @@ yg_status spmv_launch(yg_matrix A, const double *x, double *y, int precision, do
 yg_status spmv_launch_ex(yg_matrix A, const double *x, double *y, int precision, const double *w, double *partials,
                          int dot_mode, const int32_t *flag, int grid);
 int spmv_default_grid(yg_matrix A);
+int spmv_grid_for(yg_matrix A, int precision);
 void spmv_autotune(yg_matrix A);
 yg_status spmv_autotune_device(yg_matrix A);
 yg_status vector_dot(yg_context ctx, const double *a, const double *b, int64_t n, double *out);

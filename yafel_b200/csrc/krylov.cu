@@ -334,7 +334,7 @@ static yg_status pcg_core(yg_matrix A, yg_precond M, const double *b, double *x,
     const bool fused = !M || precond_fusable(M);
     const double *dinv = M ? precond_dinv(M) : nullptr;
     const int G = ctx->reduce_blocks;
-    const int spmv_grid = std::min(spmv_default_grid(A), kMaxReduceBlocks);
+    const int spmv_grid = std::min(spmv_grid_for(A, precision), kMaxReduceBlocks);
     double *P = ctx->d_partials;  // [0,G): p.q ; [2G,4G): r.z/r.r pairs ; [4G, 7G): init triples
     KrylovScalars *S = ctx->d_scalars;
     cudaStream_t st = ctx->stream;
@@ -480,6 +480,7 @@ yg_status solve_cg(yg_matrix A, yg_precond M, yg_vector bv, yg_vector xv, const 
         // FP64, or FP32 matrix values in the iteration with the residual replaced
         // by the FP64 true residual each time it fell 10x (refinement steps).
         if (o.precision == YG_PREC_MIXED && !A->d_val32) YG_TRY(yg_matrix_make_fp32(A));
+        YG_TRY(spmv_autotune_device(A));  // the FP32-value kernel has its own tuning
         int64_t repl = 0;
         YG_TRY(pcg_core(A, M, bv->d, xv->d, o.precision, o.criterion, o.tol, maxiter, m, w, &its, &flag, &prof,
                         &repl));
@@ -490,6 +491,7 @@ yg_status solve_cg(yg_matrix A, yg_precond M, yg_vector bv, yg_vector xv, const 
         // SpMV reads FP32 values (FP64 vectors and accumulation).  Outer residuals
         // and the final check are FP64.
         if (!A->d_val32) YG_TRY(yg_matrix_make_fp32(A));
+        YG_TRY(spmv_autotune_device(A));
         YG_TRY(alloc_vec(ctx, &w.d, n));
         YG_TRY(alloc_vec(ctx, &w.t, n));
         double bnorm = 0;

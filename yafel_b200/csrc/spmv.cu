@@ -447,33 +447,60 @@ static yg_status launch_tma_cfg(yg_matrix A, const VT *val, const double *x, dou
     return YG_OK;
 }
 
-// TMA configurations (chunk blocks, ring depth, warps per CTA) the autotuner tries.
-template <int B, typename VT>
-using TmaA = TmaCfg<B, VT, 64, 3, 4>;
-template <int B, typename VT>
-using TmaB = TmaCfg<B, VT, 32, 4, 8>;
+// TMA configurations (chunk blocks, ring depth, warps per CTA) the autotuner
+// tries, selected by the `lanes` field of a variant-2 matrix.
+template <int B, typename VT> using TmaL32 = TmaCfg<B, VT, 64, 3, 4>;
+template <int B, typename VT> using TmaL1 = TmaCfg<B, VT, 32, 4, 8>;
+template <int B, typename VT> using TmaL2 = TmaCfg<B, VT, 32, 3, 8>;
+template <int B, typename VT> using TmaL4 = TmaCfg<B, VT, 32, 2, 8>;
+template <int B, typename VT> using TmaL8 = TmaCfg<B, VT, 32, 3, 12>;
+template <int B, typename VT> using TmaL16 = TmaCfg<B, VT, 48, 3, 8>;
 
 template <int B, typename VT, int DOT>
-static yg_status launch_tma(yg_matrix A, const VT *val, const double *x, double *y, const double *w, double *partials,
-                            const int32_t *flag, int grid, cudaStream_t st) {
-    if (A->lanes == 1) return launch_tma_cfg<B, VT, DOT, TmaB<B, VT>>(A, val, x, y, w, partials, flag, grid, st);
-    return launch_tma_cfg<B, VT, DOT, TmaA<B, VT>>(A, val, x, y, w, partials, flag, grid, st);
+static yg_status launch_tma(yg_matrix A, int lanes, const VT *val, const double *x, double *y, const double *w,
+                            double *partials, const int32_t *flag, int grid, cudaStream_t st) {
+    switch (lanes) {
+    case 1: return launch_tma_cfg<B, VT, DOT, TmaL1<B, VT>>(A, val, x, y, w, partials, flag, grid, st);
+    case 2: return launch_tma_cfg<B, VT, DOT, TmaL2<B, VT>>(A, val, x, y, w, partials, flag, grid, st);
+    case 4: return launch_tma_cfg<B, VT, DOT, TmaL4<B, VT>>(A, val, x, y, w, partials, flag, grid, st);
+    case 8: return launch_tma_cfg<B, VT, DOT, TmaL8<B, VT>>(A, val, x, y, w, partials, flag, grid, st);
+    case 16: return launch_tma_cfg<B, VT, DOT, TmaL16<B, VT>>(A, val, x, y, w, partials, flag, grid, st);
+    default: return launch_tma_cfg<B, VT, DOT, TmaL32<B, VT>>(A, val, x, y, w, partials, flag, grid, st);
+    }
 }
 
-// CTAs per SM and warps per CTA of a TMA configuration (for the grid size).
-static void tma_shape(yg_matrix A, int *ctas_per_sm, int *warps) {
-    int smem, wp;
-    const bool f32 = false;
-    (void)f32;
+template <typename C>
+static void shape_of(int *smem, int *warps) {
+    *smem = C::SMEM;
+    *warps = C::WARPS;
+}
+template <int B, typename VT>
+static void tma_shape_bv(int lanes, int *smem, int *wp) {
+    switch (lanes) {
+    case 1: shape_of<TmaL1<B, VT>>(smem, wp); break;
+    case 2: shape_of<TmaL2<B, VT>>(smem, wp); break;
+    case 4: shape_of<TmaL4<B, VT>>(smem, wp); break;
+    case 8: shape_of<TmaL8<B, VT>>(smem, wp); break;
+    case 16: shape_of<TmaL16<B, VT>>(smem, wp); break;
+    default: shape_of<TmaL32<B, VT>>(smem, wp); break;
+    }
+}
+
+// CTAs per SM and warps per CTA of a TMA configuration (for the grid size): as
+// many CTAs as the shared memory holds, at most 64 warps and 8 CTAs per SM (the
+// Krylov kernels reserve 8 partial sums per SM for the SpMV).
+static void tma_shape(yg_matrix A, int lanes, bool f32, int *ctas_per_sm, int *warps) {
+    int smem = 0, wp = 1;
     if (A->block == 3) {
-        smem = A->lanes == 1 ? TmaB<3, double>::SMEM : TmaA<3, double>::SMEM;
-        wp = A->lanes == 1 ? TmaB<3, double>::WARPS : TmaA<3, double>::WARPS;
+        if (f32) tma_shape_bv<3, float>(lanes, &smem, &wp);
+        else tma_shape_bv<3, double>(lanes, &smem, &wp);
     } else {
-        smem = A->lanes == 1 ? TmaB<2, double>::SMEM : TmaA<2, double>::SMEM;
-        wp = A->lanes == 1 ? TmaB<2, double>::WARPS : TmaA<2, double>::WARPS;
+        if (f32) tma_shape_bv<2, float>(lanes, &smem, &wp);
+        else tma_shape_bv<2, double>(lanes, &smem, &wp);
     }
     int per = (220 * 1024) / (smem + 1024);
-    if (per > 32 / wp * 2) per = 64 / wp;
+    if (per * wp > 64) per = 64 / wp;
+    if (per > 8) per = 8;
     *ctas_per_sm = per < 1 ? 1 : per;
     *warps = wp;
 }
@@ -494,9 +521,9 @@ static yg_status launch_staged(yg_matrix A, const VT *val, const double *x, doub
 }
 
 template <int B, typename VT, int DOT>
-static yg_status launch_l(yg_matrix A, const VT *val, const double *x, double *y, const double *w, double *partials,
-                          const int32_t *flag, int grid, cudaStream_t st) {
-    switch (A->lanes) {
+static yg_status launch_l(yg_matrix A, int lanes, const VT *val, const double *x, double *y, const double *w,
+                          double *partials, const int32_t *flag, int grid, cudaStream_t st) {
+    switch (lanes) {
     case 2: k_bcsr_spmv<B, 2, VT, DOT><<<grid, kThreads, 0, st>>>(A->nbrows, A->d_rowptr, A->d_col, val, x, y, w, partials, flag); break;
     case 4: k_bcsr_spmv<B, 4, VT, DOT><<<grid, kThreads, 0, st>>>(A->nbrows, A->d_rowptr, A->d_col, val, x, y, w, partials, flag); break;
     case 8: k_bcsr_spmv<B, 8, VT, DOT><<<grid, kThreads, 0, st>>>(A->nbrows, A->d_rowptr, A->d_col, val, x, y, w, partials, flag); break;
@@ -508,26 +535,39 @@ static yg_status launch_l(yg_matrix A, const VT *val, const double *x, double *y
 }
 
 template <typename VT, int DOT>
-static yg_status launch_b(yg_matrix A, const VT *val, const double *x, double *y, const double *w, double *partials,
-                          const int32_t *flag, int grid, cudaStream_t st) {
-    if (A->variant == 2 && A->block == 3) return launch_tma<3, VT, DOT>(A, val, x, y, w, partials, flag, grid, st);
-    if (A->variant == 2 && A->block == 2) return launch_tma<2, VT, DOT>(A, val, x, y, w, partials, flag, grid, st);
-    if (A->variant == 1 && A->block == 3) return launch_staged<3, VT, DOT>(A, val, x, y, w, partials, flag, grid, st);
-    if (A->variant == 1 && A->block == 2) return launch_staged<2, VT, DOT>(A, val, x, y, w, partials, flag, grid, st);
+static yg_status launch_b(yg_matrix A, int variant, int lanes, const VT *val, const double *x, double *y,
+                          const double *w, double *partials, const int32_t *flag, int grid, cudaStream_t st) {
+    if (variant == 2 && A->block == 3) return launch_tma<3, VT, DOT>(A, lanes, val, x, y, w, partials, flag, grid, st);
+    if (variant == 2 && A->block == 2) return launch_tma<2, VT, DOT>(A, lanes, val, x, y, w, partials, flag, grid, st);
+    if (variant == 1 && A->block == 3) return launch_staged<3, VT, DOT>(A, val, x, y, w, partials, flag, grid, st);
+    if (variant == 1 && A->block == 2) return launch_staged<2, VT, DOT>(A, val, x, y, w, partials, flag, grid, st);
     switch (A->block) {
-    case 1: return launch_l<1, VT, DOT>(A, val, x, y, w, partials, flag, grid, st);
-    case 2: return launch_l<2, VT, DOT>(A, val, x, y, w, partials, flag, grid, st);
-    case 3: return launch_l<3, VT, DOT>(A, val, x, y, w, partials, flag, grid, st);
+    case 1: return launch_l<1, VT, DOT>(A, lanes, val, x, y, w, partials, flag, grid, st);
+    case 2: return launch_l<2, VT, DOT>(A, lanes, val, x, y, w, partials, flag, grid, st);
+    case 3: return launch_l<3, VT, DOT>(A, lanes, val, x, y, w, partials, flag, grid, st);
     default: return fail(YG_UNSUPPORTED, "SpMV block size %d not supported (1, 2, 3)", A->block);
     }
 }
 
 template <typename VT>
-static yg_status launch_v(yg_matrix A, const VT *val, const double *x, double *y, const double *w, double *partials,
-                          int dot_mode, const int32_t *flag, int grid, cudaStream_t st) {
-    if (dot_mode == 0) return launch_b<VT, 0>(A, val, x, y, w, partials, flag, grid, st);
-    if (dot_mode == 1) return launch_b<VT, 1>(A, val, x, y, w, partials, flag, grid, st);
-    return launch_b<VT, 2>(A, val, x, y, w, partials, flag, grid, st);
+static yg_status launch_v(yg_matrix A, int variant, int lanes, const VT *val, const double *x, double *y,
+                          const double *w, double *partials, int dot_mode, const int32_t *flag, int grid,
+                          cudaStream_t st) {
+    if (dot_mode == 0) return launch_b<VT, 0>(A, variant, lanes, val, x, y, w, partials, flag, grid, st);
+    if (dot_mode == 1) return launch_b<VT, 1>(A, variant, lanes, val, x, y, w, partials, flag, grid, st);
+    return launch_b<VT, 2>(A, variant, lanes, val, x, y, w, partials, flag, grid, st);
+}
+
+// The kernel choice for a precision: FP32-value SpMVs have their own tuning.
+static void choice(yg_matrix A, int precision, int *variant, int *lanes) {
+    const bool f32 = precision == YG_PREC_MIXED || precision == YG_PREC_MIXED_IR;
+    if (f32 && A->variant32 >= 0) {
+        *variant = A->variant32;
+        *lanes = A->lanes32;
+    } else {
+        *variant = A->variant;
+        *lanes = A->lanes;
+    }
 }
 
 // y = A x.  With `partials`: per-block sums of w.y (dot_mode 1; w defaults to
@@ -540,11 +580,13 @@ yg_status spmv_launch_ex(yg_matrix A, const double *x, double *y, int precision,
     if (!partials) dot_mode = 0;
     if (!w) w = x;
     yg_status s;
+    int variant, lanes;
+    choice(A, precision, &variant, &lanes);
     if (precision == YG_PREC_MIXED || precision == YG_PREC_MIXED_IR) {
         if (!A->d_val32) return fail(YG_BAD_ARG, "mixed-precision SpMV without FP32 values");
-        s = launch_v<float>(A, A->d_val32, x, y, w, partials, dot_mode, flag, grid, st);
+        s = launch_v<float>(A, variant, lanes, A->d_val32, x, y, w, partials, dot_mode, flag, grid, st);
     } else {
-        s = launch_v<double>(A, A->d_val, x, y, w, partials, dot_mode, flag, grid, st);
+        s = launch_v<double>(A, variant, lanes, A->d_val, x, y, w, partials, dot_mode, flag, grid, st);
     }
     if (s != YG_OK) return s;
     YG_CUDA(cudaGetLastError());
@@ -556,16 +598,21 @@ yg_status spmv_launch(yg_matrix A, const double *x, double *y, int precision, do
     return spmv_launch_ex(A, x, y, precision, x, partials, partials ? 1 : 0, flag, grid);
 }
 
-int spmv_default_grid(yg_matrix A) {
-    if (A->variant == 2) {  // TMA: as many CTAs as fit, a warp per row
+int spmv_default_grid(yg_matrix A) { return spmv_grid_for(A, YG_PREC_FP64); }
+
+int spmv_grid_for(yg_matrix A, int precision) {
+    int variant, lanes;
+    choice(A, precision, &variant, &lanes);
+    const bool f32 = precision == YG_PREC_MIXED || precision == YG_PREC_MIXED_IR;
+    if (variant == 2) {  // TMA: as many CTAs as fit, a warp per row
         int per, wp;
-        tma_shape(A, &per, &wp);
+        tma_shape(A, lanes, f32, &per, &wp);
         int64_t need = (A->nbrows + wp - 1) / wp;
         int64_t g = (int64_t)A->ctx->num_sms * per;
         if (need < g) g = need;
         return (int)(g < 1 ? 1 : g);
     }
-    if (A->variant == 1) {  // staged: 3 blocks of 4 warps per SM, a warp per row
+    if (variant == 1) {  // staged: 3 blocks of 4 warps per SM, a warp per row
         int64_t need = (A->nbrows + 3) / 4;
         int64_t g = (int64_t)A->ctx->num_sms * 3;
         if (need < g) g = need;
@@ -573,7 +620,7 @@ int spmv_default_grid(yg_matrix A) {
     }
     // enough resident warps to keep HBM busy: 8 blocks of 256 threads per SM,
     // but no more row groups than rows.
-    int64_t groups_per_block = kThreads / A->lanes;
+    int64_t groups_per_block = kThreads / lanes;
     int64_t need = (A->nbrows + groups_per_block - 1) / groups_per_block;
     int64_t g = (int64_t)A->ctx->num_sms * 8;
     if (need < g) g = need;
@@ -600,31 +647,16 @@ void spmv_autotune(yg_matrix A) {
 // matrix of the same pattern reuses the choice without timing again.
 struct TuneKey {
     int64_t nbrows, nnzb;
-    int block;
-    bool operator==(const TuneKey &o) const { return nbrows == o.nbrows && nnzb == o.nnzb && block == o.block; }
+    int block, f32;
+    bool operator==(const TuneKey &o) const {
+        return nbrows == o.nbrows && nnzb == o.nnzb && block == o.block && f32 == o.f32;
+    }
 };
 static std::vector<std::pair<TuneKey, std::pair<int, int>>> g_tune_cache;
 
-yg_status spmv_autotune_device(yg_matrix A) {
-    if (A->tuned) return YG_OK;
-    const TuneKey key{A->nbrows, A->nnzb, A->block};
-    for (const auto &kv : g_tune_cache)
-        if (kv.first == key) {
-            A->variant = kv.second.first;
-            A->lanes = kv.second.second;
-            A->tuned = true;
-            return YG_OK;
-        }
+// Time every candidate for one precision on this matrix; returns the fastest.
+static yg_status tune_precision(yg_matrix A, int precision, double *x, double *y, int *best_variant, int *best_lanes) {
     yg_context ctx = A->ctx;
-    cudaStreamCaptureStatus cs;
-    YG_CUDA(cudaStreamIsCapturing(ctx->stream, &cs));
-    if (cs != cudaStreamCaptureStatusNone) return YG_OK;
-    const int64_t n = A->rows(), m = A->cols();
-    double *x = nullptr, *y = nullptr;
-    YG_TRY(dev_alloc_t(ctx, &x, m + 1));
-    yg_status s = dev_alloc_t(ctx, &y, n + 1);
-    if (s != YG_OK) { dev_free(ctx, x); return s; }
-    cudaMemsetAsync(x, 0, sizeof(double) * (m + 1), ctx->stream);
     struct Cand { int variant, lanes; };
     std::vector<Cand> cands;
     double per_row = A->nbrows ? (double)A->nnzb * A->block * A->block / (double)A->nbrows : 1.0;
@@ -632,22 +664,25 @@ yg_status spmv_autotune_device(yg_matrix A) {
         if (L <= 4 * per_row + 4) cands.push_back({0, L});
     if (A->block == 2 || A->block == 3) {
         cands.push_back({1, 32});
-        cands.push_back({2, 32});  // TMA, 64-block chunks, 3 stages, 4 warps
-        cands.push_back({2, 1});   // TMA, 32-block chunks, 4 stages, 8 warps
+        for (int L : {32, 1, 2, 4, 8, 16}) cands.push_back({2, L});  // TMA configurations
     }
+    const bool f32 = precision != YG_PREC_FP64;
+    int *pv = f32 ? &A->variant32 : &A->variant, *pl = f32 ? &A->lanes32 : &A->lanes;
+    const int save_v = *pv, save_l = *pl;
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     float best = 1e30f;
     Cand bestc = {A->variant, A->lanes};
+    yg_status s = YG_OK;
     const int reps = 3;
     for (const Cand &c : cands) {
-        A->variant = c.variant;
-        A->lanes = c.lanes;
-        int grid = spmv_default_grid(A);
-        if ((s = spmv_launch(A, x, y, YG_PREC_FP64, nullptr, nullptr, grid)) != YG_OK) break;  // warm-up
+        *pv = c.variant;
+        *pl = c.lanes;
+        const int grid = spmv_grid_for(A, precision);
+        if ((s = spmv_launch(A, x, y, precision, nullptr, nullptr, grid)) != YG_OK) break;  // warm-up
         cudaEventRecord(e0, ctx->stream);
-        for (int r = 0; r < reps; ++r) spmv_launch(A, x, y, YG_PREC_FP64, nullptr, nullptr, grid);
+        for (int r = 0; r < reps; ++r) spmv_launch(A, x, y, precision, nullptr, nullptr, grid);
         cudaEventRecord(e1, ctx->stream);
         cudaEventSynchronize(e1);
         float ms = 0;
@@ -656,13 +691,65 @@ yg_status spmv_autotune_device(yg_matrix A) {
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    A->variant = bestc.variant;
-    A->lanes = bestc.lanes;
-    A->tuned = true;
-    if (s == YG_OK) g_tune_cache.push_back({key, {bestc.variant, bestc.lanes}});
-    dev_free(ctx, x);
-    dev_free(ctx, y);
-    if (s != YG_OK) return s;
+    *pv = save_v;
+    *pl = save_l;
+    *best_variant = bestc.variant;
+    *best_lanes = bestc.lanes;
+    return s;
+}
+
+// Device autotuner: time each candidate (flat with 2..32 lanes, cp.async
+// staged and six TMA configurations for 2x2 and 3x3 blocks) on this matrix with
+// CUDA events and keep the fastest, separately for FP64 values and, when the
+// matrix has them, FP32 values.  Must not run during stream capture.  Results
+// are cached per (rows, blocks, block size, precision): a re-assembled matrix of
+// the same pattern reuses the choice without timing again.
+yg_status spmv_autotune_device(yg_matrix A) {
+    const bool need64 = !A->tuned, need32 = A->d_val32 && !A->tuned32;
+    if (!need64 && !need32) return YG_OK;
+    yg_context ctx = A->ctx;
+    cudaStreamCaptureStatus cs;
+    YG_CUDA(cudaStreamIsCapturing(ctx->stream, &cs));
+    if (cs != cudaStreamCaptureStatusNone) return YG_OK;
+    double *x = nullptr, *y = nullptr;
+    bool allocated = false;
+    for (int f32 = 0; f32 <= 1; ++f32) {
+        if (f32 ? !need32 : !need64) continue;
+        const TuneKey key{A->nbrows, A->nnzb, A->block, f32};
+        bool hit = false;
+        for (const auto &kv : g_tune_cache)
+            if (kv.first == key) {
+                (f32 ? A->variant32 : A->variant) = kv.second.first;
+                (f32 ? A->lanes32 : A->lanes) = kv.second.second;
+                hit = true;
+                break;
+            }
+        if (!hit) {
+            if (!allocated) {
+                const int64_t n = A->rows(), m = A->cols();
+                YG_TRY(dev_alloc_t(ctx, &x, m + 1));
+                yg_status s = dev_alloc_t(ctx, &y, n + 1);
+                if (s != YG_OK) { dev_free(ctx, x); return s; }
+                cudaMemsetAsync(x, 0, sizeof(double) * (m + 1), ctx->stream);
+                allocated = true;
+            }
+            int v = 0, l = 32;
+            yg_status s = tune_precision(A, f32 ? YG_PREC_MIXED : YG_PREC_FP64, x, y, &v, &l);
+            if (s != YG_OK) {
+                dev_free(ctx, x);
+                dev_free(ctx, y);
+                return s;
+            }
+            (f32 ? A->variant32 : A->variant) = v;
+            (f32 ? A->lanes32 : A->lanes) = l;
+            g_tune_cache.push_back({key, {v, l}});
+        }
+        (f32 ? A->tuned32 : A->tuned) = true;
+    }
+    if (allocated) {
+        dev_free(ctx, x);
+        dev_free(ctx, y);
+    }
     YG_CUDA(cudaGetLastError());
     return YG_OK;
 }
