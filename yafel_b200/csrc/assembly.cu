@@ -614,26 +614,36 @@ __global__ void k_sub_inplace(int64_t n, double *__restrict__ rhs, const double 
 
 // Zero BC rows and columns, unit diagonal and rhs_r = g_r on BC rows
 // (DirichletBC.cpp:137-149).  One thread per scalar row.
+// Zero the rows and columns of the Dirichlet dofs (mask) and put 1 on their
+// diagonal with rhs = g there (DirichletBC.cpp:58-89).  One warp per block row,
+// lanes over its blocks (coalesced column reads); only masked entries are written.
 __global__ void k_bc_zero(int64_t nbrows, int B, const int32_t *__restrict__ rp, const int32_t *__restrict__ col,
                           double *__restrict__ val, const uint8_t *__restrict__ mask, const double *__restrict__ g,
                           double *__restrict__ rhs) {
-    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < nbrows * B; r += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t I = r / B;
-        const int i = (int)(r % B);
-        const bool mr = mask[r];
-        for (int32_t k = rp[I]; k < rp[I + 1]; ++k) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t I = warp; I < nbrows; I += nwarps) {
+        int mr = 0;  // bit i: scalar row I*B+i is a Dirichlet row
+        for (int i = 0; i < B; ++i) mr |= mask[I * B + i] ? (1 << i) : 0;
+        const int32_t k0 = rp[I], k1 = rp[I + 1];
+        for (int32_t k = k0 + lane; k < k1; k += 32) {
             const int64_t J = col[k];
-            for (int j = 0; j < B; ++j) {
-                const int64_t c = J * B + j;
-                if (mr || mask[c]) {
+            int mc = 0;
+            for (int j = 0; j < B; ++j) mc |= mask[J * B + j] ? (1 << j) : 0;
+            if (!mr && !mc) continue;
+            for (int i = 0; i < B; ++i)
+                for (int j = 0; j < B; ++j) {
+                    if (!((mr >> i) & 1) && !((mc >> j) & 1)) continue;
+                    const int64_t r = I * B + i, c = J * B + j;
                     double *v = &val[(int64_t)k * B * B + i * B + j];
-                    *v = 0;
                     if (r == c) {
                         rhs[r] = g[c];
                         *v = 1;
+                    } else {
+                        *v = 0;
                     }
                 }
-            }
         }
     }
 }
@@ -785,37 +795,60 @@ extern "C" yg_status yg_dirichlet_apply(yg_matrix K, yg_vector rhs, const int64_
         if (bc_dofs[i] < 0 || bc_dofs[i] >= K->rows()) return fail(YG_BAD_ARG, "BC dof %lld out of range", (long long)bc_dofs[i]);
     yg_context ctx = K->ctx;
     const int64_t n = K->rows();
-    uint8_t *mask = nullptr;
-    double *g = nullptr, *q = nullptr, *vals = nullptr;
-    int64_t *dofs = nullptr;
-    yg_status s;
-    auto cleanup = [&]() { dev_free(ctx, mask); dev_free(ctx, g); dev_free(ctx, q); dev_free(ctx, dofs); dev_free(ctx, vals); };
-    if ((s = dev_alloc_t(ctx, &mask, n)) != YG_OK || (s = dev_alloc_t(ctx, &g, n)) != YG_OK ||
-        (s = dev_alloc_t(ctx, &q, n)) != YG_OK || (s = dev_alloc_t(ctx, &dofs, n_bc + 1)) != YG_OK ||
-        (s = dev_alloc_t(ctx, &vals, n_bc + 1)) != YG_OK) {
-        cleanup();
-        return s;
+    // scratch kept on the matrix between calls
+    if (!K->d_bcmask) {
+        yg_status s;
+        if ((s = dev_alloc_t(ctx, &K->d_bcmask, n)) != YG_OK || (s = dev_alloc_t(ctx, &K->d_bcg, n)) != YG_OK ||
+            (s = dev_alloc_t(ctx, &K->d_bcq, n)) != YG_OK)
+            return s;
     }
+    if (n_bc > K->bc_cap) {
+        YG_CUDA(cudaStreamSynchronize(ctx->stream));
+        dev_free(ctx, K->d_bcdofs);
+        dev_free(ctx, K->d_bcvals);
+        K->d_bcdofs = nullptr;
+        K->d_bcvals = nullptr;
+        K->bc_cap = 0;
+        const int64_t cap = n_bc + n_bc / 2 + 16;
+        YG_TRY(dev_alloc_t(ctx, &K->d_bcdofs, cap));
+        YG_TRY(dev_alloc_t(ctx, &K->d_bcvals, cap));
+        K->bc_cap = cap;
+    }
+    bool homogeneous = true;
+    for (int64_t i = 0; i < n_bc && homogeneous; ++i) homogeneous = bc_values[i] == 0.0;
+    uint8_t *mask = K->d_bcmask;
+    double *g = K->d_bcg, *q = K->d_bcq;
     cudaStream_t st = ctx->stream;
     cudaMemsetAsync(mask, 0, n, st);
     cudaMemsetAsync(g, 0, sizeof(double) * n, st);
-    cudaMemcpyAsync(dofs, bc_dofs, sizeof(int64_t) * n_bc, cudaMemcpyHostToDevice, st);
-    cudaMemcpyAsync(vals, bc_values, sizeof(double) * n_bc, cudaMemcpyHostToDevice, st);
+    yg_status s = YG_OK;
     if (n_bc) {
-        k_bc_scatter<<<stream_grid(ctx, n_bc), kThreads, 0, st>>>(n_bc, dofs, vals, mask, g);
+        // the host arrays are pageable: the copies complete before the call returns
+        YG_CUDA(cudaMemcpyAsync(K->d_bcdofs, bc_dofs, sizeof(int64_t) * n_bc, cudaMemcpyHostToDevice, st));
+        YG_CUDA(cudaMemcpyAsync(K->d_bcvals, bc_values, sizeof(double) * n_bc, cudaMemcpyHostToDevice, st));
+        k_bc_scatter<<<stream_grid(ctx, n_bc), kThreads, 0, st>>>(n_bc, K->d_bcdofs, K->d_bcvals, mask, g);
         YG_LAUNCHED(ctx);
     }
-    s = spmv_launch(K, g, q, YG_PREC_FP64, nullptr, nullptr, spmv_default_grid(K));
-    if (s == YG_OK) {
-        k_sub_inplace<<<stream_grid(ctx, n), kThreads, 0, st>>>(n, rhs->d, q);
-        YG_LAUNCHED(ctx);
-        k_bc_zero<<<stream_grid(ctx, n), kThreads, 0, st>>>(K->nbrows, K->block, K->d_rowptr, K->d_col, K->d_val, mask,
-                                                             g, rhs->d);
-        YG_LAUNCHED(ctx);
-        if (K->d_val32) s = yg_matrix_make_fp32(K);
+    // F -= K g (skipped when every prescribed value is 0: K g = 0)
+    if (!homogeneous) {
+        s = spmv_launch(K, g, q, YG_PREC_FP64, nullptr, nullptr, spmv_default_grid(K));
+        if (s == YG_OK) {
+            k_sub_inplace<<<stream_grid(ctx, n), kThreads, 0, st>>>(n, rhs->d, q);
+            YG_LAUNCHED(ctx);
+        }
     }
+    if (s == YG_OK && n_bc) {
+        const int64_t warps_needed = K->nbrows;
+        int64_t blocks = (warps_needed * 32 + kThreads - 1) / kThreads;
+        const int64_t cap = (int64_t)ctx->num_sms * 16;
+        if (blocks > cap) blocks = cap;
+        if (blocks < 1) blocks = 1;
+        k_bc_zero<<<(int)blocks, kThreads, 0, st>>>(K->nbrows, K->block, K->d_rowptr, K->d_col, K->d_val, mask, g,
+                                                    rhs->d);
+        YG_LAUNCHED(ctx);
+    }
+    if (s == YG_OK && K->d_val32) s = yg_matrix_make_fp32(K);
     cudaError_t e = cudaStreamSynchronize(st);
-    cleanup();
     if (s != YG_OK) return s;
     if (e != cudaSuccess) return fail(YG_CUDA_ERROR, "Dirichlet apply: %s", cudaGetErrorString(e));
     return YG_OK;

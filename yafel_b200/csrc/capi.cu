@@ -32,17 +32,49 @@ yg_status fail(yg_status s, const char *fmt, ...) {
     return s;
 }
 
+// Blocks of at most kCacheBlock bytes are kept after release, up to kCacheTotal
+// bytes per context, and handed out again for an allocation of the same size:
+// solver work vectors, iterates and Dirichlet scratch are allocated and freed on
+// every solve, and cudaMalloc / cudaFree would otherwise map pages and
+// synchronise the device each time.
+constexpr size_t kCacheBlock = 256ull << 20, kCacheTotal = 2ull << 30;
+
+void flush_alloc_cache(yg_context ctx) {
+    for (auto &kv : ctx->cache) {
+        cudaEventSynchronize(kv.second.ev);
+        cudaEventDestroy(kv.second.ev);
+        cudaFree(kv.second.p);
+    }
+    ctx->cache.clear();
+    ctx->cached_bytes = 0;
+}
+
 yg_status dev_alloc(yg_context ctx, void **p, size_t bytes) {
     *p = nullptr;
     if (bytes == 0) bytes = 16;
     if (ctx->budget && ctx->in_use + bytes > ctx->budget)
         return fail(YG_OVER_BUDGET, "allocation of %zu bytes exceeds the HBM budget (%llu of %llu in use)",
                     bytes, (unsigned long long)ctx->in_use, (unsigned long long)ctx->budget);
-    cudaError_t e = cudaMalloc(p, bytes);
-    if (e != cudaSuccess) {
-        cudaGetLastError();
-        *p = nullptr;
-        return fail(YG_OUT_OF_MEMORY, "cudaMalloc(%zu) failed: %s", bytes, cudaGetErrorString(e));
+    auto hit = ctx->cache.find(bytes);
+    if (hit != ctx->cache.end()) {
+        yg_context_t::CachedBlock b = hit->second;
+        ctx->cache.erase(hit);
+        ctx->cached_bytes -= bytes;
+        cudaEventSynchronize(b.ev);
+        cudaEventDestroy(b.ev);
+        *p = b.p;
+    } else {
+        cudaError_t e = cudaMalloc(p, bytes);
+        if (e != cudaSuccess && !ctx->cache.empty()) {  // give the cached blocks back and retry
+            cudaGetLastError();
+            flush_alloc_cache(ctx);
+            e = cudaMalloc(p, bytes);
+        }
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            *p = nullptr;
+            return fail(YG_OUT_OF_MEMORY, "cudaMalloc(%zu) failed: %s", bytes, cudaGetErrorString(e));
+        }
     }
     ctx->in_use += bytes;
     ctx->allocs[*p] = bytes;
@@ -52,9 +84,23 @@ yg_status dev_alloc(yg_context ctx, void **p, size_t bytes) {
 void dev_free(yg_context ctx, void *p) {
     if (!p) return;
     auto it = ctx->allocs.find(p);
+    size_t bytes = 0;
     if (it != ctx->allocs.end()) {
-        ctx->in_use -= it->second;
+        bytes = it->second;
+        ctx->in_use -= bytes;
         ctx->allocs.erase(it);
+    }
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(ctx->stream, &cs);
+    if (bytes && bytes <= kCacheBlock && ctx->cached_bytes + bytes <= kCacheTotal && cs == cudaStreamCaptureStatusNone) {
+        cudaEvent_t ev;
+        if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) == cudaSuccess) {
+            cudaEventRecord(ev, ctx->stream);
+            ctx->cache.insert({bytes, {p, ev}});
+            ctx->cached_bytes += bytes;
+            return;
+        }
+        cudaGetLastError();
     }
     cudaFree(p);
 }
@@ -232,6 +278,7 @@ extern "C" yg_status yg_context_destroy(yg_context ctx) {
     if (!ctx) return YG_OK;
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    flush_alloc_cache(ctx);
     for (auto &kv : ctx->allocs) cudaFree(kv.first);
     ctx->allocs.clear();
     if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
@@ -418,6 +465,8 @@ extern "C" yg_status yg_matrix_destroy(yg_matrix A) {
     dev_free(ctx, A->d_val);
     dev_free(ctx, A->d_val32);
     dev_free(ctx, A->d_diag);
+    for (void *p : {(void *)A->d_bcmask, (void *)A->d_bcg, (void *)A->d_bcq, (void *)A->d_bcvals, (void *)A->d_bcdofs})
+        dev_free(ctx, p);
     delete A;
     return YG_OK;
 }

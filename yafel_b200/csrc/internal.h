@@ -9,6 +9,7 @@
 #include <string>
 #include <vector>
 #include <unordered_map>
+#include <map>
 
 namespace yg {
 
@@ -64,6 +65,14 @@ struct yg_context_t {
     uint64_t in_use = 0;
     int64_t launches = 0;
     std::unordered_map<void *, size_t> allocs;
+    // freed blocks kept for reuse (exact size), each with an event recorded on the
+    // stream at its release: a reuse waits for the work that used it before
+    struct CachedBlock {
+        void *p;
+        cudaEvent_t ev;
+    };
+    std::multimap<size_t, CachedBlock> cache;
+    size_t cached_bytes = 0;
     // reduction scratch (device) and pinned host mailbox
     double *d_partials = nullptr;   // 8 * kMaxReduceBlocks doubles
     double *h_pinned = nullptr;     // 64 doubles of pinned host memory
@@ -96,6 +105,12 @@ struct yg_matrix_t {
     bool tuned = false;
     const void *owner = nullptr;  // dofmap whose pattern this is (assembly re-use)
     int32_t owner_format = -1;
+    // Dirichlet scratch, kept between calls: row/column mask, prescribed values
+    // g, K g, and the staged dof / value lists (bc_cap entries)
+    uint8_t *d_bcmask = nullptr;
+    double *d_bcg = nullptr, *d_bcq = nullptr, *d_bcvals = nullptr;
+    int64_t *d_bcdofs = nullptr;
+    int64_t bc_cap = 0;
     int64_t rows() const { return nbrows * block; }
     int64_t cols() const { return nbcols * block; }
 };
@@ -135,6 +150,7 @@ yg_status spmv_autotune_device(yg_matrix A);
 yg_status vector_dot(yg_context ctx, const double *a, const double *b, int64_t n, double *out);
 yg_status check_device_error(yg_context ctx);
 yg_status matrix_build_diag(yg_matrix A);
+void flush_alloc_cache(yg_context ctx);
 // batch engine, host side (batch.cu)
 bool batch_slot_running(yg_batch bt, int32_t slot);
 void batch_slot_stats(yg_batch bt, int32_t slot, yg_solve_stats *out);
