@@ -40,7 +40,8 @@ def _newest(paths):
 
 
 def _compile(src, obj, extra):
-    cmd = [nvcc()] + ARCH + NVCC_FLAGS + extra + ["-c", src, "-o", obj]
+    host = ["-Xcompiler", "-fopenmp"] if src.endswith(".cpp") else []  # host-side numbering runs on all cores
+    cmd = [nvcc()] + ARCH + NVCC_FLAGS + host + extra + ["-c", src, "-o", obj]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError("nvcc failed for %s:\n%s\n%s" % (os.path.basename(src), r.stdout, r.stderr))
@@ -65,7 +66,7 @@ def build(force=False, verbose=False, extra=()):
                 if verbose and msg:
                     sys.stderr.write(msg)
     if jobs or force or not os.path.exists(OUT) or os.path.getmtime(OUT) < _newest(objs):
-        cmd = [nvcc()] + ARCH + ["-shared", "-Xcompiler", "-fPIC", "-o", OUT] + objs + ["-lcudart"]
+        cmd = [nvcc()] + ARCH + ["-shared", "-Xcompiler", "-fPIC", "-o", OUT] + objs + ["-lcudart", "-lgomp"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError("link failed:\n%s\n%s" % (r.stdout, r.stderr))

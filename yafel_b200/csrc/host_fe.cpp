@@ -2,9 +2,14 @@
 // colouring on the host.
 #include "host_fe.h"
 
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <memory>
 #include <numeric>
 
 namespace yg {
@@ -407,6 +412,59 @@ static void interpolate_from_corners(const double *xl, const double *c, int ct, 
     }
 }
 
+// Stable LSD radix sort of the N keys `ka` (only the low `nbits` bits are set;
+// the array is used as scratch) into the permutation `out_idx` (out_idx[j] =
+// position of the j-th smallest key; equal keys keep their original order).  11-bit digits; each pass counts per thread and
+// scatters each thread's contiguous chunk in order, so the result does not
+// depend on the thread count.
+static void radix_sort_index(uint64_t *ka, int64_t N, int nbits, int64_t *out_idx) {
+    constexpr int D = 11, R = 1 << D;
+    std::unique_ptr<uint64_t[]> kb(new uint64_t[N]);
+    std::unique_ptr<int64_t[]> ia_buf(new int64_t[N]), ib_buf(new int64_t[N]);
+    uint64_t *kin = ka, *kout = kb.get();
+    int64_t *iin = ia_buf.get(), *iout = ib_buf.get();
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < N; ++i) iin[i] = i;
+    int T = 1;
+#ifdef _OPENMP
+    T = omp_get_max_threads();
+#endif
+    std::vector<int64_t> hist((size_t)T * R);
+    for (int shift = 0; shift < nbits; shift += D) {
+        std::fill(hist.begin(), hist.end(), 0);
+#pragma omp parallel num_threads(T)
+        {
+            int t = 0;
+#ifdef _OPENMP
+            t = omp_get_thread_num();
+#endif
+            const int64_t lo = N * t / T, hi = N * (t + 1) / T;
+            int64_t *h = &hist[(size_t)t * R];
+            for (int64_t i = lo; i < hi; ++i) ++h[(kin[i] >> shift) & (R - 1)];
+#pragma omp barrier
+#pragma omp single
+            {
+                int64_t sum = 0;
+                for (int q = 0; q < R; ++q)
+                    for (int u = 0; u < T; ++u) {
+                        int64_t c = hist[(size_t)u * R + q];
+                        hist[(size_t)u * R + q] = sum;
+                        sum += c;
+                    }
+            }
+            for (int64_t i = lo; i < hi; ++i) {
+                const int64_t dst = h[(kin[i] >> shift) & (R - 1)]++;
+                kout[dst] = kin[i];
+                iout[dst] = iin[i];
+            }
+        }
+        std::swap(kin, kout);
+        std::swap(iin, iout);
+    }
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < N; ++i) out_idx[i] = iin[i];
+}
+
 bool build_dofmap(const double *xyz, int32_t n_nodes, const int32_t *cell_nodes, const int32_t *cell_offsets,
                   const int32_t *cell_types, int32_t n_cells, int32_t p, int32_t dpn, HostDofmap &d) {
     if (p < 1) return false;
@@ -428,93 +486,123 @@ bool build_dofmap(const double *xyz, int32_t n_nodes, const int32_t *cell_nodes,
         d.elements.assign(cell_nodes, cell_nodes + cell_offsets[n_cells]);
         return true;
     }
-    // make_raw_dofs (DoFManager.cpp:176-229)
-    std::vector<double> raw;
-    std::vector<double> loc;
+    // make_raw_dofs (DoFManager.cpp:176-229): every element's nodes at the
+    // element's local node coordinates, cells in mesh order (offsets first, then
+    // the coordinates of all cells in parallel)
     std::vector<double> tabs[3][4];
     int nloc[3][4] = {{0}};
-    int offset = 0;
+    int64_t offset = 0;
+    for (int c = 0; c < n_cells; ++c) {
+        int t = d.topology[c], td = d.topo_dim[c];
+        d.offsets[c] = (int32_t)offset;
+        if (t == TOPO_NONE) continue;
+        if (!nloc[t][td]) nloc[t][td] = local_nodes(t, td, p, tabs[t][td]);
+        offset += nloc[t][td];
+    }
+    d.offsets[n_cells] = (int32_t)offset;
+    const int64_t N = offset;
+    std::unique_ptr<double[]> raw(new double[3 * N]);  // written (first touched) in parallel below
+#pragma omp parallel for schedule(static)
     for (int c = 0; c < n_cells; ++c) {
         int t = d.topology[c], td = d.topo_dim[c];
         if (t == TOPO_NONE) continue;
-        if (!nloc[t][td]) nloc[t][td] = local_nodes(t, td, p, tabs[t][td]);
         const std::vector<double> &L = tabs[t][td];
-        int nl = nloc[t][td];
+        const int nl = nloc[t][td];
         double corners[24] = {0};
         int nc = cell_offsets[c + 1] - cell_offsets[c];
         for (int i = 0; i < nc && i < 8; ++i)
             for (int k = 0; k < 3; ++k) corners[3 * i + k] = xyz[3 * (int64_t)cell_nodes[cell_offsets[c] + i] + k];
-        for (int a = 0; a < nl; ++a) {
-            double o[3];
-            interpolate_from_corners(&L[3 * a], corners, cell_types[c], o);
-            raw.insert(raw.end(), o, o + 3);
-        }
-        d.offsets[c] = offset;
-        offset += nl;
+        double *o = &raw[3 * (int64_t)d.offsets[c]];
+        for (int a = 0; a < nl; ++a) interpolate_from_corners(&L[3 * a], corners, cell_types[c], o + 3 * a);
     }
-    d.offsets[n_cells] = offset;
-    const int64_t N = (int64_t)raw.size() / 3;
-    d.elements.resize(N);
     // recombine_all_duplicates (DoFManager.cpp:340-414): sort on the snapped
     // coordinates (z, y, x), merge neighbours closer than 1e-6.  The snapped value
     // is k*s with k = round(x/s) an integer, so the order of the snapped doubles is
-    // the order of the integer triples, which pack into one 64-bit key.
+    // the order of the integer triples, which pack into one 64-bit key; a stable
+    // sort keeps equal keys in raw order, as a (key, index) sort does.
     if (N == 0) { d.nodes.clear(); return true; }
     double bmin[3] = {raw[0], raw[1], raw[2]}, bmax[3] = {raw[0], raw[1], raw[2]};
-    for (int64_t i = 0; i < N; ++i)
-        for (int k = 0; k < 3; ++k) {
-            bmin[k] = std::min(bmin[k], raw[3 * i + k]);
-            bmax[k] = std::max(bmax[k], raw[3 * i + k]);
+    for (int k = 0; k < 3; ++k) {
+        double lo = raw[k], hi = raw[k];
+#pragma omp parallel for reduction(min : lo) reduction(max : hi) schedule(static)
+        for (int64_t i = 0; i < N; ++i) {
+            lo = std::min(lo, raw[3 * i + k]);
+            hi = std::max(hi, raw[3 * i + k]);
         }
+        bmin[k] = lo;
+        bmax[k] = hi;
+    }
     double max_dim = std::max(bmax[0] - bmin[0], std::max(bmax[1] - bmin[1], bmax[2] - bmin[2]));
     double snapv = max_dim * 1.0e-6;
-    std::vector<int64_t> kq(3 * N);
-    int64_t kmin[3] = {INT64_MAX, INT64_MAX, INT64_MAX}, kmax[3] = {INT64_MIN, INT64_MIN, INT64_MIN};
-    for (int64_t i = 0; i < N; ++i)
-        for (int k = 0; k < 3; ++k) {
-            int64_t v = (snapv > 0) ? (int64_t)std::llround(std::round(raw[3 * i + k] / snapv)) : 0;
-            kq[3 * i + k] = v;
-            kmin[k] = std::min(kmin[k], v);
-            kmax[k] = std::max(kmax[k], v);
-        }
-    bool packable = true;
-    for (int k = 0; k < 3; ++k) packable &= (kmax[k] - kmin[k]) < (int64_t(1) << 21);
-    std::vector<int64_t> idx(N);
-    std::iota(idx.begin(), idx.end(), 0);
-    if (packable) {
-        std::vector<std::pair<uint64_t, int64_t>> keys(N);
+    // snapped integer coordinates: ranges first, keys second (nothing stored)
+    auto snapped = [&](int64_t i, int k) -> int64_t {
+        return (snapv > 0) ? (int64_t)std::llround(std::round(raw[3 * i + k] / snapv)) : 0;
+    };
+    int64_t kmin[3], kmax[3];
+    for (int k = 0; k < 3; ++k) {
+        int64_t lo = INT64_MAX, hi = INT64_MIN;
+#pragma omp parallel for reduction(min : lo) reduction(max : hi) schedule(static)
         for (int64_t i = 0; i < N; ++i) {
-            uint64_t key = ((uint64_t)(kq[3 * i + 2] - kmin[2]) << 42) | ((uint64_t)(kq[3 * i + 1] - kmin[1]) << 21) |
-                           (uint64_t)(kq[3 * i + 0] - kmin[0]);
-            keys[i] = {key, i};
+            const int64_t v = snapped(i, k);
+            lo = std::min(lo, v);
+            hi = std::max(hi, v);
         }
-        std::sort(keys.begin(), keys.end());
-        for (int64_t i = 0; i < N; ++i) idx[i] = keys[i].second;
+        kmin[k] = lo;
+        kmax[k] = hi;
+    }
+    int bits[3];
+    for (int k = 0; k < 3; ++k) {
+        const uint64_t span = (uint64_t)(kmax[k] - kmin[k]);
+        bits[k] = 0;
+        while (bits[k] < 63 && (span >> bits[k]) != 0) ++bits[k];
+    }
+    const bool packable = bits[0] + bits[1] + bits[2] <= 64;
+    std::unique_ptr<int64_t[]> idx(new int64_t[N]);
+    if (packable) {
+        std::unique_ptr<uint64_t[]> keys(new uint64_t[N]);
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < N; ++i)
+            keys[i] = ((uint64_t)(snapped(i, 2) - kmin[2]) << (bits[0] + bits[1])) |
+                      ((uint64_t)(snapped(i, 1) - kmin[1]) << bits[0]) | (uint64_t)(snapped(i, 0) - kmin[0]);
+        radix_sort_index(keys.get(), N, bits[0] + bits[1] + bits[2], idx.get());
     } else {
-        std::sort(idx.begin(), idx.end(), [&](int64_t a, int64_t b) {
+        std::vector<int64_t> kq(3 * N);
+        for (int64_t i = 0; i < N; ++i)
+            for (int k = 0; k < 3; ++k) kq[3 * i + k] = snapped(i, k);
+        std::iota(idx.get(), idx.get() + N, 0);
+        std::sort(idx.get(), idx.get() + N, [&](int64_t a, int64_t b) {
             for (int k = 2; k >= 0; --k)
                 if (kq[3 * a + k] != kq[3 * b + k]) return kq[3 * a + k] < kq[3 * b + k];
             return a < b;
         });
     }
-    std::vector<int32_t> raw_to_new(N);
+    // merge: a sorted entry starts a new node unless it lies within 1e-6 of the
+    // previous one; node numbers are the running count of starts
+    std::unique_ptr<int32_t[]> start(new int32_t[N]);
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < N; ++i) {
+        int32_t newg = 1;
+        if (i > 0) {
+            const double *a = &raw[3 * idx[i]], *b = &raw[3 * idx[i - 1]];
+            double s2 = 0;
+            for (int k = 0; k < 3; ++k) s2 += (a[k] - b[k]) * (a[k] - b[k]);
+            if (std::sqrt(s2) < 1.0e-6) newg = 0;
+        }
+        start[i] = newg;
+    }
     std::vector<int64_t> first;
     first.reserve(N / 2 + 1);
     for (int64_t i = 0; i < N; ++i) {
-        bool newg = true;
-        if (i > 0) {
-            const double *a = &raw[3 * idx[i]], *b = &raw[3 * idx[i - 1]];
-            double s = 0;
-            for (int k = 0; k < 3; ++k) s += (a[k] - b[k]) * (a[k] - b[k]);
-            if (std::sqrt(s) < 1.0e-6) newg = false;
-        }
-        if (newg) first.push_back(idx[i]);
-        raw_to_new[idx[i]] = (int32_t)(first.size() - 1);
+        if (start[i]) first.push_back(idx[i]);
+        start[i] = (int32_t)(first.size() - 1);  // now the node number of sorted entry i
     }
+    d.elements.resize(N);
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < N; ++i) d.elements[idx[i]] = start[i];
     d.nodes.resize(3 * first.size());
-    for (size_t g = 0; g < first.size(); ++g)
+#pragma omp parallel for schedule(static)
+    for (int64_t g = 0; g < (int64_t)first.size(); ++g)
         for (int k = 0; k < 3; ++k) d.nodes[3 * g + k] = raw[3 * first[g] + k];
-    for (int64_t i = 0; i < N; ++i) d.elements[i] = raw_to_new[i];
     return true;
 }
 
