@@ -222,9 +222,11 @@ def run_gpu(args):
             bc.apply(Kx, Fx)
         xe, ste = yb.solve(Kx, Fx, M=yb.JacobiPreconditioner(Kx), tol=TOL)
         sol = xe.numpy()
+        # mesh arrays, the numbered nodes and element lists the DoFManager uploads,
+        # the traction vector and the BC lists (counted, not read back)
         h2d = mesh["nodes"].nbytes + mesh["cell_nodes"].nbytes + mesh["offsets"].nbytes + \
             mesh["cell_types"].nbytes + traction.nbytes + 3 * clamp.size * 16 + \
-            X.nbytes + dme.elements.nbytes  # numbering and element lists uploaded by DoFManager
+            24 * dme.nNodes() + 4 * dme._n_el
         d2h = sol.nbytes
     e2e_s = rep.max((time.perf_counter() - t0) / e2e_steps)
     # roofline of the dominant kernel (BCSR3 SpMV inside the PCG iterations)
@@ -244,7 +246,7 @@ def run_gpu(args):
     achieved = spmv_bytes / (spmv_ms * 1e-3) / 1e9 if spmv_ms > 0 else None
     # DRAM bytes (read + write) of one launch of this kernel on the 60^3 matrix,
     # measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum)
-    traffic = 8.555e9 if args.nx == 60 else None
+    traffic = 8.729e9 if args.nx == 60 else None
     iters64 = statistics.mean(s.iterations for s in st64)
     itersmx = statistics.mean(s.iterations for s in stmx)
     mixed_step = wallmx / args.steps

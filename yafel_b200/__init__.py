@@ -507,6 +507,7 @@ class DirichletBC:
     def __init__(self, dofm, bcval=0.0, comp=0):
         self.dofm, self.component = dofm, int(comp)
         self.value_func = bcval if callable(bcval) else (lambda x, t, v=float(bcval): v)
+        self.constant = None if callable(bcval) else float(bcval)
         self.bc_nodes = np.zeros(0, np.int64)
 
     def selectByFunction(self, func):
@@ -540,8 +541,11 @@ class DirichletBC:
     def dofs_and_values(self, time=0.0):
         d = self.dofm.dof_per_node
         dofs = self.bc_nodes * d + self.component
-        X = self.dofm.dof_nodes[self.bc_nodes] if self.bc_nodes.size else np.zeros((0, 3))
-        vals = np.array([self.value_func(x, time) for x in X], dtype=np.float64)
+        if self.constant is not None:  # a constant value needs no node coordinates
+            vals = np.full(self.bc_nodes.size, self.constant)
+        else:
+            X = self.dofm.dof_nodes[self.bc_nodes] if self.bc_nodes.size else np.zeros((0, 3))
+            vals = np.array([self.value_func(x, time) for x in X], dtype=np.float64)
         return np.ascontiguousarray(dofs, dtype=np.int64), np.ascontiguousarray(vals)
 
     def apply(self, A, rhs, time=0.0):
