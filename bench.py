@@ -283,6 +283,7 @@ def run_gpu(args):
     if ws == 1 and not args.no_extra:
         out["small_poisson64"] = run_small_poisson(ctx)
         out["q3_30cubed"] = run_q3(ctx)
+        out["ilu0_vs_jacobi_30cubed"] = run_ilu(ctx)
     if rank == 0 and not args.no_cpu_baseline and ws == 1:
         out["cpu_baseline"] = cpu_baseline(args)
     if rank == 0:
@@ -371,6 +372,40 @@ def run_q3(ctx, nx=30, steps=2):
         del K, F, fe, x
     out["mixed_speedup"] = out["fp64"]["s_per_solve"] / out["mixed"]["s_per_solve"]
     out["mixed_rel_diff_vs_fp64"] = float(np.linalg.norm(sol["mixed"] - sol["fp64"]) / np.linalg.norm(sol["fp64"]))
+    return out
+
+
+def run_ilu(ctx, nx=30):
+    """ILU(0)-PCG beside Jacobi-PCG on the nx^3 Q2 elasticity problem (the
+    reference's ILUPreconditioner on the scalar pattern, level-scheduled
+    triangular solves): set-up (factorisation) and solve times, iterations."""
+    import yafel_b200 as yb
+    from yafel_b200 import loads
+    dm = yb.DoFManager(problem(nx), 2, 3, ctx=ctx)
+    X = dm.dof_nodes
+    clamp = np.nonzero(np.abs(X[:, 0]) < 1e-9)[0].astype(np.int64)
+    trac = yb.DeviceVector(loads.hex_face_traction(dm, lambda Y: np.abs(Y[:, 0] - 1.0) < 1e-9, (1.0, 0.0, 0.0)), ctx)
+    fe = yb.FESystem(dm, 3, format=yb.BCSR)
+    yb.CGAssembly(yb.LinearElasticity(3, E=E, nu=NU), fe)
+    K, F = fe.getGlobalTangent(), fe.getGlobalResidual()
+    F.axpy(1.0, trac)
+    for c in range(3):
+        bc = yb.DirichletBC(dm, 0.0, c)
+        bc.bc_nodes = clamp
+        bc.apply(K, F)
+    out = {"workload": "elasticity_q2_hex_%d^3_pcg_1e-10" % nx, "dofs": dm.ndofs}
+    for name, cls in (("jacobi", yb.JacobiPreconditioner), ("ilu0", yb.ILUPreconditioner)):
+        ctx.synchronize()
+        t0 = time.perf_counter()
+        M = cls(K)
+        ctx.synchronize()
+        t1 = time.perf_counter()
+        x, st = yb.solve(K, F, M=M, tol=TOL)
+        ctx.synchronize()
+        t2 = time.perf_counter()
+        out[name] = {"setup_s": t1 - t0, "solve_s": t2 - t1, "iterations": st.iterations,
+                     "relres": st.rel_residual, "status": st.status}
+        del M, x
     return out
 
 
@@ -723,7 +758,7 @@ def main():
     ap.add_argument("--nx", type=int, default=NX)
     ap.add_argument("--cpu-nx", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-extra", action="store_true", help="skip the 64x64 Poisson and 30^3 Q3 side measurements")
+    ap.add_argument("--no-extra", action="store_true", help="skip the 64x64 Poisson, 30^3 Q3 and ILU(0) side measurements")
     ap.add_argument("--spmv-profile", action="store_true", help="time the SpMV kernel alone (roofline/ncu)")
     ap.add_argument("--variant", type=int, default=None, help="SpMV variant for --spmv-profile (0 flat, 1 staged, 2 TMA)")
     ap.add_argument("--lanes", type=int, default=32, help="SpMV lanes / TMA configuration for --spmv-profile")
