@@ -295,6 +295,10 @@ YG_API yg_status yg_batch_tune(yg_batch B);
 /* The tuning in use: out[3*(b-1) + {0,1,2}] = variant, lanes, tiles per item
  * for block size b = 1, 2, 3. */
 YG_API yg_status yg_batch_get_tuning(yg_batch B, int32_t *out);
+/* Set the tuning of one block size (variant 0 or 1; lanes 1, 2, 4, ..., 32 --
+ * lanes 1 means a lane per block with a segmented row sum in variant 0 and a
+ * thread per row in variant 1; tiles per work item >= 1), between runs. */
+YG_API yg_status yg_batch_set_tuning(yg_batch B, int32_t block, int32_t variant, int32_t lanes, int32_t tiles);
 
 /* A continuous-batching solve server on one context.  No reference
  * counterpart.  A request is submitted with an estimate of the device bytes it

@@ -140,3 +140,21 @@ def test_bicgstab_same_result_alone_and_in_mix(ctx):
     assert B.run() == 0
     for i, s in enumerate(slots):
         assert np.array_equal(B.solution(s).numpy(), alone[i]), i
+
+
+@pytest.mark.parametrize("variant,lanes,tiles", [(0, 1, 4), (0, 2, 1), (0, 32, 16), (1, 1, 4), (1, 4, 1),
+                                                 (1, 32, 16)])
+def test_every_spmv_variant_solves_the_mix(ctx, variant, lanes, tiles):
+    """Each SpMV variant (staged tiles with a lane per block and segmented row
+    sums, or L lanes per row; direct loads with a thread or L lanes per row) on
+    PCG and BiCGSTAB systems of 1x1 and 2x2 blocks: every system reaches 1e-10."""
+    probs = [assemble_problem(s, ctx) for s in MIXED_SPECS]
+    B = yb.Batch(len(probs), ctx)
+    slots = [B.add(K, b, method=workloads.method(s)) for s, (_, K, b, _) in zip(MIXED_SPECS, probs)]
+    for blk in (1, 2, 3):
+        B.set_tuning(blk, variant, lanes, tiles)
+    assert B.run() == 0
+    for spec, (mesh, K, b, dofs), s in zip(MIXED_SPECS, probs, slots):
+        st = B.stats(s)
+        assert st.status == 0 and st.rel_residual <= 1e-10, (spec, st.status, st.rel_residual)
+        assert oracle_relres(spec, mesh, dofs, b.numpy(), B.solution(s).numpy()) <= 1e-10

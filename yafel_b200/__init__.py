@@ -684,6 +684,9 @@ class Batch:
         check(lib().yg_batch_get_tuning(self.h, a), "Batch.tuning")
         return {b: (a[3 * (b - 1)], a[3 * (b - 1) + 1], a[3 * (b - 1) + 2]) for b in (1, 2, 3)}
 
+    def set_tuning(self, block, variant, lanes, tiles):
+        check(lib().yg_batch_set_tuning(self.h, int(block), int(variant), int(lanes), int(tiles)), "Batch.set_tuning")
+
     def launch(self):
         """One block of iterations without waiting; pair with wait()."""
         check(lib().yg_batch_launch(self.h), "Batch.launch")

@@ -80,6 +80,7 @@ SIGNATURES = {
     "yg_batch_launch": (i32, [vp]),
     "yg_batch_wait": (i32, [vp, P(i32)]),
     "yg_batch_get_tuning": (i32, [vp, P(i32)]),
+    "yg_batch_set_tuning": (i32, [vp, i32, i32, i32, i32]),
     "yg_server_create": (i32, [vp, u64, i32, P(vp)]),
     "yg_server_destroy": (i32, [vp]),
     "yg_server_submit": (i32, [vp, u64, P(i64)]),

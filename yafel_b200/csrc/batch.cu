@@ -288,6 +288,87 @@ struct TileHdr {
     int32_t item, r0, r1, b0, nb, last, pad0, pad1;
 };
 
+// The same with every lane on consecutive blocks of the tile (lanes == 1 in the
+// tuning): 32 blocks per round, each lane's block product, a segmented
+// inclusive warp scan by row (rows are contiguous runs of blocks), and the lane
+// that ends a row's run writes the row (a row continuing into the next round
+// carries its partial sum).  Rows without blocks are written as zero.
+template <int B, int KIND, typename VT>
+__device__ __forceinline__ void tile_rows_seg(const int32_t *rows, int r0, int r1, int b0, const VT *vals,
+                                              const int32_t *cols, const double *__restrict__ xin,
+                                              double *__restrict__ out, const double *__restrict__ w, double &dot1,
+                                              double &dot2, int lane) {
+    constexpr int B2 = B * B;
+    const int nrows = r1 - r0;
+    const int nb = rows[nrows] - b0;
+    double carry[B];
+#pragma unroll
+    for (int i = 0; i < B; ++i) carry[i] = 0;
+    int carry_row = -1;
+    int rl = 0;  // local row of this lane's block (only grows)
+    for (int base = 0; base < nb; base += 32) {
+        const int j = base + lane;
+        const bool valid = j < nb;
+        double v[B];
+#pragma unroll
+        for (int i = 0; i < B; ++i) v[i] = 0;
+        int myrow = 1 << 30;
+        if (valid) {
+            while (rows[rl + 1] - b0 <= j) ++rl;
+            myrow = rl;
+            const int c = cols[j];
+            double x[B];
+#pragma unroll
+            for (int k = 0; k < B; ++k) x[k] = __ldg(xin + (int64_t)B * c + k);
+#pragma unroll
+            for (int i = 0; i < B; ++i)
+#pragma unroll
+                for (int k = 0; k < B; ++k) v[i] = fma((double)vals[j * B2 + i * B + k], x[k], v[i]);
+        }
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int ro = __shfl_up_sync(0xffffffffu, myrow, o);
+#pragma unroll
+            for (int i = 0; i < B; ++i) {
+                const double vo = __shfl_up_sync(0xffffffffu, v[i], o);
+                if (lane >= o && ro == myrow) v[i] += vo;
+            }
+        }
+        const int next_row = __shfl_down_sync(0xffffffffu, myrow, 1);
+        const bool seg_end = valid && (lane == 31 || next_row != myrow);
+        // the run of this segment continues a row carried from the previous round
+        if (seg_end && myrow == carry_row) {
+#pragma unroll
+            for (int i = 0; i < B; ++i) v[i] += carry[i];
+        }
+        const bool row_done = seg_end && (rows[myrow + 1] - b0 - 1 == j);
+        if (row_done) {
+            const int r = r0 + myrow;
+#pragma unroll
+            for (int i = 0; i < B; ++i) {
+                out[(int64_t)B * r + i] = v[i];
+                if (KIND != SP_VERIFY) dot1 = fma(v[i], w[(int64_t)B * r + i], dot1);
+                if (KIND == SP_BICG_T) dot2 = fma(v[i], v[i], dot2);
+            }
+        }
+        // lane 31 ends the round: an unfinished row is carried
+        const int last_open = __shfl_sync(0xffffffffu, (valid && !row_done) ? 1 : 0, 31);
+        if (last_open) {
+#pragma unroll
+            for (int i = 0; i < B; ++i) carry[i] = __shfl_sync(0xffffffffu, v[i], 31);
+            carry_row = __shfl_sync(0xffffffffu, myrow, 31);
+        } else {
+            carry_row = -1;
+        }
+    }
+    // rows without blocks
+    for (int k = lane; k < nrows; k += 32)
+        if (rows[k + 1] == rows[k]) {
+#pragma unroll
+            for (int i = 0; i < B; ++i) out[(int64_t)B * (r0 + k) + i] = 0;
+        }
+}
+
 // Lane 0 issues the bulk copies of tile t of a system (values, block columns,
 // row pointers) into stage seq % NST of this warp's ring and writes the tile's
 // header; an empty or oversized tile completes its phase with no transfer and
@@ -636,10 +717,12 @@ k_batch_spmv(const BatchMItem *__restrict__ items, const int32_t *__restrict__ r
                                          : c_rowptr + h.r0;
             if (c_f32) {
                 const float *v = staged ? reinterpret_cast<const float *>(stg + lv) : c_val32 + (int64_t)h.b0 * B2;
-                tile_rows<B, L, KIND, float>(rows, h.r0, h.r1, h.b0, v, cols, xin, out, w, dot1, dot2, lane);
+                if (L == 1) tile_rows_seg<B, KIND, float>(rows, h.r0, h.r1, h.b0, v, cols, xin, out, w, dot1, dot2, lane);
+                else tile_rows<B, L, KIND, float>(rows, h.r0, h.r1, h.b0, v, cols, xin, out, w, dot1, dot2, lane);
             } else {
                 const double *v = staged ? reinterpret_cast<const double *>(stg + lv) : c_val + (int64_t)h.b0 * B2;
-                tile_rows<B, L, KIND, double>(rows, h.r0, h.r1, h.b0, v, cols, xin, out, w, dot1, dot2, lane);
+                if (L == 1) tile_rows_seg<B, KIND, double>(rows, h.r0, h.r1, h.b0, v, cols, xin, out, w, dot1, dot2, lane);
+                else tile_rows<B, L, KIND, double>(rows, h.r0, h.r1, h.b0, v, cols, xin, out, w, dot1, dot2, lane);
             }
         }
         ++seq_wait;
@@ -1048,6 +1131,7 @@ static void launch_spmv_l(yg_batch bt, int variant, int g, int parity, int commi
 template <int B, int KIND>
 static void launch_spmv_b(yg_batch bt, int V, int L, int g, int parity, int commit) {
     switch (L) {
+    case 1: launch_spmv_l<B, 1, KIND>(bt, V, g, parity, commit); break;
     case 2: launch_spmv_l<B, 2, KIND>(bt, V, g, parity, commit); break;
     case 4: launch_spmv_l<B, 4, KIND>(bt, V, g, parity, commit); break;
     case 8: launch_spmv_l<B, 8, KIND>(bt, V, g, parity, commit); break;
@@ -1080,6 +1164,7 @@ static void launch_spmv(yg_batch bt, int kind, int g, int parity, int commit, in
 // set the shared-memory attribute of every SpMV instantiation (outside capture)
 template <int B, int KIND>
 static void prepare_spmv_bk(yg_context ctx) {
+    spmv_grid<B, 1, KIND>(ctx); direct_grid<B, 1, KIND>(ctx);
     spmv_grid<B, 2, KIND>(ctx); spmv_grid<B, 4, KIND>(ctx); spmv_grid<B, 8, KIND>(ctx);
     spmv_grid<B, 16, KIND>(ctx); spmv_grid<B, 32, KIND>(ctx);
     direct_grid<B, 2, KIND>(ctx); direct_grid<B, 4, KIND>(ctx); direct_grid<B, 8, KIND>(ctx);
@@ -1552,7 +1637,7 @@ extern "C" yg_status yg_batch_tune(yg_batch bt) {
             bt->tiles_per_item[B] = T;
             YG_TRY(rebuild_items(bt));
             for (int V : {0, 1})
-                for (int L : {2, 4, 8, 16, 32}) {
+                for (int L : {1, 2, 4, 8, 16, 32}) {
                     auto launch = [&]() {
                         if (cg) launch_spmv(bt, SP_CG, B - 1, 0, 0, L, V);
                         if (bi) launch_spmv(bt, SP_BICG_V, 3 + B - 1, 0, 0, L, V);
@@ -1586,5 +1671,17 @@ extern "C" yg_status yg_batch_get_tuning(yg_batch bt, int32_t *out) {
         out[3 * (B - 1) + 1] = bt->lanes[B];
         out[3 * (B - 1) + 2] = bt->tiles_per_item[B];
     }
+    return YG_OK;
+}
+
+extern "C" yg_status yg_batch_set_tuning(yg_batch bt, int32_t block, int32_t variant, int32_t lanes, int32_t tiles) {
+    if (!bt || block < 1 || block > 3 || (variant != 0 && variant != 1) || tiles < 1 ||
+        (lanes != 1 && lanes != 2 && lanes != 4 && lanes != 8 && lanes != 16 && lanes != 32))
+        return fail(YG_BAD_ARG, "yg_batch_set_tuning: bad argument");
+    bt->variant[block] = variant;
+    bt->lanes[block] = lanes;
+    bt->tiles_per_item[block] = tiles;
+    bt->dirty = true;
+    drop_graph(bt);
     return YG_OK;
 }
