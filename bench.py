@@ -281,6 +281,7 @@ def run_gpu(args):
         "clocks": clk,
     }
     if ws == 1 and not args.no_extra:
+        out["assembly"] = run_assembly(ctx, dm, phys, args.nx)
         out["small_poisson64"] = run_small_poisson(ctx)
         out["q3_30cubed"] = run_q3(ctx)
         out["ilu0_vs_jacobi_30cubed"] = run_ilu(ctx)
@@ -373,6 +374,64 @@ def run_q3(ctx, nx=30, steps=2):
     out["mixed_speedup"] = out["fp64"]["s_per_solve"] / out["mixed"]["s_per_solve"]
     out["mixed_rel_diff_vs_fp64"] = float(np.linalg.norm(sol["mixed"] - sol["fp64"]) / np.linalg.norm(sol["fp64"]))
     return out
+
+
+def assembly_flops_per_element(nq, nen, dpn, nsd):
+    """Algorithmic flops of the element-local B^T D B product per element:
+    2 nq (s^2 n + s n^2) with s = 3 (2D) or 6 (3D) strain components and
+    n = nen * dpn element dofs."""
+    s = 3 if nsd == 2 else 6
+    n = nen * dpn
+    return 2 * nq * (s * s * n + s * n * n)
+
+
+def fp64_peak_tflops():
+    """FP64 dense rate measured here: torch float64 8192^3 matmul (cuBLAS DGEMM),
+    best of 5, CUDA events; None without torch CUDA."""
+    try:
+        import torch
+        if not torch.cuda.is_available():
+            return None
+        a = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
+        b = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
+        torch.matmul(a, b)
+        best = 1e30
+        for _ in range(5):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            torch.matmul(a, b)
+            e1.record()
+            torch.cuda.synchronize()
+            best = min(best, e0.elapsed_time(e1))
+        del a, b
+        torch.cuda.empty_cache()
+        return 2 * 8192 ** 3 / (best * 1e-3) / 1e12
+    except Exception:
+        return None
+
+
+def run_assembly(ctx, dm, phys, nx, reps=5):
+    """Element kernels alone: re-assembly of the tangent's values on an existing
+    pattern (CGAssembly on an FESystem that already holds K), wall time with the
+    device synchronised on both sides, against the algorithmic B^T D B flops of
+    the Q2 hexes (27 Gauss points, 27 nodes, 3 dofs per node)."""
+    import yafel_b200 as yb
+    fe = yb.FESystem(dm, 3, format=yb.BCSR)
+    yb.CGAssembly(phys, fe, [yb.AssemblyRequirement.Tangent])
+    ts = []
+    for _ in range(reps):
+        ctx.synchronize()
+        t0 = time.perf_counter()
+        yb.CGAssembly(phys, fe, [yb.AssemblyRequirement.Tangent])
+        ctx.synchronize()
+        ts.append(time.perf_counter() - t0)
+    t = min(ts)
+    flops = assembly_flops_per_element(27, 27, 3, 3) * nx ** 3
+    peak = fp64_peak_tflops()
+    achieved = flops / t / 1e12
+    return {"elements": nx ** 3, "ms": t * 1e3, "algorithmic_flops": flops, "achieved_TFLOPs": achieved,
+            "fp64_dgemm_TFLOPs_measured": peak, "frac_of_dgemm": (achieved / peak) if peak else None,
+            "bound": "FP64 FMA pipe (tcgen05 has no FP64 kind; element matrices use FP64 FMAs)"}
 
 
 def run_ilu(ctx, nx=30):

@@ -32,12 +32,13 @@ yg_status fail(yg_status s, const char *fmt, ...) {
     return s;
 }
 
-// Blocks of at most kCacheBlock bytes are kept after release, up to kCacheTotal
-// bytes per context, and handed out again for an allocation of the same size:
-// solver work vectors, iterates and Dirichlet scratch are allocated and freed on
-// every solve, and cudaMalloc / cudaFree would otherwise map pages and
-// synchronise the device each time.
-constexpr size_t kCacheBlock = 256ull << 20, kCacheTotal = 2ull << 30;
+// Released blocks are kept, up to kCacheTotal bytes per context, and handed out
+// again for an allocation of the same size: solver work vectors, iterates,
+// Dirichlet scratch and re-assembled matrices are allocated and freed over and
+// over, and cudaMalloc / cudaFree would otherwise map and unmap pages and
+// synchronise the device each time.  A cudaMalloc that fails releases the
+// cached blocks and tries again.
+constexpr size_t kCacheBlock = 16ull << 30, kCacheTotal = 32ull << 30;
 
 void flush_alloc_cache(yg_context ctx) {
     for (auto &kv : ctx->cache) {
