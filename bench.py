@@ -809,6 +809,10 @@ def run_reference(args):
 
 
 def main():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    if ws > 1 and "OMP_NUM_THREADS" not in os.environ:
+        # one process per GPU on one host: share the host cores among the ranks
+        os.environ["OMP_NUM_THREADS"] = str(max(1, (os.cpu_count() or ws) // ws))
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
