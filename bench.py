@@ -329,7 +329,34 @@ def run_small_poisson(ctx, reps=30):
             "iterations": st.iterations, "relres": st.rel_residual, "status": st.status,
             "latency_ms_p50": 1e3 * lat[len(lat) // 2], "latency_ms_p99": 1e3 * lat[min(len(lat) - 1, int(0.99 * len(lat)))],
             "solve_device_ms_p50": sorted(solve_ms)[len(solve_ms) // 2], "solves_per_s": len(lat) / sum(lat),
-            "l2": "L2-resident (%.2f MB): latency, not a roofline" % ((K.nnz() * 12 + dm.ndofs * 40) / 1e6)}
+            "l2": "L2-resident (%.2f MB): latency, not a roofline" % ((K.nnz() * 12 + dm.ndofs * 40) / 1e6),
+            "cpu": cpu_small_poisson(mesh)}
+
+
+def cpu_small_poisson(mesh, reps=5):
+    """The same 64x64 Q1 Poisson solve on the host: oracle assembly and
+    Dirichlet conditions, then the reference's sparse_csr(triplets) and
+    pcg_solve with its Jacobi preconditioner (TOL 1e-24 on the squared
+    preconditioned ratio).  Median latency over `reps` solves, DoF numbering
+    outside the timed region as on the device."""
+    from oracle import oracle as O
+    if not O.ref_available():
+        return None
+    odm = O.dofmanager(mesh, 1)
+    X = odm.nodes
+    mask = ((X[:, 0] < 1e-9) | (X[:, 0] > 1 - 1e-9) | (X[:, 1] < 1e-9) | (X[:, 1] > 1 - 1e-9)).astype(np.uint8)
+    lat, rel = [], None
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        K, F = O.assemble(odm, 1, 2, O.POISSON, [1.0, 1.0])
+        O.dirichlet_apply(K, F, mask, np.zeros(K.nrows))
+        x = O.RefCsr(*O.csr_to_triplets(K)).pcg_jacobi(F, np.zeros(K.nrows), 1e-24)
+        lat.append(time.perf_counter() - t0)
+        rel = O.true_relres(K, F, x)
+    lat.sort()
+    return {"latency_ms_p50": 1e3 * lat[len(lat) // 2], "relres": rel, "kind": "reference",
+            "cores": int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1)),
+            "sample": "%d solves: oracle assembly + the reference's sparse_csr + pcg_solve/Jacobi" % reps}
 
 
 def run_q3(ctx, nx=30, steps=2):
@@ -584,6 +611,8 @@ def run_batch(args):
            "gpu_launches": int(mixed["launches"] / args.steps),
            "setup": {"assembly_s": t_setup},
            "clocks": clk}
+    if not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_problems(specs)
     print(json.dumps(out), flush=True)
 
 
@@ -733,6 +762,9 @@ def run_serve(args):
                    "d2h_bytes_per_step": int(8 * sum(dofs)),
                    "includes": "DoF numbering, mesh upload, assembly, solve, solution download per request"},
            "gpu_launches": int(launches), "clocks": clk}
+    if not args.no_cpu_baseline:
+        # requests in arrival order up to 1e5 dofs (the large 3D ones take minutes on the CPU)
+        out["cpu_baseline"] = cpu_problems(specs, meshes, max_dofs=100000)
     print(json.dumps(out), flush=True)
 
 
@@ -771,6 +803,61 @@ def cpu_sample(nx, threads):
         kind = "port"
     dt = time.perf_counter() - t0
     return K.nrows, dt, O.true_relres(K, F, x), kind
+
+
+def cpu_problem(spec, mesh=None):
+    """The reference's CPU path on one seeded problem: oracle assembly and
+    Dirichlet conditions (the reference's own assembly needs Eigen), the
+    reference's sparse_csr(triplets), then its pcg_solve with the Jacobi
+    preconditioner (TOL 1e-24 on the squared preconditioned ratio), or for SUPG
+    its unpreconditioned bicgstab_solve (whose tolerance is fixed: 1e-14 on the
+    squared true residual).  Returns (dofs, seconds, FP64 relative residual)."""
+    from oracle import oracle as O
+    from yafel_b200 import workloads
+    if mesh is None:
+        mesh = workloads.build_mesh(spec)
+    t0 = time.perf_counter()
+    odm = O.dofmanager(mesh, spec["order"])
+    dim, dpn = spec["dim"], spec["dpn"]
+    if spec["kind"] == "supg":
+        h = 1.0 / spec["n"]
+        kind, params = O.SUPG, [h / (2.0 * spec["peclet"]), h, 1.0, 0.0]
+    elif spec["kind"] == "poisson":
+        kind, params = O.POISSON, [1.0, 0.0]
+    else:
+        lam, mu = (1.0 * 0.3) / (1.3 * 0.4), 1.0 / 2.6
+        kind, params = O.ELASTICITY, [1.0, lam, mu, 0.0, 0.0, 0.0]
+    K, _ = O.assemble(odm, dpn, dim, kind, params)
+    b = workloads.rhs(spec, K.nrows)
+    mask = np.zeros(K.nrows, np.uint8)
+    mask[workloads.clamp_dofs(odm.nodes, dpn)] = 1
+    O.dirichlet_apply(K, b, mask, np.zeros(K.nrows))
+    R = O.RefCsr(*O.csr_to_triplets(K))
+    x0 = np.zeros(K.nrows)
+    x = R.bicgstab(b, x0) if spec["kind"] == "supg" else R.pcg_jacobi(b, x0, 1e-24)
+    dt = time.perf_counter() - t0
+    return K.nrows, dt, O.true_relres(K, b, x)
+
+
+def cpu_problems(specs, meshes=None, budget_s=30.0, max_dofs=None):
+    """The reference's CPU path over problems in order until the time budget is
+    spent (a bounded sample); returns the cpu_baseline object."""
+    from oracle import oracle as O
+    if not O.ref_available():
+        return None
+    n, dofs, t, rels = 0, 0, 0.0, []
+    for i, spec in enumerate(specs):
+        if max_dofs and spec["dpn"] * (spec["order"] * spec["n"] + 1) ** spec["dim"] > max_dofs:
+            continue
+        d, dt, rel = cpu_problem(spec, meshes[i] if meshes else None)
+        n, dofs, t = n + 1, dofs + d, t + dt
+        rels.append(rel)
+        if t > budget_s:
+            break
+    return {"value": n / t, "unit": "solves/s", "cores": os.cpu_count() or 1, "kind": "reference",
+            "dofs_per_s": dofs / t,
+            "sample": "%d problems (%d dofs), oracle assembly + the reference's pcg_solve/Jacobi (bicgstab_solve "
+                      "for SUPG) on sparse_csr, %.1f s, max relres %.1e" % (n, dofs, t, max(rels))}
 
 
 def cpu_baseline(args):
