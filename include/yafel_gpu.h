@@ -180,7 +180,11 @@ YG_API yg_status yg_spmv_ex(yg_matrix A, yg_vector x, yg_vector y, int32_t preci
 /* SpMV kernel choice (no reference counterpart; the reference has one loop).
  * variant 0: flat, `lanes` lanes per block row read the value stream coalesced;
  * variant 1: each warp stages its rows' values in shared memory with cp.async
- * (2x2 and 3x3 blocks).  variant -1 re-runs the device autotuner, which times
+ * (2x2 and 3x3 blocks); variant 2: bulk asynchronous copies (cp.async.bulk) of
+ * row chunks into per-warp rings (2x2 and 3x3 blocks, `lanes` 1..32 selects the
+ * ring shape); variant 3: bulk copies of tiles of whole rows with at most 256,
+ * 512 or 1024 entries (CSR only, `lanes` 1, 2, 4, 8 selects the shape; every
+ * row must hold 1..capacity entries).  variant -1 re-runs the device autotuner, which times
  * the candidates on this matrix and keeps the fastest (it also runs on the
  * first SpMV or solve of a matrix). */
 YG_API yg_status yg_matrix_set_spmv(yg_matrix A, int32_t variant, int32_t lanes);

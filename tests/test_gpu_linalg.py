@@ -48,17 +48,65 @@ def test_spmv_matches_oracle(ctx, B, per_row):
     yo = Ao.spmv(x)
     scale = np.abs(val).max() * np.abs(x).max() * (per_row + 1) * B
     tma = [(2, L) for L in (32, 1, 2, 4, 8, 16)]
-    variants = [(0, 4), (0, 32)] + ([(1, 32)] + tma if B in (2, 3) else []) + [(-1, 32)]
+    tiles = [(3, L) for L in (1, 2, 4, 8)]
+    variants = [(0, 4), (0, 32)] + ([(1, 32)] + tma if B in (2, 3) else tiles) + [(-1, 32)]
     for v, L in variants:
         A.set_spmv(v, L)
         y = A * x
         assert np.abs(y - yo).max() <= 1e-14 * scale, (v, L)
         # determinism: same bits twice
         assert np.array_equal(y, A * x)
-        if B in (2, 3):
+        if v == 3:
+            # row tiles sum each row's rounded products left to right from 0, as the
+            # oracle's csr_spmv loop does (built without contraction): same bits
+            assert np.array_equal(y, yo), L
+        if B in (2, 3) or v == 3:
             y32 = A.spmv(x, precision=yb.PREC_MIXED).numpy()
             yo32 = bcsr_to_oracle_csr(rp, col, val.astype(np.float32).astype(np.float64), B).spmv(x)
             assert np.abs(y32 - yo32).max() <= 1e-13 * np.abs(yo32).max(), (v, L)
+            if v == 3:
+                assert np.array_equal(y32, yo32), L
+
+
+def test_csr_row_tiles_edge_cases(ctx):
+    """Row tiles (SpMV variant 3): a row longer than a tile's capacity rules out
+    that capacity only; an empty row rules the variant out; a one-row matrix and
+    rows of one entry work; the autotuner skips what does not apply."""
+    rng = np.random.Generator(np.random.PCG64(11))
+    n = 700
+    cols = [np.unique(np.concatenate([[i], rng.integers(0, n, 6)])) for i in range(n)]
+    cols[5] = np.unique(np.concatenate([[5], rng.choice(n, 400, replace=False)]))  # 400+ entries
+    rp = np.concatenate([[0], np.cumsum([c.size for c in cols])]).astype(np.int64)
+    col = np.concatenate(cols).astype(np.int64)
+    val = rng.standard_normal(col.size)
+    A = yb.sparse_csr.from_csr(rp, col, val)
+    x = rng.standard_normal(n)
+    yo = O.Csr(n, n, rp, col, val).spmv(x)
+    with pytest.raises(Exception):
+        A.set_spmv(3, 4)  # capacity 256 < the long row
+    for L in (1, 2, 8):  # capacities 512, 512, 1024
+        A.set_spmv(3, L)
+        assert np.array_equal(A * x, yo), L
+    A.set_spmv(-1)
+    assert np.abs(A * x - yo).max() <= 1e-13 * np.abs(yo).max()
+    # an empty row
+    rp2 = np.array([0, 2, 2, 3], dtype=np.int64)
+    col2 = np.array([0, 2, 2], dtype=np.int64)
+    val2 = np.array([1.0, 2.0, 3.0])
+    A2 = yb.sparse_csr.from_csr(rp2, col2, val2)
+    with pytest.raises(Exception):
+        A2.set_spmv(3, 1)
+    A2.set_spmv(-1)
+    assert np.array_equal(A2 * np.array([1.0, 1.0, 1.0]), np.array([3.0, 0.0, 3.0]))
+    # one row; rows of a single entry (diagonal)
+    A3 = yb.sparse_csr.from_csr(np.array([0, 3]), np.array([0, 1, 2]), np.array([1.0, 2.0, 4.0]), ncols=3)
+    A3.set_spmv(3, 2)
+    assert np.array_equal(A3 * np.ones(3), np.array([7.0]))
+    d = rng.standard_normal(5000)
+    A4 = yb.sparse_csr.from_csr(np.arange(5001), np.arange(5000), d)
+    for L in (1, 2, 4, 8):
+        A4.set_spmv(3, L)
+        assert np.array_equal(A4 * x[:1].repeat(5000), d * x[0]), L
 
 
 @pytest.mark.parametrize("B", [1, 3])

@@ -346,7 +346,8 @@ class _Matrix:
         check(lib().yg_matrix_make_fp32(self.h))
 
     def set_spmv(self, variant, lanes=32):
-        """variant 0 flat (lanes per row), 1 shared-memory staged, -1 autotune."""
+        """variant 0 flat (lanes per row), 1 shared-memory staged, 2 bulk-copy
+        row chunks (2x2/3x3 blocks), 3 bulk-copy row tiles (CSR), -1 autotune."""
         check(lib().yg_matrix_set_spmv(self.h, int(variant), int(lanes)))
 
     def get_spmv(self):

@@ -81,7 +81,9 @@ struct BatchScal {
 };
 
 struct BatchMItem {
-    int32_t sys, tile_begin, tile_end, pad;
+    int32_t sys, tile_begin, tile_end;  // tiles [tile_begin, tile_end) of system sys
+    int32_t row_begin, row_end;         // their block rows
+    int32_t pad[3];
 };
 struct BatchVItem {
     int32_t sys, row_begin, row_end, pad;  // block rows
@@ -105,9 +107,10 @@ struct yg_batch_t {
     BatchVItem *d_vitems = nullptr;
     int32_t *d_ranges = nullptr;
     double *d_mpart = nullptr;          // SpMV partials: 2 per matrix item
+    int32_t *d_cticket = nullptr;       // per matrix item: finished items of the chunk it starts (zero between kernels)
     double *d_vpart = nullptr;          // vector partials: 2 per vector item
     double *d_vpart2 = nullptr;         // b.b partials of the verification
-    int32_t max_mitems = 0, max_vitems = 0;
+    int32_t max_mitems = 0, max_vitems = 0, cticket_cap = 0;
     int32_t tiles_per_item[4] = {0, 4, 4, 4};
     int32_t lanes[4] = {4, 4, 8, 16};
     int32_t variant[4] = {1, 1, 1, 0};   // SpMV variant per block size: 0 staged, 1 direct
@@ -191,19 +194,23 @@ __device__ __forceinline__ bool last_of_system(BatchScal *sc, int n_items, int *
     return *flag_sm != 0;
 }
 
-// The same for one warp (lane 0 publishes, the verdict is broadcast).
-__device__ __forceinline__ bool warp_last_of_system(BatchScal *sc, int n_items, int lane) {
+// The same for one warp and any ticket (lane 0 publishes, the verdict is
+// broadcast).
+__device__ __forceinline__ bool warp_last_of(int32_t *ticket, int n_items, int lane) {
     int last = 0;
     if (lane == 0) {
         __threadfence();
-        const int old = atomicAdd(&sc->ticket, 1);
+        const int old = atomicAdd(ticket, 1);
         last = (old == n_items - 1);
         if (last) {
-            sc->ticket = 0;
+            *ticket = 0;
             __threadfence();
         }
     }
     return __shfl_sync(0xffffffffu, last, 0) != 0;
+}
+__device__ __forceinline__ bool warp_last_of_system(BatchScal *sc, int n_items, int lane) {
+    return warp_last_of(&sc->ticket, n_items, lane);
 }
 
 // Fixed-order sums of partials [ib, ie) (stride 2, offset off): by a CTA (result
@@ -223,6 +230,19 @@ __device__ __forceinline__ double warp_sum_items(const double *part, int ib, int
     for (int i = ib + lane; i < ie; i += 32) v += __ldcg(part + 2 * (int64_t)i + off);
     return warp_sum(v);
 }
+// Sum of the partials of items ib, ib + step, ib + 2 step, ... (n of them).
+__device__ __forceinline__ double warp_sum_strided(const double *part, int ib, int n, int step, int off, int lane) {
+    double v = 0;
+#pragma unroll 4
+    for (int k = lane; k < n; k += 32) v += __ldcg(part + 2 * ((int64_t)ib + (int64_t)k * step) + off);
+    return warp_sum(v);
+}
+
+// Matrix items per reduction chunk: a system with more items than this sums
+// its item partials in two levels (chunks of kChunk items, then the chunk sums),
+// so the warp that finishes a large system reads a few thousand partials
+// instead of tens of thousands one after the other.
+constexpr int kChunk = 32;
 
 // Rows [r0, r1) of one tile, by one warp with L lanes per block row; vals / cols
 // point at the tile's first block and rowptr at row r0's pointer (shared
@@ -478,10 +498,14 @@ __device__ __forceinline__ bool warp_stage_wait(uint64_t *bar, unsigned parity, 
 
 // End of a matrix item in a warp: publish its partials; the warp that
 // completes the system's last item takes the reduction and the decision.
+// Systems with more than kChunk items: the warp that finishes a chunk's last
+// item sums the chunk (in item order) into the partial slot of the chunk's
+// first item (cticket[first item] counts the chunk's finished items); the warp
+// that finishes the last chunk sums the chunk sums in chunk order.
 template <int KIND>
 __device__ __forceinline__ void finish_item(const BatchSys *__restrict__ sys, BatchScal *__restrict__ scal,
-                                            double *__restrict__ part, int it, int s, int parity, double dot1,
-                                            double dot2, int lane) {
+                                            double *__restrict__ part, int32_t *__restrict__ cticket, int it, int s,
+                                            int parity, double dot1, double dot2, int lane) {
     dot1 = warp_sum(dot1);
     if (KIND == SP_BICG_T) dot2 = warp_sum(dot2);
     if (lane == 0) {
@@ -489,9 +513,25 @@ __device__ __forceinline__ void finish_item(const BatchSys *__restrict__ sys, Ba
         if (KIND == SP_BICG_T) part[2 * (int64_t)it + 1] = dot2;
     }
     const int ib = sys[s].mitem_begin, ie = sys[s].mitem_end;
-    if (!warp_last_of_system(&scal[s], ie - ib, lane)) return;
-    const double a = warp_sum_items(part, ib, ie, 0, lane);
-    const double tt = KIND == SP_BICG_T ? warp_sum_items(part, ib, ie, 1, lane) : 0.0;
+    double a, tt = 0.0;
+    if (ie - ib <= kChunk) {
+        if (!warp_last_of_system(&scal[s], ie - ib, lane)) return;
+        a = warp_sum_items(part, ib, ie, 0, lane);
+        if (KIND == SP_BICG_T) tt = warp_sum_items(part, ib, ie, 1, lane);
+    } else {
+        const int cb = ib + (it - ib) / kChunk * kChunk, ce = min(ie, cb + kChunk);
+        if (!warp_last_of(&cticket[cb], ce - cb, lane)) return;
+        const double ca = warp_sum_items(part, cb, ce, 0, lane);
+        const double ct = KIND == SP_BICG_T ? warp_sum_items(part, cb, ce, 1, lane) : 0.0;
+        if (lane == 0) {
+            part[2 * (int64_t)cb] = ca;
+            if (KIND == SP_BICG_T) part[2 * (int64_t)cb + 1] = ct;
+        }
+        const int nch = (ie - ib + kChunk - 1) / kChunk;
+        if (!warp_last_of_system(&scal[s], nch, lane)) return;
+        a = warp_sum_strided(part, ib, nch, kChunk, 0, lane);
+        if (KIND == SP_BICG_T) tt = warp_sum_strided(part, ib, nch, kChunk, 1, lane);
+    }
     if (lane != 0) return;
     BatchScal &sc = scal[s];
     if (KIND == SP_CG) {
@@ -509,9 +549,10 @@ __device__ __forceinline__ void finish_item(const BatchSys *__restrict__ sys, Ba
 }
 
 // Direct-load SpMV of one group (no staging): each warp takes whole items; L
-// lanes per block row, each lane loading up to four whole blocks (values with
-// vector loads and an L2 evict-first hint, columns, gathered x) before using
-// them.  Same operations and reductions as k_batch_spmv.
+// lanes per block row, each lane loading up to U whole blocks (values with
+// vector loads and an L2 evict-first hint, columns) and then the gathered x
+// before using them; the next row group's bounds are loaded one step ahead.
+// Same operations and reductions as k_batch_spmv.
 template <int B, int L, int KIND, typename VT>
 __device__ __forceinline__ void direct_rows(const int32_t *__restrict__ rowptr, int r0, int r1,
                                             const VT *__restrict__ val, const int32_t *__restrict__ col,
@@ -520,39 +561,41 @@ __device__ __forceinline__ void direct_rows(const int32_t *__restrict__ rowptr, 
                                             uint64_t pol) {
     constexpr int B2 = B * B;
     constexpr int G = 32 / L;
-    constexpr int U = 4;
+    constexpr int U = B == 1 ? 4 : (B == 2 ? 2 : 1);
     const int glane = lane % L, grp = lane / L;
-    for (int rb = r0; rb < r1; rb += G) {
-        const int r = rb + grp;
+    int r = r0 + grp;
+    int rs = 0, re = 0;
+    if (r < r1) { rs = __ldg(rowptr + r); re = __ldg(rowptr + r + 1); }
+#pragma unroll 1
+    for (int rb = r0; rb < r1; rb += G, r += G) {
+        int rs_n = 0, re_n = 0;
+        if (r + G < r1) { rs_n = __ldg(rowptr + r + G); re_n = __ldg(rowptr + r + G + 1); }
         double acc[B];
 #pragma unroll
         for (int i = 0; i < B; ++i) acc[i] = 0;
-        if (r < r1) {
-            const int rs = rowptr[r], re = rowptr[r + 1];
-            for (int j0 = rs + glane; j0 < re; j0 += U * L) {
-                int c[U];
-                double v[U][B2], x[U][B];
+#pragma unroll 1
+        for (int j0 = rs + glane; j0 < re; j0 += U * L) {
+            int c[U];
+            double v[U][B2], x[U][B];
 #pragma unroll
-                for (int u = 0; u < U; ++u) {
-                    const int j = j0 + u * L;
-                    c[u] = j < re ? __ldg(col + j) : -1;
+            for (int u = 0; u < U; ++u) {
+                const int j = j0 + u * L;
+                c[u] = 0;
+                if (j < re) {
+                    c[u] = ld_stream_i(col + j, pol);
+                    load_block<B2>(val + (int64_t)j * B2, v[u], pol);
                 }
+            }
 #pragma unroll
-                for (int u = 0; u < U; ++u) {
-                    const int j = j0 + u * L;
-                    if (c[u] >= 0) {
-                        load_block<B2>(val + (int64_t)j * B2, v[u], pol);
-                        load_x<B>(xin + (int64_t)B * c[u], x[u]);
-                    }
-                }
+            for (int u = 0; u < U; ++u)
+                if (j0 + u * L < re) load_x<B>(xin + (int64_t)B * c[u], x[u]);
 #pragma unroll
-                for (int u = 0; u < U; ++u) {
-                    if (c[u] >= 0) {
+            for (int u = 0; u < U; ++u) {
+                if (j0 + u * L < re) {
 #pragma unroll
-                        for (int i = 0; i < B; ++i)
+                    for (int i = 0; i < B; ++i)
 #pragma unroll
-                            for (int k = 0; k < B; ++k) acc[i] = fma(v[u][i * B + k], x[u][k], acc[i]);
-                    }
+                        for (int k = 0; k < B; ++k) acc[i] = fma(v[u][i * B + k], x[u][k], acc[i]);
                 }
             }
         }
@@ -568,35 +611,42 @@ __device__ __forceinline__ void direct_rows(const int32_t *__restrict__ rowptr, 
                 if (KIND == SP_BICG_T) dot2 = fma(acc[i], acc[i], dot2);
             }
         }
+        rs = rs_n;
+        re = re_n;
     }
 }
 
+// Each warp walks its items (grid stride), loading the next item's descriptor
+// while it works on the current one.
 template <int B, int L, int KIND>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 3)
 k_batch_spmv_direct(const BatchMItem *__restrict__ items, const int32_t *__restrict__ ranges, int g,
                     const BatchSys *__restrict__ sys, BatchScal *__restrict__ scal, double *__restrict__ part,
-                    int parity, int commit) {
+                    int32_t *__restrict__ cticket, int parity, int commit) {
     const int lane = threadIdx.x & 31;
     const int W = gridDim.x * (blockDim.x >> 5);
     const int g1 = ranges[g + 1];
     const uint64_t pol = evict_first_policy();
-    for (int it = ranges[g] + blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); it < g1; it += W) {
-        const BatchMItem item = items[it];
-        const int s = item.sys;
+    int it = ranges[g] + blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    int s_n = 0, r0_n = 0, r1_n = 0;  // the item to work on next
+    if (it < g1) { s_n = items[it].sys; r0_n = items[it].row_begin; r1_n = items[it].row_end; }
+    for (; it < g1; it += W) {
+        const int s = s_n, r0 = r0_n, r1 = r1_n;
+        if (it + W < g1) { s_n = items[it + W].sys; r0_n = items[it + W].row_begin; r1_n = items[it + W].row_end; }
         int act = lane == 0 ? activity(&scal[s], KIND == SP_VERIFY ? ACT_VERIFY : ACT_ITER) : 0;
-        if (!__shfl_sync(0xffffffffu, act, 0)) continue;
-        const BatchSys &d = sys[s];
-        const double *xin = KIND == SP_CG ? d.p : KIND == SP_VERIFY ? d.x : KIND == SP_BICG_V ? d.ph : d.sh;
-        double *out = (KIND == SP_CG || KIND == SP_VERIFY) ? d.q : KIND == SP_BICG_V ? d.v : d.t;
-        const double *w = KIND == SP_CG ? d.p : KIND == SP_BICG_V ? d.r0 : d.s;
-        const int r0 = item.tile_begin < item.tile_end ? d.tiles[item.tile_begin] : 0;
-        const int r1 = item.tile_begin < item.tile_end ? d.tiles[item.tile_end] : 0;
-        double dot1 = 0, dot2 = 0;
-        if (KIND != SP_VERIFY && d.precision == YG_PREC_MIXED)
-            direct_rows<B, L, KIND, float>(d.rowptr, r0, r1, d.val32, d.col, xin, out, w, dot1, dot2, lane, pol);
-        else
-            direct_rows<B, L, KIND, double>(d.rowptr, r0, r1, d.val, d.col, xin, out, w, dot1, dot2, lane, pol);
-        if (KIND != SP_VERIFY && commit) finish_item<KIND>(sys, scal, part, it, s, parity, dot1, dot2, lane);
+        if (__shfl_sync(0xffffffffu, act, 0)) {
+            const BatchSys &d = sys[s];
+            const double *xin = KIND == SP_CG ? d.p : KIND == SP_VERIFY ? d.x : KIND == SP_BICG_V ? d.ph : d.sh;
+            double *out = (KIND == SP_CG || KIND == SP_VERIFY) ? d.q : KIND == SP_BICG_V ? d.v : d.t;
+            const double *w = KIND == SP_CG ? d.p : KIND == SP_BICG_V ? d.r0 : d.s;
+            double dot1 = 0, dot2 = 0;
+            if (KIND != SP_VERIFY && d.precision == YG_PREC_MIXED)
+                direct_rows<B, L, KIND, float>(d.rowptr, r0, r1, d.val32, d.col, xin, out, w, dot1, dot2, lane, pol);
+            else
+                direct_rows<B, L, KIND, double>(d.rowptr, r0, r1, d.val, d.col, xin, out, w, dot1, dot2, lane, pol);
+            if (KIND != SP_VERIFY && commit)
+                finish_item<KIND>(sys, scal, part, cticket, it, s, parity, dot1, dot2, lane);
+        }
     }
 }
 
@@ -615,8 +665,8 @@ k_batch_spmv_direct(const BatchMItem *__restrict__ items, const int32_t *__restr
 template <int B, int L, int KIND>
 __global__ void __launch_bounds__(WCfg<B>::WARPS * 32)
 k_batch_spmv(const BatchMItem *__restrict__ items, const int32_t *__restrict__ ranges, int g,
-             const BatchSys *__restrict__ sys, BatchScal *__restrict__ scal, double *__restrict__ part, int parity,
-             int commit, int32_t *__restrict__ err) {
+             const BatchSys *__restrict__ sys, BatchScal *__restrict__ scal, double *__restrict__ part,
+             int32_t *__restrict__ cticket, int parity, int commit, int32_t *__restrict__ err) {
     using S = WStage<B>;
     constexpr int B2 = B * B;
     constexpr int CAP = WCfg<B>::CAP, NST = WCfg<B>::NST, WARPS = WCfg<B>::WARPS;
@@ -728,7 +778,8 @@ k_batch_spmv(const BatchMItem *__restrict__ items, const int32_t *__restrict__ r
         ++seq_wait;
         __syncwarp();  // the stage is free for the next issue
         if (h.last) {
-            if (KIND != SP_VERIFY && commit) finish_item<KIND>(sys, scal, part, ci, cs, parity, dot1, dot2, lane);
+            if (KIND != SP_VERIFY && commit)
+                finish_item<KIND>(sys, scal, part, cticket, ci, cs, parity, dot1, dot2, lane);
             dot1 = dot2 = 0;
         }
     }
@@ -1120,10 +1171,11 @@ static void launch_spmv_l(yg_batch bt, int variant, int g, int parity, int commi
     yg_context ctx = bt->ctx;
     if (variant == 1) {
         k_batch_spmv_direct<B, L, KIND><<<direct_grid<B, L, KIND>(ctx), 256, 0, ctx->stream>>>(
-            bt->d_mitems, bt->d_ranges, g, bt->d_sys, bt->d_scal, bt->d_mpart, parity, commit);
+            bt->d_mitems, bt->d_ranges, g, bt->d_sys, bt->d_scal, bt->d_mpart, bt->d_cticket, parity, commit);
     } else {
         k_batch_spmv<B, L, KIND><<<spmv_grid<B, L, KIND>(ctx), WCfg<B>::WARPS * 32, WStage<B>::SMEM, ctx->stream>>>(
-            bt->d_mitems, bt->d_ranges, g, bt->d_sys, bt->d_scal, bt->d_mpart, parity, commit, ctx->d_err);
+            bt->d_mitems, bt->d_ranges, g, bt->d_sys, bt->d_scal, bt->d_mpart, bt->d_cticket, parity, commit,
+            ctx->d_err);
     }
     YG_LAUNCHED(ctx);
 }
@@ -1269,8 +1321,12 @@ static yg_status rebuild_items(yg_batch bt) {
             d.mitem_begin = (int32_t)mitems.size();
             d.vitem_begin = (int32_t)vitems.size();
             if (sys_live(bt, s)) {
-                for (int t0 = 0; t0 < d.ntiles; t0 += T) mitems.push_back({s, t0, std::min(d.ntiles, t0 + T), 0});
-                if (d.ntiles == 0) mitems.push_back({s, 0, 0, 0});
+                const std::vector<int32_t> &tl = bt->tiles[s];
+                for (int t0 = 0; t0 < d.ntiles; t0 += T) {
+                    const int t1 = std::min(d.ntiles, t0 + T);
+                    mitems.push_back({s, t0, t1, tl[t0], tl[t1], {0, 0, 0}});
+                }
+                if (d.ntiles == 0) mitems.push_back({s, 0, 0, 0, 0, {0, 0, 0}});
                 for (int r0 = 0; r0 < d.nbrows; r0 += VR) vitems.push_back({s, r0, std::min(d.nbrows, r0 + VR), 0});
                 if (d.nbrows == 0) vitems.push_back({s, 0, 0, 0});
             }
@@ -1282,6 +1338,14 @@ static yg_status rebuild_items(yg_batch bt) {
     ranges[kVR + kGroups] = ranges[kVR + kGroups + 1] = (int32_t)vitems.size();
     const bool regrow = (int64_t)mitems.size() > bt->max_mitems || (int64_t)vitems.size() > bt->max_vitems;
     YG_TRY(grow(ctx, &bt->d_mitems, &bt->max_mitems, mitems.size(), &bt->d_mpart, (double **)nullptr));
+    if (bt->cticket_cap < bt->max_mitems) {  // grew: the stream is idle (grow synchronised it)
+        dev_free(ctx, bt->d_cticket);
+        bt->d_cticket = nullptr;
+        bt->cticket_cap = 0;
+        YG_TRY(dev_alloc_t(ctx, &bt->d_cticket, bt->max_mitems));
+        YG_CUDA(cudaMemsetAsync(bt->d_cticket, 0, sizeof(int32_t) * bt->max_mitems, ctx->stream));
+        bt->cticket_cap = bt->max_mitems;
+    }
     YG_TRY(grow(ctx, &bt->d_vitems, &bt->max_vitems, vitems.size(), &bt->d_vpart, &bt->d_vpart2));
     if (regrow) drop_graph(bt);  // the graph captured the old pointers
     YG_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -1406,7 +1470,7 @@ extern "C" yg_status yg_batch_destroy(yg_batch bt) {
     for (int s = 0; s < bt->capacity; ++s)
         if (bt->used[s]) release_slot(bt, s);
     for (void *p : {(void *)bt->d_sys, (void *)bt->d_scal, (void *)bt->d_mitems, (void *)bt->d_vitems, (void *)bt->d_ranges,
-                    (void *)bt->d_mpart, (void *)bt->d_vpart, (void *)bt->d_vpart2})
+                    (void *)bt->d_mpart, (void *)bt->d_cticket, (void *)bt->d_vpart, (void *)bt->d_vpart2})
         dev_free(bt->ctx, p);
     delete bt;
     return YG_OK;

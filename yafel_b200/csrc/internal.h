@@ -99,7 +99,8 @@ struct yg_matrix_t {
     float *d_val32 = nullptr;     // optional FP32 copy
     int32_t *d_diag = nullptr;    // position of the diagonal block in each block row, -1 if absent
     int lanes = 32;               // SpMV lanes per block row (flat variant)
-    int variant = 0;              // SpMV variant: 0 flat lane-strided, 1 cp.async staged, 2 TMA bulk staged (B = 2, 3)
+    int variant = 0;              // SpMV variant: 0 flat lane-strided, 1 cp.async staged, 2 TMA bulk staged (B = 2, 3),
+                                  // 3 TMA row tiles (B = 1)
     int variant32 = -1, lanes32 = 32;  // choice for FP32 values (-1: as for FP64)
     bool tuned32 = false;
     bool tuned = false;
@@ -111,6 +112,11 @@ struct yg_matrix_t {
     double *d_bcg = nullptr, *d_bcq = nullptr, *d_bcvals = nullptr;
     int64_t *d_bcdofs = nullptr;
     int64_t bc_cap = 0;
+    // Row tiles of the tiled CSR SpMV (variant 3): table k holds the first row
+    // of each tile of at most (256 << k) entries, then the row count
+    int32_t *d_ctiles[3] = {nullptr, nullptr, nullptr};
+    int64_t nctiles[3] = {0, 0, 0};
+    int32_t row_min = -1, row_max = -1;  // entries per row, -1 until measured
     int64_t rows() const { return nbrows * block; }
     int64_t cols() const { return nbcols * block; }
 };
@@ -147,6 +153,9 @@ int spmv_default_grid(yg_matrix A);
 int spmv_grid_for(yg_matrix A, int precision);
 void spmv_autotune(yg_matrix A);
 yg_status spmv_autotune_device(yg_matrix A);
+// Builds what SpMV variant/lanes needs before its first launch (the row tiles of
+// variant 3); YG_UNSUPPORTED when the matrix cannot use it.  Not during capture.
+yg_status spmv_prepare(yg_matrix A, int variant, int lanes);
 yg_status vector_dot(yg_context ctx, const double *a, const double *b, int64_t n, double *out);
 yg_status check_device_error(yg_context ctx);
 yg_status matrix_build_diag(yg_matrix A);

@@ -22,7 +22,7 @@ namespace yg {
 // DOT = 0: y = A x.  DOT = 1: also per-block sums of w.y.  DOT = 2: per-block
 // sums of w.y and y.y (partials[2b], partials[2b+1]).
 template <int B, int L, typename VT, int DOT>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, B == 1 ? 8 : 1)
 k_bcsr_spmv(int64_t nbrows, const int32_t *__restrict__ rowptr, const int32_t *__restrict__ col,
             const VT *__restrict__ val, const double *__restrict__ x, double *__restrict__ y,
             const double *__restrict__ w, double *__restrict__ partials, const int32_t *__restrict__ flag) {
@@ -36,6 +36,49 @@ k_bcsr_spmv(int64_t nbrows, const int32_t *__restrict__ rowptr, const int32_t *_
     const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     double dot = 0, yy = 0;
+    if constexpr (B == 1) {
+        // Scalar rows: a lane issues the loads of up to U of its entries before
+        // the first gather, and the next step's row bounds are fetched one step
+        // ahead, so a step costs one value/column round trip and one gather round
+        // trip instead of one per U/4 entries.  The accumulation order (the lane's
+        // entries left to right, then the butterfly) is that of the loop below.
+        constexpr int U = 8;
+        const int64_t step = nwarps * GPW;
+        int64_t r = warp * GPW + lane / L;
+        int rs = 0, re = 0;
+        if (r < nbrows) { rs = __ldg(rowptr + r); re = __ldg(rowptr + r + 1); }
+        for (int64_t rb = warp * GPW; rb < nbrows; rb += step, r += step) {
+            int rs_n = 0, re_n = 0;
+            if (r + step < nbrows) { rs_n = __ldg(rowptr + r + step); re_n = __ldg(rowptr + r + step + 1); }
+            double acc = 0;
+            for (int k0 = rs + glane; k0 < re; k0 += L * U) {
+                double v[U];
+                int c[U];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int k = k0 + u * L;
+                    v[u] = 0;
+                    c[u] = 0;
+                    if (k < re) {
+                        v[u] = ld_stream(val + k, pol);
+                        c[u] = ld_stream_i(col + k, pol);
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u)
+                    if (k0 + u * L < re) acc = fma(v[u], __ldg(x + c[u]), acc);
+            }
+#pragma unroll
+            for (int o = L / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+            if (r < nbrows && glane == 0) {
+                y[r] = acc;
+                if (DOT >= 1) dot = fma(acc, w[r], dot);
+                if (DOT == 2) yy = fma(acc, acc, yy);
+            }
+            rs = rs_n;
+            re = re_n;
+        }
+    } else
     for (int64_t rb = warp * GPW; rb < nbrows; rb += nwarps * GPW) {
         const int64_t r = rb + lane / L;
         double acc[B];
@@ -433,6 +476,327 @@ k_bcsr_spmv_tma(int64_t nbrows, const int32_t *__restrict__ rowptr, const int32_
     }
 }
 
+// ---------------------------------------------------------------------------
+// Row-tile variant for CSR (block size 1, variant 3).  Long scalar rows (3D
+// order-2 elements: 27-125 entries) leave the flat kernel latency bound: each
+// warp's row costs a row-pointer load, then the value and column loads, then
+// the gathers of x, one after the other.  Here the rows are cut once into
+// tiles of whole consecutive rows holding at most CAP entries (a table of tile
+// starts, built on the device from the row pointers).  Each warp streams its
+// tiles (grid stride) through a ring of NST shared-memory stages: one lane
+// fetches a tile's values, columns and row pointers with three bulk
+// asynchronous copies completing on the stage's mbarrier, running NST-1 tiles
+// ahead, with the tile bounds of the next 32 tiles prefetched by the whole
+// warp.  Consuming a tile, the lanes first form all its products v_k x[c_k]
+// (up to U independent gathers per lane in flight) into a per-warp buffer,
+// then lane r sums row r's products in entry order.  So each row is summed
+// left to right, the order of the reference's csr_spmv loop, and the result
+// does not depend on the launch shape.  Waits are bounded as in the TMA
+// variant above.
+template <typename VT, int CAP_, int NST_, int WARPS_>
+struct CsrCfg {
+    static constexpr int CAP = CAP_, NST = NST_, WARPS = WARPS_;
+    static constexpr int U = CAP / 32 < 16 ? CAP / 32 : 16;  // products per lane per round
+    static constexpr int VB = (CAP * (int)sizeof(VT) + 32 + 15) & ~15;
+    static constexpr int CB = (CAP * 4 + 32 + 15) & ~15;
+    static constexpr int RB = ((CAP + 1) * 4 + 32 + 15) & ~15;
+    static constexpr int STAGE = VB + CB + RB;
+    static constexpr int PB = CAP * 8;
+    static constexpr int WARP_BYTES = NST * STAGE + PB;
+    static constexpr int SMEM = WARPS * WARP_BYTES + WARPS * NST * 8;
+};
+
+template <typename VT, int DOT, typename C>
+__global__ void __launch_bounds__(C::WARPS * 32)
+k_csr_spmv_tiles(int64_t ntiles, const int32_t *__restrict__ tiles, const int32_t *__restrict__ rowptr,
+                 const int32_t *__restrict__ col, const VT *__restrict__ val, const double *__restrict__ x,
+                 double *__restrict__ y, const double *__restrict__ w, double *__restrict__ partials,
+                 const int32_t *__restrict__ flag, int32_t *__restrict__ err) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ double red[C::WARPS + 1];
+    __shared__ int hdr[C::WARPS][C::NST][4];  // r0, r1, e0, e1 of the tile in each stage
+    if (flag && read_flag(flag)) return;
+    constexpr int VS = (int)sizeof(VT);
+    const uint64_t pol = evict_first_policy();
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    unsigned char *ring = smem_raw + (size_t)wib * C::WARP_BYTES;
+    double *prod = reinterpret_cast<double *>(ring + (size_t)C::NST * C::STAGE);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw + (size_t)C::WARPS * C::WARP_BYTES) + wib * C::NST;
+    if (lane == 0)
+        for (int k = 0; k < C::NST; ++k) mbar_init(&bars[k], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    __syncwarp();
+    const int64_t stride = (int64_t)gridDim.x * C::WARPS;
+    const char *vbytes = reinterpret_cast<const char *>(val);
+    const char *cbytes = reinterpret_cast<const char *>(col);
+    const char *rbytes = reinterpret_cast<const char *>(rowptr);
+
+    // tile bounds of the next 32 tiles of this warp, lane k holding tile tb + k*stride
+    int64_t t_issue = (int64_t)blockIdx.x * C::WARPS + wib;
+    int64_t tb = t_issue;
+    int nb_used = 32;
+    int d_r0 = 0, d_r1 = 0, d_e0 = 0, d_e1 = 0;
+    auto issue = [&](int st) {
+        if (nb_used == 32) {
+            tb = t_issue;
+            const int64_t t = tb + (int64_t)lane * stride;
+            d_r0 = d_r1 = d_e0 = d_e1 = 0;
+            if (t < ntiles) {
+                d_r0 = __ldg(tiles + t);
+                d_r1 = __ldg(tiles + t + 1);
+                d_e0 = __ldg(rowptr + d_r0);
+                d_e1 = __ldg(rowptr + d_r1);
+            }
+            nb_used = 0;
+        }
+        const int r0 = __shfl_sync(0xffffffffu, d_r0, nb_used), r1 = __shfl_sync(0xffffffffu, d_r1, nb_used);
+        const int e0 = __shfl_sync(0xffffffffu, d_e0, nb_used), e1 = __shfl_sync(0xffffffffu, d_e1, nb_used);
+        ++nb_used;
+        t_issue += stride;
+        if (lane == 0) {
+            hdr[wib][st][0] = r0;
+            hdr[wib][st][1] = r1;
+            hdr[wib][st][2] = e0;
+            hdr[wib][st][3] = e1;
+            if (r1 > r0) {
+                const int64_t vs = (int64_t)e0 * VS, va = vs & ~(int64_t)15, ve = ((int64_t)e1 * VS + 15) & ~(int64_t)15;
+                const int64_t cs = (int64_t)e0 * 4, ca = cs & ~(int64_t)15, ce = ((int64_t)e1 * 4 + 15) & ~(int64_t)15;
+                const int64_t rs = (int64_t)r0 * 4, ra = rs & ~(int64_t)15, re = ((int64_t)(r1 + 1) * 4 + 15) & ~(int64_t)15;
+                unsigned char *dst = ring + (size_t)st * C::STAGE;
+                mbar_expect_tx(&bars[st], (unsigned)((ve - va) + (ce - ca) + (re - ra)));
+                bulk_g2s(dst, vbytes + va, (unsigned)(ve - va), &bars[st], pol);
+                bulk_g2s(dst + C::VB, cbytes + ca, (unsigned)(ce - ca), &bars[st], pol);
+                bulk_g2s(dst + C::VB + C::CB, rbytes + ra, (unsigned)(re - ra), &bars[st], pol);
+            } else {
+                mbar_expect_tx(&bars[st], 0);  // completes the phase with no transfer
+            }
+        }
+    };
+
+#pragma unroll
+    for (int k = 0; k < C::NST - 1; ++k) issue(k);
+    double dot = 0, yy = 0;
+    int st = 0;
+    unsigned phase = 0;  // bit k: parity of stage k's next completion
+    bool timed_out = false;
+    for (int64_t t = (int64_t)blockIdx.x * C::WARPS + wib; t < ntiles; t += stride) {
+        issue((st + C::NST - 1) % C::NST);
+        int ok = 1;
+        if (lane == 0) {
+            long long spins = 0;
+            while (!mbar_try_wait(&bars[st], (phase >> st) & 1u))
+                if (++spins > kSpinLimit) { ok = 0; break; }
+        }
+        ok = __shfl_sync(0xffffffffu, ok, 0);
+        if (!ok) { timed_out = true; break; }
+        if (lane != 0) mbar_try_wait(&bars[st], (phase >> st) & 1u);
+        phase ^= (1u << st);
+        __syncwarp();
+        const int r0 = hdr[wib][st][0], r1 = hdr[wib][st][1], e0 = hdr[wib][st][2], e1 = hdr[wib][st][3];
+        const int E = e1 - e0, R = r1 - r0;
+        const unsigned char *stg = ring + (size_t)st * C::STAGE;
+        const VT *v = reinterpret_cast<const VT *>(stg + (((int64_t)e0 * VS) & 15));
+        const int32_t *c = reinterpret_cast<const int32_t *>(stg + C::VB + (((int64_t)e0 * 4) & 15));
+        const int32_t *rp = reinterpret_cast<const int32_t *>(stg + C::VB + C::CB + (((int64_t)r0 * 4) & 15));
+        for (int k0 = 0; k0 < E; k0 += 32 * C::U) {
+            double pv[C::U];
+#pragma unroll
+            for (int u = 0; u < C::U; ++u) {
+                const int k = k0 + u * 32 + lane;
+                pv[u] = 0;
+                if (k < E) pv[u] = (double)v[k] * __ldg(x + c[k]);
+            }
+#pragma unroll
+            for (int u = 0; u < C::U; ++u) {
+                const int k = k0 + u * 32 + lane;
+                if (k < E) prod[k] = pv[u];
+            }
+        }
+        __syncwarp();
+        for (int r = lane; r < R; r += 32) {
+            const int a = rp[r] - e0, b = rp[r + 1] - e0;
+            double sum = 0;
+            for (int k = a; k < b; ++k) sum += prod[k];
+            y[r0 + r] = sum;
+            if (DOT >= 1) dot = fma(sum, w[r0 + r], dot);
+            if (DOT == 2) yy = fma(sum, sum, yy);
+        }
+        __syncwarp();  // the stage and the product buffer are free again
+        st = (st + 1) % C::NST;
+    }
+    if (timed_out && lane == 0 && err) atomicExch(err, (int32_t)YG_TIMEOUT);
+    // drain the copies still in flight into this warp's stages (bounded): NST-1
+    // after the loop, all NST after a timeout (the failed stage included)
+    if (lane == 0) {
+        const int outstanding = timed_out ? C::NST : C::NST - 1;
+        for (int k = 0; k < outstanding; ++k) {
+            const int s2 = (st + k) % C::NST;
+            long long spins = 0;
+            while (!mbar_try_wait(&bars[s2], (phase >> s2) & 1u) && ++spins <= kSpinLimit) {
+            }
+            phase ^= (1u << s2);
+        }
+    }
+    __syncwarp();
+    if (DOT) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            dot += __shfl_xor_sync(0xffffffffu, dot, o);
+            if (DOT == 2) yy += __shfl_xor_sync(0xffffffffu, yy, o);
+        }
+        if (lane == 0) red[wib] = dot;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double sum = 0;
+            for (int i = 0; i < C::WARPS; ++i) sum += red[i];
+            if (DOT == 1) partials[blockIdx.x] = sum;
+            else partials[2 * blockIdx.x] = sum;
+        }
+        if (DOT == 2) {
+            __syncthreads();
+            if (lane == 0) red[wib] = yy;
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                double sum = 0;
+                for (int i = 0; i < C::WARPS; ++i) sum += red[i];
+                partials[2 * blockIdx.x + 1] = sum;
+            }
+        }
+    }
+}
+
+// Row-tile configurations (tile entries, ring depth, warps per CTA), selected by
+// the `lanes` field of a variant-3 matrix; each fills one SM's shared memory.
+template <typename VT> using CsrL1 = CsrCfg<VT, 512, 3, 6>;
+template <typename VT> using CsrL2 = CsrCfg<VT, 512, 2, 8>;
+template <typename VT> using CsrL4 = CsrCfg<VT, 256, 3, 12>;
+template <typename VT> using CsrL8 = CsrCfg<VT, 1024, 2, 4>;
+
+// tile-table index of a configuration: capacity 256 << k entries
+static int csr_table(int lanes) { return lanes == 4 ? 0 : lanes == 8 ? 2 : 1; }
+static bool csr_lanes_ok(int lanes) { return lanes == 1 || lanes == 2 || lanes == 4 || lanes == 8; }
+
+__global__ void k_row_extent(int64_t n, const int32_t *__restrict__ rowptr, int32_t *__restrict__ out) {
+    int lo = INT32_MAX, hi = 0;
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
+        const int len = rowptr[r + 1] - rowptr[r];
+        lo = min(lo, len);
+        hi = max(hi, len);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+        hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMin(out, lo);
+        atomicMax(out + 1, hi);
+    }
+}
+
+// tiles[t] = first row whose first entry is at or after t*per (t = 0..nt; the
+// last is n): the rows starting in [t*per, (t+1)*per) form tile t, whose entries
+// then span at most per - 1 + (longest row) positions.
+__global__ void k_row_tiles(int64_t n, int64_t nt, int64_t per, const int32_t *__restrict__ rowptr,
+                            int32_t *__restrict__ tiles) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t <= nt; t += (int64_t)gridDim.x * blockDim.x) {
+        if (t == nt) { tiles[t] = (int32_t)n; continue; }
+        const int64_t target = t * per;
+        int64_t lo = 0, hi = n;  // first r in [0, n] with rowptr[r] >= target
+        while (lo < hi) {
+            const int64_t mid = (lo + hi) >> 1;
+            if (rowptr[mid] < target) lo = mid + 1;
+            else hi = mid;
+        }
+        tiles[t] = (int32_t)lo;
+    }
+}
+
+// Row tiles of capacity 256 << k for A (block size 1).  Needs every row to hold
+// at least one and at most `cap` entries.
+static yg_status csr_tiles_build(yg_matrix A, int k) {
+    if (A->block != 1 || A->nbrows < 1) return fail(YG_UNSUPPORTED, "row-tile SpMV needs a non-empty CSR matrix");
+    if (A->d_ctiles[k]) return YG_OK;
+    yg_context ctx = A->ctx;
+    cudaStreamCaptureStatus cs;
+    YG_CUDA(cudaStreamIsCapturing(ctx->stream, &cs));
+    if (cs != cudaStreamCaptureStatusNone) return fail(YG_BAD_ARG, "row tiles cannot be built during stream capture");
+    if (A->row_min < 0) {
+        int32_t *d = nullptr;
+        YG_TRY(dev_alloc_t(ctx, &d, 2));
+        const int32_t init[2] = {INT32_MAX, 0};
+        int32_t h[2];
+        cudaMemcpyAsync(d, init, sizeof(init), cudaMemcpyHostToDevice, ctx->stream);
+        int blocks = (int)std::min<int64_t>((A->nbrows + kThreads - 1) / kThreads, (int64_t)ctx->num_sms * 4);
+        k_row_extent<<<blocks, kThreads, 0, ctx->stream>>>(A->nbrows, A->d_rowptr, d);
+        YG_LAUNCHED(ctx);
+        cudaMemcpyAsync(h, d, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream);
+        cudaError_t e = cudaStreamSynchronize(ctx->stream);
+        dev_free(ctx, d);
+        if (e != cudaSuccess) return fail(YG_CUDA_ERROR, "row extent: %s", cudaGetErrorString(e));
+        A->row_min = h[0];
+        A->row_max = h[1];
+    }
+    const int cap = 256 << k;
+    if (A->row_min < 1 || A->row_max > cap)
+        return fail(YG_UNSUPPORTED, "row-tile SpMV needs 1..%d entries per row (rows hold %d..%d)", cap, A->row_min,
+                    A->row_max);
+    const int64_t per = cap - A->row_max + 1;
+    const int64_t nt = (A->nnzb + per - 1) / per;
+    YG_TRY(dev_alloc_t(ctx, &A->d_ctiles[k], nt + 1));
+    int blocks = (int)std::min<int64_t>((nt + kThreads) / kThreads, (int64_t)ctx->num_sms * 4);
+    k_row_tiles<<<blocks, kThreads, 0, ctx->stream>>>(A->nbrows, nt, per, A->d_rowptr, A->d_ctiles[k]);
+    YG_LAUNCHED(ctx);
+    YG_CUDA(cudaGetLastError());
+    A->nctiles[k] = nt;
+    return YG_OK;
+}
+
+yg_status spmv_prepare(yg_matrix A, int variant, int lanes) {
+    if (variant != 3) return YG_OK;
+    if (!csr_lanes_ok(lanes)) return fail(YG_BAD_ARG, "row-tile SpMV configurations are lanes 1, 2, 4, 8");
+    return csr_tiles_build(A, csr_table(lanes));
+}
+
+template <typename VT, int DOT, typename C>
+static yg_status launch_csr_cfg(yg_matrix A, int k, const VT *val, const double *x, double *y, const double *w,
+                                double *partials, const int32_t *flag, int grid, cudaStream_t st) {
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_csr_spmv_tiles<VT, DOT, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM);
+        attr = true;
+    }
+    k_csr_spmv_tiles<VT, DOT, C><<<grid, C::WARPS * 32, C::SMEM, st>>>(A->nctiles[k], A->d_ctiles[k], A->d_rowptr,
+                                                                       A->d_col, val, x, y, w, partials, flag,
+                                                                       A->ctx->d_err);
+    YG_LAUNCHED(A->ctx);
+    return YG_OK;
+}
+
+template <typename VT, int DOT>
+static yg_status launch_csr(yg_matrix A, int lanes, const VT *val, const double *x, double *y, const double *w,
+                            double *partials, const int32_t *flag, int grid, cudaStream_t st) {
+    const int k = csr_table(lanes);
+    if (A->block != 1 || !csr_lanes_ok(lanes) || !A->d_ctiles[k])
+        return fail(YG_BAD_ARG, "row-tile SpMV launched without its row tiles (block %d, lanes %d)", A->block, lanes);
+    switch (lanes) {
+    case 1: return launch_csr_cfg<VT, DOT, CsrL1<VT>>(A, k, val, x, y, w, partials, flag, grid, st);
+    case 2: return launch_csr_cfg<VT, DOT, CsrL2<VT>>(A, k, val, x, y, w, partials, flag, grid, st);
+    case 4: return launch_csr_cfg<VT, DOT, CsrL4<VT>>(A, k, val, x, y, w, partials, flag, grid, st);
+    default: return launch_csr_cfg<VT, DOT, CsrL8<VT>>(A, k, val, x, y, w, partials, flag, grid, st);
+    }
+}
+
+template <typename VT>
+static void csr_shape_v(int lanes, int *smem, int *wp) {
+    switch (lanes) {
+    case 1: *smem = CsrL1<VT>::SMEM; *wp = CsrL1<VT>::WARPS; break;
+    case 2: *smem = CsrL2<VT>::SMEM; *wp = CsrL2<VT>::WARPS; break;
+    case 4: *smem = CsrL4<VT>::SMEM; *wp = CsrL4<VT>::WARPS; break;
+    default: *smem = CsrL8<VT>::SMEM; *wp = CsrL8<VT>::WARPS; break;
+    }
+}
+
 template <int B, typename VT, int DOT, typename C>
 static yg_status launch_tma_cfg(yg_matrix A, const VT *val, const double *x, double *y, const double *w,
                                 double *partials, const int32_t *flag, int grid, cudaStream_t st) {
@@ -537,6 +901,7 @@ static yg_status launch_l(yg_matrix A, int lanes, const VT *val, const double *x
 template <typename VT, int DOT>
 static yg_status launch_b(yg_matrix A, int variant, int lanes, const VT *val, const double *x, double *y,
                           const double *w, double *partials, const int32_t *flag, int grid, cudaStream_t st) {
+    if (variant == 3) return launch_csr<VT, DOT>(A, lanes, val, x, y, w, partials, flag, grid, st);
     if (variant == 2 && A->block == 3) return launch_tma<3, VT, DOT>(A, lanes, val, x, y, w, partials, flag, grid, st);
     if (variant == 2 && A->block == 2) return launch_tma<2, VT, DOT>(A, lanes, val, x, y, w, partials, flag, grid, st);
     if (variant == 1 && A->block == 3) return launch_staged<3, VT, DOT>(A, val, x, y, w, partials, flag, grid, st);
@@ -598,12 +963,53 @@ yg_status spmv_launch(yg_matrix A, const double *x, double *y, int precision, do
     return spmv_launch_ex(A, x, y, precision, x, partials, partials ? 1 : 0, flag, grid);
 }
 
+// Resident blocks per SM of the flat kernel (the heaviest, DOT = 2, form) for a
+// block size, lane count and value type; at most 8.
+template <int B, typename VT>
+static int flat_occupancy(int lanes) {
+    static int cache[6] = {0, 0, 0, 0, 0, 0};
+    const int li = lanes == 2 ? 0 : lanes == 4 ? 1 : lanes == 8 ? 2 : lanes == 16 ? 3 : 4;
+    if (!cache[li]) {
+        int n = 0;
+        cudaError_t e;
+        switch (lanes) {
+        case 2: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_bcsr_spmv<B, 2, VT, 2>, kThreads, 0); break;
+        case 4: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_bcsr_spmv<B, 4, VT, 2>, kThreads, 0); break;
+        case 8: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_bcsr_spmv<B, 8, VT, 2>, kThreads, 0); break;
+        case 16: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_bcsr_spmv<B, 16, VT, 2>, kThreads, 0); break;
+        default: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_bcsr_spmv<B, 32, VT, 2>, kThreads, 0); break;
+        }
+        if (e != cudaSuccess) cudaGetLastError();
+        cache[li] = (e != cudaSuccess || n < 1) ? 1 : (n > 8 ? 8 : n);
+    }
+    return cache[li];
+}
+static int flat_blocks_per_sm(int block, int lanes, bool f32) {
+    if (block == 1) return f32 ? flat_occupancy<1, float>(lanes) : flat_occupancy<1, double>(lanes);
+    if (block == 2) return f32 ? flat_occupancy<2, float>(lanes) : flat_occupancy<2, double>(lanes);
+    return f32 ? flat_occupancy<3, float>(lanes) : flat_occupancy<3, double>(lanes);
+}
+
 int spmv_default_grid(yg_matrix A) { return spmv_grid_for(A, YG_PREC_FP64); }
 
 int spmv_grid_for(yg_matrix A, int precision) {
     int variant, lanes;
     choice(A, precision, &variant, &lanes);
     const bool f32 = precision == YG_PREC_MIXED || precision == YG_PREC_MIXED_IR;
+    if (variant == 3) {  // row tiles: as many CTAs as the shared memory holds, a warp per tile
+        int smem = 0, wp = 1;
+        if (f32) csr_shape_v<float>(lanes, &smem, &wp);
+        else csr_shape_v<double>(lanes, &smem, &wp);
+        int per = (220 * 1024) / (smem + 1024);
+        if (per * wp > 64) per = 64 / wp;
+        if (per > 8) per = 8;
+        if (per < 1) per = 1;
+        const int64_t nt = A->nctiles[csr_table(lanes)];
+        int64_t need = (nt + wp - 1) / wp;
+        int64_t g = (int64_t)A->ctx->num_sms * per;
+        if (need < g) g = need;
+        return (int)(g < 1 ? 1 : g);
+    }
     if (variant == 2) {  // TMA: as many CTAs as fit, a warp per row
         int per, wp;
         tma_shape(A, lanes, f32, &per, &wp);
@@ -618,11 +1024,12 @@ int spmv_grid_for(yg_matrix A, int precision) {
         if (need < g) g = need;
         return (int)(g < 1 ? 1 : g);
     }
-    // enough resident warps to keep HBM busy: 8 blocks of 256 threads per SM,
-    // but no more row groups than rows.
+    // as many blocks as are resident at once (one wave: a grid-stride loop over
+    // equal shares would otherwise run a second, thinner wave), at most 8 of 256
+    // threads per SM, and no more row groups than rows.
     int64_t groups_per_block = kThreads / lanes;
     int64_t need = (A->nbrows + groups_per_block - 1) / groups_per_block;
-    int64_t g = (int64_t)A->ctx->num_sms * 8;
+    int64_t g = (int64_t)A->ctx->num_sms * flat_blocks_per_sm(A->block, lanes, f32);
     if (need < g) g = need;
     if (g < 1) g = 1;
     if (g > kMaxReduceBlocks) g = kMaxReduceBlocks;
@@ -666,6 +1073,9 @@ static yg_status tune_precision(yg_matrix A, int precision, double *x, double *y
         cands.push_back({1, 32});
         for (int L : {32, 1, 2, 4, 8, 16}) cands.push_back({2, L});  // TMA configurations
     }
+    if (A->block == 1)
+        for (int L : {1, 2, 4, 8})  // row-tile configurations the matrix's rows fit
+            if (spmv_prepare(A, 3, L) == YG_OK) cands.push_back({3, L});
     const bool f32 = precision != YG_PREC_FP64;
     int *pv = f32 ? &A->variant32 : &A->variant, *pl = f32 ? &A->lanes32 : &A->lanes;
     const int save_v = *pv, save_l = *pl;
@@ -718,7 +1128,7 @@ yg_status spmv_autotune_device(yg_matrix A) {
         const TuneKey key{A->nbrows, A->nnzb, A->block, f32};
         bool hit = false;
         for (const auto &kv : g_tune_cache)
-            if (kv.first == key) {
+            if (kv.first == key && spmv_prepare(A, kv.second.first, kv.second.second) == YG_OK) {
                 (f32 ? A->variant32 : A->variant) = kv.second.first;
                 (f32 ? A->lanes32 : A->lanes) = kv.second.second;
                 hit = true;
