@@ -243,6 +243,10 @@ __device__ __forceinline__ double warp_sum_strided(const double *part, int ib, i
 // so the warp that finishes a large system reads a few thousand partials
 // instead of tens of thousands one after the other.
 constexpr int kChunk = 32;
+// Matrix items of one system at most (longer items beyond): enough for every
+// warp of the grid to take a few, few enough that the per-item publication
+// (fence, ticket, partial) stays small against the item's rows.
+constexpr int kMaxItems = 16384;
 
 // Rows [r0, r1) of one tile, by one warp with L lanes per block row; vals / cols
 // point at the tile's first block and rowptr at row r0's pointer (shared
@@ -1322,8 +1326,10 @@ static yg_status rebuild_items(yg_batch bt) {
             d.vitem_begin = (int32_t)vitems.size();
             if (sys_live(bt, s)) {
                 const std::vector<int32_t> &tl = bt->tiles[s];
-                for (int t0 = 0; t0 < d.ntiles; t0 += T) {
-                    const int t1 = std::min(d.ntiles, t0 + T);
+                // a large system takes longer items: at most kMaxItems of them
+                const int Ts = std::max(T, (d.ntiles + kMaxItems - 1) / kMaxItems);
+                for (int t0 = 0; t0 < d.ntiles; t0 += Ts) {
+                    const int t1 = std::min(d.ntiles, t0 + Ts);
                     mitems.push_back({s, t0, t1, tl[t0], tl[t1], {0, 0, 0}});
                 }
                 if (d.ntiles == 0) mitems.push_back({s, 0, 0, 0, 0, {0, 0, 0}});
