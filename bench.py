@@ -629,10 +629,15 @@ def run_serve(args):
     admitted in arrival order under an HBM budget (`--budget-gb`) and solved
     together in one batch (yg_server_*), in FP64 (the value) and in mixed
     precision; the same requests served one at a time by the plain FP64
-    single-system solvers give the baseline.  Latency = arrival to solution on the host."""
+    single-system solvers give the baseline.  Latency = arrival to solution on the host.
+    Requests are built on a second context of the GPU (its own stream), so their
+    numbering and assembly overlap the block of iterations in flight: after each
+    launch the loop builds admitted requests while the block runs (at least one,
+    at most `--build-per-block`, 0 = no limit)."""
     import yafel_b200 as yb
     from yafel_b200 import workloads
     ctx = yb.Context(0)
+    bctx = yb.Context(0)  # builds: DoF numbering, assembly, boundary conditions
     N = args.requests
     specs = workloads.serving_specs(N)
     arr = workloads.arrivals(N, args.rate)
@@ -660,16 +665,20 @@ def run_serve(args):
                 idx[S.submit(workloads.est_bytes(specs[i]))] = i
                 state["nsub"] += 1
 
-        def admit_build(limit):
-            for _ in range(limit):
+        def admit_build(limit, while_running=False):
+            k = 0
+            while limit <= 0 or k < limit:
+                if while_running and k > 0 and S.ready():
+                    return
                 r = S.admit()
                 if r is None:
                     return
                 i = idx[r]
-                _, K, b, _ = workloads.assemble(specs[i], ctx, mesh=meshes[i])
-                x = yb.DeviceVector(K.rows(), ctx)
+                _, K, b, _ = workloads.assemble(specs[i], bctx, mesh=meshes[i])
+                x = yb.DeviceVector(K.rows(), bctx)
                 x.fill(0.0)
                 pending.append((r, K, b, x, i))
+                k += 1
 
         if clocks:
             clocks.start()
@@ -691,7 +700,7 @@ def run_serve(args):
                 tuned = True
             S.launch()
             take_arrivals()
-            admit_build(args.build_per_block)  # host work overlaps the block
+            admit_build(args.build_per_block, while_running=True)  # host work overlaps the block
             S.wait()
             for r in S.finished():
                 i = idx[r]
@@ -749,7 +758,8 @@ def run_serve(args):
            "config": {"workload": "serve_%d_requests_poisson_arrivals_%g_per_s" % (N, args.rate), "requests": N,
                       "offered_rate_per_s": args.rate, "total_dofs": int(sum(dofs)), "min_dofs": int(min(dofs)),
                       "max_dofs": int(max(dofs)), "budget_GB": args.budget_gb, "max_active": args.max_active,
-                      "solo_rows": args.solo_rows,
+                      "solo_rows": args.solo_rows, "build_per_block": args.build_per_block,
+                      "builds": "second context (own stream), overlapping the block in flight",
                       "kinds": {k: sum(1 for s in specs if s["kind"] == k) for k in ("poisson", "elasticity", "supg")},
                       "dims": {str(d): sum(1 for s in specs if s["dim"] == d) for d in (2, 3)},
                       "tolerance": "relative residual 1e-10 (FP64 true residual per request)",
@@ -921,7 +931,8 @@ def main():
     ap.add_argument("--rate", type=float, default=2000.0, help="arrival rate (req/s) of the serving workload")
     ap.add_argument("--budget-gb", type=float, default=150.0, help="HBM budget of the serving workload")
     ap.add_argument("--max-active", type=int, default=1024, help="systems solved together by the server")
-    ap.add_argument("--build-per-block", type=int, default=4, help="requests the serving loop builds per block")
+    ap.add_argument("--build-per-block", type=int, default=0,
+                    help="most requests the serving loop builds while a block runs (0 = while it runs)")
     ap.add_argument("--solo-rows", type=int, default=0,
                     help="served systems of at least this many rows are solved alone (0: batch all)")
     args = ap.parse_args()

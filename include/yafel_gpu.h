@@ -260,7 +260,10 @@ YG_API yg_status yg_bicgstab(yg_matrix A, yg_precond M, yg_vector b, yg_vector x
  * reference solves one system per pcg_solve / bicgstab_solve call.  Each system
  * keeps its own matrix (CSR or 2x2/3x3 BCSR), right-hand side and iterate,
  * which must stay alive while it is in the batch; x holds x0 when added and the
- * solution when finished.  Systems may be added and removed between calls of
+ * solution when finished.  They may belong to another context of the same
+ * device (a second stream, so that systems are assembled while a block runs):
+ * yg_batch_add waits for that context's pending work, and the caller frees them
+ * only after the slot is removed between a wait and the next launch.  Systems may be added and removed between calls of
  * yg_batch_run (continuous batching); work advances in blocks of iterations
  * captured in one CUDA graph followed by an FP64 verification pass (true
  * residual b - A x for converged systems, BiCGSTAB restarts after a breakdown,
@@ -289,6 +292,9 @@ YG_API yg_status yg_batch_run(yg_batch B, int32_t max_blocks, int32_t *n_active)
  * between a wait and the next launch. */
 YG_API yg_status yg_batch_launch(yg_batch B);
 YG_API yg_status yg_batch_wait(yg_batch B, int32_t *n_active);
+/* *ready = 1 when no block is in flight or the launched block has completed
+ * (yg_batch_wait then returns without blocking), 0 while it runs.  Never blocks. */
+YG_API yg_status yg_batch_ready(yg_batch B, int32_t *ready);
 /* Status (YG_OK when converged and verified in FP64, YG_RUNNING while it
  * iterates), iterations and FP64 relative residual of a slot. */
 YG_API yg_status yg_batch_stats(yg_batch B, int32_t slot, yg_solve_stats *stats);
@@ -326,6 +332,9 @@ YG_API yg_status yg_server_attach(yg_server S, int64_t id, yg_matrix A, yg_vecto
                                   const yg_solve_opts *opts);
 YG_API yg_status yg_server_launch(yg_server S);
 YG_API yg_status yg_server_wait(yg_server S, int32_t *n_finished);
+/* *ready = 1 when no block is in flight or it has completed, 0 while it runs
+ * (build admitted requests until then).  Never blocks. */
+YG_API yg_status yg_server_ready(yg_server S, int32_t *ready);
 YG_API yg_status yg_server_finished(yg_server S, int64_t *ids, int32_t cap, int32_t *n);
 /* stats->status is YG_RUNNING until the request finished. */
 YG_API yg_status yg_server_poll(yg_server S, int64_t id, yg_solve_stats *stats);

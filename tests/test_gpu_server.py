@@ -60,3 +60,54 @@ def test_server_admits_by_budget_and_solves_everything(ctx, solo_rows):
         s = B.add(K, b, method=workloads.method(SPECS[i]))
         assert B.run() == 0
         assert np.array_equal(B.solution(s).numpy(), results[i][2]), i
+
+
+def test_server_with_requests_built_on_a_second_context(ctx):
+    """Requests assembled on another context of the device (its own stream) while
+    a block runs: ready() reports the block's completion without blocking, the
+    attached systems converge, and their results equal those of the same systems
+    built on the server's own context."""
+    bctx = yb.Context(0)
+    S = yb.Server(int(1e11), max_active=16, ctx=ctx)
+    ids = {S.submit(workloads.est_bytes(s)): i for i, s in enumerate(SPECS)}
+    pending, results, keep = [], {}, {}
+
+    def build_one():
+        rid = S.admit()
+        if rid is None:
+            return False
+        spec = SPECS[ids[rid]]
+        _, K, b, _ = workloads.assemble(spec, bctx)
+        x = yb.DeviceVector(K.rows(), bctx)
+        x.fill(0.0)
+        pending.append((rid, K, b, x))
+        return True
+
+    build_one()
+    assert S.ready()  # nothing in flight
+    while len(results) < len(SPECS):
+        for rid, K, b, x in pending:
+            S.attach(rid, K, b, x, method=workloads.method(SPECS[ids[rid]]))
+            keep[rid] = (K, b, x)
+        pending.clear()
+        S.launch()
+        while not S.ready():
+            if not build_one():
+                break
+        S.wait()
+        assert S.ready()
+        for rid in S.finished():
+            st = S.poll(rid)
+            results[ids[rid]] = (st.status, st.rel_residual, S.solution(rid).numpy())
+            S.release(rid)
+            keep.pop(rid)
+        if S.info()["active"] == 0 and not pending:
+            build_one()
+    for i, (status, rel, _) in results.items():
+        assert status == 0 and rel <= 1e-10, (SPECS[i], status, rel)
+    for i in (0, 4, 9):
+        _, K, b, _ = workloads.assemble(SPECS[i], ctx)
+        B = yb.Batch(1, ctx)
+        s = B.add(K, b, method=workloads.method(SPECS[i]))
+        assert B.run() == 0
+        assert np.array_equal(B.solution(s).numpy(), results[i][2]), i

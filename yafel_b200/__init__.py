@@ -697,6 +697,12 @@ class Batch:
         check(lib().yg_batch_wait(self.h, C.byref(n)), "Batch.wait")
         return n.value
 
+    def ready(self):
+        """True when no block is in flight or the launched one has completed."""
+        r = C.c_int32()
+        check(lib().yg_batch_ready(self.h, C.byref(r)), "Batch.ready")
+        return bool(r.value)
+
     def stats(self, slot):
         st = SolveStats()
         check(lib().yg_batch_stats(self.h, int(slot), C.byref(st)), "Batch.stats")
@@ -747,6 +753,13 @@ class Server:
         n = C.c_int32()
         check(lib().yg_server_wait(self.h, C.byref(n)), "Server.wait")
         return n.value
+
+    def ready(self):
+        """True when no block is in flight or the launched one has completed
+        (build admitted requests until then)."""
+        r = C.c_int32()
+        check(lib().yg_server_ready(self.h, C.byref(r)), "Server.ready")
+        return bool(r.value)
 
     def finished(self):
         ids = (C.c_int64 * 4096)()

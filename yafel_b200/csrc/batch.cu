@@ -119,6 +119,8 @@ struct yg_batch_t {
     int32_t live_items = 0;             // vector items of systems that may still iterate (host view)
     int m = 16;
     cudaGraphExec_t exec = nullptr;
+    cudaEvent_t done = nullptr;         // recorded after each launched block
+    bool in_flight = false;
     cudaGraph_t graph = nullptr;
     int64_t graph_kernels = 0;
     std::vector<BatchScal> h_scal;
@@ -1459,6 +1461,12 @@ extern "C" yg_status yg_batch_create(yg_context ctx, int32_t capacity, yg_batch 
     prepare_spmv_b<1>(ctx);
     prepare_spmv_b<2>(ctx);
     prepare_spmv_b<3>(ctx);
+    if (cudaEventCreateWithFlags(&bt->done, cudaEventDisableTiming) != cudaSuccess) {
+        cudaGetLastError();
+        bt->done = nullptr;
+        yg_batch_destroy(bt);
+        return fail(YG_CUDA_ERROR, "yg_batch_create: event creation failed");
+    }
     std::vector<BatchScal> init(capacity);
     for (auto &c : init) c.flag = BF_EMPTY;
     bt->h_scal = init;
@@ -1478,7 +1486,22 @@ extern "C" yg_status yg_batch_destroy(yg_batch bt) {
     for (void *p : {(void *)bt->d_sys, (void *)bt->d_scal, (void *)bt->d_mitems, (void *)bt->d_vitems, (void *)bt->d_ranges,
                     (void *)bt->d_mpart, (void *)bt->d_cticket, (void *)bt->d_vpart, (void *)bt->d_vpart2})
         dev_free(bt->ctx, p);
+    if (bt->done) cudaEventDestroy(bt->done);
     delete bt;
+    return YG_OK;
+}
+
+extern "C" yg_status yg_batch_ready(yg_batch bt, int32_t *ready) {
+    if (!bt || !ready) return fail(YG_BAD_ARG, "yg_batch_ready: NULL argument");
+    *ready = 1;
+    if (!bt->in_flight) return YG_OK;
+    const cudaError_t e = cudaEventQuery(bt->done);
+    if (e == cudaErrorNotReady) {
+        cudaGetLastError();
+        *ready = 0;
+        return YG_OK;
+    }
+    if (e != cudaSuccess) return fail(YG_CUDA_ERROR, "yg_batch_ready: %s", cudaGetErrorString(e));
     return YG_OK;
 }
 
@@ -1491,7 +1514,10 @@ extern "C" int64_t yg_batch_work_bytes(int64_t rows, int32_t method) {
 extern "C" yg_status yg_batch_add(yg_batch bt, yg_matrix A, yg_vector b, yg_vector x, int32_t method,
                                   const yg_solve_opts *opts, int32_t *slot) {
     if (!bt || !A || !b || !x || !slot) return fail(YG_BAD_ARG, "yg_batch_add: NULL argument");
-    if (A->ctx != bt->ctx || b->ctx != bt->ctx || x->ctx != bt->ctx) return fail(YG_BAD_ARG, "yg_batch_add: context mismatch");
+    for (yg_context c : {A->ctx, b->ctx, x->ctx})
+        if (c->device != bt->ctx->device)
+            return fail(YG_BAD_ARG, "yg_batch_add: the system lives on device %d, the batch on device %d", c->device,
+                        bt->ctx->device);
     if (A->rows() != A->cols() || b->n != A->rows() || x->n != A->rows()) return fail(YG_BAD_ARG, "yg_batch_add: dimension mismatch");
     if (A->block < 1 || A->block > 3) return fail(YG_UNSUPPORTED, "yg_batch_add: block size %d", A->block);
     if (method != YG_METHOD_CG && method != YG_METHOD_BICGSTAB) return fail(YG_BAD_ARG, "yg_batch_add: method %d", method);
@@ -1504,6 +1530,10 @@ extern "C" yg_status yg_batch_add(yg_batch bt, yg_matrix A, yg_vector b, yg_vect
     if (s < 0) return fail(YG_OVER_BUDGET, "yg_batch_add: all %d slots in use", bt->capacity);
     yg_context ctx = bt->ctx;
     if (o.precision == YG_PREC_MIXED && !A->d_val32) YG_TRY(yg_matrix_make_fp32(A));
+    // Objects built on another context of the device (its own stream, so their
+    // assembly overlaps a running block): their pending work completes first.
+    for (yg_context c : {A->ctx, b->ctx, x->ctx})
+        if (c != ctx) YG_CUDA(cudaStreamSynchronize(c->stream));
     // tiles of whole rows, from the row pointer
     std::vector<int32_t> rp(A->nbrows + 1);
     YG_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -1611,6 +1641,8 @@ static yg_status batch_launch(yg_batch bt) {
     ctx->launches += bt->graph_kernels;
     YG_CUDA(cudaMemcpyAsync(bt->h_scal.data(), bt->d_scal, sizeof(BatchScal) * bt->capacity, cudaMemcpyDeviceToHost,
                             ctx->stream));
+    YG_CUDA(cudaEventRecord(bt->done, ctx->stream));
+    bt->in_flight = true;
     return YG_OK;
 }
 
@@ -1619,6 +1651,7 @@ static yg_status batch_launch(yg_batch bt) {
 static yg_status batch_collect(yg_batch bt, int *active_out) {
     yg_context ctx = bt->ctx;
     YG_CUDA(cudaStreamSynchronize(ctx->stream));
+    bt->in_flight = false;
     YG_TRY(check_device_error(ctx));
     int active = 0;
     int32_t live = 0;

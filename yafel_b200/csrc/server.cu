@@ -204,6 +204,13 @@ extern "C" yg_status yg_server_wait(yg_server S, int32_t *n_finished) {
     return YG_OK;
 }
 
+extern "C" yg_status yg_server_ready(yg_server S, int32_t *ready) {
+    if (!S || !ready) return fail(YG_BAD_ARG, "yg_server_ready: NULL argument");
+    *ready = 1;
+    if (!S->in_flight) return YG_OK;
+    return yg_batch_ready(S->batch, ready);
+}
+
 extern "C" yg_status yg_server_set_solo_rows(yg_server S, int64_t rows) {
     if (!S || rows < 0) return fail(YG_BAD_ARG, "yg_server_set_solo_rows: bad argument");
     S->solo_rows = rows;
