@@ -113,20 +113,33 @@ def spmv_kernel_name(K, dot=1, vt="double"):
 
 
 def run_spmv_profile(args):
-    """SpMV alone on the nx^3 Q2 elasticity matrix (GPU-assembled), for
-    roofline and ncu captures: FP64 then FP32 values, `--reps` launches each."""
+    """SpMV alone on the nx^3 Q2 elasticity matrix (BCSR3) or, with
+    `--spmv-matrix poisson`, the nx^3 Q2 Poisson matrix (CSR, 27-125 entries a
+    row), GPU-assembled, for roofline and ncu captures: FP64 then FP32 values,
+    `--reps` launches each."""
     import yafel_b200 as yb
-    dm = yb.DoFManager(problem(args.nx), 2, 3)
-    fe = yb.FESystem(dm, 3)
-    yb.CGAssembly(yb.LinearElasticity(3, E=E, nu=NU), fe, [yb.AssemblyRequirement.Tangent])
+    poisson = args.spmv_matrix == "poisson"
+    dpn = 1 if poisson else 3
+    dm = yb.DoFManager(problem(args.nx), 2, dpn)
+    fe = yb.FESystem(dm, 3, format=yb.CSR if poisson else yb.BCSR)
+    phys = yb.PoissonEquation(3, f=0.0) if poisson else yb.LinearElasticity(3, E=E, nu=NU)
+    yb.CGAssembly(phys, fe, [yb.AssemblyRequirement.Tangent])
     K = fe.getGlobalTangent()
     if args.variant is not None:
         K.set_spmv(args.variant, args.lanes)
-    n, nnzb = K.rows(), K.nnz() // 9
+    n = K.rows()
     x = yb.DeviceVector(np.random.default_rng(0).standard_normal(n), dm.ctx)
-    out = {"mesh": "%d^3 Q2 hex" % args.nx, "dofs": n, "blocks": nnzb, "kernel": spmv_kernel_name(K, 0)}
-    for prec, name, nbytes in ((0, "fp64", bcsr3_spmv_bytes(nnzb, n)),
-                               (1, "fp32_values", nnzb * 40 + 4 * (n // 3 + 1) + 16 * n)):
+    if poisson:
+        nnz = K.nnz()
+        v, L = K.get_spmv()
+        out = {"mesh": "%d^3 Q2 hex, Poisson" % args.nx, "dofs": n, "nnz": nnz,
+               "kernel": "k_bcsr_spmv<1,%d,double,0>" % L if v == 0 else "variant %d lanes %d" % (v, L)}
+        cases = ((0, "fp64", nnz * 12 + 4 * (n + 1) + 16 * n), (1, "fp32_values", nnz * 8 + 4 * (n + 1) + 16 * n))
+    else:
+        nnzb = K.nnz() // 9
+        out = {"mesh": "%d^3 Q2 hex" % args.nx, "dofs": n, "blocks": nnzb, "kernel": spmv_kernel_name(K, 0)}
+        cases = ((0, "fp64", bcsr3_spmv_bytes(nnzb, n)), (1, "fp32_values", nnzb * 40 + 4 * (n // 3 + 1) + 16 * n))
+    for prec, name, nbytes in cases:
         ms = K.spmv_bench(reps=args.reps, precision=prec, x=x)
         out[name] = {"ms": ms, "bytes": nbytes, "GB_s": nbytes / ms / 1e6}
     print(json.dumps(out), flush=True)
@@ -650,6 +663,8 @@ def run_serve(args):
     def served(precision, idxs, clocks=None):
         S = yb.Server(budget, max_active=args.max_active, ctx=ctx)
         S.set_solo_rows(args.solo_rows)
+        if args.solo_spmv_mb is not None:
+            S.set_solo_spmv_bytes(int(args.solo_spmv_mb * 2 ** 20))
         idx, pending = {}, []
         lat, stats = {}, {}
         state = {"nsub": 0}
@@ -759,6 +774,7 @@ def run_serve(args):
                       "offered_rate_per_s": args.rate, "total_dofs": int(sum(dofs)), "min_dofs": int(min(dofs)),
                       "max_dofs": int(max(dofs)), "budget_GB": args.budget_gb, "max_active": args.max_active,
                       "solo_rows": args.solo_rows, "build_per_block": args.build_per_block,
+                      "solo_spmv_MiB": args.solo_spmv_mb,
                       "builds": "second context (own stream), overlapping the block in flight",
                       "kinds": {k: sum(1 for s in specs if s["kind"] == k) for k in ("poisson", "elasticity", "supg")},
                       "dims": {str(d): sum(1 for s in specs if s["dim"] == d) for d in (2, 3)},
@@ -923,6 +939,8 @@ def main():
     ap.add_argument("--spmv-profile", action="store_true", help="time the SpMV kernel alone (roofline/ncu)")
     ap.add_argument("--variant", type=int, default=None, help="SpMV variant for --spmv-profile (0 flat, 1 staged, 2 TMA)")
     ap.add_argument("--lanes", type=int, default=32, help="SpMV lanes / TMA configuration for --spmv-profile")
+    ap.add_argument("--spmv-matrix", default="elasticity", choices=["elasticity", "poisson"],
+                    help="matrix of --spmv-profile: Q2 elasticity (BCSR3) or Q2 Poisson (CSR)")
     ap.add_argument("--reps", type=int, default=10)
     ap.add_argument("--workload", default="fem", choices=["fem", "batch", "serve"],
                     help="fem: 60^3 Q2 elasticity assemble+solve; batch: many 2D problems solved together")
@@ -931,6 +949,9 @@ def main():
     ap.add_argument("--rate", type=float, default=2000.0, help="arrival rate (req/s) of the serving workload")
     ap.add_argument("--budget-gb", type=float, default=150.0, help="HBM budget of the serving workload")
     ap.add_argument("--max-active", type=int, default=1024, help="systems solved together by the server")
+    ap.add_argument("--solo-spmv-mb", type=float, default=None,
+                    help="serving: requests whose FP64 matrix holds at least this many MiB run their own SpMV "
+                         "launch in the batch (default: the library's)")
     ap.add_argument("--build-per-block", type=int, default=0,
                     help="most requests the serving loop builds while a block runs (0 = while it runs)")
     ap.add_argument("--solo-rows", type=int, default=0,

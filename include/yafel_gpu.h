@@ -292,6 +292,11 @@ YG_API yg_status yg_batch_run(yg_batch B, int32_t max_blocks, int32_t *n_active)
  * between a wait and the next launch. */
 YG_API yg_status yg_batch_launch(yg_batch B);
 YG_API yg_status yg_batch_wait(yg_batch B, int32_t *n_active);
+/* Systems added from now on whose FP64 matrix holds at least `bytes` bytes run
+ * their iteration SpMV as one launch of the single-system kernel (autotuned for
+ * that matrix, dot products fused) inside the batch's graph instead of sharing
+ * the batched SpMV kernels; 0 turns this off.  Default 128 MiB. */
+YG_API yg_status yg_batch_set_solo_bytes(yg_batch B, int64_t bytes);
 /* *ready = 1 when no block is in flight or the launched block has completed
  * (yg_batch_wait then returns without blocking), 0 while it runs.  Never blocks. */
 YG_API yg_status yg_batch_ready(yg_batch B, int32_t *ready);
@@ -332,6 +337,10 @@ YG_API yg_status yg_server_attach(yg_server S, int64_t id, yg_matrix A, yg_vecto
                                   const yg_solve_opts *opts);
 YG_API yg_status yg_server_launch(yg_server S);
 YG_API yg_status yg_server_wait(yg_server S, int32_t *n_finished);
+/* yg_batch_set_solo_bytes for the server's batch: requests attached from now on
+ * whose FP64 matrix holds at least `bytes` run their iteration SpMV as their own
+ * single-system launch inside the batch's graph. */
+YG_API yg_status yg_server_set_solo_spmv_bytes(yg_server S, int64_t bytes);
 /* *ready = 1 when no block is in flight or it has completed, 0 while it runs
  * (build admitted requests until then).  Never blocks. */
 YG_API yg_status yg_server_ready(yg_server S, int32_t *ready);

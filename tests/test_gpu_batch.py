@@ -158,3 +158,49 @@ def test_every_spmv_variant_solves_the_mix(ctx, variant, lanes, tiles):
         st = B.stats(s)
         assert st.status == 0 and st.rel_residual <= 1e-10, (spec, st.status, st.rel_residual)
         assert oracle_relres(spec, mesh, dofs, b.numpy(), B.solution(s).numpy()) <= 1e-10
+
+
+@pytest.mark.parametrize("precision", [yb.PREC_FP64, yb.PREC_MIXED])
+def test_systems_with_their_own_spmv_launch(ctx, precision):
+    """Systems above the matrix-size threshold run their iteration SpMV as a
+    single-system launch inside the batch's graph (PCG and BiCGSTAB): they reach
+    1e-10 on the oracle-assembled system, agree with the shared-kernel solution,
+    give the same bits alone and in the mix, and a system of that kind added
+    while the batch runs (a new graph) converges too."""
+    probs = [assemble_problem(s, ctx) for s in MIXED_SPECS]
+    sizes = sorted(K.nnz() * 8 for (_, K, _, _) in probs)
+    threshold = sizes[len(sizes) // 2]
+    solo = [K.nnz() * 8 >= threshold for (_, K, _, _) in probs]
+    assert any(solo) and not all(solo)
+    meth = [workloads.method(s) for s in MIXED_SPECS]
+    assert any(m == "bicgstab" and o for m, o in zip(meth, solo)) or any(m == "cg" and o for m, o in zip(meth, solo))
+
+    def run(idx, thr, late=None):
+        B = yb.Batch(len(MIXED_SPECS), ctx)
+        B.set_solo_bytes(thr)
+        slots = {i: B.add(probs[i][1], probs[i][2], precision=precision, method=meth[i]) for i in idx}
+        if late is not None:
+            B.run(max_blocks=2)
+            slots[late] = B.add(probs[late][1], probs[late][2], precision=precision, method=meth[late])
+        assert B.run() == 0
+        out = {}
+        for i, s in slots.items():
+            st = B.stats(s)
+            assert st.status == 0 and st.rel_residual <= 1e-10, (MIXED_SPECS[i], st.status, st.rel_residual)
+            out[i] = B.solution(s).numpy()
+        return out
+
+    everything = list(range(len(MIXED_SPECS)))
+    own = run(everything, threshold)
+    shared = run(everything, 0)
+    for i in everything:
+        spec, (mesh, K, b, dofs) = MIXED_SPECS[i], probs[i]
+        assert oracle_relres(spec, mesh, dofs, b.numpy(), own[i]) <= 1e-10, spec
+        assert np.linalg.norm(own[i] - shared[i]) <= 1e-6 * np.linalg.norm(shared[i]), spec
+    first_solo = solo.index(True)
+    alone = run([first_solo], threshold)
+    assert np.array_equal(alone[first_solo], own[first_solo])
+    late = max(i for i in everything if solo[i])
+    rest = [i for i in everything if i != late]
+    mixed_late = run(rest, threshold, late=late)
+    assert np.array_equal(mixed_late[late], own[late])

@@ -697,6 +697,11 @@ class Batch:
         check(lib().yg_batch_wait(self.h, C.byref(n)), "Batch.wait")
         return n.value
 
+    def set_solo_bytes(self, nbytes):
+        """Systems added from now on whose FP64 matrix holds at least `nbytes`
+        run their iteration SpMV as their own single-system launch (0: never)."""
+        check(lib().yg_batch_set_solo_bytes(self.h, int(nbytes)), "Batch.set_solo_bytes")
+
     def ready(self):
         """True when no block is in flight or the launched one has completed."""
         r = C.c_int32()
@@ -753,6 +758,11 @@ class Server:
         n = C.c_int32()
         check(lib().yg_server_wait(self.h, C.byref(n)), "Server.wait")
         return n.value
+
+    def set_solo_spmv_bytes(self, nbytes):
+        """Requests attached from now on whose FP64 matrix holds at least
+        `nbytes` run their iteration SpMV as their own launch (0: never)."""
+        check(lib().yg_server_set_solo_spmv_bytes(self.h, int(nbytes)), "Server.set_solo_spmv_bytes")
 
     def ready(self):
         """True when no block is in flight or the launched one has completed

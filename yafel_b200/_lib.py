@@ -80,6 +80,7 @@ SIGNATURES = {
     "yg_batch_launch": (i32, [vp]),
     "yg_batch_wait": (i32, [vp, P(i32)]),
     "yg_batch_ready": (i32, [vp, P(i32)]),
+    "yg_batch_set_solo_bytes": (i32, [vp, i64]),
     "yg_batch_get_tuning": (i32, [vp, P(i32)]),
     "yg_batch_set_tuning": (i32, [vp, i32, i32, i32, i32]),
     "yg_server_create": (i32, [vp, u64, i32, P(vp)]),
@@ -90,6 +91,7 @@ SIGNATURES = {
     "yg_server_launch": (i32, [vp]),
     "yg_server_wait": (i32, [vp, P(i32)]),
     "yg_server_ready": (i32, [vp, P(i32)]),
+    "yg_server_set_solo_spmv_bytes": (i32, [vp, i64]),
     "yg_server_finished": (i32, [vp, P(i64), i32, P(i32)]),
     "yg_server_poll": (i32, [vp, i64, P(SolveStats)]),
     "yg_server_release": (i32, [vp, i64]),

@@ -65,7 +65,8 @@ struct BatchSys {
     int32_t vitem_begin, vitem_end;  // vector items
     int32_t precision;            // YG_PREC_FP64 or YG_PREC_MIXED
     int32_t ntiles;
-    int32_t method, pad;
+    int32_t method;
+    int32_t solo;                 // 1: the iteration SpMV is the single-system kernel (large matrix)
 };
 
 struct BatchScal {
@@ -92,6 +93,16 @@ struct BatchVItem {
 constexpr int kGroups = 6;  // (method, block size): group = 3 * method + block - 1
 // d_ranges: [0, 8) first matrix item of each group then the end; [8, 16) the same for vector items
 constexpr int kVR = 8;
+// [16, 16 + kGroups): end of each group's matrix items that the iteration SpMV
+// kernels take (the items of systems with their own SpMV follow, for the
+// verification pass only)
+constexpr int kRanges = 3 * kVR;
+// A system whose FP64 matrix holds at least this many bytes runs its iteration
+// SpMV as one launch of the single-system kernel (autotuned for its matrix, fused
+// dot products) inside the batch's graph: at that size the launch is amortised
+// and the single-system kernels stream closer to the HBM roofline than the
+// shared batch kernels.
+constexpr int64_t kSoloSpmvBytes = 128ll << 20;
 
 struct yg_batch_t {
     yg_context ctx = nullptr;
@@ -121,6 +132,12 @@ struct yg_batch_t {
     cudaGraphExec_t exec = nullptr;
     cudaEvent_t done = nullptr;         // recorded after each launched block
     bool in_flight = false;
+    // live systems with their own SpMV launches (slot, matrix), and the list the
+    // captured graph holds; partial sums of those launches
+    std::vector<std::pair<int, yg_matrix>> solo, graph_solo;
+    double *d_solo_part = nullptr;
+    yg_status solo_err = YG_OK;         // first failed launch of those SpMVs while capturing
+    int64_t solo_bytes = kSoloSpmvBytes;  // threshold for systems added from now on (0: none)
     cudaGraph_t graph = nullptr;
     int64_t graph_kernels = 0;
     std::vector<BatchScal> h_scal;
@@ -504,6 +521,26 @@ __device__ __forceinline__ bool warp_stage_wait(uint64_t *bar, unsigned parity, 
 
 // End of a matrix item in a warp: publish its partials; the warp that
 // completes the system's last item takes the reduction and the decision.
+// The decision after an iteration SpMV of a system, from its dot products:
+//   SP_CG      alpha = r.z / p.q
+//   SP_BICG_V  alpha = rho / r0.v
+//   SP_BICG_T  omega = t.s / t.t
+template <int KIND>
+__device__ __forceinline__ void decide_spmv(BatchScal &sc, double a, double tt, int parity) {
+    if (KIND == SP_CG) {
+        const double alpha = sc.rz[parity] / a;
+        if (a == 0 || !isfinite(alpha)) sc.stop = isfinite(a) ? BS_BREAK : BS_NAN;
+        else sc.alpha = alpha;
+    } else if (KIND == SP_BICG_V) {
+        const double alpha = sc.rho / a;
+        sc.fresh = 0;
+        if (a == 0 || !isfinite(alpha)) sc.stop = isfinite(a) ? BS_CONV : BS_NAN;  // restart via verify
+        else sc.alpha = alpha;
+    } else {
+        sc.omega = tt > 0 ? a / tt : 0.0;
+    }
+}
+
 // Systems with more than kChunk items: the warp that finishes a chunk's last
 // item sums the chunk (in item order) into the partial slot of the chunk's
 // first item (cticket[first item] counts the chunk's finished items); the warp
@@ -539,19 +576,30 @@ __device__ __forceinline__ void finish_item(const BatchSys *__restrict__ sys, Ba
         if (KIND == SP_BICG_T) tt = warp_sum_strided(part, ib, nch, kChunk, 1, lane);
     }
     if (lane != 0) return;
-    BatchScal &sc = scal[s];
-    if (KIND == SP_CG) {
-        const double alpha = sc.rz[parity] / a;
-        if (a == 0 || !isfinite(alpha)) sc.stop = isfinite(a) ? BS_BREAK : BS_NAN;
-        else sc.alpha = alpha;
-    } else if (KIND == SP_BICG_V) {
-        const double alpha = sc.rho / a;
-        sc.fresh = 0;
-        if (a == 0 || !isfinite(alpha)) sc.stop = isfinite(a) ? BS_CONV : BS_NAN;  // restart via verify
-        else sc.alpha = alpha;
-    } else {
-        sc.omega = tt > 0 ? a / tt : 0.0;
+    decide_spmv<KIND>(scal[s], a, tt, parity);
+}
+
+// A system with its own SpMV launch: one warp sums that launch's per-CTA
+// partials (np of them; DOT 2 launches store pairs) in CTA order and takes the
+// same decision as the last item of a batched SpMV.
+template <int KIND>
+__global__ void k_batch_solo_finish(BatchScal *__restrict__ scal, const double *__restrict__ part, int np, int s,
+                                    int parity) {
+    const int lane = threadIdx.x & 31;
+    int act = lane == 0 ? activity(&scal[s], ACT_ITER) : 0;
+    if (!__shfl_sync(0xffffffffu, act, 0)) return;
+    double a = 0, tt = 0;
+    for (int i = lane; i < np; i += 32) {
+        if (KIND == SP_BICG_T) {
+            a += __ldcg(part + 2 * i);
+            tt += __ldcg(part + 2 * i + 1);
+        } else {
+            a += __ldcg(part + i);
+        }
     }
+    a = warp_sum(a);
+    if (KIND == SP_BICG_T) tt = warp_sum(tt);
+    if (lane == 0) decide_spmv<KIND>(scal[s], a, tt, parity);
 }
 
 // Direct-load SpMV of one group (no staging): each warp takes whole items; L
@@ -631,7 +679,7 @@ k_batch_spmv_direct(const BatchMItem *__restrict__ items, const int32_t *__restr
                     int32_t *__restrict__ cticket, int parity, int commit) {
     const int lane = threadIdx.x & 31;
     const int W = gridDim.x * (blockDim.x >> 5);
-    const int g1 = ranges[g + 1];
+    const int g1 = KIND == SP_VERIFY ? ranges[g + 1] : ranges[2 * kVR + g];
     const uint64_t pol = evict_first_policy();
     int it = ranges[g] + blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     int s_n = 0, r0_n = 0, r1_n = 0;  // the item to work on next
@@ -685,7 +733,7 @@ k_batch_spmv(const BatchMItem *__restrict__ items, const int32_t *__restrict__ r
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     __syncwarp();
     const uint64_t pol = evict_first_policy();
-    const int g1 = ranges[g + 1];
+    const int g1 = KIND == SP_VERIFY ? ranges[g + 1] : ranges[2 * kVR + g];
     const int W = gridDim.x * WARPS;
     const int act_kind = KIND == SP_VERIFY ? ACT_VERIFY : ACT_ITER;
 
@@ -1253,6 +1301,41 @@ static void launch_verify(yg_batch bt) {
     YG_LAUNCHED(ctx);
 }
 
+// The iteration SpMV of each system that has its own launch (kind SP_CG or
+// SP_BICG_V for the first SpMV of an iteration, SP_BICG_T for the second), each
+// followed by its one-warp decision.  The SpMV kernel skips a system whose flag
+// says it is not running; the decision also skips a stopped one.
+static void launch_solo(yg_batch bt, int kind, int parity) {
+    yg_context ctx = bt->ctx;
+    for (const auto &e : bt->solo) {
+        const int s = e.first;
+        yg_matrix A = e.second;
+        const BatchSys &d = bt->sys[s];
+        const bool bicg = d.method == BM_BICG;
+        if ((kind == SP_BICG_T || kind == SP_BICG_V) != bicg) continue;
+        const int prec = d.precision == YG_PREC_MIXED ? YG_PREC_MIXED : YG_PREC_FP64;
+        const int grid = spmv_grid_for(A, prec);
+        const int32_t *flag = &bt->d_scal[s].flag;
+        const int64_t l0 = A->ctx->launches;
+        yg_status st;
+        if (kind == SP_CG) {
+            st = spmv_launch_ex(A, d.p, d.q, prec, d.p, bt->d_solo_part, 1, flag, grid, ctx->stream);
+            k_batch_solo_finish<SP_CG><<<1, 32, 0, ctx->stream>>>(bt->d_scal, bt->d_solo_part, grid, s, parity);
+        } else if (kind == SP_BICG_V) {
+            st = spmv_launch_ex(A, d.ph, d.v, prec, d.r0, bt->d_solo_part, 1, flag, grid, ctx->stream);
+            k_batch_solo_finish<SP_BICG_V><<<1, 32, 0, ctx->stream>>>(bt->d_scal, bt->d_solo_part, grid, s, parity);
+        } else {
+            st = spmv_launch_ex(A, d.sh, d.t, prec, d.s, bt->d_solo_part, 2, flag, grid, ctx->stream);
+            k_batch_solo_finish<SP_BICG_T><<<1, 32, 0, ctx->stream>>>(bt->d_scal, bt->d_solo_part, grid, s, parity);
+        }
+        if (st != YG_OK && bt->solo_err == YG_OK) bt->solo_err = st;
+        // count the SpMV on this context (A may belong to another one), and the decision
+        const int64_t dl = A->ctx->launches - l0;
+        A->ctx->launches -= dl;
+        ctx->launches += dl + 1;
+    }
+}
+
 static void launch_iteration(yg_batch bt, int parity) {
     yg_context ctx = bt->ctx;
     const int grid = batch_grid(ctx);
@@ -1262,11 +1345,14 @@ static void launch_iteration(yg_batch bt, int parity) {
     }
     for (int g = 0; g < kGroups; ++g)
         if (has(bt, g)) launch_spmv(bt, g < 3 ? SP_CG : SP_BICG_V, g, parity, 1);
+    launch_solo(bt, SP_CG, parity);
+    launch_solo(bt, SP_BICG_V, parity);
     k_batch_v2<<<grid, kThreads, 0, ctx->stream>>>(bt->d_vitems, bt->d_ranges, bt->d_sys, bt->d_scal, parity,
                                                   bt->d_vpart);
     YG_LAUNCHED(ctx);
     for (int g = 3; g < kGroups; ++g)
         if (has(bt, g)) launch_spmv(bt, SP_BICG_T, g, parity, 1);
+    launch_solo(bt, SP_BICG_T, parity);
     k_batch_v3<<<grid, kThreads, 0, ctx->stream>>>(bt->d_vitems, bt->d_ranges, bt->d_sys, bt->d_scal, bt->d_vpart);
     YG_LAUNCHED(ctx);
 }
@@ -1313,15 +1399,21 @@ static yg_status rebuild_items(yg_batch bt) {
     yg_context ctx = bt->ctx;
     std::vector<BatchMItem> mitems;
     std::vector<BatchVItem> vitems;
-    int32_t ranges[2 * kVR] = {0};
+    int32_t ranges[kRanges] = {0};
     unsigned present = 0;
+    std::vector<std::pair<int, yg_matrix>> solo;
     for (int g = 0; g < kGroups; ++g) {
         const int method = g / 3, B = g % 3 + 1;
         ranges[g] = (int32_t)mitems.size();
         ranges[kVR + g] = (int32_t)vitems.size();
         const int T = std::max(1, bt->tiles_per_item[B]), VR = vitem_rows(B);
+        // systems of the group with batched iteration SpMVs first, then those with their own
+        for (int pass = 0; pass < 2; ++pass) {
+        if (pass == 1) ranges[2 * kVR + g] = (int32_t)mitems.size();
         for (int s = 0; s < bt->capacity; ++s) {
             if (!bt->used[s] || bt->sys[s].block != B || bt->sys[s].method != method) continue;
+            if (bt->sys[s].solo != pass) continue;
+            if (pass == 1 && sys_live(bt, s)) solo.push_back({s, bt->mats[s]});
             present |= 1u << g;
             BatchSys &d = bt->sys[s];
             d.mitem_begin = (int32_t)mitems.size();
@@ -1340,6 +1432,7 @@ static yg_status rebuild_items(yg_batch bt) {
             }
             d.mitem_end = (int32_t)mitems.size();
             d.vitem_end = (int32_t)vitems.size();
+        }
         }
     }
     ranges[kGroups] = ranges[kGroups + 1] = (int32_t)mitems.size();
@@ -1364,6 +1457,7 @@ static yg_status rebuild_items(yg_batch bt) {
     YG_CUDA(cudaMemcpy(bt->d_ranges, ranges, sizeof(ranges), cudaMemcpyHostToDevice));
     YG_CUDA(cudaMemcpy(bt->d_sys, bt->sys.data(), sizeof(BatchSys) * bt->capacity, cudaMemcpyHostToDevice));
     bt->groups_present = present;
+    bt->solo = solo;
     bt->live_items = (int32_t)vitems.size();
     bt->dirty = false;
     return YG_OK;
@@ -1373,6 +1467,7 @@ static yg_status capture_graph(yg_batch bt) {
     yg_context ctx = bt->ctx;
     drop_graph(bt);
     int64_t before = ctx->launches;
+    bt->solo_err = YG_OK;
     YG_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
     for (int it = 0; it < bt->m; ++it) launch_iteration(bt, it & 1);
     launch_verify(bt);
@@ -1381,9 +1476,14 @@ static yg_status capture_graph(yg_batch bt) {
     bt->graph_kernels = ctx->launches - before;
     ctx->launches = before;
     if (e != cudaSuccess) return fail(YG_CUDA_ERROR, "batch graph capture: %s", cudaGetErrorString(e));
+    if (bt->solo_err != YG_OK) {
+        cudaGraphDestroy(g);
+        return bt->solo_err;
+    }
     bt->graph = g;
     YG_CUDA(cudaGraphInstantiate(&bt->exec, g, 0));
     bt->graph_groups = bt->groups_present;
+    bt->graph_solo = bt->solo;
     return YG_OK;
 }
 
@@ -1454,7 +1554,8 @@ extern "C" yg_status yg_batch_create(yg_context ctx, int32_t capacity, yg_batch 
     bt->opts.assign(capacity, yg_solve_opts{});
     yg_status s;
     if ((s = dev_alloc_t(ctx, &bt->d_sys, capacity)) != YG_OK || (s = dev_alloc_t(ctx, &bt->d_scal, capacity)) != YG_OK ||
-        (s = dev_alloc_t(ctx, &bt->d_ranges, 2 * kVR)) != YG_OK) {
+        (s = dev_alloc_t(ctx, &bt->d_ranges, kRanges)) != YG_OK ||
+        (s = dev_alloc_t(ctx, &bt->d_solo_part, 2 * kMaxReduceBlocks)) != YG_OK) {
         yg_batch_destroy(bt);
         return s;
     }
@@ -1471,7 +1572,7 @@ extern "C" yg_status yg_batch_create(yg_context ctx, int32_t capacity, yg_batch 
     for (auto &c : init) c.flag = BF_EMPTY;
     bt->h_scal = init;
     cudaMemcpy(bt->d_scal, init.data(), sizeof(BatchScal) * capacity, cudaMemcpyHostToDevice);
-    cudaMemset(bt->d_ranges, 0, sizeof(int32_t) * 2 * kVR);
+    cudaMemset(bt->d_ranges, 0, sizeof(int32_t) * kRanges);
     YG_CUDA(cudaGetLastError());
     *out = bt;
     return YG_OK;
@@ -1484,10 +1585,17 @@ extern "C" yg_status yg_batch_destroy(yg_batch bt) {
     for (int s = 0; s < bt->capacity; ++s)
         if (bt->used[s]) release_slot(bt, s);
     for (void *p : {(void *)bt->d_sys, (void *)bt->d_scal, (void *)bt->d_mitems, (void *)bt->d_vitems, (void *)bt->d_ranges,
-                    (void *)bt->d_mpart, (void *)bt->d_cticket, (void *)bt->d_vpart, (void *)bt->d_vpart2})
+                    (void *)bt->d_mpart, (void *)bt->d_cticket, (void *)bt->d_vpart, (void *)bt->d_vpart2,
+                    (void *)bt->d_solo_part})
         dev_free(bt->ctx, p);
     if (bt->done) cudaEventDestroy(bt->done);
     delete bt;
+    return YG_OK;
+}
+
+extern "C" yg_status yg_batch_set_solo_bytes(yg_batch bt, int64_t bytes) {
+    if (!bt) return fail(YG_BAD_ARG, "yg_batch_set_solo_bytes: NULL batch");
+    bt->solo_bytes = bytes < 0 ? 0 : bytes;
     return YG_OK;
 }
 
@@ -1552,6 +1660,8 @@ extern "C" yg_status yg_batch_add(yg_batch bt, yg_matrix A, yg_vector b, yg_vect
     d.precision = o.precision;
     d.method = method;
     d.ntiles = (int32_t)tl.size() - 1;
+    d.solo = bt->solo_bytes > 0 && A->nnzb * (int64_t)A->block * A->block * 8 >= bt->solo_bytes;
+    if (d.solo) YG_TRY(spmv_autotune_device(A));  // its own SpMV: tune it now, outside any capture
     const int64_t n = A->rows();
     double *dinv = nullptr;
     int32_t *dtiles = nullptr;
@@ -1668,7 +1778,7 @@ static yg_status batch_collect(yg_batch bt, int *active_out) {
 
 static yg_status batch_prepare(yg_batch bt) {
     if (bt->dirty) YG_TRY(rebuild_items(bt));
-    if (!bt->exec || bt->graph_groups != bt->groups_present) YG_TRY(capture_graph(bt));
+    if (!bt->exec || bt->graph_groups != bt->groups_present || bt->graph_solo != bt->solo) YG_TRY(capture_graph(bt));
     launch_verify(bt);  // initialise systems added since the last run
     return YG_OK;
 }

@@ -148,7 +148,7 @@ yg_status dev_alloc_t(yg_context ctx, T **p, size_t count) {
 yg_status spmv_launch(yg_matrix A, const double *x, double *y, int precision, double *partials_dot,
                       const int32_t *flag, int grid);
 yg_status spmv_launch_ex(yg_matrix A, const double *x, double *y, int precision, const double *w, double *partials,
-                         int dot_mode, const int32_t *flag, int grid);
+                         int dot_mode, const int32_t *flag, int grid, cudaStream_t stream = nullptr);
 int spmv_default_grid(yg_matrix A);
 int spmv_grid_for(yg_matrix A, int precision);
 void spmv_autotune(yg_matrix A);

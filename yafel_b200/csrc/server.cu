@@ -211,6 +211,11 @@ extern "C" yg_status yg_server_ready(yg_server S, int32_t *ready) {
     return yg_batch_ready(S->batch, ready);
 }
 
+extern "C" yg_status yg_server_set_solo_spmv_bytes(yg_server S, int64_t bytes) {
+    if (!S) return fail(YG_BAD_ARG, "yg_server_set_solo_spmv_bytes: NULL server");
+    return yg_batch_set_solo_bytes(S->batch, bytes);
+}
+
 extern "C" yg_status yg_server_set_solo_rows(yg_server S, int64_t rows) {
     if (!S || rows < 0) return fail(YG_BAD_ARG, "yg_server_set_solo_rows: bad argument");
     S->solo_rows = rows;

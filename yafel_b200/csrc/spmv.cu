@@ -939,8 +939,8 @@ static void choice(yg_matrix A, int precision, int *variant, int *lanes) {
 // x) or of w.y and y.y (dot_mode 2).  The grid is persistent: `grid` blocks
 // stride over the block rows.
 yg_status spmv_launch_ex(yg_matrix A, const double *x, double *y, int precision, const double *w, double *partials,
-                         int dot_mode, const int32_t *flag, int grid) {
-    cudaStream_t st = A->ctx->stream;
+                         int dot_mode, const int32_t *flag, int grid, cudaStream_t stream) {
+    cudaStream_t st = stream ? stream : A->ctx->stream;
     if (grid > kMaxReduceBlocks) grid = kMaxReduceBlocks;
     if (!partials) dot_mode = 0;
     if (!w) w = x;
