@@ -545,6 +545,8 @@ def run_batch(args):
 
     def make_batch(precision):
         B = yb.Batch(P, ctx)
+        if args.solo_spmv_mb is not None:
+            B.set_solo_bytes(int(args.solo_spmv_mb * 2 ** 20))
         xs = []
         for K, b, n in zip(Ks, bs, ndofs):
             x = yb.DeviceVector(n, ctx)
@@ -950,8 +952,8 @@ def main():
     ap.add_argument("--budget-gb", type=float, default=150.0, help="HBM budget of the serving workload")
     ap.add_argument("--max-active", type=int, default=1024, help="systems solved together by the server")
     ap.add_argument("--solo-spmv-mb", type=float, default=None,
-                    help="serving: requests whose FP64 matrix holds at least this many MiB run their own SpMV "
-                         "launch in the batch (default: the library's)")
+                    help="batched and served: systems whose FP64 matrix holds at least this many MiB run their "
+                         "own SpMV launch in the batch (default: the library's)")
     ap.add_argument("--build-per-block", type=int, default=0,
                     help="most requests the serving loop builds while a block runs (0 = while it runs)")
     ap.add_argument("--solo-rows", type=int, default=0,
