@@ -206,7 +206,9 @@ yg_status solve_bicgstab(yg_matrix A, yg_precond M, yg_vector bv, yg_vector xv, 
     const double *dinv = precond_dinv(M);
     const int64_t maxiter = o.maxiter > 0 ? o.maxiter : 100 * n + 1000;
     const int G = ctx->reduce_blocks;
-    const int SG = std::min(spmv_default_grid(A), G);  // SpMV grid = partials count
+    // SpMV grid = partials count: up to 2G, so that r^.v (at [2G, 2G+SG)) and
+    // s.t, t.t (at [4G, 4G+2SG)) stay inside their regions and below b.b
+    const int SG = std::min(spmv_default_grid(A), 2 * G);
     cudaStream_t st = ctx->stream;
     double *P = ctx->d_partials;
     KrylovScalars *S = ctx->d_scalars;
@@ -287,7 +289,9 @@ yg_status solve_bicgstab(yg_matrix A, yg_precond M, yg_vector bv, yg_vector xv, 
                 TRYB(build(m, g));
                 int64_t total = 0;
                 // The recursive residual triggers the stop; the FP64 true residual
-                // decides.  If they drifted apart, restart from the true residual.
+                // decides.  If they drifted apart, or the iteration broke down
+                // (rho or omega vanished), restart from the true residual with
+                // r^ = r, at most 8 times (as the batched BiCGSTAB does).
                 for (int restart = 0; restart < 8; ++restart) {
                     int64_t it = 0;
                     for (;;) {
@@ -297,13 +301,16 @@ yg_status solve_bicgstab(yg_matrix A, yg_precond M, yg_vector bv, yg_vector xv, 
                     }
                     total += hs.iter;
                     flag = hs.flag;
-                    if (flag != BF_CONVERGED) break;
+                    if (flag != BF_CONVERGED && flag != BF_BREAKDOWN) break;
                     TRYB(spmv_launch(A, xv->d, q, YG_PREC_FP64, nullptr, nullptr, spmv_default_grid(A)));
                     k_axmb<<<stream_grid(ctx, n), kThreads, 0, st>>>(n, q, bv->d, q);
                     YG_LAUNCHED(ctx);
                     double rr = 0;
                     TRYB(vector_dot(ctx, q, q, n, &rr));
-                    if (std::sqrt(rr) <= o.tol * std::sqrt(bb0)) break;
+                    if (std::sqrt(rr) <= o.tol * std::sqrt(bb0)) {
+                        flag = BF_CONVERGED;
+                        break;
+                    }
                     if (total >= maxiter) { flag = BF_MAXITER; break; }
                     TRYB(init(maxiter - total));
                     TRYB(read_s(ctx, &hs));
