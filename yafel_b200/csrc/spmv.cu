@@ -1073,9 +1073,6 @@ static yg_status tune_precision(yg_matrix A, int precision, double *x, double *y
         cands.push_back({1, 32});
         for (int L : {32, 1, 2, 4, 8, 16}) cands.push_back({2, L});  // TMA configurations
     }
-    if (A->block == 1)
-        for (int L : {1, 2, 4, 8})  // row-tile configurations the matrix's rows fit
-            if (spmv_prepare(A, 3, L) == YG_OK) cands.push_back({3, L});
     const bool f32 = precision != YG_PREC_FP64;
     int *pv = f32 ? &A->variant32 : &A->variant, *pl = f32 ? &A->lanes32 : &A->lanes;
     const int save_v = *pv, save_l = *pl;
@@ -1109,7 +1106,9 @@ static yg_status tune_precision(yg_matrix A, int precision, double *x, double *y
 }
 
 // Device autotuner: time each candidate (flat with 2..32 lanes, cp.async
-// staged and six TMA configurations for 2x2 and 3x3 blocks) on this matrix with
+// staged and six TMA configurations for 2x2 and 3x3 blocks; the row-tile variant
+// is taken only when set explicitly: on the assembled CSR matrices measured it
+// stayed below the flat kernel) on this matrix with
 // CUDA events and keep the fastest, separately for FP64 values and, when the
 // matrix has them, FP32 values.  Must not run during stream capture.  Results
 // are cached per (rows, blocks, block size, precision): a re-assembled matrix of
