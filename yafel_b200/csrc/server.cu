@@ -8,11 +8,14 @@
 // it, and every attached system advances in the shared batch (batch.cu: one
 // persistent launch per step of every iteration, PCG and BiCGSTAB together).
 // A launch runs one block of iterations without blocking the host, which
-// builds the next admitted systems meanwhile; the following wait retires the
-// systems that finished, whose results the client then reads and releases.
-// Systems of at least `solo_rows` rows (when set) fill the GPU on their own:
-// they skip the batch and are solved one at a time, after a block, by the
-// single-system solvers (autotuned SpMV, fused iterations).
+// builds the next admitted systems meanwhile (yg_server_ready says, without
+// blocking, whether the block is done; building on a second context of the
+// device keeps the builds off the batch's stream); the following wait retires
+// the systems that finished, whose results the client then reads and releases.
+// Inside the batch, systems with a large matrix run their iteration SpMV as
+// their own single-system launch (yg_server_set_solo_spmv_bytes).  Systems of
+// at least `solo_rows` rows (when set; off by default) skip the batch instead
+// and are solved one at a time, after a block, by the single-system solvers.
 #include "internal.h"
 
 #include <deque>
