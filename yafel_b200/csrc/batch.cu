@@ -22,8 +22,11 @@
 //       partials of r0.r, r.r -> beta and the stopping tests
 // (V1 and S2 are launched only when BiCGSTAB systems are present).  Every
 // decision about a system is taken once, by the warp or CTA that completes the
-// system's last item of a kernel (a per-system ticket), so every CTA of the
-// next kernel sees the same state.  Sums run in a fixed order over a fixed item
+// system's last item of a kernel (a per-system ticket; systems with more than
+// kChunk matrix items sum their partials in two levels), so every CTA of the
+// next kernel sees the same state.  A system whose matrix holds at least
+// solo_bytes runs S1/S2 as its own launch of the single-system SpMV kernel
+// followed by a one-warp decision kernel, both in the captured graph.  Sums run in a fixed order over a fixed item
 // decomposition: a system's result does not depend on which other systems
 // share the batch.  Converged systems drop out of the kernels at once and out
 // of the work tables at the next compaction.  A block of m iterations plus a
@@ -34,7 +37,8 @@
 // (init).  Systems can be added and removed between replays (continuous
 // batching): only the descriptor and work tables change, and kernels read their
 // ranges from device memory, so the captured graph stays valid while the set of
-// (method, block size) groups present does not change.
+// (method, block size) groups present and of systems with their own SpMV launch
+// does not change.
 #include "internal.h"
 #include "device_common.cuh"
 
