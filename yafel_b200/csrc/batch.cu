@@ -1318,7 +1318,7 @@ static void launch_solo(yg_batch bt, int kind, int parity) {
         const bool bicg = d.method == BM_BICG;
         if ((kind == SP_BICG_T || kind == SP_BICG_V) != bicg) continue;
         const int prec = d.precision == YG_PREC_MIXED ? YG_PREC_MIXED : YG_PREC_FP64;
-        const int grid = spmv_grid_for(A, prec);
+        const int grid = std::min(spmv_grid_for(A, prec), kMaxReduceBlocks);  // the launch's CTAs = partials
         const int32_t *flag = &bt->d_scal[s].flag;
         const int64_t l0 = A->ctx->launches;
         yg_status st;
