@@ -679,7 +679,7 @@ def run_serve(args):
             t = time.perf_counter() - t0
             while state["nsub"] < n and arr[idxs[state["nsub"]]] - arr[idxs[0]] <= t:
                 i = idxs[state["nsub"]]
-                idx[S.submit(workloads.est_bytes(specs[i]))] = i
+                idx[S.submit(workloads.est_bytes(specs[i], mixed=precision == yb.PREC_MIXED))] = i
                 state["nsub"] += 1
 
         def admit_build(limit, while_running=False):

@@ -95,16 +95,17 @@ def assemble(spec, ctx, mesh=None):
     return mesh, K, b, clamp_dofs(dm.dof_nodes, dpn)
 
 
-def est_bytes(spec):
+def est_bytes(spec, mixed=False):
     """Upper estimate of the solver-resident device bytes of a problem, from its
     size alone (before it is built): matrix values and columns with at most
-    dpn * (2p+1)^dim entries per row, the right-hand side, the iterate and the
-    Krylov work vectors (4 for PCG, 9 for BiCGSTAB), plus row data."""
+    dpn * (2p+1)^dim entries per row (plus the FP32 copy of the values when
+    `mixed`), the right-hand side, the iterate and the Krylov work vectors (4 for
+    PCG, 9 for BiCGSTAB), plus row data."""
     p, dim, dpn, n = spec["order"], spec["dim"], spec["dpn"], spec["n"]
     dofs = dpn * (p * n + 1) ** dim
     nnz_row = dpn * (2 * p + 1) ** dim
     vecs = (9 if spec["kind"] == "supg" else 4) + 2
-    return int(dofs * (12 * nnz_row + 8 * vecs + 16))
+    return int(dofs * ((16 if mixed else 12) * nnz_row + 8 * vecs + 16))
 
 
 def serving_specs(count, base=BASE_SEED + 1_000_000, lo=1e3, hi=1e6):
