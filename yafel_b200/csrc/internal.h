@@ -55,6 +55,8 @@ struct KrylovScalars {
     int32_t criterion;
     int32_t check_freq;  // BiCGSTAB reference criterion: true-residual check period
     int32_t pad;
+    int64_t iter_seen;   // CG: iter as the update kernel saw it (read by the next kernel,
+                         // which increments iter: no block reads a value another block writes)
 };
 
 struct yg_context_t {

@@ -133,6 +133,7 @@ k_cg_update(int64_t n, const double *__restrict__ pq_partials, int np, KrylovSca
         if (blockIdx.x == 0 && threadIdx.x == 0) S->flag = isfinite(pq) ? FLAG_BREAKDOWN : FLAG_NAN;
         return;
     }
+    if (blockIdx.x == 0 && threadIdx.x == 0) S->iter_seen = S->iter;  // for k_cg_pupdate's iteration cap test
     int64_t lo, hi;
     block_chunk(n, lo, hi);
     double srz = 0, srr = 0;
@@ -174,11 +175,14 @@ k_cg_pupdate(int64_t n, const double *__restrict__ partials_in, int np, KrylovSc
         if (sqrt(rr) <= S->tol * sqrt(S->bb)) { done = true; flag = FLAG_CONVERGED; }
     }
     if (!isfinite(rz_new)) { done = true; flag = FLAG_NAN; }
-    if (!done && S->iter + 1 >= S->maxiter) { done = true; flag = FLAG_MAXITER; }
+    // the cap test reads the count the previous kernel recorded: S->iter itself is
+    // incremented below by block 0 while other blocks may still be deciding
+    const int64_t it = S->iter_seen;
+    if (!done && it + 1 >= S->maxiter) { done = true; flag = FLAG_MAXITER; }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         S->rz[parity ^ 1] = rz_new;
         S->rr = rr;
-        S->iter += 1;
+        S->iter = it + 1;
         if (done) S->flag = flag;
     }
     if (done) return;
