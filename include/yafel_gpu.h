@@ -140,6 +140,14 @@ enum { YG_FORMAT_CSR = 0, YG_FORMAT_BCSR = 1 };
 YG_API yg_status yg_assemble(yg_dofmap d, const yg_physics *physics, uint32_t requirements,
                       int32_t format, yg_matrix *K, yg_vector residual);
 
+/* LocalSmoothingGradient<Physics>(FESystem&) (include/assembly/LocalSmoothingGradient.hpp:20-94):
+ * the nodal gradient of `solution` (n_dofs entries) over the cells of dimension
+ * nsd, written to `gradient` (n_dofs * nsd entries, row-major: dof-major, then
+ * the nsd derivatives): the element gradient at each quadrature point, weighted
+ * by N_A jxw, summed per dof and divided by the sum of N_A jxw (a dof no such
+ * cell touches gets 0/0).  Deterministic (element-coloured sums). */
+YG_API yg_status yg_local_smoothing_gradient(yg_dofmap d, int32_t nsd, yg_vector solution, yg_vector gradient);
+
 /* DirichletBC::apply(A, rhs) for one BC object (src/boundary_conditions/DirichletBC.cpp:27-89):
  * rhs -= A*g, zero the BC rows and columns, unit diagonal, rhs_bc = g.  bc_dofs
  * are global dofs (node*dof_per_node + component), bc_values their g. */

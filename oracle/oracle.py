@@ -72,6 +72,8 @@ def lib():
         L.or_free_dofmap.argtypes = [C.POINTER(_Dofmap)]
         L.or_assemble.argtypes = [C.POINTER(_Dofmap), C.c_int32, C.c_int32, C.c_int32, f64p, C.c_void_p]
         L.or_assemble.restype = C.POINTER(_Csr)
+        L.or_local_smoothing_gradient.argtypes = [C.POINTER(_Dofmap), C.c_int32, C.c_int32, f64p, f64p]
+        L.or_local_smoothing_gradient.restype = None
         L.or_dirichlet_apply.argtypes = [C.POINTER(_Csr), f64p, u8p, f64p]
         L.or_csr_from_triplets.argtypes = [i64p, i64p, f64p, C.c_int64]
         L.or_csr_from_triplets.restype = C.POINTER(_Csr)
@@ -288,6 +290,15 @@ def assemble(dm, dpn, nsd, physics, params, residual=True):
     p = lib().or_assemble(dm._p, dpn, nsd, physics, params,
                           R.ctypes.data_as(C.c_void_p) if R is not None else None)
     return _csr_from_ptr(p), R
+
+
+def local_smoothing_gradient(dm, dpn, nsd, sol):
+    """LocalSmoothingGradient (include/assembly/LocalSmoothingGradient.hpp:20-94):
+    the nodal gradient, shape (n_nodes*dpn, nsd)."""
+    sol = np.ascontiguousarray(sol, dtype=np.float64)
+    out = np.zeros((dm.n_nodes * dpn, nsd))
+    lib().or_local_smoothing_gradient(dm._p, dpn, nsd, sol, out)
+    return out
 
 
 def dirichlet_apply(A, rhs, mask, vals):

@@ -872,6 +872,51 @@ or_csr *or_assemble(const or_dofmap *d, int32_t dpn, int32_t nsd, int32_t physic
     return K;
 }
 
+/* LocalSmoothingGradient<Physics> (include/assembly/LocalSmoothingGradient.hpp:20-94):
+ * over the cells of topology dimension nsd in cell order and their quadrature
+ * points in order, the gradient of each solution component at the point
+ * (qp_grad(comp, i) = sum over local dofs A of u_A dN_A/dx_i) is spread to the
+ * element's dofs with weights N_A jxw into VolTimesGrad, and N_A jxw into Volume;
+ * the result is VolTimesGrad / Volume per dof (0/0 where no cell touches it). */
+void or_local_smoothing_gradient(const or_dofmap *d, int32_t dpn, int32_t nsd, const double *sol, double *grad) {
+    or_eltab tabs[3][4];
+    memset(tabs, 0, sizeof(tabs));
+    const int64_t ndofs = (int64_t)d->n_nodes * dpn;
+    double *vol = (double *)calloc(ndofs > 0 ? ndofs : 1, sizeof(double));
+    double *vtg = (double *)calloc(ndofs > 0 ? ndofs * nsd : 1, sizeof(double));
+    for (int e = 0; e < d->n_cells; ++e) {
+        if (d->topo_dim[e] != nsd || d->topology[e] == OR_NONE) continue;
+        or_eltab *T = &tabs[d->topology[e]][d->topo_dim[e]];
+        if (!T->ok) build_eltab(T, d->topology[e], d->topo_dim[e], d->poly_order[e]);
+        const int nen = d->offsets[e + 1] - d->offsets[e];
+        const int32_t *gn = &d->elements[d->offsets[e]];
+        double xe[3 * OR_MAX_NEN], g[3 * OR_MAX_NEN], ul[3 * OR_MAX_NEN];
+        for (int A = 0; A < nen; ++A)
+            for (int k = 0; k < 3; ++k) xe[3 * A + k] = d->nodes[3 * (int64_t)gn[A] + k];
+        for (int A = 0; A < nen * dpn; ++A) ul[A] = sol[(int64_t)gn[A / dpn] * dpn + A % dpn];
+        for (int q = 0; q < T->nq; ++q) {
+            const double jxw = element_update(nsd, nen, xe, &T->dN[(int64_t)q * nen * T->dim], T->dim, T->w[q], g);
+            double qg[3][3] = {{0}};
+            for (int A = 0; A < nen * dpn; ++A)
+                for (int i = 0; i < nsd; ++i) qg[A % dpn][i] += ul[A] * g[(A / dpn) * nsd + i];
+            const double *Nq = &T->N[(int64_t)q * nen];
+            for (int A = 0; A < nen * dpn; ++A) {
+                const int64_t G = (int64_t)gn[A / dpn] * dpn + A % dpn;
+                const double NA = Nq[A / dpn];
+                vol[G] += NA * jxw;
+                for (int i = 0; i < nsd; ++i) vtg[G * nsd + i] += NA * qg[A % dpn][i] * jxw;
+            }
+        }
+    }
+    for (int64_t A = 0; A < ndofs; ++A)
+        for (int i = 0; i < nsd; ++i) grad[A * nsd + i] = vtg[A * nsd + i] / vol[A];
+    free(vol);
+    free(vtg);
+    for (int t = 0; t < 3; ++t)
+        for (int td = 0; td < 4; ++td)
+            if (tabs[t][td].ok) { free(tabs[t][td].N); free(tabs[t][td].dN); }
+}
+
 /* DirichletBC::apply, RowMajor form (src/boundary_conditions/DirichletBC.cpp:27-56):
  * rhs -= A g, then zero BC rows and columns, unit diagonal, rhs_bc = g. */
 void or_dirichlet_apply(or_csr *A, double *rhs, const uint8_t *mask, const double *vals) {

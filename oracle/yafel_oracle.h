@@ -82,6 +82,8 @@ void or_free_dofmap(or_dofmap *d);
 or_csr *or_assemble(const or_dofmap *d, int32_t dpn, int32_t nsd, int32_t physics,
                     const double *params, double *residual /* nullable, n_nodes*dpn */);
 void or_dirichlet_apply(or_csr *A, double *rhs, const uint8_t *mask, const double *vals);
+/* LocalSmoothingGradient: grad is n_nodes*dpn rows of nsd (row-major). */
+void or_local_smoothing_gradient(const or_dofmap *d, int32_t dpn, int32_t nsd, const double *sol, double *grad);
 
 /* ---- sparse containers ---- */
 or_csr *or_csr_from_triplets(const int64_t *r, const int64_t *c, const double *v, int64_t n);

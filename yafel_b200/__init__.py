@@ -17,7 +17,7 @@ from ._lib import (lib, check, YafelError, Physics, SolveOpts, SolveStats, YG_OK
                    YG_UNSUPPORTED)
 from . import meshgen
 
-__all__ = ["Context", "default_context", "Mesh", "DoFManager", "FESystem", "CGAssembly",
+__all__ = ["Context", "default_context", "Mesh", "DoFManager", "FESystem", "CGAssembly", "LocalSmoothingGradient",
            "AssemblyRequirement", "PoissonEquation", "LinearElasticity", "AdvectionDiffusionSUPG",
            "DirichletBC", "DeviceVector", "sparse_csr", "sparse_bcsr", "JacobiPreconditioner",
            "ILUPreconditioner", "IdentityPreconditioner", "cg_solve", "pcg_solve",
@@ -465,6 +465,7 @@ class FESystem:
         n = dofm.ndofs
         self.global_residual = DeviceVector(n, self.ctx)
         self.solution = DeviceVector(n, self.ctx)
+        self.solution_gradient = None
         self.global_tangent = None
         self.time = 0.0
 
@@ -476,6 +477,11 @@ class FESystem:
 
     def getSolution(self):
         return self.solution
+
+    def getSolutionGradient(self):
+        """The nodal gradient of the last LocalSmoothingGradient call: a
+        DeviceVector of n_dofs * nsd entries (row-major, one row per dof)."""
+        return self.solution_gradient
 
     def getDoFManager(self):
         return self.dofm
@@ -498,6 +504,18 @@ def CGAssembly(physics, feSystem, requirements=(AssemblyRequirement.Residual, As
                             feSystem.global_residual.h), "CGAssembly")
     if K is None and (mask & AssemblyRequirement.Tangent):
         feSystem.global_tangent = _wrap_matrix(h, feSystem.ctx)
+    return feSystem
+
+
+def LocalSmoothingGradient(physics, feSystem):
+    """LocalSmoothingGradient<Physics>(FESystem&)
+    (include/assembly/LocalSmoothingGradient.hpp:20-94): the gradient of the
+    FESystem's solution averaged to the dofs with weights N_A jxw over the cells
+    of dimension physics.nsd(); stored as the FESystem's solution gradient."""
+    nsd = physics.nsd()
+    g = DeviceVector(feSystem.dofm.ndofs * nsd, feSystem.ctx)
+    check(lib().yg_local_smoothing_gradient(feSystem.dofm.h, nsd, feSystem.solution.h, g.h), "LocalSmoothingGradient")
+    feSystem.solution_gradient = g
     return feSystem
 
 

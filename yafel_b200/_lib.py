@@ -80,6 +80,7 @@ SIGNATURES = {
     "yg_batch_launch": (i32, [vp]),
     "yg_batch_wait": (i32, [vp, P(i32)]),
     "yg_batch_ready": (i32, [vp, P(i32)]),
+    "yg_local_smoothing_gradient": (i32, [vp, i32, vp, vp]),
     "yg_batch_set_solo_bytes": (i32, [vp, i64]),
     "yg_batch_get_tuning": (i32, [vp, P(i32)]),
     "yg_batch_set_tuning": (i32, [vp, i32, i32, i32, i32]),

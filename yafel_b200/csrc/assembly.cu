@@ -853,3 +853,192 @@ extern "C" yg_status yg_dirichlet_apply(yg_matrix K, yg_vector rhs, const int64_
     if (e != cudaSuccess) return fail(YG_CUDA_ERROR, "Dirichlet apply: %s", cudaGetErrorString(e));
     return YG_OK;
 }
+
+// ------------------------------------------------------------------ gradient recovery
+
+namespace yg {
+
+// LocalSmoothingGradient<Physics> (include/assembly/LocalSmoothingGradient.hpp:20-94):
+// per cell of dimension NSD (one CTA), per quadrature point, the gradient of each
+// of the DPN solution components, qg(comp, i) = sum_A u_A dN_A/dx_i, is spread to
+// the cell's dofs: vtg(dof, i) += N_A qg(comp_A, i) jxw and vol(dof) += N_A jxw.
+// A CTA first sums its quadrature points, then adds into the global arrays; the
+// cells of one launch share no node (one colour), so the adds need no atomics and
+// the sums are deterministic.  The geometry is that of k_assemble's Element::update.
+template <int NSD, int DPN>
+__global__ void __launch_bounds__(128)
+k_smooth_gradient(const int32_t *__restrict__ order, int ncell, const int32_t *__restrict__ off,
+                  const int32_t *__restrict__ el, const double *__restrict__ nodes, const double *__restrict__ tab,
+                  int nen, int nq, int tdim, const double *__restrict__ sol, double *__restrict__ vol,
+                  double *__restrict__ vtg) {
+    extern __shared__ double sm[];
+    double *xe = sm;                           // nen*3
+    double *G = xe + 3 * nen;                  // nq*nen*NSD
+    double *jxw = G + (size_t)nq * nen * NSD;  // nq
+    double *Ji = jxw + nq;                     // nq*9
+    double *ul = Ji + 9 * nq;                  // nen*DPN
+    double *qg = ul + nen * DPN;               // nq*DPN*NSD
+    int32_t *gn = reinterpret_cast<int32_t *>(qg + (size_t)nq * DPN * NSD);  // nen
+    const double *tN = tab;
+    const double *tdN = tab + (size_t)nq * nen;
+    const double *tw = tdN + (size_t)nq * nen * tdim;
+    for (int t = blockIdx.x; t < ncell; t += gridDim.x) {
+        const int c = order[t];
+        const int base = off[c];
+        for (int a = threadIdx.x; a < nen; a += blockDim.x) {
+            const int n = el[base + a];
+            gn[a] = n;
+            xe[3 * a + 0] = nodes[3 * (int64_t)n + 0];
+            xe[3 * a + 1] = nodes[3 * (int64_t)n + 1];
+            xe[3 * a + 2] = nodes[3 * (int64_t)n + 2];
+        }
+        __syncthreads();
+        for (int a = threadIdx.x; a < nen * DPN; a += blockDim.x) ul[a] = sol[(int64_t)gn[a / DPN] * DPN + a % DPN];
+        for (int q = threadIdx.x; q < nq; q += blockDim.x) {
+            double J[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+            for (int A = 0; A < nen; ++A) {
+                const double *d = tdN + ((size_t)q * nen + A) * tdim;
+#pragma unroll
+                for (int i = 0; i < NSD; ++i)
+#pragma unroll
+                    for (int j = 0; j < NSD; ++j) J[i][j] += xe[3 * A + i] * d[j];
+            }
+            double det, inv[3][3];
+            if (NSD == 1) {
+                det = J[0][0];
+                inv[0][0] = 1.0 / J[0][0];
+            } else if (NSD == 2) {
+                det = J[0][0] * J[1][1] - J[0][1] * J[1][0];
+                const double di = 1.0 / det;
+                inv[0][0] = J[1][1] * di; inv[1][1] = J[0][0] * di;
+                inv[0][1] = -J[0][1] * di; inv[1][0] = -J[1][0] * di;
+            } else {
+                det = J[0][0] * (J[1][1] * J[2][2] - J[1][2] * J[2][1]) - J[0][1] * (J[1][0] * J[2][2] - J[2][0] * J[1][2]) +
+                      J[0][2] * (J[1][0] * J[2][1] - J[2][0] * J[1][1]);
+                const double di = 1.0 / det;
+                inv[0][0] = (J[1][1] * J[2][2] - J[1][2] * J[2][1]) * di;
+                inv[0][1] = -(J[0][1] * J[2][2] - J[2][1] * J[0][2]) * di;
+                inv[0][2] = (J[0][1] * J[1][2] - J[1][1] * J[0][2]) * di;
+                inv[1][0] = -(J[1][0] * J[2][2] - J[2][0] * J[1][2]) * di;
+                inv[1][1] = (J[0][0] * J[2][2] - J[0][2] * J[2][0]) * di;
+                inv[1][2] = -(J[0][0] * J[1][2] - J[1][0] * J[0][2]) * di;
+                inv[2][0] = (J[1][0] * J[2][1] - J[2][0] * J[1][1]) * di;
+                inv[2][1] = -(J[0][0] * J[2][1] - J[2][0] * J[0][1]) * di;
+                inv[2][2] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) * di;
+            }
+            jxw[q] = det * tw[q];
+#pragma unroll
+            for (int i = 0; i < NSD; ++i)
+#pragma unroll
+                for (int j = 0; j < NSD; ++j) Ji[9 * q + 3 * i + j] = inv[i][j];
+        }
+        __syncthreads();
+        for (int idx = threadIdx.x; idx < nq * nen; idx += blockDim.x) {
+            const int q = idx / nen;
+            const double *d = tdN + (size_t)idx * tdim;
+#pragma unroll
+            for (int dd = 0; dd < NSD; ++dd) {
+                double s = 0;
+#pragma unroll
+                for (int j = 0; j < NSD; ++j) s += Ji[9 * q + 3 * j + dd] * d[j];
+                G[(size_t)idx * NSD + dd] = s;
+            }
+        }
+        __syncthreads();
+        // qg[(q*DPN + comp)*NSD + i] = sum over the cell's nodes A of u(A, comp) dN_A/dx_i at q
+        for (int idx = threadIdx.x; idx < nq * DPN * NSD; idx += blockDim.x) {
+            const int q = idx / (DPN * NSD), comp = (idx / NSD) % DPN, i = idx % NSD;
+            double s = 0;
+            for (int A = 0; A < nen; ++A) s += ul[A * DPN + comp] * G[((size_t)q * nen + A) * NSD + i];
+            qg[idx] = s;
+        }
+        __syncthreads();
+        for (int a = threadIdx.x; a < nen * DPN; a += blockDim.x) {
+            const int A = a / DPN, comp = a % DPN;
+            double v = 0, w[NSD];
+#pragma unroll
+            for (int i = 0; i < NSD; ++i) w[i] = 0;
+            for (int q = 0; q < nq; ++q) {
+                const double NA = tN[(size_t)q * nen + A];
+                v += NA * jxw[q];
+#pragma unroll
+                for (int i = 0; i < NSD; ++i) w[i] += NA * qg[(q * DPN + comp) * NSD + i] * jxw[q];
+            }
+            const int64_t g = (int64_t)gn[A] * DPN + comp;
+            vol[g] += v;
+#pragma unroll
+            for (int i = 0; i < NSD; ++i) vtg[g * NSD + i] += w[i];
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void k_divide_rows(int64_t n, int nsd, const double *__restrict__ vol, double *__restrict__ g) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n * nsd; i += (int64_t)gridDim.x * blockDim.x)
+        g[i] = g[i] / vol[i / nsd];
+}
+
+template <int NSD, int DPN>
+static yg_status launch_smooth_gradient(yg_context ctx, const ElementGroup &g, yg_dofmap d, const double *sol,
+                                        double *vol, double *vtg) {
+    const int nen = g.tab.nen, nq = g.tab.nq;
+    const size_t smem = sizeof(double) * (3 * nen + (size_t)nq * nen * NSD + nq + 9 * nq + nen * DPN +
+                                          (size_t)nq * DPN * NSD) + sizeof(int32_t) * nen + 16;
+    auto kern = k_smooth_gradient<NSD, DPN>;
+    if (smem > 48 * 1024) YG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    for (size_t c = 0; c + 1 < g.color_ptr.size(); ++c) {
+        const int n = g.color_ptr[c + 1] - g.color_ptr[c];
+        if (n == 0) continue;
+        const int grid = std::min(n, ctx->num_sms * 16);
+        kern<<<grid, 128, smem, ctx->stream>>>(g.d_order + g.color_ptr[c], n, d->d_offsets, d->d_elements, d->d_nodes,
+                                               g.d_tab, nen, nq, g.tab.dim, sol, vol, vtg);
+        YG_LAUNCHED(ctx);
+    }
+    YG_CUDA(cudaGetLastError());
+    return YG_OK;
+}
+
+template <int NSD>
+static yg_status smooth_gradient_dpn(yg_context ctx, const ElementGroup &g, yg_dofmap d, int dpn, const double *sol,
+                                     double *vol, double *vtg) {
+    if (dpn == 1) return launch_smooth_gradient<NSD, 1>(ctx, g, d, sol, vol, vtg);
+    if (dpn == 2) return launch_smooth_gradient<NSD, 2>(ctx, g, d, sol, vol, vtg);
+    return launch_smooth_gradient<NSD, 3>(ctx, g, d, sol, vol, vtg);
+}
+
+}  // namespace yg
+
+extern "C" yg_status yg_local_smoothing_gradient(yg_dofmap d, int32_t nsd, yg_vector solution, yg_vector gradient) {
+    if (!d || !solution || !gradient) return fail(YG_BAD_ARG, "yg_local_smoothing_gradient: NULL argument");
+    if (nsd < 1 || nsd > 3) return fail(YG_BAD_ARG, "yg_local_smoothing_gradient: nsd must be 1..3");
+    yg_context ctx = d->ctx;
+    if (!ctx) return fail(YG_BAD_ARG, "yg_local_smoothing_gradient: dofmap was created without a context");
+    const int dpn = d->host.dof_per_node;
+    if (dpn < 1 || dpn > 3) return fail(YG_UNSUPPORTED, "yg_local_smoothing_gradient: dof_per_node %d (1..3)", dpn);
+    const int64_t ndofs = (int64_t)d->host.n_nodes() * dpn;
+    if (solution->n != ndofs || gradient->n != ndofs * nsd)
+        return fail(YG_BAD_ARG, "yg_local_smoothing_gradient: solution needs %lld entries, gradient %lld",
+                    (long long)ndofs, (long long)(ndofs * nsd));
+    YG_TRY(build_pattern(d, nsd));  // element groups and colourings of the cells of dimension nsd
+    double *vol = nullptr;
+    YG_TRY(dev_alloc_t(ctx, &vol, ndofs));
+    YG_CUDA(cudaMemsetAsync(vol, 0, sizeof(double) * ndofs, ctx->stream));
+    YG_CUDA(cudaMemsetAsync(gradient->d, 0, sizeof(double) * ndofs * nsd, ctx->stream));
+    yg_status s = YG_OK;
+    for (const ElementGroup &g : d->groups) {
+        switch (nsd) {
+        case 1: s = smooth_gradient_dpn<1>(ctx, g, d, dpn, solution->d, vol, gradient->d); break;
+        case 2: s = smooth_gradient_dpn<2>(ctx, g, d, dpn, solution->d, vol, gradient->d); break;
+        default: s = smooth_gradient_dpn<3>(ctx, g, d, dpn, solution->d, vol, gradient->d); break;
+        }
+        if (s != YG_OK) break;
+    }
+    if (s == YG_OK && ndofs > 0) {
+        k_divide_rows<<<stream_grid(ctx, ndofs * nsd), kThreads, 0, ctx->stream>>>(ndofs, nsd, vol, gradient->d);
+        YG_LAUNCHED(ctx);
+    }
+    dev_free(ctx, vol);
+    if (s != YG_OK) return s;
+    YG_CUDA(cudaGetLastError());
+    return YG_OK;
+}
