@@ -1,6 +1,6 @@
 // yafel_gpu.hpp -- header-only C++ adapters with the reference's spellings over
 // the C ABI of yafel_gpu.h.  Code written against the reference's
-//   DoFManager / FESystem / CGAssembly<Physics> / DirichletBC
+//   DoFManager / FESystem / CGAssembly<Physics> / LocalSmoothingGradient<Physics> / DirichletBC
 //   sparse_csr / sparse_bcsr / cg_solve / pcg_solve / bicgstab_solve /
 //   JacobiPreconditioner / ILUPreconditioner / IdentityPreconditioner
 // switches to the GPU by including this header and using namespace yafel::gpu.
@@ -321,6 +321,16 @@ public:
     }
     DeviceVector &getGlobalResidual() { return residual_; }
     DeviceVector &getSolution() { return solution_; }
+    // the nodal gradient of the last LocalSmoothingGradient call: n_dofs * nsd
+    // entries, row-major (one row of nsd derivatives per dof)
+    DeviceVector &getSolutionGradient() {
+        if (!gradient_) throw std::runtime_error("FESystem: no solution gradient computed");
+        return *gradient_;
+    }
+    void reset_gradient(int nsd) {
+        const int64_t n = (int64_t)dofm.nNodes() * dofm.dof_per_node * nsd;
+        if (!gradient_ || gradient_->size() != n) gradient_.reset(new DeviceVector(dofm.context(), n));
+    }
     DoFManager &getDoFManager() { return dofm; }
     double &currentTime() { return time_; }
     int format() const { return format_; }
@@ -336,6 +346,7 @@ private:
     double time_ = 0;
     DeviceVector residual_, solution_;
     std::unique_ptr<matrix_base> tangent_;
+    std::unique_ptr<DeviceVector> gradient_;
 };
 
 enum class AssemblyRequirement : int { Residual, Tangent, DtMass, LumpedDtMassInverse, DtDtMass };
@@ -380,6 +391,18 @@ void CGAssembly(FESystem &fe, std::vector<AssemblyRequirement> requirements = {A
     yg_matrix K = fe.tangent_handle();
     check(yg_assemble(fe.dofm.get(), &p, mask, fe.format(), &K, fe.getGlobalResidual().get()), "CGAssembly");
     if (mask & YG_REQ_TANGENT) fe.adopt_tangent(K);
+}
+
+// LocalSmoothingGradient<Physics>(FESystem&)
+// (include/assembly/LocalSmoothingGradient.hpp:20-94): the gradient of the
+// solution averaged to the dofs with weights N_A jxw over the cells of dimension
+// Physics::nsd(); read it with fe.getSolutionGradient().
+template <typename Physics>
+void LocalSmoothingGradient(FESystem &fe) {
+    fe.reset_gradient(Physics::nsd());
+    check(yg_local_smoothing_gradient(fe.dofm.get(), Physics::nsd(), fe.getSolution().get(),
+                                      fe.getSolutionGradient().get()),
+          "LocalSmoothingGradient");
 }
 
 // DirichletBC (include/boundary_conditions/DirichletBC.hpp:23-89)

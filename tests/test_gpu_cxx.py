@@ -27,6 +27,13 @@ def test_cxx_adapter_compiles(tmp_path):
     assert os.path.exists(build_example(tmp_path))
 
 
+def test_cxx_gradient_adapter_compiles(tmp_path):
+    obj = str(tmp_path / "gradient_compile.o")
+    subprocess.run(["g++", "-std=c++17", "-O2", "-c", "-I", os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "tests", "cxx", "gradient_compile.cpp"), "-o", obj], check=True)
+    assert os.path.exists(obj)
+
+
 @pytest.mark.gpu
 def test_cxx_drop_in_poisson_matches_oracle(tmp_path):
     exe = build_example(tmp_path)
