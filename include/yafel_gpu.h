@@ -105,6 +105,27 @@ YG_API yg_status yg_dofmap_sizes(yg_dofmap d, int32_t *n_dof_nodes, int32_t *n_c
  * (DoFManager.hpp:67-73); any pointer may be NULL. */
 YG_API yg_status yg_dofmap_get(yg_dofmap d, double *dof_nodes_xyz, int32_t *element_offsets,
                         int32_t *elements, int8_t *topology, int8_t *topo_dim, int8_t *poly_order);
+/* A dofmap from a numbering the caller already has: the public members of a
+ * host DoFManager (dof_nodes, element_offsets, elements, element_types;
+ * include/utils/DoFManager.hpp:62-70) after DoFManager(M, CG, p, dpn).  For a
+ * caller that keeps the reference's own DoFManager and hands only assembly and
+ * the solve to the GPU.  cell_types are the mesh CellType codes of each cell
+ * (they give the element topology and dimension); every cell has poly_order.
+ * Fails with YG_BAD_ARG when an element lists a node outside dof_nodes or its
+ * node count is not that of its element type. */
+YG_API yg_status yg_dofmap_create_from_numbering(yg_context ctx, const double *dof_nodes_xyz, int32_t n_dof_nodes,
+                                          const int32_t *element_offsets, const int32_t *elements,
+                                          const int32_t *cell_types, int32_t n_cells, int32_t poly_order,
+                                          int32_t dof_per_node, yg_dofmap *out);
+/* Element(ElementType{topology, dim, p}) tables as the GPU uses them
+ * (src/element/Element.cpp:11-31, make_tensorproduct_element.cpp:17-145,
+ * make_simplex_element.cpp:17-142, ShapeFunctionUtils.cpp:16-304): local node
+ * coordinates (nen x 3), volume quadrature points (nq x 3) and weights (nq),
+ * shape values N (nq x nen) and reference gradients dN/dxi (nq x nen x dim).
+ * Host only.  Call with NULL arrays to get nen and nq; YG_UNSUPPORTED for an
+ * element the reference cannot build either (tetrahedra above p = 2). */
+YG_API yg_status yg_element_table(int32_t topology, int32_t dim, int32_t poly_order, int32_t *nen, int32_t *nq,
+                           double *local_nodes_xyz, double *qp_xyz, double *qw, double *N, double *dN);
 
 /* ------------------------------------------------------------------ assembly */
 

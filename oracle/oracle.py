@@ -160,8 +160,133 @@ def ref():
         R.ref_ilu_factor.restype = C.c_void_p
         R.ref_ilu_apply.argtypes = [C.c_void_p, f64p]
         R.ref_jacobi_apply.argtypes = [C.c_void_p, f64p]
+        # the assembly half (ref_assembly.cpp)
+        R.refa_set_threads.argtypes = [C.c_int]
+        R.refa_dofmanager.argtypes = [f64p, C.c_int, i32p, i32p, i32p, C.c_int, C.c_int, C.c_int]
+        R.refa_dofmanager.restype = C.c_void_p
+        R.refa_dofmanager_free.argtypes = [C.c_void_p]
+        R.refa_dofmanager_sizes.argtypes = [C.c_void_p] + [C.POINTER(C.c_int)] * 3
+        R.refa_dofmanager_get.argtypes = [C.c_void_p, f64p, i32p, i32p, i8p, i8p, i8p]
+        R.refa_assemble.argtypes = [C.c_void_p, C.c_int, C.c_int, f64p, C.c_int, C.c_int]
+        R.refa_assemble.restype = C.c_void_p
+        R.refa_system_free.argtypes = [C.c_void_p]
+        R.refa_system_sizes.argtypes = [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+        R.refa_system_get.argtypes = [C.c_void_p, i32p, i32p, f64p, f64p]
+        R.refa_system_set_residual.argtypes = [C.c_void_p, f64p]
+        R.refa_dirichlet_plane.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double,
+                                           C.c_double, C.POINTER(C.c_int)]
+        R.refa_dirichlet_nodes.argtypes = [C.c_void_p, C.c_int, i32p, C.c_int, C.c_double]
+        R.refa_local_smoothing_gradient.argtypes = [C.c_void_p, C.c_int, f64p, f64p]
+        R.refa_element.argtypes = [C.c_int] * 4 + [C.POINTER(C.c_int)] * 2 + [C.c_void_p] * 5
         _REF = R
     return _REF
+
+
+def ref_element(topology, dim, p, qrm=2):
+    """The reference's Element(ElementType{topology, dim, p}, 1, qrm) tables:
+    (local nodes nen x 3, quadrature points nq x 3, weights, N nq x nen,
+    dN/dxi nq x nen x dim)."""
+    R = ref()
+    nen, nq = C.c_int(), C.c_int()
+    R.refa_element(topology, dim, p, qrm, C.byref(nen), C.byref(nq), None, None, None, None, None)
+    a, q = nen.value, nq.value
+    L, X, W = np.zeros((a, 3)), np.zeros((q, 3)), np.zeros(q)
+    N, dN = np.zeros((q, a)), np.zeros((q, a, dim))
+    ptr = lambda x: x.ctypes.data_as(C.c_void_p)
+    R.refa_element(topology, dim, p, qrm, C.byref(nen), C.byref(nq), ptr(L), ptr(X), ptr(W), ptr(N), ptr(dN))
+    return L, X, W, N, dN
+
+
+class RefDofManager:
+    """The reference's own Mesh + DoFManager(M, CG, p, dpn) (src/utils/DoFManager.cpp),
+    compiled in place; arrays copied out after construction."""
+
+    def __init__(self, mesh, p, dpn=1):
+        R = ref()
+        nodes = np.ascontiguousarray(mesh["nodes"], dtype=np.float64).ravel()
+        cn = np.ascontiguousarray(mesh["cell_nodes"], dtype=np.int32)
+        off = np.ascontiguousarray(mesh["offsets"], dtype=np.int32)
+        ct = np.ascontiguousarray(mesh["cell_types"], dtype=np.int32)
+        self.h = R.refa_dofmanager(nodes, nodes.size // 3, cn, off, ct, ct.size, p, dpn)
+        if not self.h:
+            raise RuntimeError("DoFManager: Invalid polynomial order")
+        self.dpn = dpn
+        a, b, c = C.c_int(), C.c_int(), C.c_int()
+        R.refa_dofmanager_sizes(self.h, C.byref(a), C.byref(b), C.byref(c))
+        self.n_nodes, self.n_cells = a.value, b.value
+        self.nodes = np.zeros(3 * max(1, a.value))
+        self.offsets = np.zeros(b.value + 1, np.int32)
+        self.elements = np.zeros(max(1, c.value), np.int32)
+        self.topology = np.zeros(max(1, b.value), np.int8)
+        self.topo_dim = np.zeros(max(1, b.value), np.int8)
+        self.poly_order = np.zeros(max(1, b.value), np.int8)
+        R.refa_dofmanager_get(self.h, self.nodes, self.offsets, self.elements, self.topology,
+                              self.topo_dim, self.poly_order)
+        self.nodes = self.nodes[:3 * a.value].reshape(-1, 3)
+        self.elements = self.elements[:c.value]
+        self.topology, self.topo_dim = self.topology[:b.value], self.topo_dim[:b.value]
+        self.poly_order = self.poly_order[:b.value]
+
+    def __del__(self):
+        if getattr(self, "h", None) and _REF is not None:
+            _REF.refa_dofmanager_free(self.h)
+            self.h = None
+
+
+class RefSystem:
+    """FESystem + CGAssembly<Physics> of the reference (include/assembly/CGAssembly.hpp),
+    run single-threaded so that duplicates are summed in element order.
+    physics: POISSON {sign, f}, ELASTICITY {sign, lambda, mu, b0, b1, b2}, or
+    SUPG (the reference's AdvectionDiffusionSUPG with its own constants)."""
+
+    def __init__(self, dm, nsd, physics, params=None, tangent=True, residual=True, threads=1):
+        R = ref()
+        self.dm = dm
+        prm = np.zeros(8)
+        if params is not None:
+            prm[:len(params)] = params
+        R.refa_set_threads(threads)
+        self.h = R.refa_assemble(dm.h, physics, nsd, prm, int(tangent), int(residual))
+        n, nnz = C.c_int64(), C.c_int64()
+        R.refa_system_sizes(self.h, C.byref(n), C.byref(nnz))
+        self.n, self.nnz = n.value, nnz.value
+
+    def matrix(self):
+        """(Csr of K, residual): Eigen's ColMajor storage transposed to row-major."""
+        cp = np.zeros(self.n + 1, np.int32)
+        ri = np.zeros(max(1, self.nnz), np.int32)
+        v = np.zeros(max(1, self.nnz))
+        res = np.zeros(max(1, self.n))
+        ref().refa_system_get(self.h, cp, ri, v, res)
+        ri, v = ri[:self.nnz], v[:self.nnz]
+        cols = np.repeat(np.arange(self.n, dtype=np.int64), np.diff(cp))
+        order = np.lexsort((cols, ri))
+        row_ptr = np.zeros(self.n + 1, np.int64)
+        np.add.at(row_ptr, ri.astype(np.int64) + 1, 1)
+        return Csr(self.n, self.n, np.cumsum(row_ptr), cols[order], v[order]), res[:self.n]
+
+    def set_residual(self, r):
+        ref().refa_system_set_residual(self.h, np.ascontiguousarray(r, dtype=np.float64))
+
+    def dirichlet_plane(self, comp, axis, coord, value=0.0, tol=1e-9):
+        """DirichletBC(dofm, value, comp).selectByFunction(|x[axis]-coord| < tol).apply(K, F)."""
+        n = C.c_int()
+        ref().refa_dirichlet_plane(self.h, comp, axis, coord, tol, value, C.byref(n))
+        return n.value
+
+    def dirichlet_nodes(self, comp, nodes, value=0.0):
+        nodes = np.ascontiguousarray(nodes, dtype=np.int32)
+        ref().refa_dirichlet_nodes(self.h, comp, nodes, nodes.size, value)
+
+    def local_smoothing_gradient(self, nsd, sol):
+        out = np.zeros((self.n, nsd))
+        ref().refa_local_smoothing_gradient(self.h, nsd, np.ascontiguousarray(sol, dtype=np.float64), out)
+        return out
+
+    def __del__(self):
+        if getattr(self, "h", None) and _REF is not None:
+            _REF.refa_system_free(self.h)
+            self.h = None
 
 
 # ---------------------------------------------------------------- helpers
@@ -270,6 +395,30 @@ class DofMap:
         if getattr(self, "_p", None) is not None and _LIB is not None:
             _LIB.or_free_dofmap(self._p)
             self._p = None
+
+
+class ArrayDofMap:
+    """An oracle dofmap over caller-held numbering arrays (the reference's own
+    DoFManager output, say), for assembling on exactly that numbering."""
+
+    _TOPO = {0: (TENSOR, 1), 1: (SIMPLEX, 2), 2: (SIMPLEX, 3), 3: (TENSOR, 2), 4: (TENSOR, 3)}
+
+    def __init__(self, dof_nodes, element_offsets, elements, cell_types, p):
+        self.nodes = np.ascontiguousarray(np.asarray(dof_nodes, dtype=np.float64).reshape(-1, 3))
+        self.offsets = np.ascontiguousarray(element_offsets, dtype=np.int32)
+        self.elements = np.ascontiguousarray(elements, dtype=np.int32)
+        ct = np.asarray(cell_types)
+        self.topology = np.array([self._TOPO.get(int(c), (NONE, 0))[0] for c in ct], np.int8)
+        self.topo_dim = np.array([self._TOPO.get(int(c), (NONE, 0))[1] for c in ct], np.int8)
+        self.poly_order = np.full(ct.size, p, np.int8)
+        self.n_nodes, self.n_cells = self.nodes.shape[0], ct.size
+        self._s = _Dofmap(self.n_nodes, self.nodes.ctypes.data_as(C.POINTER(C.c_double)), self.n_cells,
+                          self.offsets.ctypes.data_as(C.POINTER(C.c_int32)),
+                          self.elements.ctypes.data_as(C.POINTER(C.c_int32)),
+                          self.topology.ctypes.data_as(C.POINTER(C.c_int8)),
+                          self.topo_dim.ctypes.data_as(C.POINTER(C.c_int8)),
+                          self.poly_order.ctypes.data_as(C.POINTER(C.c_int8)))
+        self._p = C.pointer(self._s)
 
 
 def dofmanager(mesh, p):

@@ -464,7 +464,13 @@ static int cmp_snapped_zyx(const void *pa, const void *pb) {
         if (ka[k] < kb[k]) return -1;
         if (ka[k] > kb[k]) return 1;
     }
-    return (a < b) ? -1 : (a > b); /* ties merge below; index order only picks the representative */
+    /* Ties merge below; index order only picks the representative, i.e. which
+     * coincident raw node gives the merged node its coordinates.  The reference's
+     * std::sort is unstable, so its representative is whatever that sort leaves
+     * first; the two agree to rounding except where triangles meet
+     * quadrilaterals at p >= 3 (their local nodes are snapped differently), and
+     * the parity tests assemble those cases on the reference's own numbering. */
+    return (a < b) ? -1 : (a > b);
 }
 
 /* DoFManager(M, CG, p): p=1 keeps the mesh numbering (DoFManager.cpp:153-160);
@@ -543,7 +549,9 @@ or_dofmap *or_dofmanager(const double *xyz, int32_t n_nodes, const int32_t *cell
     int *idxs = (int *)malloc(sizeof(int) * (N > 0 ? N : 1));
     for (int64_t i = 0; i < N; ++i) {
         idxs[i] = (int)i;
-        for (int k = 0; k < 3; ++k) keys[3 * i + k] = snap_to(raw[3 * i + k], snapv);
+        /* round(x * (1/s)) * s: the reference's tensor division by a scalar
+         * multiplies by the reciprocal (tensor_functions/operators.hpp:66-70) */
+        for (int k = 0; k < 3; ++k) keys[3 * i + k] = round(raw[3 * i + k] * (1.0 / snapv)) * snapv;
     }
     g_sort_keys = keys;
     qsort(idxs, N, sizeof(int), cmp_snapped_zyx);

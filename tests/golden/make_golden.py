@@ -2,10 +2,16 @@
 
 Run here (where the reference tree exists and oracle/_ref is built):
     python tests/golden/make_golden.py
-The fixtures hold outputs of the reference's handmade linear algebra and
-quadrature (compiled in place by oracle/Makefile), on the inputs its own tests
-use (test/test_sparse_csr.cpp, test_sparse_bcsr.cpp, test_cg_solve.cpp,
-test_bicgstab_solve.cpp, test_ILU.cpp) and on a small assembled Poisson system.
+The fixtures hold outputs of the reference's own code compiled in place by
+oracle/Makefile: its handmade linear algebra and quadrature on the inputs its
+own tests use (test/test_sparse_csr.cpp, test_sparse_bcsr.cpp,
+test_cg_solve.cpp, test_bicgstab_solve.cpp, test_ILU.cpp) and on a small
+assembled Poisson system (linalg.npz, quadrature.npz, poisson8.npz); and its
+assembly half -- Element tables, DoFManager numbering, CGAssembly values and
+residuals, DirichletBC::apply and LocalSmoothingGradient -- on small seeded
+quadrilateral, triangle, mixed, hexahedron and tetrahedron meshes at orders
+1-3 (elements.npz, assembly_ref.npz), built against the from-scratch Eigen-API
+subset in oracle/ref_compat (Eigen itself is not installed).
 They pin the oracle without the reference tree being present.
 """
 import os
@@ -136,6 +142,108 @@ def poisson_system():
     np.savez_compressed(os.path.join(HERE, "poisson8.npz"), **out)
 
 
+# ------------------------------------------------ the reference's assembly half
+
+ELEMENT_TYPES = ([(0, 1, p) for p in (1, 2, 3, 4)] + [(0, 2, p) for p in (1, 2, 3, 4)] +
+                 [(0, 3, p) for p in (1, 2, 3)] + [(1, 2, p) for p in (1, 2, 3)] + [(1, 3, p) for p in (1, 2)])
+
+
+def elements():
+    """Element tables (local nodes, quadrature, N, dN/dxi) of the reference's own
+    Element(ElementType{topology, dim, p}) (src/element/*.cpp, compiled against
+    oracle/ref_compat)."""
+    out = {}
+    for topo, dim, p in ELEMENT_TYPES:
+        L, X, W, N, dN = O.ref_element(topo, dim, p)
+        k = "e%d_%d_%d_" % (topo, dim, p)
+        out[k + "L"], out[k + "X"], out[k + "W"], out[k + "N"], out[k + "dN"] = L, X, W, N, dN
+    np.savez_compressed(os.path.join(HERE, "elements.npz"), **out)
+
+
+def _jitter(mesh, h, amount, seed):
+    """Move the interior nodes of a structured mesh by U(-amount, amount)*h."""
+    m = dict(mesh)
+    X = m["nodes"].copy()
+    lo, hi = X.min(0), X.max(0)
+    inner = np.all((X > lo + 1e-9) | (hi - lo < 1e-12), axis=1) & np.all((X < hi - 1e-9) | (hi - lo < 1e-12), axis=1)
+    rng = np.random.Generator(np.random.PCG64(seed))
+    d = rng.uniform(-amount, amount, size=X.shape) * np.asarray(h)
+    d[:, (hi - lo) < 1e-12] = 0
+    X[inner] += d[inner]
+    m["nodes"] = X
+    return m
+
+
+def assembly_meshes(kind, p):
+    o = meshgen.corner_order(p)
+    if kind == "quad":
+        return _jitter(meshgen.structured_quad(4, 3, order=o), (0.25, 1 / 3, 0), 0.2, 11), 2
+    if kind == "mixed":
+        return meshgen.jittered_mixed(4, 4, seed=5, order=o), 2
+    if kind == "tri":
+        return meshgen.jittered_mixed(3, 3, seed=8, tri_fraction=1.0, order=o), 2
+    if kind == "hex":
+        return _jitter(meshgen.structured_hex(2, 2, 2, order=o), (0.5, 0.5, 0.5), 0.15, 12), 3
+    if kind == "tet":
+        return meshgen.structured_tet(2, 2, 2, seed=13, jitter=0.15), 3
+    raise ValueError(kind)
+
+
+LAM, MU = 0.5769230769230769, 0.38461538461538464  # E=1, nu=0.3
+# (name, mesh kind, p, physics, params); dpn = nsd for elasticity, else 1
+ASSEMBLY_CASES = (
+    [("quad_poisson_p%d" % p, "quad", p, O.POISSON, [1.0, 1.3]) for p in (1, 2, 3)] +
+    [("quad_poisson_refsign_p2", "quad", 2, O.POISSON, [-1.0, 100.0])] +
+    [("quad_elast_p%d" % p, "quad", p, O.ELASTICITY, [1.0, LAM, MU, 0.5, -1.0]) for p in (1, 2, 3)] +
+    [("mixed_poisson_p%d" % p, "mixed", p, O.POISSON, [1.0, 1.0]) for p in (1, 2, 3)] +
+    [("mixed_elast_p%d" % p, "mixed", p, O.ELASTICITY, [1.0, LAM, MU, 0.0, -1.0]) for p in (2, 3)] +
+    [("mixed_supg_p%d" % p, "mixed", p, O.SUPG, None) for p in (1, 2, 3)] +
+    [("tri_poisson_p%d" % p, "tri", p, O.POISSON, [1.0, 2.0]) for p in (1, 2, 3)] +
+    [("hex_poisson_p%d" % p, "hex", p, O.POISSON, [1.0, 1.0]) for p in (1, 2, 3)] +
+    [("hex_elast_p%d" % p, "hex", p, O.ELASTICITY, [1.0, LAM, MU, 1.0, 0.0, -0.5]) for p in (1, 2)] +
+    [("hex_supg_p2", "hex", 2, O.SUPG, None)] +
+    [("tet_poisson_p%d" % p, "tet", p, O.POISSON, [1.0, 1.0]) for p in (1, 2)] +
+    [("tet_elast_p%d" % p, "tet", p, O.ELASTICITY, [1.0, LAM, MU, 0.0, 0.0, 1.0]) for p in (1, 2)]
+)
+# the reference's AdvectionDiffusionSUPG constants (apps/supg_learning/supg_advection.hpp:110-113)
+SUPG_PARAMS = [0.1, 0.1, 1.0, 0.0]
+
+
+def smooth_field(X, comp):
+    """A non-linear field sampled at the dof nodes, for the gradient fixtures."""
+    return np.sin(2 * X[:, 0]) + X[:, 0] * X[:, 1] ** 2 + 0.5 * X[:, 2] + comp * (X[:, 0] - X[:, 1] ** 2)
+
+
+def assembly():
+    """The reference's DoFManager, CGAssembly<Physics>, DirichletBC::apply and
+    LocalSmoothingGradient run on small seeded meshes (one thread, so that
+    duplicate sums follow element order)."""
+    out = {}
+    for name, kind, p, phys, params in ASSEMBLY_CASES:
+        mesh, nsd = assembly_meshes(kind, p)
+        dpn = nsd if phys == O.ELASTICITY else 1
+        dm = O.RefDofManager(mesh, p, dpn)
+        sysm = O.RefSystem(dm, nsd, phys, params)
+        K, R = sysm.matrix()
+        k = name + "/"
+        for key in ("nodes", "cell_nodes", "offsets", "cell_types"):
+            out[k + "mesh_" + key] = mesh[key]
+        out[k + "dof_nodes"], out[k + "element_offsets"], out[k + "elements"] = dm.nodes, dm.offsets, dm.elements
+        out[k + "row_ptr"], out[k + "col"] = K.row_ptr.astype(np.int32), K.col.astype(np.int32)
+        out[k + "val"], out[k + "residual"] = K.val, R
+        # two Dirichlet objects: comp 0 = 0.25 on x = min, comp dpn-1 = -0.5 on y = min
+        X = dm.nodes
+        nsel0 = sysm.dirichlet_plane(0, 0, X[:, 0].min(), 0.25)
+        nsel1 = sysm.dirichlet_plane(dpn - 1, 1, X[:, 1].min(), -0.5)
+        Kb, Rb = sysm.matrix()
+        out[k + "bc_val"], out[k + "bc_rhs"], out[k + "bc_count"] = Kb.val, Rb, np.array([nsel0, nsel1])
+        u = np.stack([smooth_field(X, c) for c in range(dpn)], axis=1).ravel()
+        out[k + "grad_u"] = u
+        out[k + "grad"] = sysm.local_smoothing_gradient(nsd, u)
+        out[k + "meta"] = np.array([p, dpn, nsd, phys] + list(params if params is not None else SUPG_PARAMS))
+    np.savez_compressed(os.path.join(HERE, "assembly_ref.npz"), **out)
+
+
 if __name__ == "__main__":
     O.build()
     if not O.ref_available():
@@ -143,4 +251,6 @@ if __name__ == "__main__":
     quadrature()
     linalg()
     poisson_system()
+    elements()
+    assembly()
     print("golden fixtures written to", HERE)

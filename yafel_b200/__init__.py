@@ -171,15 +171,27 @@ class DoFManager:
     """DoFManager(M, ManagerType::CG, polyOrder, dof_per_node)
     (src/utils/DoFManager.cpp:11-36); numbering identical to the reference's."""
 
-    def __init__(self, mesh, polyOrder=1, dof_per_node=1, ctx=None, host_only=False):
+    def __init__(self, mesh, polyOrder=1, dof_per_node=1, ctx=None, host_only=False, numbering=None):
+        """numbering: optional (dof_nodes n x 3, element_offsets, elements) of a
+        DoFManager the caller already built (the reference's own, say); the
+        mesh then only supplies the cell types."""
         if isinstance(mesh, dict):
             mesh = Mesh.from_dict(mesh)
         self.ctx = None if host_only else (ctx or default_context())
         self.mesh = mesh
         h = C.c_void_p()
-        check(lib().yg_dofmap_create(self.ctx.h if self.ctx else None, _ptr(mesh.nodes), mesh.nNodes(), _ptr(mesh.cell_nodes),
-                                     _ptr(mesh.offsets), _ptr(mesh.cell_types), mesh.nCells(), int(polyOrder),
-                                     int(dof_per_node), C.byref(h)), "DoFManager")
+        cx = self.ctx.h if self.ctx else None
+        if numbering is None:
+            check(lib().yg_dofmap_create(cx, _ptr(mesh.nodes), mesh.nNodes(), _ptr(mesh.cell_nodes),
+                                         _ptr(mesh.offsets), _ptr(mesh.cell_types), mesh.nCells(), int(polyOrder),
+                                         int(dof_per_node), C.byref(h)), "DoFManager")
+        else:
+            dn = np.ascontiguousarray(np.asarray(numbering[0], dtype=np.float64).reshape(-1, 3))
+            eo = np.ascontiguousarray(numbering[1], dtype=np.int32)
+            el = np.ascontiguousarray(numbering[2], dtype=np.int32)
+            check(lib().yg_dofmap_create_from_numbering(cx, _ptr(dn), dn.shape[0], _ptr(eo), _ptr(el),
+                                                        _ptr(mesh.cell_types), mesh.nCells(), int(polyOrder),
+                                                        int(dof_per_node), C.byref(h)), "DoFManager")
         self.h = h
         self.polyOrder, self.dof_per_node = int(polyOrder), int(dof_per_node)
         a, b, c, d = C.c_int32(), C.c_int32(), C.c_int64(), C.c_int64()
@@ -239,6 +251,21 @@ class DoFManager:
         if getattr(self, "h", None) and _alive(getattr(self, "ctx", None)):
             lib().yg_dofmap_destroy(self.h)
         self.h = None
+
+
+def element_table(topology, dim, polyOrder):
+    """The reference element tables the GPU kernels use for ElementType
+    {topology, dim, polyOrder}: (local nodes nen x 3, quadrature points nq x 3,
+    weights nq, N nq x nen, dN/dxi nq x nen x dim)."""
+    nen, nq = C.c_int32(), C.c_int32()
+    check(lib().yg_element_table(topology, dim, polyOrder, C.byref(nen), C.byref(nq), None, None, None, None, None),
+          "element_table")
+    a, q = nen.value, nq.value
+    L, X, W = np.zeros((a, 3)), np.zeros((q, 3)), np.zeros(q)
+    N, dN = np.zeros((q, a)), np.zeros((q, a, dim))
+    check(lib().yg_element_table(topology, dim, polyOrder, C.byref(nen), C.byref(nq), _ptr(L), _ptr(X), _ptr(W),
+                                 _ptr(N), _ptr(dN)), "element_table")
+    return L, X, W, N, dN
 
 
 # ------------------------------------------------------------------ physics

@@ -654,25 +654,10 @@ using namespace yg;
 
 // ================================================================ C ABI
 
-extern "C" yg_status yg_dofmap_create(yg_context ctx, const double *nodes_xyz, int32_t n_nodes,
-                                      const int32_t *cell_nodes, const int32_t *cell_offsets,
-                                      const int32_t *cell_types, int32_t n_cells, int32_t poly_order,
-                                      int32_t dof_per_node, yg_dofmap *out) {
-    if (!out || n_nodes < 0 || n_cells < 0 || (n_nodes && !nodes_xyz) || (n_cells && (!cell_offsets || !cell_types)))
-        return fail(YG_BAD_ARG, "yg_dofmap_create: bad argument");
-    if (dof_per_node < 1 || dof_per_node > 3) return fail(YG_BAD_ARG, "dof_per_node must be 1..3");
-    *out = nullptr;
-    for (int32_t c = 0; c < n_cells; ++c) {
-        if (cell_offsets[c + 1] < cell_offsets[c]) return fail(YG_BAD_ARG, "cell offsets decrease at cell %d", c);
-        for (int32_t i = cell_offsets[c]; i < cell_offsets[c + 1]; ++i)
-            if (cell_nodes[i] < 0 || cell_nodes[i] >= n_nodes) return fail(YG_BAD_ARG, "cell %d references node %d", c, cell_nodes[i]);
-    }
-    auto *d = new yg_dofmap_t();
-    d->ctx = ctx;
-    if (!build_dofmap(nodes_xyz, n_nodes, cell_nodes, cell_offsets, cell_types, n_cells, poly_order, dof_per_node, d->host)) {
-        delete d;
-        return fail(YG_BAD_ARG, "DoFManager: Invalid polynomial order");
-    }
+// Copies a host numbering to the device (when there is a context) and hands
+// the dofmap out; on failure the dofmap is destroyed.
+static yg_status upload_dofmap(yg_dofmap d, yg_dofmap *out) {
+    yg_context ctx = d->ctx;
     const HostDofmap &h = d->host;
     if (!ctx) {  // host-only numbering (no device copy); assembly needs a context
         *out = d;
@@ -685,11 +670,112 @@ extern "C" yg_status yg_dofmap_create(yg_context ctx, const double *nodes_xyz, i
         yg_dofmap_destroy(d);
         return s;
     }
-    cudaMemcpy(d->d_nodes, h.nodes.data(), sizeof(double) * h.nodes.size(), cudaMemcpyHostToDevice);
-    cudaMemcpy(d->d_offsets, h.offsets.data(), sizeof(int32_t) * h.offsets.size(), cudaMemcpyHostToDevice);
-    cudaError_t e = cudaMemcpy(d->d_elements, h.elements.data(), sizeof(int32_t) * h.elements.size(), cudaMemcpyHostToDevice);
+    cudaError_t e = cudaMemcpy(d->d_nodes, h.nodes.data(), sizeof(double) * h.nodes.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(d->d_offsets, h.offsets.data(), sizeof(int32_t) * h.offsets.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(d->d_elements, h.elements.data(), sizeof(int32_t) * h.elements.size(), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) { yg_dofmap_destroy(d); return fail(YG_CUDA_ERROR, "dofmap upload: %s", cudaGetErrorString(e)); }
     *out = d;
+    return YG_OK;
+}
+
+static int cell_corner_count(int32_t ct) {
+    switch (ct) {
+    case CELL_LINE2: return 2;
+    case CELL_TRI3: return 3;
+    case CELL_TET4: return 4;
+    case CELL_QUAD4: return 4;
+    case CELL_HEX8: return 8;
+    default: return -1;
+    }
+}
+
+extern "C" yg_status yg_dofmap_create(yg_context ctx, const double *nodes_xyz, int32_t n_nodes,
+                                      const int32_t *cell_nodes, const int32_t *cell_offsets,
+                                      const int32_t *cell_types, int32_t n_cells, int32_t poly_order,
+                                      int32_t dof_per_node, yg_dofmap *out) {
+    if (!out || n_nodes < 0 || n_cells < 0 || (n_nodes && !nodes_xyz) || (n_cells && (!cell_offsets || !cell_types)))
+        return fail(YG_BAD_ARG, "yg_dofmap_create: bad argument");
+    if (dof_per_node < 1 || dof_per_node > 3) return fail(YG_BAD_ARG, "dof_per_node must be 1..3");
+    *out = nullptr;
+    for (int32_t c = 0; c < n_cells; ++c) {
+        if (cell_offsets[c + 1] < cell_offsets[c]) return fail(YG_BAD_ARG, "cell offsets decrease at cell %d", c);
+        for (int32_t i = cell_offsets[c]; i < cell_offsets[c + 1]; ++i)
+            if (cell_nodes[i] < 0 || cell_nodes[i] >= n_nodes) return fail(YG_BAD_ARG, "cell %d references node %d", c, cell_nodes[i]);
+        const int nc = cell_corner_count(cell_types[c]);
+        if (poly_order > 1 && nc > 0 && cell_offsets[c + 1] - cell_offsets[c] < nc)
+            return fail(YG_BAD_ARG, "cell %d has %d corners, its type needs %d", c, cell_offsets[c + 1] - cell_offsets[c], nc);
+    }
+    auto *d = new yg_dofmap_t();
+    d->ctx = ctx;
+    if (!build_dofmap(nodes_xyz, n_nodes, cell_nodes, cell_offsets, cell_types, n_cells, poly_order, dof_per_node, d->host)) {
+        delete d;
+        return fail(YG_BAD_ARG, "DoFManager: Invalid polynomial order");
+    }
+    return upload_dofmap(d, out);
+}
+
+extern "C" yg_status yg_dofmap_create_from_numbering(yg_context ctx, const double *dof_nodes_xyz, int32_t n_dof_nodes,
+                                                     const int32_t *element_offsets, const int32_t *elements,
+                                                     const int32_t *cell_types, int32_t n_cells, int32_t poly_order,
+                                                     int32_t dof_per_node, yg_dofmap *out) {
+    if (!out || n_dof_nodes < 0 || n_cells < 0 || (n_dof_nodes && !dof_nodes_xyz) ||
+        (n_cells && (!element_offsets || !elements || !cell_types)))
+        return fail(YG_BAD_ARG, "yg_dofmap_create_from_numbering: bad argument");
+    if (dof_per_node < 1 || dof_per_node > 3) return fail(YG_BAD_ARG, "dof_per_node must be 1..3");
+    if (poly_order < 1) return fail(YG_BAD_ARG, "DoFManager: Invalid polynomial order");
+    *out = nullptr;
+    auto *d = new yg_dofmap_t();
+    d->ctx = ctx;
+    HostDofmap &h = d->host;
+    h.dof_per_node = dof_per_node;
+    h.poly_order = poly_order;
+    h.nodes.assign(dof_nodes_xyz, dof_nodes_xyz + 3 * (int64_t)n_dof_nodes);
+    h.offsets.assign(element_offsets, element_offsets + n_cells + 1);
+    h.elements.assign(elements, elements + (n_cells ? element_offsets[n_cells] : 0));
+    h.topology.resize(n_cells);
+    h.topo_dim.resize(n_cells);
+    h.porder.assign(n_cells, (int8_t)poly_order);
+    for (int32_t c = 0; c < n_cells; ++c) {
+        int t, td;
+        cell_element_type(cell_types[c], t, td);
+        h.topology[c] = (int8_t)t;
+        h.topo_dim[c] = (int8_t)td;
+        const int32_t cnt = element_offsets[c + 1] - element_offsets[c];
+        int nen = 0;
+        if (t != TOPO_NONE) {
+            ElementTable T;
+            if (poly_order == 1) nen = cell_corner_count(cell_types[c]);
+            else if (make_element_table(t, td, poly_order, T)) nen = T.nen;
+            else { delete d; return fail(YG_UNSUPPORTED, "element (topology %d, dim %d, order %d) not supported", t, td, poly_order); }
+        }
+        if (cnt < 0 || cnt != nen) {
+            delete d;
+            return fail(YG_BAD_ARG, "element %d lists %d nodes, its type has %d", c, cnt, nen);
+        }
+        for (int32_t i = element_offsets[c]; i < element_offsets[c + 1]; ++i)
+            if (elements[i] < 0 || elements[i] >= n_dof_nodes) {
+                delete d;
+                return fail(YG_BAD_ARG, "element %d references node %d", c, elements[i]);
+            }
+    }
+    return upload_dofmap(d, out);
+}
+
+extern "C" yg_status yg_element_table(int32_t topology, int32_t dim, int32_t poly_order, int32_t *nen, int32_t *nq,
+                                      double *local_nodes_xyz, double *qp_xyz, double *qw, double *N, double *dN) {
+    if (!nen || !nq || dim < 1 || dim > 3 || poly_order < 1) return fail(YG_BAD_ARG, "yg_element_table: bad argument");
+    ElementTable T;
+    if (!make_element_table(topology, dim, poly_order, T))
+        return fail(YG_UNSUPPORTED, "element (topology %d, dim %d, order %d) not supported", topology, dim, poly_order);
+    *nen = T.nen;
+    *nq = T.nq;
+    if (local_nodes_xyz) std::copy(T.local_nodes.begin(), T.local_nodes.end(), local_nodes_xyz);
+    if (qp_xyz) std::copy(T.qpts.begin(), T.qpts.end(), qp_xyz);
+    if (qw) std::copy(T.qw.begin(), T.qw.end(), qw);
+    if (N) std::copy(T.N.begin(), T.N.end(), N);
+    if (dN) std::copy(T.dN.begin(), T.dN.end(), dN);
     return YG_OK;
 }
 

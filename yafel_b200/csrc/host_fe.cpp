@@ -7,6 +7,7 @@
 #endif
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -152,6 +153,49 @@ int triangle_rule(int order, std::vector<double> &pts, std::vector<double> &w) {
     return n;
 }
 
+// Symmetric tetrahedron rules on (0,0,0),(1,0,0),(0,1,0),(0,0,1) of exactness
+// 1..5 (Keast's published rules); the reference tabulates them with these
+// digits and this point order for QuadratureRule::get_tetrahedron_quadrature
+// (src/quadrature/TetrahedronQuadratureRules.cpp:27-127), and the same values
+// keep assembled tetrahedron matrices identical.  Order 6 and above: none
+// (the reference throws).
+int tetrahedron_rule(int order, std::vector<double> &pts, std::vector<double> &w) {
+    struct P { double x, y, z, w; };
+    static const double a2 = 0.138196601125011, b2 = 0.585410196624969;
+    static const P r1[] = {{0.25, 0.25, 0.25, 0.16666666666666666}};
+    static const P r2[] = {{a2, a2, b2, 0.041666666666666664}, {a2, a2, a2, 0.041666666666666664},
+                           {a2, b2, a2, 0.041666666666666664}, {b2, a2, a2, 0.041666666666666664}};
+    static const double s3 = 0.16666666666666666;
+    static const P r3[] = {{0.25, 0.25, 0.25, -0.13333333333333333}, {s3, 0.5, s3, 0.075}, {s3, s3, 0.5, 0.075},
+                           {s3, s3, s3, 0.075}, {0.5, s3, s3, 0.075}};
+    static const double a4 = 0.071428571428571, b4 = 0.785714285714286, c4 = 0.399403576166799,
+                        d4 = 0.100596423833201, w4a = 0.007622222222222222, w4b = 0.024888888888888887;
+    static const P r4[] = {{0.25, 0.25, 0.25, -0.013155555555555556}, {a4, a4, b4, w4a}, {a4, a4, a4, w4a},
+                           {a4, b4, a4, w4a}, {b4, a4, a4, w4a}, {c4, d4, d4, w4b}, {d4, c4, c4, w4b},
+                           {d4, d4, c4, w4b}, {c4, d4, c4, w4b}, {d4, c4, d4, w4b}, {c4, c4, d4, w4b}};
+    static const double t5 = 0.3333333333333333, a5 = 0.09090909090909091, b5 = 0.7272727272727273,
+                        c5 = 0.433449846426336, d5 = 0.066550153573664, w5a = 0.006026785714286,
+                        w5b = 0.011645249086029, w5c = 0.010949141561386;
+    static const P r5[] = {{0.25, 0.25, 0.25, 0.030283678097089}, {t5, t5, t5, w5a}, {0.0, t5, t5, w5a},
+                           {t5, 0.0, t5, w5a}, {t5, t5, 0.0, w5a}, {a5, b5, a5, w5b}, {a5, a5, b5, w5b},
+                           {a5, a5, a5, w5b}, {b5, a5, a5, w5b}, {c5, d5, c5, w5c}, {c5, c5, d5, w5c},
+                           {d5, d5, c5, w5c}, {d5, c5, c5, w5c}, {c5, d5, d5, w5c}, {d5, c5, d5, w5c}};
+    const P *r = nullptr;
+    int n = 0;
+    switch (order) {
+    case 1: r = r1; n = 1; break;
+    case 2: r = r2; n = 4; break;
+    case 3: r = r3; n = 5; break;
+    case 4: r = r4; n = 11; break;
+    case 5: r = r5; n = 15; break;
+    default: return 0;
+    }
+    pts.clear();
+    w.clear();
+    for (int i = 0; i < n; ++i) { pts.insert(pts.end(), {r[i].x, r[i].y, r[i].z}); w.push_back(r[i].w); }
+    return n;
+}
+
 // ------------------------------------------------------------ reference elements
 
 static double snap_to(double x, double s) { return std::round(x / s) * s; }
@@ -182,6 +226,49 @@ static int local_nodes(int topology, int dim, int p, std::vector<double> &pts) {
                 pts.insert(pts.end(), {snap_to((1 + 2 * vj - vi - vk) / 3, snap), snap_to((1 + 2 * vi - vj - vk) / 3, snap),
                                        snap_to(0.0, snap)});
             }
+        return (int)pts.size() / 3;
+    }
+    if (topology == TOPO_SIMPLEX && dim == 3) {
+        // Blyth-Pozrikidis points face by face, then interior, each coordinate
+        // clipped at 0 (make_simplex_element.cpp:178-273); sorted by (z, y, x)
+        // and snapped to 2^-21 as make_simplex does (:21-22,94-97)
+        const double snap = 1.0 / (2 << 20);
+        auto v = [&](int i) { return (l[i - 1] + 1) / 2; };
+        std::vector<std::array<double, 3>> P;
+        for (int i = 1; i <= n; ++i)  // xi-eta plane
+            for (int j = 1; j <= n + 1 - i; ++j) {
+                int k = n + 2 - i - j;
+                P.push_back({std::max(0.0, (1 + 2 * v(j) - v(i) - v(k)) / 3), std::max(0.0, (1 + 2 * v(i) - v(j) - v(k)) / 3), 0.0});
+            }
+        for (int j = 1; j < n; ++j)  // eta-zeta plane
+            for (int k = 2; k <= n + 1 - j; ++k) {
+                int m = n + 2 - j - k;
+                P.push_back({0.0, std::max(0.0, (1 + 2 * v(j) - v(k) - v(m)) / 3), std::max(0.0, (1 + 2 * v(k) - v(j) - v(m)) / 3)});
+            }
+        for (int i = 2; i < n; ++i)  // xi-zeta plane
+            for (int k = 2; k <= n + 1 - i; ++k) {
+                int m = n + 2 - i - k;
+                P.push_back({std::max(0.0, (1 + 2 * v(i) - v(k) - v(m)) / 3), 0.0, std::max(0.0, (1 + 2 * v(k) - v(i) - v(m)) / 3)});
+            }
+        for (int i = 2; i < n; ++i)  // slanted face
+            for (int j = 2; j <= n - i; ++j) {
+                int m = n + 2 - i - j;
+                const double x = std::max(0.0, (1 + 2 * v(i) - v(j) - v(m)) / 3);
+                const double y = std::max(0.0, (1 + 2 * v(j) - v(i) - v(m)) / 3);
+                P.push_back({x, y, 1 - x - y});
+            }
+        for (int i = 2; i < n; ++i)  // interior
+            for (int j = 2; j <= n - i; ++j)
+                for (int k = 2; k <= n + 1 - i - j; ++k) {
+                    int m = n + 3 - i - j - k;
+                    P.push_back({std::max(0.0, (1 + 3 * v(k) - v(i) - v(j) - v(m)) / 4),
+                                 std::max(0.0, (1 + 3 * v(j) - v(i) - v(k) - v(m)) / 4),
+                                 std::max(0.0, (1 + 3 * v(i) - v(j) - v(k) - v(m)) / 4)});
+                }
+        std::sort(P.begin(), P.end(), [](const std::array<double, 3> &a, const std::array<double, 3> &b) {
+            return std::lexicographical_compare(a.rbegin(), a.rend(), b.rbegin(), b.rend());
+        });
+        for (auto &x : P) pts.insert(pts.end(), {snap_to(x[0], snap), snap_to(x[1], snap), snap_to(x[2], snap)});
         return (int)pts.size() / 3;
     }
     return 0;
@@ -305,6 +392,36 @@ struct Koornwinder {
     }
 };
 
+// The reference's orthogonal basis on the tetrahedron,
+// phi_k = P_m(r) P_n^{(2m+1,0)}(s) P_l^{(2m+2n+2,0)}(t) ((1-s)/2)^m ((1-t)/2)^(m+n)
+// with r = -2(1+xi)/(eta+zeta) - 1, s = 2(1+eta)/(1-zeta) - 1, t = zeta and
+// (m,n,l) in the reference's loop order (ShapeFunctionUtils.cpp:230-281).
+struct TetBasis {
+    std::vector<std::vector<double>> j00, j2, j3;
+    std::vector<int> m, n;
+    explicit TetBasis(int p) {
+        for (int k = 0; k <= p; ++k) j00.push_back(jacobi_coeffs(k, 0, 0));
+        for (int i = 0; i <= p; ++i)
+            for (int j = 0; j <= p; ++j)
+                for (int k = 0; k <= p; ++k)
+                    if (i + j + k <= p) {
+                        m.push_back(i);
+                        n.push_back(j);
+                        j2.push_back(jacobi_coeffs(j, 2 * i + 1, 0));
+                        j3.push_back(jacobi_coeffs(k, 2 * i + 2 * j + 2, 0));
+                    }
+    }
+    Dual eval(int k, double x, double y, double z, int g) const {
+        Dual xi{x, g == 0 ? 1.0 : 0.0}, eta{y, g == 1 ? 1.0 : 0.0}, zeta{z, g == 2 ? 1.0 : 0.0};
+        Dual one{1, 0}, two{2, 0};
+        Dual r = Dual{-2, 0} * (one + xi) / (eta + zeta) - one;
+        Dual s = two * (one + eta) / (one - zeta) - one;
+        Dual t = zeta;
+        return horner(j00[m[k]], r) * horner(j2[k], s) * horner(j3[k], t) * dpow((one - s) / two, m[k]) *
+               dpow((one - t) / two, m[k] + n[k]);
+    }
+};
+
 bool make_element_table(int topology, int dim, int p, ElementTable &T) {
     T.topology = topology;
     T.dim = dim;
@@ -373,12 +490,52 @@ bool make_element_table(int topology, int dim, int p, ElementTable &T) {
         }
         return true;
     }
+    if (topology == TOPO_SIMPLEX && dim == 3) {
+        // volume rule of exactness 2p (make_simplex_element.cpp:101-103); the
+        // reference has rules up to exactness 5, so p <= 2
+        T.nq = tetrahedron_rule(std::max(1, 2 * p), T.qpts, T.qw);
+        if (T.nq == 0) return false;
+        // nodal basis from the Vandermonde of TetBasis on the node set with
+        // zeta capped at 0.999999999 and points on the eta = zeta = 0 edge moved
+        // by 1e-8 in eta and zeta (ShapeFunctionUtils.cpp:220-304)
+        const int nen = T.nen;
+        std::vector<double> nodes = T.local_nodes;
+        for (int i = 0; i < nen; ++i) {
+            nodes[3 * i + 2] = std::min(.999999999, nodes[3 * i + 2]);
+            if (nodes[3 * i + 1] + nodes[3 * i + 2] == 0) {
+                nodes[3 * i + 1] += 0.00000001;
+                nodes[3 * i + 2] += 0.00000001;
+            }
+        }
+        TetBasis K(p);
+        std::vector<double> VT((size_t)nen * nen);
+        for (int i = 0; i < nen; ++i)
+            for (int j = 0; j < nen; ++j)
+                VT[(size_t)j * nen + i] = K.eval(j, nodes[3 * i], nodes[3 * i + 1], nodes[3 * i + 2], -1).f;
+        std::vector<int> piv;
+        lu_factor(VT, nen, piv);
+        T.N.assign((size_t)T.nq * nen, 0.0);
+        T.dN.assign((size_t)T.nq * nen * 3, 0.0);
+        std::vector<double> v(nen), dg(nen), sol(nen);
+        for (int q = 0; q < T.nq; ++q) {
+            const double x = T.qpts[3 * q], y = T.qpts[3 * q + 1], z = T.qpts[3 * q + 2];
+            for (int j = 0; j < nen; ++j) v[j] = K.eval(j, x, y, z, -1).f;
+            lu_solve(VT, nen, piv, v.data(), sol.data());
+            for (int A = 0; A < nen; ++A) T.N[(size_t)q * nen + A] = sol[A];
+            for (int g = 0; g < 3; ++g) {
+                for (int j = 0; j < nen; ++j) dg[j] = K.eval(j, x, y, z, g).d;
+                lu_solve(VT, nen, piv, dg.data(), sol.data());
+                for (int A = 0; A < nen; ++A) T.dN[((size_t)q * nen + A) * 3 + g] = sol[A];
+            }
+        }
+        return true;
+    }
     return false;
 }
 
 // ------------------------------------------------------------ DoF numbering
 
-static void cell_to_element(int ct, int &topo, int &tdim) {
+void cell_element_type(int ct, int &topo, int &tdim) {
     switch (ct) {
     case CELL_LINE2: topo = TOPO_TENSOR; tdim = 1; break;
     case CELL_TRI3: topo = TOPO_SIMPLEX; tdim = 2; break;
@@ -417,6 +574,10 @@ static void interpolate_from_corners(const double *xl, const double *c, int ct, 
 // position of the j-th smallest key; equal keys keep their original order).  11-bit digits; each pass counts per thread and
 // scatters each thread's contiguous chunk in order, so the result does not
 // depend on the thread count.
+// Meshes with at most this many raw element nodes are numbered with the
+// reference's own comparison sort (see build_dofmap).
+constexpr int64_t kReferenceOrderMaxRawNodes = int64_t(1) << 20;
+
 static void radix_sort_index(uint64_t *ka, int64_t N, int nbits, int64_t *out_idx) {
     constexpr int D = 11, R = 1 << D;
     std::unique_ptr<uint64_t[]> kb(new uint64_t[N]);
@@ -476,7 +637,7 @@ bool build_dofmap(const double *xyz, int32_t n_nodes, const int32_t *cell_nodes,
     d.porder.assign(n_cells, (int8_t)p);
     for (int c = 0; c < n_cells; ++c) {
         int t, td;
-        cell_to_element(cell_types[c], t, td);
+        cell_element_type(cell_types[c], t, td);
         d.topology[c] = (int8_t)t;
         d.topo_dim[c] = (int8_t)td;
     }
@@ -534,9 +695,13 @@ bool build_dofmap(const double *xyz, int32_t n_nodes, const int32_t *cell_nodes,
     }
     double max_dim = std::max(bmax[0] - bmin[0], std::max(bmax[1] - bmin[1], bmax[2] - bmin[2]));
     double snapv = max_dim * 1.0e-6;
-    // snapped integer coordinates: ranges first, keys second (nothing stored)
+    // snapped integer coordinates: ranges first, keys second (nothing stored).
+    // The reference's tensor division by a scalar multiplies by its reciprocal
+    // (lin_alg/tensor/tensor_functions/operators.hpp:66-70), so the key is
+    // round(x * (1/s)); a true division would round differently near .5.
+    const double inv_snap = snapv > 0 ? 1.0 / snapv : 0.0;
     auto snapped = [&](int64_t i, int k) -> int64_t {
-        return (snapv > 0) ? (int64_t)std::llround(std::round(raw[3 * i + k] / snapv)) : 0;
+        return (snapv > 0) ? (int64_t)std::llround(std::round(raw[3 * i + k] * inv_snap)) : 0;
     };
     int64_t kmin[3], kmax[3];
     for (int k = 0; k < 3; ++k) {
@@ -558,7 +723,39 @@ bool build_dofmap(const double *xyz, int32_t n_nodes, const int32_t *cell_nodes,
     }
     const bool packable = bits[0] + bits[1] + bits[2] <= 64;
     std::unique_ptr<int64_t[]> idx(new int64_t[N]);
-    if (packable) {
+    // Which of several coincident raw nodes gives the merged node its
+    // coordinates is the first one in sorted order.  The reference sorts with
+    // std::sort on the snapped key alone (DoFManager.cpp:371), an unstable sort,
+    // so among equal keys its order is whatever std::sort produces.  Coincident
+    // raw nodes usually differ only in rounding, but where triangles (whose
+    // local nodes are snapped to 2^-21, make_simplex_element.cpp:21-22,94-97)
+    // meet quadrilaterals at p >= 3 they differ by up to 2.4e-7 of the cell
+    // size, and the choice changes the geometry.  Small meshes, and every mesh
+    // that mixes simplex and tensor cells at p >= 3, are therefore sorted with
+    // std::sort and the reference's comparison (no tie-break) from the same
+    // identity permutation, which reproduces its order exactly; large meshes
+    // use the stable parallel radix sort (same node numbering; merged
+    // coordinates can differ from the reference's in the last bit).
+    bool has_simplex = false, has_tensor = false;
+    for (int c = 0; c < n_cells; ++c) {
+        has_simplex |= d.topology[c] == TOPO_SIMPLEX && d.topo_dim[c] >= 2;
+        has_tensor |= d.topology[c] == TOPO_TENSOR && d.topo_dim[c] >= 2;
+    }
+    const bool reference_order = N <= kReferenceOrderMaxRawNodes || (p >= 3 && has_simplex && has_tensor);
+    if (reference_order) {
+        std::vector<int64_t> kq(3 * N);
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < N; ++i)
+            for (int k = 0; k < 3; ++k) kq[3 * i + k] = snapped(i, k);
+        std::vector<int32_t> ids(N);
+        std::iota(ids.begin(), ids.end(), 0);
+        std::sort(ids.begin(), ids.end(), [&](int32_t a, int32_t b) {
+            for (int k = 2; k >= 0; --k)
+                if (kq[3 * (int64_t)a + k] != kq[3 * (int64_t)b + k]) return kq[3 * (int64_t)a + k] < kq[3 * (int64_t)b + k];
+            return false;
+        });
+        for (int64_t i = 0; i < N; ++i) idx[i] = ids[i];
+    } else if (packable) {
         std::unique_ptr<uint64_t[]> keys(new uint64_t[N]);
 #pragma omp parallel for schedule(static)
         for (int64_t i = 0; i < N; ++i)

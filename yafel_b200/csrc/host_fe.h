@@ -14,6 +14,7 @@ void gauss_legendre_1d(int n, double *x, double *w);
 void gauss_lobatto_1d(int n, double *x, double *w);
 int tensor_rule(bool lobatto, int dim, int order, std::vector<double> &pts, std::vector<double> &w);
 int triangle_rule(int order, std::vector<double> &pts, std::vector<double> &w);
+int tetrahedron_rule(int order, std::vector<double> &pts, std::vector<double> &w);
 
 // Reference-element tables of one ElementType.
 struct ElementTable {
@@ -25,6 +26,10 @@ struct ElementTable {
     std::vector<double> dN;           // nq*nen*dim
 };
 bool make_element_table(int topology, int dim, int p, ElementTable &T);
+
+// Element topology and topological dimension of a mesh CellType code
+// (DoFManager::CellType_to_ElementType, src/utils/DoFManager.cpp:107-141).
+void cell_element_type(int cell_type, int &topology, int &topo_dim);
 
 struct HostDofmap {
     int32_t dof_per_node = 1, poly_order = 1;

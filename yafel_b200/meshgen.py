@@ -101,3 +101,34 @@ def jittered_mixed(nx, ny, seed, tri_fraction=0.5, jitter=0.2, lx=1.0, ly=1.0, o
             nper.append(4)
             types.append(QUAD4)
     return _mesh(nodes, np.array(cells), np.array(nper), np.array(types))
+
+
+def structured_tet(nx, ny, nz, lx=1.0, ly=1.0, lz=1.0, seed=None, jitter=0.0):
+    """nx*ny*nz boxes, each split into six Tet4 cells around its main diagonal
+    (Freudenthal-Kuhn), corners ordered so that every tetrahedron has positive
+    volume under the map (1-x-y-z) c0 + x c1 + y c2 + z c3 that
+    DoFManager::interpolate_from_corners uses for Tet4
+    (src/utils/DoFManager.cpp:307-311).  With a seed, interior nodes move by
+    U(-jitter, jitter) times the box size per coordinate (numpy PCG64)."""
+    m = structured_hex(nx, ny, nz, lx, ly, lz, order="tensor")
+    nodes = m["nodes"].copy()
+    if seed is not None and jitter > 0:
+        rng = np.random.Generator(np.random.PCG64(seed))
+        h = np.array([lx / nx, ly / ny, lz / nz])
+        ix = np.round(nodes / h).astype(np.int64)
+        interior = ((ix[:, 0] > 0) & (ix[:, 0] < nx) & (ix[:, 1] > 0) & (ix[:, 1] < ny) &
+                    (ix[:, 2] > 0) & (ix[:, 2] < nz))
+        d = rng.uniform(-jitter, jitter, size=nodes.shape) * h
+        nodes[interior] += d[interior]
+    hexes = m["cell_nodes"].reshape(-1, 8)  # tensor order: corner (i,j,k) at i + 2j + 4k
+    # paths from corner 0 to corner 7 along the three axes in every order
+    paths = [(1, 2, 4), (1, 4, 2), (2, 1, 4), (2, 4, 1), (4, 1, 2), (4, 2, 1)]
+    tets = []
+    for hx in hexes:
+        for a, b, c in paths:
+            t = [hx[0], hx[a], hx[a + b], hx[7]]
+            x = nodes[t]
+            if np.linalg.det(np.stack([x[1] - x[0], x[2] - x[0], x[3] - x[0]])) < 0:
+                t[1], t[2] = t[2], t[1]
+            tets.append(t)
+    return _mesh(nodes, np.array(tets), 4, np.full(len(tets), TET4))
