@@ -157,7 +157,9 @@ enum { YG_FORMAT_CSR = 0, YG_FORMAT_BCSR = 1 };
  * replaced, like setFromTriplets (CGAssembly.hpp:185).  Residual: added into
  * `residual` (length n_dofs), like GlobalResidual += private_residual
  * (CGAssembly.hpp:181).  Duplicate summation is deterministic (element-coloured
- * scatter, colours in ascending order). */
+ * scatter, colours in ascending order).  An element's shape gradients at all its
+ * quadrature points are staged in shared memory, which limits hexahedra to
+ * p <= 3 (p = 4 needs 375 KB); larger elements return YG_UNSUPPORTED. */
 YG_API yg_status yg_assemble(yg_dofmap d, const yg_physics *physics, uint32_t requirements,
                       int32_t format, yg_matrix *K, yg_vector residual);
 
@@ -166,7 +168,8 @@ YG_API yg_status yg_assemble(yg_dofmap d, const yg_physics *physics, uint32_t re
  * nsd, written to `gradient` (n_dofs * nsd entries, row-major: dof-major, then
  * the nsd derivatives): the element gradient at each quadrature point, weighted
  * by N_A jxw, summed per dof and divided by the sum of N_A jxw (a dof no such
- * cell touches gets 0/0).  Deterministic (element-coloured sums). */
+ * cell touches gets 0/0).  Deterministic (element-coloured sums).  Same element
+ * limit as yg_assemble (hexahedra p <= 3, else YG_UNSUPPORTED). */
 YG_API yg_status yg_local_smoothing_gradient(yg_dofmap d, int32_t nsd, yg_vector solution, yg_vector gradient);
 
 /* DirichletBC::apply(A, rhs) for one BC object (src/boundary_conditions/DirichletBC.cpp:27-89):

@@ -23,6 +23,7 @@ f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
 
 TENSOR, SIMPLEX, NONE = 0, 1, 2
 POISSON, ELASTICITY, SUPG = 0, 1, 2
+SUPG_PARAM = 3  # reference assembly only: SUPG formulas with run-time k, h, U0, Q
 PRECOND_NONE, PRECOND_JACOBI, PRECOND_ILU0 = 0, 1, 2
 CRIT_REFERENCE, CRIT_RELRES = 0, 1
 
@@ -144,6 +145,8 @@ def ref():
         R.ref_csr_info.argtypes = [C.c_void_p] + [C.POINTER(C.c_int64)] * 3
         R.ref_csr_get.argtypes = [C.c_void_p, i64p, i64p, f64p]
         R.ref_csr_free.argtypes = [C.c_void_p]
+        R.ref_csr_from_csc.argtypes = [C.c_int64, i32p, i32p, f64p]
+        R.ref_csr_from_csc.restype = C.c_void_p
         R.ref_csr_spmv.argtypes = [C.c_void_p, f64p, f64p]
         R.ref_bcsr_from_triplets.argtypes = [C.c_int, i64p, i64p, f64p, C.c_int64]
         R.ref_bcsr_from_triplets.restype = C.c_void_p
@@ -236,8 +239,9 @@ class RefDofManager:
 class RefSystem:
     """FESystem + CGAssembly<Physics> of the reference (include/assembly/CGAssembly.hpp),
     run single-threaded so that duplicates are summed in element order.
-    physics: POISSON {sign, f}, ELASTICITY {sign, lambda, mu, b0, b1, b2}, or
-    SUPG (the reference's AdvectionDiffusionSUPG with its own constants)."""
+    physics: POISSON {sign, f}, ELASTICITY {sign, lambda, mu, b0, b1, b2},
+    SUPG (the reference's AdvectionDiffusionSUPG with its own constants), or
+    SUPG_PARAM {k, h, U0, Q} (the same formulas with run-time constants)."""
 
     def __init__(self, dm, nsd, physics, params=None, tangent=True, residual=True, threads=1):
         R = ref()
@@ -264,6 +268,22 @@ class RefSystem:
         row_ptr = np.zeros(self.n + 1, np.int64)
         np.add.at(row_ptr, ri.astype(np.int64) + 1, 1)
         return Csr(self.n, self.n, np.cumsum(row_ptr), cols[order], v[order]), res[:self.n]
+
+    def csc(self):
+        """Eigen's ColMajor arrays of the tangent (column pointers, row indices,
+        values) and the residual, copied out."""
+        cp = np.zeros(self.n + 1, np.int32)
+        ri = np.zeros(max(1, self.nnz), np.int32)
+        v = np.zeros(max(1, self.nnz))
+        res = np.zeros(max(1, self.n))
+        ref().refa_system_get(self.h, cp, ri, v, res)
+        return cp, ri, v, res[:self.n]
+
+    def to_ref_csr(self):
+        """The tangent as the reference's handmade sparse_csr (its triplet
+        constructor over Eigen's entries) and the residual."""
+        cp, ri, v, res = self.csc()
+        return RefCsr.from_handle(ref().ref_csr_from_csc(self.n, cp, ri, v)), res
 
     def set_residual(self, r):
         ref().refa_system_set_residual(self.h, np.ascontiguousarray(r, dtype=np.float64))
@@ -539,6 +559,15 @@ class RefCsr:
         R.ref_csr_info(self.h, C.byref(a), C.byref(b), C.byref(n))
         self.nrows, self.ncols, self.nnz = a.value, b.value, n.value
 
+    @classmethod
+    def from_handle(cls, h):
+        self = cls.__new__(cls)
+        self.h = h
+        a, b, n = C.c_int64(), C.c_int64(), C.c_int64()
+        ref().ref_csr_info(self.h, C.byref(a), C.byref(b), C.byref(n))
+        self.nrows, self.ncols, self.nnz = a.value, b.value, n.value
+        return self
+
     def arrays(self):
         rp = np.zeros(self.nrows + 1, np.int64)
         col = np.zeros(max(self.nnz, 1), np.int64)
@@ -555,6 +584,11 @@ class RefCsr:
         x = np.ascontiguousarray(x0, dtype=np.float64).copy()
         ref().ref_cg(self.h, np.ascontiguousarray(b, dtype=np.float64), x, tol)
         return x
+
+    def true_relres(self, b, x):
+        """||b - A x|| / ||b|| with A x from the reference's csr_spmv."""
+        r = np.asarray(b, dtype=np.float64) - self.spmv(x)
+        return float(np.linalg.norm(r) / np.linalg.norm(b))
 
     def pcg_jacobi(self, b, x0, tol):
         x = np.ascontiguousarray(x0, dtype=np.float64).copy()

@@ -100,6 +100,52 @@ struct ElasticityPhysics {
     }
 };
 
+// Steady SUPG advection-diffusion with run-time constants: the tangent and
+// residual of apps/supg_learning/supg_advection.hpp:24-131 (advection summed
+// inside the Acomp loop, as there), with k, h, U0 and Q as parameters instead
+// of that header's compile-time constants, for problems of any Peclet number.
+double g_k = 0.1, g_h = 0.1, g_U0 = 1.0, g_Q = 0.0;
+
+template <int NSD>
+struct SupgPhysics {
+    static constexpr int nsd() { return NSD; }
+    static double alpha() {
+        const double Pe = g_U0 * g_h / (2 * g_k);
+        return Pe == 0 ? 0.0 : std::cosh(Pe) / std::sinh(Pe) - 1.0 / Pe;
+    }
+    static void LocalResidual(const Element &E, int qpi, coordinate<> &, double,
+                              Eigen::Map<Eigen::Matrix<double, Eigen::Dynamic, 1>> &,
+                              Eigen::Map<Eigen::Matrix<double, Eigen::Dynamic, 1>> &R_el) {
+        const double a = alpha(), normU = std::abs(g_U0);
+        double Uhat[NSD] = {0};
+        if (normU > 0) Uhat[0] = (a * g_h / 2) * g_U0 * (1.0 / normU);
+        for (int A = 0; A < E.localMesh.nNodes(); ++A)
+            for (int i = 0; i < NSD; ++i)
+                R_el(A) -= (E.shapeValues[qpi](A) * g_Q + Uhat[i] * E.shapeGrad(A, i)) * E.jxw;
+    }
+    static void LocalTangent(const Element &E, int qpi, coordinate<> &, double,
+                             Eigen::Map<Eigen::Matrix<double, Eigen::Dynamic, 1>> &,
+                             Eigen::Map<Eigen::Matrix<double, Eigen::Dynamic, Eigen::Dynamic, Eigen::RowMajor>> &K_el) {
+        const double a = alpha(), normU = std::abs(g_U0);
+        double U[NSD] = {0}, K[NSD][NSD];
+        U[0] = g_U0;
+        for (int i = 0; i < NSD; ++i)
+            for (int j = 0; j < NSD; ++j) K[i][j] = (i == j ? 1.0 : 0.0) * g_k;
+        if (normU > 0) {
+            const double c = a * g_h / (normU * 2);
+            for (int i = 0; i < NSD; ++i)
+                for (int j = 0; j < NSD; ++j) K[i][j] += c * (U[i] * U[j]);
+        }
+        const int n = E.localMesh.nNodes();
+        for (int A = 0; A < n; ++A)
+            for (int ac = 0; ac < NSD; ++ac)
+                for (int B = 0; B < n; ++B)
+                    for (int bc = 0; bc < NSD; ++bc)
+                        K_el(A, B) += (E.shapeValues[qpi](A) * U[bc] * E.shapeGrad(B, bc) +
+                                       E.shapeGrad(A, ac) * E.shapeGrad(B, bc) * K[ac][bc]) * E.jxw;
+    }
+};
+
 struct RefMesh {
     Mesh mesh;
     DoFManager dofm;
@@ -200,7 +246,8 @@ void refa_element(int topology, int dim, int p, int qrm, int *nen, int *nq, doub
 
 // FESystem(dofm, nsd) + CGAssembly<Physics>(sys, {Residual?, Tangent?}).
 // kind 0: Poisson {sign, f}; 1: elasticity {sign, lambda, mu, b0, b1, b2};
-// 2: the reference's steady AdvectionDiffusionSUPG (its own constants).
+// 2: the reference's steady AdvectionDiffusionSUPG (its own constants);
+// 3: the same SUPG formulas with params {k, h, U0, Q}.
 void *refa_assemble(void *mesh, int kind, int nsd, const double *params, int want_tangent, int want_residual) {
     auto *m = static_cast<RefMesh *>(mesh);
     auto *s = new RefSystem(m, nsd);
@@ -217,6 +264,12 @@ void *refa_assemble(void *mesh, int kind, int nsd, const double *params, int wan
         g_mu = params[2];
         for (int k = 0; k < 3; ++k) g_body[k] = params[3 + k];
         assemble_nsd<ElasticityPhysics>(s->sys, nsd, req);
+    } else if (kind == 3) {
+        g_k = params[0];
+        g_h = params[1];
+        g_U0 = params[2];
+        g_Q = params[3];
+        assemble_nsd<SupgPhysics>(s->sys, nsd, req);
     } else {
         assemble_nsd<SupgSteady>(s->sys, nsd, req);
     }

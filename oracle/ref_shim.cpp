@@ -81,6 +81,16 @@ extern "C" void ref_csr_get(void *h, int64_t *row_ptr, int64_t *col, double *val
     for (std::size_t i = 0; i < A->row_ptr.size(); ++i) row_ptr[i] = (int64_t)A->row_ptr[i];
     for (std::size_t i = 0; i < A->col_index.size(); ++i) { col[i] = (int64_t)A->col_index[i]; val[i] = A->_data[i]; }
 }
+// The bridge from the current stack to the handmade one (the reference has
+// none): Eigen's ColMajor compressed tangent (column pointers, row indices,
+// values) as a triplet list, then the reference's own sparse_csr(triplets).
+extern "C" void *ref_csr_from_csc(int64_t n, const int *col_ptr, const int *row_idx, const double *val) {
+    std::vector<Trip> t;
+    t.reserve((std::size_t)col_ptr[n]);
+    for (int64_t c = 0; c < n; ++c)
+        for (int k = col_ptr[c]; k < col_ptr[c + 1]; ++k) t.emplace_back((std::size_t)row_idx[k], (std::size_t)c, val[k]);
+    return new sparse_csr<double>(t);
+}
 extern "C" void ref_csr_free(void *h) { delete static_cast<sparse_csr<double> *>(h); }
 extern "C" void ref_csr_spmv(void *h, const double *x, double *y) {
     auto *A = static_cast<sparse_csr<double> *>(h);

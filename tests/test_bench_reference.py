@@ -1,6 +1,8 @@
 """The reference arm of bench.py (`--impl reference`) on the host: one JSON line
-with the contract's keys, the reference's CPU path reaching the oracle's
-residual on a small sample of the workload (no GPU needed)."""
+with the contract's keys and the GPU arm's config, the reference's own CPU path
+(its DoFManager, CGAssembly, DirichletBC, sparse_csr and pcg_solve) reaching a
+1e-10 relative residual on a small sample of the workload, with no part of the
+yafel_b200 library loaded (no GPU needed)."""
 import json
 import os
 import subprocess
@@ -23,4 +25,21 @@ def test_reference_arm_prints_one_contract_line():
     assert d["impl"] == "reference" and d["value"] > 0 and d["unit"] == "dofs/s"
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["value"] == d["value"]
     assert d["cpu_baseline"]["kind"] in ("reference", "port")
-    assert d["config"]["max_relres"] <= 1e-10
+    assert d["config"] == bench_config()
+    assert 1e-12 <= d["sample"]["relres_min"] and d["sample"]["relres_max"] <= 1e-10
+    assert d["sample"]["mesh"] == "3^3 Q2 hex" and d["sample"]["dofs"] == 3 * 7 ** 3
+
+
+def bench_config():
+    sys.path.insert(0, ROOT)
+    import bench
+    return bench.base_config(60, 1)
+
+
+def test_reference_arm_loads_no_library_of_the_product():
+    code = ("import sys, bench; bench.cpu_sample(2, 2, 1e-20); "
+            "m = open('/proc/self/maps').read(); "
+            "sys.exit(3 if 'libyafel_b200' in m else (0 if 'libyafel_ref' in m else 4))")
+    out = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True, timeout=300,
+                         env=dict(os.environ, OMP_NUM_THREADS="2"))
+    assert out.returncode == 0, (out.returncode, out.stderr[-2000:])

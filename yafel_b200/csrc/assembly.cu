@@ -447,6 +447,9 @@ static yg_status launch_assemble(yg_context ctx, const ElementGroup &g, yg_dofma
     const int nen = g.tab.nen, nq = g.tab.nq;
     size_t smem = assemble_smem(nen, nq, NSD);
     auto kern = k_assemble<NSD, DPN, PHYS>;
+    if (smem > ctx->smem_optin)
+        return fail(YG_UNSUPPORTED, "CGAssembly: element (nen %d, nq %d) needs %zu B of shared memory, the device "
+                    "allows %zu", nen, nq, smem, ctx->smem_optin);
     if (smem > 48 * 1024) YG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     for (size_t c = 0; c + 1 < g.color_ptr.size(); ++c) {
         int n = g.color_ptr[c + 1] - g.color_ptr[c];
@@ -1071,6 +1074,11 @@ static yg_status launch_smooth_gradient(yg_context ctx, const ElementGroup &g, y
     const size_t smem = sizeof(double) * (3 * nen + (size_t)nq * nen * NSD + nq + 9 * nq + nen * DPN +
                                           (size_t)nq * DPN * NSD) + sizeof(int32_t) * nen + 16;
     auto kern = k_smooth_gradient<NSD, DPN>;
+    // the element's shape gradients at every quadrature point sit in shared
+    // memory: hexahedra of order 4 and above need more than a block can hold
+    if (smem > ctx->smem_optin)
+        return fail(YG_UNSUPPORTED, "LocalSmoothingGradient: element (nen %d, nq %d) needs %zu B of shared memory, "
+                    "the device allows %zu", nen, nq, smem, ctx->smem_optin);
     if (smem > 48 * 1024) YG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     for (size_t c = 0; c + 1 < g.color_ptr.size(); ++c) {
         const int n = g.color_ptr[c + 1] - g.color_ptr[c];
@@ -1108,10 +1116,12 @@ extern "C" yg_status yg_local_smoothing_gradient(yg_dofmap d, int32_t nsd, yg_ve
     YG_TRY(build_pattern(d, nsd));  // element groups and colourings of the cells of dimension nsd
     double *vol = nullptr;
     YG_TRY(dev_alloc_t(ctx, &vol, ndofs));
-    YG_CUDA(cudaMemsetAsync(vol, 0, sizeof(double) * ndofs, ctx->stream));
-    YG_CUDA(cudaMemsetAsync(gradient->d, 0, sizeof(double) * ndofs * nsd, ctx->stream));
     yg_status s = YG_OK;
+    cudaError_t e = cudaMemsetAsync(vol, 0, sizeof(double) * ndofs, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(gradient->d, 0, sizeof(double) * ndofs * nsd, ctx->stream);
+    if (e != cudaSuccess) s = fail(YG_CUDA_ERROR, "LocalSmoothingGradient: %s", cudaGetErrorString(e));
     for (const ElementGroup &g : d->groups) {
+        if (s != YG_OK) break;
         switch (nsd) {
         case 1: s = smooth_gradient_dpn<1>(ctx, g, d, dpn, solution->d, vol, gradient->d); break;
         case 2: s = smooth_gradient_dpn<2>(ctx, g, d, dpn, solution->d, vol, gradient->d); break;

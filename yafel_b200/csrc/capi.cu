@@ -257,6 +257,7 @@ extern "C" yg_status yg_context_create(int32_t device, uint64_t hbm_budget_bytes
     cudaDeviceProp prop;
     YG_CUDA(cudaGetDeviceProperties(&prop, device));
     ctx->num_sms = prop.multiProcessorCount;
+    ctx->smem_optin = prop.sharedMemPerBlockOptin;
     ctx->reduce_blocks = ctx->num_sms * 4;
     YG_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
     yg_status s;
