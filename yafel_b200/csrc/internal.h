@@ -62,6 +62,7 @@ struct KrylovScalars {
 struct yg_context_t {
     int device = 0;
     int num_sms = 148;
+    size_t smem_optin = 227 * 1024;  // largest dynamic shared memory a block may opt in to
     cudaStream_t stream = nullptr;
     uint64_t budget = 0;
     uint64_t in_use = 0;
@@ -147,10 +148,17 @@ yg_status dev_alloc_t(yg_context ctx, T **p, size_t count) {
 }
 
 // ---- kernels-side entry points (implemented in .cu files) ----
+// x32 (optional, FP32-value precisions only): the same vector rounded to FP32 in
+// the node-padded layout of spmv_x32_stride(); the TMA kernels then gather it
+// with one vector load per block instead of B scalar FP64 loads.
 yg_status spmv_launch(yg_matrix A, const double *x, double *y, int precision, double *partials_dot,
-                      const int32_t *flag, int grid);
+                      const int32_t *flag, int grid, const float *x32 = nullptr);
 yg_status spmv_launch_ex(yg_matrix A, const double *x, double *y, int precision, const double *w, double *partials,
-                         int dot_mode, const int32_t *flag, int grid, cudaStream_t stream = nullptr);
+                         int dot_mode, const int32_t *flag, int grid, cudaStream_t stream = nullptr,
+                         const float *x32 = nullptr);
+// Floats per block row of an FP32 gather copy: 4 for 3x3 blocks (16-byte rows),
+// else the block size.
+inline int spmv_x32_stride(int block) { return block == 3 ? 4 : block; }
 int spmv_default_grid(yg_matrix A);
 int spmv_grid_for(yg_matrix A, int precision);
 void spmv_autotune(yg_matrix A);

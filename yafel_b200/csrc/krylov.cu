@@ -156,11 +156,23 @@ k_cg_update(int64_t n, const double *__restrict__ pq_partials, int np, KrylovSca
 }
 
 // Kernel 3: beta, p = z + beta p, scalars and convergence (block 0).
+// FP32 gather copy of the direction for the mixed-precision SpMV: entry i of a
+// vector with `blk`-sized node blocks goes to p32[(i / blk) * xs + i % blk].
+struct Dir32 {
+    float *p32 = nullptr;
+    int blk = 1, xs = 1;
+    __device__ __forceinline__ void put(int64_t i, double v) const {
+        if (!p32) return;
+        if (blk == 1) p32[i] = (float)v;
+        else p32[(i / blk) * xs + i % blk] = (float)v;
+    }
+};
+
 template <bool FUSED>
 __global__ void __launch_bounds__(kThreads)
 k_cg_pupdate(int64_t n, const double *__restrict__ partials_in, int np, KrylovScalars *S, int parity,
              double *__restrict__ p, const double *__restrict__ r, const double *__restrict__ z,
-             const double *__restrict__ dinv) {
+             const double *__restrict__ dinv, Dir32 d32) {
     __shared__ double sm[kThreads / 32 + 1];
     if (read_flag(&S->flag)) return;
     const double rz_new = reduce_partials<kThreads>(partials_in, np, 2, 0, sm);
@@ -191,15 +203,20 @@ k_cg_pupdate(int64_t n, const double *__restrict__ partials_in, int np, KrylovSc
     block_chunk(n, lo, hi);
     for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
         double zi = FUSED ? (dinv ? dinv[i] * r[i] : r[i]) : z[i];
-        p[i] = zi + beta * p[i];
+        const double pi = zi + beta * p[i];
+        p[i] = pi;
+        d32.put(i, pi);
     }
 }
 
 // p = z (start of the iteration); z is dinv*r or r in the fused path
 __global__ void k_p_init(int64_t n, double *__restrict__ p, const double *__restrict__ r,
-                         const double *__restrict__ z, const double *__restrict__ dinv) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        p[i] = z ? z[i] : (dinv ? dinv[i] * r[i] : r[i]);
+                         const double *__restrict__ z, const double *__restrict__ dinv, Dir32 d32) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double pi = z ? z[i] : (dinv ? dinv[i] * r[i] : r[i]);
+        p[i] = pi;
+        d32.put(i, pi);
+    }
 }
 
 __global__ void k_sub(int64_t n, const double *__restrict__ b, const double *__restrict__ q, double *__restrict__ r) {
@@ -224,8 +241,10 @@ struct Work {
     int64_t n;
     double *r = nullptr, *p = nullptr, *q = nullptr, *z = nullptr, *t = nullptr, *s = nullptr, *v = nullptr,
            *rhat = nullptr, *ph = nullptr, *sh = nullptr, *d = nullptr;
+    Dir32 d32;  // FP32 copy of p for the mixed-precision SpMV (p32 NULL otherwise)
     ~Work() {
         for (double *ptr : {r, p, q, z, t, s, v, rhat, ph, sh, d}) dev_free(ctx, ptr);
+        dev_free(ctx, d32.p32);
     }
 };
 
@@ -342,13 +361,15 @@ static yg_status pcg_core(yg_matrix A, yg_precond M, const double *b, double *x,
     double *P = ctx->d_partials;  // [0,G): p.q ; [2G,4G): r.z/r.r pairs ; [4G, 7G): init triples
     KrylovScalars *S = ctx->d_scalars;
     cudaStream_t st = ctx->stream;
+    // the FP32 direction copy serves the FP32-value iteration SpMV only
+    const Dir32 d32 = (precision == YG_PREC_MIXED || precision == YG_PREC_MIXED_IR) ? w.d32 : Dir32{};
 
     // r = b - A x ; z = M^-1 r ; p = z
     YG_TRY(spmv_launch(A, x, w.q, precision, nullptr, nullptr, spmv_grid));
     if (fused) {
         k_residual_init<<<G, kThreads, 0, st>>>(n, b, w.q, w.r, nullptr, dinv, P + 4 * G);
         YG_LAUNCHED(ctx);
-        k_p_init<<<stream_grid(ctx, n), kThreads, 0, st>>>(n, w.p, w.r, nullptr, dinv);
+        k_p_init<<<stream_grid(ctx, n), kThreads, 0, st>>>(n, w.p, w.r, nullptr, dinv, d32);
         YG_LAUNCHED(ctx);
     } else {
         k_residual_init<<<G, kThreads, 0, st>>>(n, b, w.q, w.r, nullptr, nullptr, P + 4 * G);
@@ -356,7 +377,7 @@ static yg_status pcg_core(yg_matrix A, yg_precond M, const double *b, double *x,
         YG_TRY(precond_apply_dev(M, w.r, w.z));
         k_dot2_partials<<<G, kThreads, 0, st>>>(n, w.r, w.z, P + 4 * G, nullptr, 0, 3);
         YG_LAUNCHED(ctx);
-        k_p_init<<<stream_grid(ctx, n), kThreads, 0, st>>>(n, w.p, w.r, w.z, nullptr);
+        k_p_init<<<stream_grid(ctx, n), kThreads, 0, st>>>(n, w.p, w.r, w.z, nullptr, d32);
         YG_LAUNCHED(ctx);
     }
     k_cg_scalars_init<<<1, kThreads, 0, st>>>(S, P + 4 * G, G, 3, tol, maxiter, criterion);
@@ -366,13 +387,13 @@ static yg_status pcg_core(yg_matrix A, yg_precond M, const double *b, double *x,
     int slot = 0;
     auto one = [&](int parity) -> yg_status {
         if (prof && prof->on) YG_CUDA(cudaEventRecordWithFlags(prof->start[slot], st, cudaEventRecordExternal));
-        YG_TRY(spmv_launch(A, w.p, w.q, precision, P, &S->flag, spmv_grid));
+        YG_TRY(spmv_launch(A, w.p, w.q, precision, P, &S->flag, spmv_grid, d32.p32));
         if (prof && prof->on) YG_CUDA(cudaEventRecordWithFlags(prof->stop[slot], st, cudaEventRecordExternal));
         ++slot;
         if (fused) {
             k_cg_update<true><<<G, kThreads, 0, st>>>(n, P, spmv_grid, S, parity, x, w.r, w.p, w.q, dinv, P + 2 * G);
             YG_LAUNCHED(ctx);
-            k_cg_pupdate<true><<<G, kThreads, 0, st>>>(n, P + 2 * G, G, S, parity, w.p, w.r, nullptr, dinv);
+            k_cg_pupdate<true><<<G, kThreads, 0, st>>>(n, P + 2 * G, G, S, parity, w.p, w.r, nullptr, dinv, d32);
             YG_LAUNCHED(ctx);
         } else {
             k_cg_update<false><<<G, kThreads, 0, st>>>(n, P, spmv_grid, S, parity, x, w.r, w.p, w.q, nullptr, P + 2 * G);
@@ -380,7 +401,7 @@ static yg_status pcg_core(yg_matrix A, yg_precond M, const double *b, double *x,
             YG_TRY(precond_apply_dev(M, w.r, w.z));
             k_dot2_partials<<<G, kThreads, 0, st>>>(n, w.r, w.z, P + 2 * G, &S->flag, 0, 2);
             YG_LAUNCHED(ctx);
-            k_cg_pupdate<false><<<G, kThreads, 0, st>>>(n, P + 2 * G, G, S, parity, w.p, w.r, w.z, nullptr);
+            k_cg_pupdate<false><<<G, kThreads, 0, st>>>(n, P + 2 * G, G, S, parity, w.p, w.r, w.z, nullptr, d32);
             YG_LAUNCHED(ctx);
         }
         return YG_OK;
@@ -442,9 +463,9 @@ static yg_status pcg_core(yg_matrix A, yg_precond M, const double *b, double *x,
                 }
                 // continue from the true residual with a fresh direction p = M^-1 r
                 if (fused) {
-                    k_p_init<<<stream_grid(ctx, n), kThreads, 0, st>>>(n, w.p, w.r, nullptr, dinv);
+                    k_p_init<<<stream_grid(ctx, n), kThreads, 0, st>>>(n, w.p, w.r, nullptr, dinv, d32);
                 } else {
-                    k_p_init<<<stream_grid(ctx, n), kThreads, 0, st>>>(n, w.p, w.r, w.z, nullptr);
+                    k_p_init<<<stream_grid(ctx, n), kThreads, 0, st>>>(n, w.p, w.r, w.z, nullptr, d32);
                 }
                 YG_LAUNCHED(ctx);
                 continue;
@@ -471,6 +492,15 @@ yg_status solve_cg(yg_matrix A, yg_precond M, yg_vector bv, yg_vector xv, const 
     YG_TRY(alloc_vec(ctx, &w.p, n));
     YG_TRY(alloc_vec(ctx, &w.q, n));
     if (M && !precond_fusable(M)) YG_TRY(alloc_vec(ctx, &w.z, n));
+    if (o.precision != YG_PREC_FP64 && (A->block == 2 || A->block == 3)) {
+        // FP32 gather copy of p (node-padded) for the FP32-value TMA SpMV
+        const int xs = spmv_x32_stride(A->block);
+        const int64_t m32 = (n / A->block + 1) * xs;
+        YG_TRY(dev_alloc_t(ctx, &w.d32.p32, m32));
+        YG_CUDA(cudaMemsetAsync(w.d32.p32, 0, sizeof(float) * m32, ctx->stream));
+        w.d32.blk = A->block;
+        w.d32.xs = xs;
+    }
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);

@@ -17,6 +17,8 @@
 #include "internal.h"
 #include "device_common.cuh"
 
+#include <type_traits>
+
 namespace yg {
 
 // DOT = 0: y = A x.  DOT = 1: also per-block sums of w.y.  DOT = 2: per-block
@@ -309,12 +311,32 @@ struct TmaCfg {
     static constexpr int SMEM = WARPS * NST * STAGE + WARPS * NST * 8;  // stages + mbarriers
 };
 
-template <int B, typename VT, int DOT, typename C>
+// XF: gather x from the FP32 node-padded copy x32 (one 16-byte load for a 3x3
+// block, one 8-byte load for a 2x2 block) instead of B FP64 loads from x.
+template <int B, bool XF>
+__device__ __forceinline__ void gather_x(const double *__restrict__ x, const float *__restrict__ x32, int c,
+                                         double (&xo)[B]) {
+    if constexpr (XF && B == 3) {
+        const float4 v = __ldg(reinterpret_cast<const float4 *>(x32) + c);
+        xo[0] = v.x;
+        xo[1] = v.y;
+        xo[2] = v.z;
+    } else if constexpr (XF && B == 2) {
+        const float2 v = __ldg(reinterpret_cast<const float2 *>(x32) + c);
+        xo[0] = v.x;
+        xo[1] = v.y;
+    } else {
+#pragma unroll
+        for (int k = 0; k < B; ++k) xo[k] = __ldg(x + (int64_t)B * c + k);
+    }
+}
+
+template <int B, typename VT, int DOT, typename C, bool XF>
 __global__ void __launch_bounds__(C::WARPS * 32)
 k_bcsr_spmv_tma(int64_t nbrows, const int32_t *__restrict__ rowptr, const int32_t *__restrict__ col,
-                const VT *__restrict__ val, const double *__restrict__ x, double *__restrict__ y,
-                const double *__restrict__ w, double *__restrict__ partials, const int32_t *__restrict__ flag,
-                int32_t *__restrict__ err) {
+                const VT *__restrict__ val, const double *__restrict__ x, const float *__restrict__ x32,
+                double *__restrict__ y, const double *__restrict__ w, double *__restrict__ partials,
+                const int32_t *__restrict__ flag, int32_t *__restrict__ err) {
     constexpr int B2 = B * B;
     constexpr int BB = B2 * (int)sizeof(VT);
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -396,11 +418,8 @@ k_bcsr_spmv_tma(int64_t nbrows, const int32_t *__restrict__ rowptr, const int32_
         for (; j + 32 < nb; j += 64) {
             const int c0 = cix[j], c1 = cix[j + 32];
             double x0[B], x1[B];
-#pragma unroll
-            for (int k = 0; k < B; ++k) {
-                x0[k] = __ldg(x + (int64_t)B * c0 + k);
-                x1[k] = __ldg(x + (int64_t)B * c1 + k);
-            }
+            gather_x<B, XF>(x, x32, c0, x0);
+            gather_x<B, XF>(x, x32, c1, x1);
 #pragma unroll
             for (int i = 0; i < B; ++i)
 #pragma unroll
@@ -412,8 +431,7 @@ k_bcsr_spmv_tma(int64_t nbrows, const int32_t *__restrict__ rowptr, const int32_
         if (j < nb) {
             const int c0 = cix[j];
             double x0[B];
-#pragma unroll
-            for (int k = 0; k < B; ++k) x0[k] = __ldg(x + (int64_t)B * c0 + k);
+            gather_x<B, XF>(x, x32, c0, x0);
 #pragma unroll
             for (int i = 0; i < B; ++i)
 #pragma unroll
@@ -797,18 +815,29 @@ static void csr_shape_v(int lanes, int *smem, int *wp) {
     }
 }
 
-template <int B, typename VT, int DOT, typename C>
-static yg_status launch_tma_cfg(yg_matrix A, const VT *val, const double *x, double *y, const double *w,
-                                double *partials, const int32_t *flag, int grid, cudaStream_t st) {
+template <int B, typename VT, int DOT, typename C, bool XF>
+static yg_status launch_tma_xf(yg_matrix A, const VT *val, const double *x, const float *x32, double *y,
+                               const double *w, double *partials, const int32_t *flag, int grid, cudaStream_t st) {
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(k_bcsr_spmv_tma<B, VT, DOT, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM);
+        cudaFuncSetAttribute(k_bcsr_spmv_tma<B, VT, DOT, C, XF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             C::SMEM);
         attr = true;
     }
-    k_bcsr_spmv_tma<B, VT, DOT, C><<<grid, C::WARPS * 32, C::SMEM, st>>>(A->nbrows, A->d_rowptr, A->d_col, val, x, y, w,
-                                                                        partials, flag, A->ctx->d_err);
+    k_bcsr_spmv_tma<B, VT, DOT, C, XF><<<grid, C::WARPS * 32, C::SMEM, st>>>(
+        A->nbrows, A->d_rowptr, A->d_col, val, x, x32, y, w, partials, flag, A->ctx->d_err);
     YG_LAUNCHED(A->ctx);
     return YG_OK;
+}
+
+// FP32 gathers only with FP32 values (the mixed-precision iteration SpMV).
+template <int B, typename VT, int DOT, typename C>
+static yg_status launch_tma_cfg(yg_matrix A, const VT *val, const double *x, const float *x32, double *y,
+                                const double *w, double *partials, const int32_t *flag, int grid, cudaStream_t st) {
+    if constexpr (std::is_same<VT, float>::value) {
+        if (x32) return launch_tma_xf<B, VT, DOT, C, true>(A, val, x, x32, y, w, partials, flag, grid, st);
+    }
+    return launch_tma_xf<B, VT, DOT, C, false>(A, val, x, nullptr, y, w, partials, flag, grid, st);
 }
 
 // TMA configurations (chunk blocks, ring depth, warps per CTA) the autotuner
@@ -821,15 +850,15 @@ template <int B, typename VT> using TmaL8 = TmaCfg<B, VT, 32, 3, 12>;
 template <int B, typename VT> using TmaL16 = TmaCfg<B, VT, 48, 3, 8>;
 
 template <int B, typename VT, int DOT>
-static yg_status launch_tma(yg_matrix A, int lanes, const VT *val, const double *x, double *y, const double *w,
-                            double *partials, const int32_t *flag, int grid, cudaStream_t st) {
+static yg_status launch_tma(yg_matrix A, int lanes, const VT *val, const double *x, const float *x32, double *y,
+                            const double *w, double *partials, const int32_t *flag, int grid, cudaStream_t st) {
     switch (lanes) {
-    case 1: return launch_tma_cfg<B, VT, DOT, TmaL1<B, VT>>(A, val, x, y, w, partials, flag, grid, st);
-    case 2: return launch_tma_cfg<B, VT, DOT, TmaL2<B, VT>>(A, val, x, y, w, partials, flag, grid, st);
-    case 4: return launch_tma_cfg<B, VT, DOT, TmaL4<B, VT>>(A, val, x, y, w, partials, flag, grid, st);
-    case 8: return launch_tma_cfg<B, VT, DOT, TmaL8<B, VT>>(A, val, x, y, w, partials, flag, grid, st);
-    case 16: return launch_tma_cfg<B, VT, DOT, TmaL16<B, VT>>(A, val, x, y, w, partials, flag, grid, st);
-    default: return launch_tma_cfg<B, VT, DOT, TmaL32<B, VT>>(A, val, x, y, w, partials, flag, grid, st);
+    case 1: return launch_tma_cfg<B, VT, DOT, TmaL1<B, VT>>(A, val, x, x32, y, w, partials, flag, grid, st);
+    case 2: return launch_tma_cfg<B, VT, DOT, TmaL2<B, VT>>(A, val, x, x32, y, w, partials, flag, grid, st);
+    case 4: return launch_tma_cfg<B, VT, DOT, TmaL4<B, VT>>(A, val, x, x32, y, w, partials, flag, grid, st);
+    case 8: return launch_tma_cfg<B, VT, DOT, TmaL8<B, VT>>(A, val, x, x32, y, w, partials, flag, grid, st);
+    case 16: return launch_tma_cfg<B, VT, DOT, TmaL16<B, VT>>(A, val, x, x32, y, w, partials, flag, grid, st);
+    default: return launch_tma_cfg<B, VT, DOT, TmaL32<B, VT>>(A, val, x, x32, y, w, partials, flag, grid, st);
     }
 }
 
@@ -899,11 +928,14 @@ static yg_status launch_l(yg_matrix A, int lanes, const VT *val, const double *x
 }
 
 template <typename VT, int DOT>
-static yg_status launch_b(yg_matrix A, int variant, int lanes, const VT *val, const double *x, double *y,
-                          const double *w, double *partials, const int32_t *flag, int grid, cudaStream_t st) {
+static yg_status launch_b(yg_matrix A, int variant, int lanes, const VT *val, const double *x, const float *x32,
+                          double *y, const double *w, double *partials, const int32_t *flag, int grid,
+                          cudaStream_t st) {
     if (variant == 3) return launch_csr<VT, DOT>(A, lanes, val, x, y, w, partials, flag, grid, st);
-    if (variant == 2 && A->block == 3) return launch_tma<3, VT, DOT>(A, lanes, val, x, y, w, partials, flag, grid, st);
-    if (variant == 2 && A->block == 2) return launch_tma<2, VT, DOT>(A, lanes, val, x, y, w, partials, flag, grid, st);
+    if (variant == 2 && A->block == 3)
+        return launch_tma<3, VT, DOT>(A, lanes, val, x, x32, y, w, partials, flag, grid, st);
+    if (variant == 2 && A->block == 2)
+        return launch_tma<2, VT, DOT>(A, lanes, val, x, x32, y, w, partials, flag, grid, st);
     if (variant == 1 && A->block == 3) return launch_staged<3, VT, DOT>(A, val, x, y, w, partials, flag, grid, st);
     if (variant == 1 && A->block == 2) return launch_staged<2, VT, DOT>(A, val, x, y, w, partials, flag, grid, st);
     switch (A->block) {
@@ -915,12 +947,12 @@ static yg_status launch_b(yg_matrix A, int variant, int lanes, const VT *val, co
 }
 
 template <typename VT>
-static yg_status launch_v(yg_matrix A, int variant, int lanes, const VT *val, const double *x, double *y,
-                          const double *w, double *partials, int dot_mode, const int32_t *flag, int grid,
+static yg_status launch_v(yg_matrix A, int variant, int lanes, const VT *val, const double *x, const float *x32,
+                          double *y, const double *w, double *partials, int dot_mode, const int32_t *flag, int grid,
                           cudaStream_t st) {
-    if (dot_mode == 0) return launch_b<VT, 0>(A, variant, lanes, val, x, y, w, partials, flag, grid, st);
-    if (dot_mode == 1) return launch_b<VT, 1>(A, variant, lanes, val, x, y, w, partials, flag, grid, st);
-    return launch_b<VT, 2>(A, variant, lanes, val, x, y, w, partials, flag, grid, st);
+    if (dot_mode == 0) return launch_b<VT, 0>(A, variant, lanes, val, x, x32, y, w, partials, flag, grid, st);
+    if (dot_mode == 1) return launch_b<VT, 1>(A, variant, lanes, val, x, x32, y, w, partials, flag, grid, st);
+    return launch_b<VT, 2>(A, variant, lanes, val, x, x32, y, w, partials, flag, grid, st);
 }
 
 // The kernel choice for a precision: FP32-value SpMVs have their own tuning.
@@ -939,7 +971,7 @@ static void choice(yg_matrix A, int precision, int *variant, int *lanes) {
 // x) or of w.y and y.y (dot_mode 2).  The grid is persistent: `grid` blocks
 // stride over the block rows.
 yg_status spmv_launch_ex(yg_matrix A, const double *x, double *y, int precision, const double *w, double *partials,
-                         int dot_mode, const int32_t *flag, int grid, cudaStream_t stream) {
+                         int dot_mode, const int32_t *flag, int grid, cudaStream_t stream, const float *x32) {
     cudaStream_t st = stream ? stream : A->ctx->stream;
     if (grid > kMaxReduceBlocks) grid = kMaxReduceBlocks;
     if (!partials) dot_mode = 0;
@@ -949,9 +981,9 @@ yg_status spmv_launch_ex(yg_matrix A, const double *x, double *y, int precision,
     choice(A, precision, &variant, &lanes);
     if (precision == YG_PREC_MIXED || precision == YG_PREC_MIXED_IR) {
         if (!A->d_val32) return fail(YG_BAD_ARG, "mixed-precision SpMV without FP32 values");
-        s = launch_v<float>(A, variant, lanes, A->d_val32, x, y, w, partials, dot_mode, flag, grid, st);
+        s = launch_v<float>(A, variant, lanes, A->d_val32, x, x32, y, w, partials, dot_mode, flag, grid, st);
     } else {
-        s = launch_v<double>(A, variant, lanes, A->d_val, x, y, w, partials, dot_mode, flag, grid, st);
+        s = launch_v<double>(A, variant, lanes, A->d_val, x, nullptr, y, w, partials, dot_mode, flag, grid, st);
     }
     if (s != YG_OK) return s;
     YG_CUDA(cudaGetLastError());
@@ -959,8 +991,8 @@ yg_status spmv_launch_ex(yg_matrix A, const double *x, double *y, int precision,
 }
 
 yg_status spmv_launch(yg_matrix A, const double *x, double *y, int precision, double *partials,
-                      const int32_t *flag, int grid) {
-    return spmv_launch_ex(A, x, y, precision, x, partials, partials ? 1 : 0, flag, grid);
+                      const int32_t *flag, int grid, const float *x32) {
+    return spmv_launch_ex(A, x, y, precision, x, partials, partials ? 1 : 0, flag, grid, nullptr, x32);
 }
 
 // Resident blocks per SM of the flat kernel (the heaviest, DOT = 2, form) for a
@@ -1062,7 +1094,8 @@ struct TuneKey {
 static std::vector<std::pair<TuneKey, std::pair<int, int>>> g_tune_cache;
 
 // Time every candidate for one precision on this matrix; returns the fastest.
-static yg_status tune_precision(yg_matrix A, int precision, double *x, double *y, int *best_variant, int *best_lanes) {
+static yg_status tune_precision(yg_matrix A, int precision, double *x, const float *x32, double *y,
+                                int *best_variant, int *best_lanes) {
     yg_context ctx = A->ctx;
     struct Cand { int variant, lanes; };
     std::vector<Cand> cands;
@@ -1087,9 +1120,9 @@ static yg_status tune_precision(yg_matrix A, int precision, double *x, double *y
         *pv = c.variant;
         *pl = c.lanes;
         const int grid = spmv_grid_for(A, precision);
-        if ((s = spmv_launch(A, x, y, precision, nullptr, nullptr, grid)) != YG_OK) break;  // warm-up
+        if ((s = spmv_launch(A, x, y, precision, nullptr, nullptr, grid, x32)) != YG_OK) break;  // warm-up
         cudaEventRecord(e0, ctx->stream);
-        for (int r = 0; r < reps; ++r) spmv_launch(A, x, y, precision, nullptr, nullptr, grid);
+        for (int r = 0; r < reps; ++r) spmv_launch(A, x, y, precision, nullptr, nullptr, grid, x32);
         cudaEventRecord(e1, ctx->stream);
         cudaEventSynchronize(e1);
         float ms = 0;
@@ -1121,6 +1154,7 @@ yg_status spmv_autotune_device(yg_matrix A) {
     YG_CUDA(cudaStreamIsCapturing(ctx->stream, &cs));
     if (cs != cudaStreamCaptureStatusNone) return YG_OK;
     double *x = nullptr, *y = nullptr;
+    float *x32 = nullptr;  // FP32 gather copy: the mixed-precision solvers pass one to the TMA kernels
     bool allocated = false;
     for (int f32 = 0; f32 <= 1; ++f32) {
         if (f32 ? !need32 : !need64) continue;
@@ -1136,17 +1170,21 @@ yg_status spmv_autotune_device(yg_matrix A) {
         if (!hit) {
             if (!allocated) {
                 const int64_t n = A->rows(), m = A->cols();
+                const int64_t m32 = (m / A->block + 1) * spmv_x32_stride(A->block);
                 YG_TRY(dev_alloc_t(ctx, &x, m + 1));
                 yg_status s = dev_alloc_t(ctx, &y, n + 1);
-                if (s != YG_OK) { dev_free(ctx, x); return s; }
+                if (s == YG_OK) s = dev_alloc_t(ctx, &x32, m32);
+                if (s != YG_OK) { dev_free(ctx, x); dev_free(ctx, y); return s; }
                 cudaMemsetAsync(x, 0, sizeof(double) * (m + 1), ctx->stream);
+                cudaMemsetAsync(x32, 0, sizeof(float) * m32, ctx->stream);
                 allocated = true;
             }
             int v = 0, l = 32;
-            yg_status s = tune_precision(A, f32 ? YG_PREC_MIXED : YG_PREC_FP64, x, y, &v, &l);
+            yg_status s = tune_precision(A, f32 ? YG_PREC_MIXED : YG_PREC_FP64, x, f32 ? x32 : nullptr, y, &v, &l);
             if (s != YG_OK) {
                 dev_free(ctx, x);
                 dev_free(ctx, y);
+                dev_free(ctx, x32);
                 return s;
             }
             (f32 ? A->variant32 : A->variant) = v;
@@ -1158,6 +1196,7 @@ yg_status spmv_autotune_device(yg_matrix A) {
     if (allocated) {
         dev_free(ctx, x);
         dev_free(ctx, y);
+        dev_free(ctx, x32);
     }
     YG_CUDA(cudaGetLastError());
     return YG_OK;
