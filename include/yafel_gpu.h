@@ -172,6 +172,17 @@ YG_API yg_status yg_assemble(yg_dofmap d, const yg_physics *physics, uint32_t re
  * limit as yg_assemble (hexahedra p <= 3, else YG_UNSUPPORTED). */
 YG_API yg_status yg_local_smoothing_gradient(yg_dofmap d, int32_t nsd, yg_vector solution, yg_vector gradient);
 
+/* ZZGradientRecovery<Physics>(FESystem&) (include/assembly/ZZGradientRecovery.hpp:33-140):
+ * Zienkiewicz-Zhu patch recovery of the nodal gradient of a p = 1 scalar field
+ * (one dof per node, as the reference asserts): each node fits a linear
+ * polynomial by least squares to the FE gradient at the quadrature points of
+ * the cells of dimension nsd (2 or 3) around it and takes its value at the
+ * node.  `gradient` has n_nodes * nsd entries, row-major.  Solved through the
+ * patch's normal equations in coordinates centred at the node (the reference
+ * uses a column-pivoted QR in absolute coordinates; same fit to rounding).
+ * A node whose patch has fewer samples than nsd + 1 gets NaN.  Deterministic. */
+YG_API yg_status yg_zz_gradient_recovery(yg_dofmap d, int32_t nsd, yg_vector solution, yg_vector gradient);
+
 /* DirichletBC::apply(A, rhs) for one BC object (src/boundary_conditions/DirichletBC.cpp:27-89):
  * rhs -= A*g, zero the BC rows and columns, unit diagonal, rhs_bc = g.  bc_dofs
  * are global dofs (node*dof_per_node + component), bc_values their g. */

@@ -181,6 +181,7 @@ def ref():
         R.refa_dirichlet_nodes.argtypes = [C.c_void_p, C.c_int, i32p, C.c_int, C.c_double]
         R.refa_local_smoothing_gradient.argtypes = [C.c_void_p, C.c_int, f64p, f64p]
         R.refa_element.argtypes = [C.c_int] * 4 + [C.POINTER(C.c_int)] * 2 + [C.c_void_p] * 5
+        R.refa_zz_gradient.argtypes = [C.c_void_p, C.c_int, f64p, f64p]
         _REF = R
     return _REF
 
@@ -301,6 +302,13 @@ class RefSystem:
     def local_smoothing_gradient(self, nsd, sol):
         out = np.zeros((self.n, nsd))
         ref().refa_local_smoothing_gradient(self.h, nsd, np.ascontiguousarray(sol, dtype=np.float64), out)
+        return out
+
+    def zz_gradient(self, nsd, sol):
+        """ZZGradientRecovery (include/assembly/ZZGradientRecovery.hpp:33-140): the
+        patch-recovered nodal gradient of a p = 1 scalar field, (n_nodes, nsd)."""
+        out = np.zeros((self.n, nsd))
+        ref().refa_zz_gradient(self.h, nsd, np.ascontiguousarray(sol, dtype=np.float64), out)
         return out
 
     def __del__(self):

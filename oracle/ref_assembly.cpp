@@ -13,6 +13,7 @@
 //   src/boundary_conditions/DirichletBC.cpp:58-89    DirichletBC::apply (ColMajor)
 //   include/boundary_conditions/DirichletBC.hpp:80-89 selectByFunction
 //   include/assembly/LocalSmoothingGradient.hpp:20-94 LocalSmoothingGradient<Physics>
+//   include/assembly/ZZGradientRecovery.hpp:33-140   ZZGradientRecovery<Physics>
 //   apps/supg_learning/supg_advection.hpp:19-132     AdvectionDiffusionSUPG<NSD> (the physics itself)
 //
 // The Poisson and elasticity Physics structs of the reference live in the apps'
@@ -23,6 +24,7 @@
 // mirrored entry), generalised to a sign and load parameters.
 #include "assembly/CGAssembly.hpp"
 #include "assembly/LocalSmoothingGradient.hpp"
+#include "assembly/ZZGradientRecovery.hpp"
 #include "boundary_conditions/DirichletBC.hpp"
 #include "fe_system/FESystem.hpp"
 #include "mesh/Mesh.hpp"
@@ -324,6 +326,19 @@ void refa_local_smoothing_gradient(void *h, int nsd, const double *solution, dou
     if (nsd == 1) LocalSmoothingGradient<PoissonPhysics<1>>(s);
     if (nsd == 2) LocalSmoothingGradient<PoissonPhysics<2>>(s);
     if (nsd == 3) LocalSmoothingGradient<PoissonPhysics<3>>(s);
+    auto &G = s.getSolutionGradient();
+    for (Eigen::Index i = 0; i < G.rows(); ++i)
+        for (int d = 0; d < nsd; ++d) gradient[i * nsd + d] = G(i, d);
+}
+
+// ZZGradientRecovery<Physics>(sys) on a given solution (p = 1, one dof per
+// node); gradient row-major (n_nodes x nsd).
+void refa_zz_gradient(void *h, int nsd, const double *solution, double *gradient) {
+    auto &s = static_cast<RefSystem *>(h)->sys;
+    auto &U = s.getSolution();
+    for (Eigen::Index i = 0; i < U.rows(); ++i) U(i) = solution[i];
+    if (nsd == 2) ZZGradientRecovery<PoissonPhysics<2>>(s);
+    if (nsd == 3) ZZGradientRecovery<PoissonPhysics<3>>(s);
     auto &G = s.getSolutionGradient();
     for (Eigen::Index i = 0; i < G.rows(); ++i)
         for (int d = 0; d < nsd; ++d) gradient[i * nsd + d] = G(i, d);

@@ -8,10 +8,11 @@ own tests use (test/test_sparse_csr.cpp, test_sparse_bcsr.cpp,
 test_cg_solve.cpp, test_bicgstab_solve.cpp, test_ILU.cpp) and on a small
 assembled Poisson system (linalg.npz, quadrature.npz, poisson8.npz); and its
 assembly half -- Element tables, DoFManager numbering, CGAssembly values and
-residuals, DirichletBC::apply and LocalSmoothingGradient -- on small seeded
-quadrilateral, triangle, mixed, hexahedron and tetrahedron meshes at orders
-1-3 (elements.npz, assembly_ref.npz), built against the from-scratch Eigen-API
-subset in oracle/ref_compat (Eigen itself is not installed).
+residuals, DirichletBC::apply, LocalSmoothingGradient and ZZGradientRecovery
+-- on small seeded quadrilateral, triangle, mixed, hexahedron and tetrahedron
+meshes at orders 1-3 (elements.npz, assembly_ref.npz, zz_ref.npz), built
+against the from-scratch Eigen-API subset in oracle/ref_compat (Eigen itself is
+not installed).
 They pin the oracle without the reference tree being present.
 """
 import os
@@ -244,6 +245,22 @@ def assembly():
     np.savez_compressed(os.path.join(HERE, "assembly_ref.npz"), **out)
 
 
+def zz():
+    """The reference's ZZGradientRecovery (p = 1, one dof per node) of a
+    non-linear field on the p = 1 meshes of assembly_meshes."""
+    out = {}
+    for kind in ("quad", "mixed", "tri", "hex", "tet"):
+        mesh, nsd = assembly_meshes(kind, 1)
+        dm = O.RefDofManager(mesh, 1, 1)
+        sysm = O.RefSystem(dm, nsd, O.POISSON, [1.0, 1.0])
+        u = smooth_field(dm.nodes, 0)
+        k = kind + "/"
+        for key in ("nodes", "cell_nodes", "offsets", "cell_types"):
+            out[k + "mesh_" + key] = mesh[key]
+        out[k + "u"], out[k + "grad"], out[k + "nsd"] = u, sysm.zz_gradient(nsd, u), np.array(nsd)
+    np.savez_compressed(os.path.join(HERE, "zz_ref.npz"), **out)
+
+
 if __name__ == "__main__":
     O.build()
     if not O.ref_available():
@@ -253,4 +270,5 @@ if __name__ == "__main__":
     poisson_system()
     elements()
     assembly()
+    zz()
     print("golden fixtures written to", HERE)

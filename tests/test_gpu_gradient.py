@@ -3,7 +3,10 @@ oracle's restatement of include/assembly/LocalSmoothingGradient.hpp:20-94, on th
 same numbering: random solution fields on jittered mixed triangle/quad meshes
 (orders 1 and 3; quads at order 2, where a quadratic triangle's vertex functions
 integrate to zero) and hex meshes, scalar and vector fields; and the exact
-constant gradient of a linear field."""
+constant gradient of a linear field.  ZZGradientRecovery (yg_zz_gradient_recovery)
+against the reference's own, run on the fixtures of tests/golden/zz_ref.npz."""
+import os
+
 import numpy as np
 import pytest
 
@@ -34,7 +37,9 @@ def test_gradient_matches_oracle(ctx, dim, p, dpn, n):
     fe.getSolution().upload(u)
     yb.LocalSmoothingGradient(yb.PoissonEquation(dim), fe)
     g = fe.getSolutionGradient().numpy().reshape(-1, dim)
-    go = O.local_smoothing_gradient(O.dofmanager(mesh, p), dpn, dim, u)
+    # the oracle on the GPU's numbering (the reference's merged coordinates)
+    odm = O.ArrayDofMap(dm.dof_nodes, dm.element_offsets, dm.elements, mesh["cell_types"], p)
+    go = O.local_smoothing_gradient(odm, dpn, dim, u)
     assert g.shape == go.shape
     assert np.abs(g - go).max() <= 1e-11 * np.abs(go).max(), (dim, p, dpn)
     # same bits on a second call
@@ -54,3 +59,42 @@ def test_linear_field_has_its_constant_gradient(ctx, dim, p, dpn, n):
     yb.LocalSmoothingGradient(yb.PoissonEquation(dim), fe)
     g = fe.getSolutionGradient().numpy().reshape(-1, dim)
     assert np.abs(g - np.tile(a, (dm.dof_nodes.shape[0], 1))).max() <= 1e-11
+
+
+ZZ = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "zz_ref.npz"))
+
+
+@pytest.mark.parametrize("kind", ["quad", "mixed", "tri", "hex", "tet"])
+def test_zz_recovery_matches_reference(ctx, kind):
+    """ZZGradientRecovery on the GPU against the reference's own (compiled in
+    place, column-pivoted QR in absolute coordinates) on a non-linear field:
+    the GPU solves the same least-squares fits through normal equations in
+    coordinates centred at the node, so the two agree to rounding."""
+    k = kind + "/"
+    mesh = {"nodes": ZZ[k + "mesh_nodes"], "cell_nodes": ZZ[k + "mesh_cell_nodes"],
+            "offsets": ZZ[k + "mesh_offsets"], "cell_types": ZZ[k + "mesh_cell_types"]}
+    nsd = int(ZZ[k + "nsd"])
+    dm = yb.DoFManager(mesh, 1, 1, ctx=ctx)
+    fe = yb.FESystem(dm, nsd)
+    fe.getSolution().upload(ZZ[k + "u"])
+    yb.ZZGradientRecovery(yb.PoissonEquation(nsd), fe)
+    g = fe.getSolutionGradient().numpy().reshape(-1, nsd)
+    ref = ZZ[k + "grad"]
+    assert np.abs(g - ref).max() <= 1e-10 * np.abs(ref).max(), np.abs(g - ref).max()
+    # deterministic
+    yb.ZZGradientRecovery(yb.PoissonEquation(nsd), fe)
+    assert np.array_equal(fe.getSolutionGradient().numpy().reshape(-1, nsd), g)
+
+
+def test_zz_recovers_linear_fields_exactly_and_rejects_p2(ctx):
+    mesh = meshgen.jittered_mixed(12, 10, seed=4, order="tensor")
+    dm = yb.DoFManager(mesh, 1, 1, ctx=ctx)
+    fe = yb.FESystem(dm, 2)
+    X = dm.dof_nodes
+    fe.getSolution().upload(0.5 + 3.0 * X[:, 0] - 2.0 * X[:, 1])
+    yb.ZZGradientRecovery(yb.PoissonEquation(2), fe)
+    g = fe.getSolutionGradient().numpy().reshape(-1, 2)
+    assert np.abs(g - np.array([3.0, -2.0])).max() <= 1e-11
+    dm2 = yb.DoFManager(meshgen.structured_quad(4, 4), 2, 1, ctx=ctx)
+    with pytest.raises(yb.YafelError):
+        yb.ZZGradientRecovery(yb.PoissonEquation(2), yb.FESystem(dm2, 2))

@@ -546,6 +546,18 @@ def LocalSmoothingGradient(physics, feSystem):
     return feSystem
 
 
+def ZZGradientRecovery(physics, feSystem):
+    """ZZGradientRecovery<Physics>(FESystem&)
+    (include/assembly/ZZGradientRecovery.hpp:33-140): Zienkiewicz-Zhu patch
+    recovery of the gradient of the FESystem's p = 1 scalar solution, stored as
+    the FESystem's solution gradient (n_nodes x nsd)."""
+    nsd = physics.nsd()
+    g = DeviceVector(feSystem.dofm.nNodes() * nsd, feSystem.ctx)
+    check(lib().yg_zz_gradient_recovery(feSystem.dofm.h, nsd, feSystem.solution.h, g.h), "ZZGradientRecovery")
+    feSystem.solution_gradient = g
+    return feSystem
+
+
 class DirichletBC:
     """DirichletBC(dofm, value, comp) (include/boundary_conditions/DirichletBC.hpp:23-89);
     value is a number or a function f(x, t)."""

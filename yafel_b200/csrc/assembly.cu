@@ -947,6 +947,68 @@ extern "C" yg_status yg_dirichlet_apply(yg_matrix K, yg_vector rhs, const int64_
 
 namespace yg {
 
+// Element::update for one cell, cooperatively by the CTA (include/element/Element.hpp:109-149):
+// the Jacobian sum_A x_A (x) dN_A/dxi, jxw = det J * w_q and the physical
+// gradients G[(q*nen + A)*NSD + i] = sum_j Jinv(j, i) dN_A/dxi_j, from the
+// cell's node coordinates xe (nen x 3, already in shared memory).  Ends with
+// the CTA synchronised.
+template <int NSD>
+__device__ void cell_gradients(const double *__restrict__ xe, const double *__restrict__ tdN, const double *__restrict__ tw,
+                               int nen, int nq, int tdim, double *__restrict__ G, double *__restrict__ jxw,
+                               double *__restrict__ Ji) {
+    for (int q = threadIdx.x; q < nq; q += blockDim.x) {
+        double J[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+        for (int A = 0; A < nen; ++A) {
+            const double *d = tdN + ((size_t)q * nen + A) * tdim;
+#pragma unroll
+            for (int i = 0; i < NSD; ++i)
+#pragma unroll
+                for (int j = 0; j < NSD; ++j) J[i][j] += xe[3 * A + i] * d[j];
+        }
+        double det, inv[3][3];
+        if (NSD == 1) {
+            det = J[0][0];
+            inv[0][0] = 1.0 / J[0][0];
+        } else if (NSD == 2) {
+            det = J[0][0] * J[1][1] - J[0][1] * J[1][0];
+            const double di = 1.0 / det;
+            inv[0][0] = J[1][1] * di; inv[1][1] = J[0][0] * di;
+            inv[0][1] = -J[0][1] * di; inv[1][0] = -J[1][0] * di;
+        } else {
+            det = J[0][0] * (J[1][1] * J[2][2] - J[1][2] * J[2][1]) - J[0][1] * (J[1][0] * J[2][2] - J[2][0] * J[1][2]) +
+                  J[0][2] * (J[1][0] * J[2][1] - J[2][0] * J[1][1]);
+            const double di = 1.0 / det;
+            inv[0][0] = (J[1][1] * J[2][2] - J[1][2] * J[2][1]) * di;
+            inv[0][1] = -(J[0][1] * J[2][2] - J[2][1] * J[0][2]) * di;
+            inv[0][2] = (J[0][1] * J[1][2] - J[1][1] * J[0][2]) * di;
+            inv[1][0] = -(J[1][0] * J[2][2] - J[2][0] * J[1][2]) * di;
+            inv[1][1] = (J[0][0] * J[2][2] - J[0][2] * J[2][0]) * di;
+            inv[1][2] = -(J[0][0] * J[1][2] - J[1][0] * J[0][2]) * di;
+            inv[2][0] = (J[1][0] * J[2][1] - J[2][0] * J[1][1]) * di;
+            inv[2][1] = -(J[0][0] * J[2][1] - J[2][0] * J[0][1]) * di;
+            inv[2][2] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) * di;
+        }
+        jxw[q] = det * tw[q];
+#pragma unroll
+        for (int i = 0; i < NSD; ++i)
+#pragma unroll
+            for (int j = 0; j < NSD; ++j) Ji[9 * q + 3 * i + j] = inv[i][j];
+    }
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < nq * nen; idx += blockDim.x) {
+        const int q = idx / nen;
+        const double *d = tdN + (size_t)idx * tdim;
+#pragma unroll
+        for (int dd = 0; dd < NSD; ++dd) {
+            double s = 0;
+#pragma unroll
+            for (int j = 0; j < NSD; ++j) s += Ji[9 * q + 3 * j + dd] * d[j];
+            G[(size_t)idx * NSD + dd] = s;
+        }
+    }
+    __syncthreads();
+}
+
 // LocalSmoothingGradient<Physics> (include/assembly/LocalSmoothingGradient.hpp:20-94):
 // per cell of dimension NSD (one CTA), per quadrature point, the gradient of each
 // of the DPN solution components, qg(comp, i) = sum_A u_A dN_A/dx_i, is spread to
@@ -983,57 +1045,7 @@ k_smooth_gradient(const int32_t *__restrict__ order, int ncell, const int32_t *_
         }
         __syncthreads();
         for (int a = threadIdx.x; a < nen * DPN; a += blockDim.x) ul[a] = sol[(int64_t)gn[a / DPN] * DPN + a % DPN];
-        for (int q = threadIdx.x; q < nq; q += blockDim.x) {
-            double J[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-            for (int A = 0; A < nen; ++A) {
-                const double *d = tdN + ((size_t)q * nen + A) * tdim;
-#pragma unroll
-                for (int i = 0; i < NSD; ++i)
-#pragma unroll
-                    for (int j = 0; j < NSD; ++j) J[i][j] += xe[3 * A + i] * d[j];
-            }
-            double det, inv[3][3];
-            if (NSD == 1) {
-                det = J[0][0];
-                inv[0][0] = 1.0 / J[0][0];
-            } else if (NSD == 2) {
-                det = J[0][0] * J[1][1] - J[0][1] * J[1][0];
-                const double di = 1.0 / det;
-                inv[0][0] = J[1][1] * di; inv[1][1] = J[0][0] * di;
-                inv[0][1] = -J[0][1] * di; inv[1][0] = -J[1][0] * di;
-            } else {
-                det = J[0][0] * (J[1][1] * J[2][2] - J[1][2] * J[2][1]) - J[0][1] * (J[1][0] * J[2][2] - J[2][0] * J[1][2]) +
-                      J[0][2] * (J[1][0] * J[2][1] - J[2][0] * J[1][1]);
-                const double di = 1.0 / det;
-                inv[0][0] = (J[1][1] * J[2][2] - J[1][2] * J[2][1]) * di;
-                inv[0][1] = -(J[0][1] * J[2][2] - J[2][1] * J[0][2]) * di;
-                inv[0][2] = (J[0][1] * J[1][2] - J[1][1] * J[0][2]) * di;
-                inv[1][0] = -(J[1][0] * J[2][2] - J[2][0] * J[1][2]) * di;
-                inv[1][1] = (J[0][0] * J[2][2] - J[0][2] * J[2][0]) * di;
-                inv[1][2] = -(J[0][0] * J[1][2] - J[1][0] * J[0][2]) * di;
-                inv[2][0] = (J[1][0] * J[2][1] - J[2][0] * J[1][1]) * di;
-                inv[2][1] = -(J[0][0] * J[2][1] - J[2][0] * J[0][1]) * di;
-                inv[2][2] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) * di;
-            }
-            jxw[q] = det * tw[q];
-#pragma unroll
-            for (int i = 0; i < NSD; ++i)
-#pragma unroll
-                for (int j = 0; j < NSD; ++j) Ji[9 * q + 3 * i + j] = inv[i][j];
-        }
-        __syncthreads();
-        for (int idx = threadIdx.x; idx < nq * nen; idx += blockDim.x) {
-            const int q = idx / nen;
-            const double *d = tdN + (size_t)idx * tdim;
-#pragma unroll
-            for (int dd = 0; dd < NSD; ++dd) {
-                double s = 0;
-#pragma unroll
-                for (int j = 0; j < NSD; ++j) s += Ji[9 * q + 3 * j + dd] * d[j];
-                G[(size_t)idx * NSD + dd] = s;
-            }
-        }
-        __syncthreads();
+        cell_gradients<NSD>(xe, tdN, tw, nen, nq, tdim, G, jxw, Ji);
         // qg[(q*DPN + comp)*NSD + i] = sum over the cell's nodes A of u(A, comp) dN_A/dx_i at q
         for (int idx = threadIdx.x; idx < nq * DPN * NSD; idx += blockDim.x) {
             const int q = idx / (DPN * NSD), comp = (idx / NSD) % DPN, i = idx % NSD;
@@ -1059,6 +1071,139 @@ k_smooth_gradient(const int32_t *__restrict__ order, int ncell, const int32_t *_
             for (int i = 0; i < NSD; ++i) vtg[g * NSD + i] += w[i];
         }
         __syncthreads();
+    }
+}
+
+// ZZGradientRecovery<Physics> (include/assembly/ZZGradientRecovery.hpp:33-140), p = 1:
+// every node fits a linear polynomial a_0 + a.(x - x_n) by least squares to the
+// FE gradient sampled at the quadrature points of the cells around it; the
+// recovered gradient is a_0.  Centred coordinates give the same fit as the
+// reference's [1 x y z] basis with a better conditioned system.  This kernel
+// accumulates, per node, the normal equations of its patch: the symmetric
+// (NSD+1)^2 matrix sum P^T P (packed upper triangle) and P^T g (NSD+1 rows of
+// NSD), P = [1, x_q - x_n].  One CTA per cell of one colour, as in
+// k_smooth_gradient, so the sums need no atomics and are deterministic.
+template <int NSD>
+__global__ void __launch_bounds__(128)
+k_zz_accumulate(const int32_t *__restrict__ order, int ncell, const int32_t *__restrict__ off,
+                const int32_t *__restrict__ el, const double *__restrict__ nodes, const double *__restrict__ tab,
+                int nen, int nq, int tdim, const double *__restrict__ sol, double *__restrict__ acc) {
+    constexpr int NB = NSD + 1, NM = NB * (NB + 1) / 2, NA = NM + NB * NSD;
+    extern __shared__ double sm[];
+    double *xe = sm;                           // nen*3
+    double *G = xe + 3 * nen;                  // nq*nen*NSD
+    double *jxw = G + (size_t)nq * nen * NSD;  // nq
+    double *Ji = jxw + nq;                     // nq*9
+    double *ul = Ji + 9 * nq;                  // nen
+    double *qg = ul + nen;                     // nq*NSD: field gradient at q
+    double *xq = qg + (size_t)nq * NSD;        // nq*3: point location
+    int32_t *gn = reinterpret_cast<int32_t *>(xq + (size_t)nq * 3);  // nen
+    const double *tN = tab;
+    const double *tdN = tab + (size_t)nq * nen;
+    const double *tw = tdN + (size_t)nq * nen * tdim;
+    for (int t = blockIdx.x; t < ncell; t += gridDim.x) {
+        const int c = order[t];
+        const int base = off[c];
+        for (int a = threadIdx.x; a < nen; a += blockDim.x) {
+            const int n = el[base + a];
+            gn[a] = n;
+            xe[3 * a + 0] = nodes[3 * (int64_t)n + 0];
+            xe[3 * a + 1] = nodes[3 * (int64_t)n + 1];
+            xe[3 * a + 2] = nodes[3 * (int64_t)n + 2];
+        }
+        __syncthreads();
+        for (int a = threadIdx.x; a < nen; a += blockDim.x) ul[a] = sol[gn[a]];
+        cell_gradients<NSD>(xe, tdN, tw, nen, nq, tdim, G, jxw, Ji);
+        // sample point x_q = sum_A N_A x_A and field gradient sum_A u_A dN_A/dx
+        for (int idx = threadIdx.x; idx < nq * 3; idx += blockDim.x) {
+            const int q = idx / 3, k = idx % 3;
+            double s = 0;
+            for (int A = 0; A < nen; ++A) s += tN[(size_t)q * nen + A] * xe[3 * A + k];
+            xq[idx] = s;
+        }
+        for (int idx = threadIdx.x; idx < nq * NSD; idx += blockDim.x) {
+            const int q = idx / NSD, i = idx % NSD;
+            double s = 0;
+            for (int A = 0; A < nen; ++A) s += ul[A] * G[((size_t)q * nen + A) * NSD + i];
+            qg[idx] = s;
+        }
+        __syncthreads();
+        // node A of the cell: its patch rows, one per quadrature point
+        for (int A = threadIdx.x; A < nen; A += blockDim.x) {
+            double a[NA];
+#pragma unroll
+            for (int k = 0; k < NA; ++k) a[k] = 0;
+            for (int q = 0; q < nq; ++q) {
+                double P[NB];
+                P[0] = 1;
+#pragma unroll
+                for (int i = 0; i < NSD; ++i) P[i + 1] = xq[3 * q + i] - xe[3 * A + i];
+                int k = 0;
+#pragma unroll
+                for (int r = 0; r < NB; ++r)
+#pragma unroll
+                    for (int cc = r; cc < NB; ++cc) a[k++] += P[r] * P[cc];
+#pragma unroll
+                for (int r = 0; r < NB; ++r)
+#pragma unroll
+                    for (int i = 0; i < NSD; ++i) a[NM + r * NSD + i] += P[r] * qg[q * NSD + i];
+            }
+            double *dst = acc + (int64_t)gn[A] * NA;
+#pragma unroll
+            for (int k = 0; k < NA; ++k) dst[k] += a[k];
+        }
+        __syncthreads();
+    }
+}
+
+// Per node: solve the (NSD+1)^2 normal equations by Cholesky and keep the
+// constant term of each of the NSD fits.  A node with too few samples (a
+// singular system) gets NaN; a node no cell of the dimension touches gets 0/0.
+template <int NSD>
+__global__ void k_zz_solve(int64_t n, const double *__restrict__ acc, double *__restrict__ grad) {
+    constexpr int NB = NSD + 1, NM = NB * (NB + 1) / 2, NA = NM + NB * NSD;
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
+        const double *a = acc + v * NA;
+        double L[NB][NB], y[NB][NSD];
+        int k = 0;
+#pragma unroll
+        for (int r = 0; r < NB; ++r)
+#pragma unroll
+            for (int cc = r; cc < NB; ++cc) { L[cc][r] = a[k]; ++k; }  // lower triangle of the symmetric matrix
+#pragma unroll
+        for (int j = 0; j < NB; ++j) {
+            double d = L[j][j];
+#pragma unroll
+            for (int m = 0; m < j; ++m) d -= L[j][m] * L[j][m];
+            d = sqrt(d);
+            L[j][j] = d;
+#pragma unroll
+            for (int i = j + 1; i < NB; ++i) {
+                double s = L[i][j];
+#pragma unroll
+                for (int m = 0; m < j; ++m) s -= L[i][m] * L[j][m];
+                L[i][j] = s / d;
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < NSD; ++i) {
+            double z[NB];
+#pragma unroll
+            for (int r = 0; r < NB; ++r) {  // L z = P^T g
+                double s = a[NM + r * NSD + i];
+#pragma unroll
+                for (int m = 0; m < r; ++m) s -= L[r][m] * z[m];
+                z[r] = s / L[r][r];
+            }
+#pragma unroll
+            for (int r = NB - 1; r >= 0; --r) {  // L^T y = z
+                double s = z[r];
+#pragma unroll
+                for (int m = r + 1; m < NB; ++m) s -= L[m][r] * y[m][i];
+                y[r][i] = s / L[r][r];
+            }
+            grad[v * NSD + i] = y[0][i];
+        }
     }
 }
 
@@ -1100,7 +1245,64 @@ static yg_status smooth_gradient_dpn(yg_context ctx, const ElementGroup &g, yg_d
     return launch_smooth_gradient<NSD, 3>(ctx, g, d, sol, vol, vtg);
 }
 
+template <int NSD>
+static yg_status launch_zz(yg_context ctx, const ElementGroup &g, yg_dofmap d, const double *sol, double *acc) {
+    const int nen = g.tab.nen, nq = g.tab.nq;
+    const size_t smem = sizeof(double) * (3 * nen + (size_t)nq * nen * NSD + nq + 9 * nq + nen + (size_t)nq * NSD +
+                                          (size_t)nq * 3) + sizeof(int32_t) * nen + 16;
+    auto kern = k_zz_accumulate<NSD>;
+    if (smem > ctx->smem_optin)
+        return fail(YG_UNSUPPORTED, "ZZGradientRecovery: element (nen %d, nq %d) needs %zu B of shared memory", nen, nq,
+                    smem);
+    if (smem > 48 * 1024) YG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    for (size_t c = 0; c + 1 < g.color_ptr.size(); ++c) {
+        const int n = g.color_ptr[c + 1] - g.color_ptr[c];
+        if (n == 0) continue;
+        const int grid = std::min(n, ctx->num_sms * 16);
+        kern<<<grid, 128, smem, ctx->stream>>>(g.d_order + g.color_ptr[c], n, d->d_offsets, d->d_elements, d->d_nodes,
+                                               g.d_tab, nen, nq, g.tab.dim, sol, acc);
+        YG_LAUNCHED(ctx);
+    }
+    YG_CUDA(cudaGetLastError());
+    return YG_OK;
+}
+
 }  // namespace yg
+
+extern "C" yg_status yg_zz_gradient_recovery(yg_dofmap d, int32_t nsd, yg_vector solution, yg_vector gradient) {
+    if (!d || !solution || !gradient) return fail(YG_BAD_ARG, "yg_zz_gradient_recovery: NULL argument");
+    if (nsd < 2 || nsd > 3) return fail(YG_BAD_ARG, "yg_zz_gradient_recovery: nsd must be 2 or 3");
+    yg_context ctx = d->ctx;
+    if (!ctx) return fail(YG_BAD_ARG, "yg_zz_gradient_recovery: dofmap was created without a context");
+    // the reference asserts p = 1 (ZZGradientRecovery.hpp:44) and reads one dof per node
+    if (d->host.poly_order != 1 || d->host.dof_per_node != 1)
+        return fail(YG_UNSUPPORTED, "ZZGradientRecovery: p = 1 and one dof per node only (got p %d, dpn %d)",
+                    d->host.poly_order, d->host.dof_per_node);
+    const int64_t nn = d->host.n_nodes();
+    if (solution->n != nn || gradient->n != nn * nsd)
+        return fail(YG_BAD_ARG, "yg_zz_gradient_recovery: solution needs %lld entries, gradient %lld", (long long)nn,
+                    (long long)(nn * nsd));
+    YG_TRY(build_pattern(d, nsd));
+    const int na = (nsd + 1) * (nsd + 2) / 2 + (nsd + 1) * nsd;
+    double *acc = nullptr;
+    YG_TRY(dev_alloc_t(ctx, &acc, nn * na));
+    yg_status s = YG_OK;
+    cudaError_t e = cudaMemsetAsync(acc, 0, sizeof(double) * nn * na, ctx->stream);
+    if (e != cudaSuccess) s = fail(YG_CUDA_ERROR, "ZZGradientRecovery: %s", cudaGetErrorString(e));
+    for (const ElementGroup &g : d->groups) {
+        if (s != YG_OK) break;
+        s = nsd == 2 ? launch_zz<2>(ctx, g, d, solution->d, acc) : launch_zz<3>(ctx, g, d, solution->d, acc);
+    }
+    if (s == YG_OK && nn > 0) {
+        if (nsd == 2) k_zz_solve<2><<<stream_grid(ctx, nn), kThreads, 0, ctx->stream>>>(nn, acc, gradient->d);
+        else k_zz_solve<3><<<stream_grid(ctx, nn), kThreads, 0, ctx->stream>>>(nn, acc, gradient->d);
+        YG_LAUNCHED(ctx);
+    }
+    dev_free(ctx, acc);
+    if (s != YG_OK) return s;
+    YG_CUDA(cudaGetLastError());
+    return YG_OK;
+}
 
 extern "C" yg_status yg_local_smoothing_gradient(yg_dofmap d, int32_t nsd, yg_vector solution, yg_vector gradient) {
     if (!d || !solution || !gradient) return fail(YG_BAD_ARG, "yg_local_smoothing_gradient: NULL argument");
