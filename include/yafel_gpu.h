@@ -189,6 +189,20 @@ YG_API yg_status yg_zz_gradient_recovery(yg_dofmap d, int32_t nsd, yg_vector sol
 YG_API yg_status yg_dirichlet_apply(yg_matrix K, yg_vector rhs, const int64_t *bc_dofs,
                              const double *bc_values, int64_t n_bc);
 
+/* ------------------------------------------------------------------ output */
+
+/* SimulationOutput(fname_base, BackendType::VTU).captureFrame(FESystem&) with the
+ * default capture (include/output/SimulationOutput.hpp:47-116,
+ * src/output/VTUBackend.cpp:20-269, src/output/OutputMesh.cpp:10-50): writes
+ * fname_base.vtu, an ASCII UnstructuredGrid of the dof nodes and the linear
+ * sub-cells of every element, with the components of `solution` (device, NULL
+ * for the mesh alone) as scalar arrays Solution_0.. -- point data when it holds
+ * dof_per_node values per dof node, cell data when it holds dof_per_node values
+ * per cell.  The text is the reference's character for character (six
+ * significant digits).  The vector is copied off the device in chunks through
+ * pinned buffers.  The HDF5 backend is not provided (no HDF5 library here). */
+YG_API yg_status yg_output_vtu(yg_dofmap d, const char *fname_base, yg_vector solution);
+
 /* ------------------------------------------------------------------ matrices */
 
 /* sparse_csr<T>(triplets) for block=1 (include/old_handmade_linalg/sparse_csr.hpp:90-149)

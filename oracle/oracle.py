@@ -182,6 +182,7 @@ def ref():
         R.refa_local_smoothing_gradient.argtypes = [C.c_void_p, C.c_int, f64p, f64p]
         R.refa_element.argtypes = [C.c_int] * 4 + [C.POINTER(C.c_int)] * 2 + [C.c_void_p] * 5
         R.refa_zz_gradient.argtypes = [C.c_void_p, C.c_int, f64p, f64p]
+        R.refa_write_vtu.argtypes = [C.c_void_p, C.c_char_p, C.c_void_p, C.c_int]
         _REF = R
     return _REF
 
@@ -303,6 +304,15 @@ class RefSystem:
         out = np.zeros((self.n, nsd))
         ref().refa_local_smoothing_gradient(self.h, nsd, np.ascontiguousarray(sol, dtype=np.float64), out)
         return out
+
+    def write_vtu(self, fname_base, sol=None):
+        """SimulationOutput(fname_base, VTU).captureFrame(system) (default capture
+        of `sol`, or no data); returns the file's text."""
+        a = None if sol is None else np.ascontiguousarray(sol, dtype=np.float64)
+        ref().refa_write_vtu(self.h, fname_base.encode(), None if a is None else a.ctypes.data_as(C.c_void_p),
+                             0 if a is None else 1)
+        with open(fname_base + ".vtu") as f:
+            return f.read()
 
     def zz_gradient(self, nsd, sol):
         """ZZGradientRecovery (include/assembly/ZZGradientRecovery.hpp:33-140): the

@@ -14,6 +14,7 @@
 //   include/boundary_conditions/DirichletBC.hpp:80-89 selectByFunction
 //   include/assembly/LocalSmoothingGradient.hpp:20-94 LocalSmoothingGradient<Physics>
 //   include/assembly/ZZGradientRecovery.hpp:33-140   ZZGradientRecovery<Physics>
+//   src/output/{SimulationOutput,OutputMesh,VTUBackend}.cpp  VTU output (default capture)
 //   apps/supg_learning/supg_advection.hpp:19-132     AdvectionDiffusionSUPG<NSD> (the physics itself)
 //
 // The Poisson and elasticity Physics structs of the reference live in the apps'
@@ -28,6 +29,7 @@
 #include "boundary_conditions/DirichletBC.hpp"
 #include "fe_system/FESystem.hpp"
 #include "mesh/Mesh.hpp"
+#include "output/SimulationOutput.hpp"
 #include "utils/DoFManager.hpp"
 #include "supg_learning/supg_advection.hpp"
 
@@ -342,6 +344,23 @@ void refa_zz_gradient(void *h, int nsd, const double *solution, double *gradient
     auto &G = s.getSolutionGradient();
     for (Eigen::Index i = 0; i < G.rows(); ++i)
         for (int d = 0; d < nsd; ++d) gradient[i * nsd + d] = G(i, d);
+}
+
+// SimulationOutput(fname_base, VTU).captureFrame(sys) with the default capture
+// of the system's solution (with_solution) or a capture that adds no data.
+void refa_write_vtu(void *h, const char *fname_base, const double *solution, int with_solution) {
+    auto &s = static_cast<RefSystem *>(h)->sys;
+    if (with_solution) {
+        auto &U = s.getSolution();
+        for (Eigen::Index i = 0; i < U.rows(); ++i) U(i) = solution[i];
+    }
+    SimulationOutput out(fname_base, BackendType::VTU);
+    if (with_solution) {
+        out.captureFrame(s);
+    } else {
+        std::function<void(FESystem &, OutputFrame &)> none = [](FESystem &, OutputFrame &) {};
+        out.captureFrame(s, none);
+    }
 }
 
 }  // extern "C"

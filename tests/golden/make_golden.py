@@ -8,9 +8,10 @@ own tests use (test/test_sparse_csr.cpp, test_sparse_bcsr.cpp,
 test_cg_solve.cpp, test_bicgstab_solve.cpp, test_ILU.cpp) and on a small
 assembled Poisson system (linalg.npz, quadrature.npz, poisson8.npz); and its
 assembly half -- Element tables, DoFManager numbering, CGAssembly values and
-residuals, DirichletBC::apply, LocalSmoothingGradient and ZZGradientRecovery
--- on small seeded quadrilateral, triangle, mixed, hexahedron and tetrahedron
-meshes at orders 1-3 (elements.npz, assembly_ref.npz, zz_ref.npz), built
+residuals, DirichletBC::apply, LocalSmoothingGradient, ZZGradientRecovery and
+the VTU writer's text -- on small seeded quadrilateral, triangle, mixed,
+hexahedron and tetrahedron meshes at orders 1-3 (elements.npz,
+assembly_ref.npz, zz_ref.npz, vtu_ref.npz), built
 against the from-scratch Eigen-API subset in oracle/ref_compat (Eigen itself is
 not installed).
 They pin the oracle without the reference tree being present.
@@ -261,6 +262,31 @@ def zz():
     np.savez_compressed(os.path.join(HERE, "zz_ref.npz"), **out)
 
 
+VTU_CASES = [("quad", 2, 1), ("mixed", 3, 1), ("tri", 1, 1), ("hex", 2, 3), ("tet", 2, 1)]
+
+
+def vtu():
+    """The reference's SimulationOutput(VTU).captureFrame text, mesh only and with
+    the default capture of a solution (dof_per_node components)."""
+    import tempfile
+    out = {}
+    with tempfile.TemporaryDirectory() as tmp:
+        for kind, p, dpn in VTU_CASES:
+            mesh, nsd = assembly_meshes(kind, p)
+            dm = O.RefDofManager(mesh, p, dpn)
+            phys = O.ELASTICITY if dpn > 1 else O.POISSON
+            sysm = O.RefSystem(dm, nsd, phys, [1.0, 1.0, 1.0])
+            u = np.stack([smooth_field(dm.nodes, c) for c in range(dpn)], axis=1).ravel()
+            k = "%s_p%d/" % (kind, p)
+            for key in ("nodes", "cell_nodes", "offsets", "cell_types"):
+                out[k + "mesh_" + key] = mesh[key]
+            out[k + "meta"] = np.array([p, dpn])
+            out[k + "u"] = u
+            out[k + "text_mesh"] = np.array(sysm.write_vtu(os.path.join(tmp, "m")))
+            out[k + "text_solution"] = np.array(sysm.write_vtu(os.path.join(tmp, "s"), u))
+    np.savez_compressed(os.path.join(HERE, "vtu_ref.npz"), **out)
+
+
 if __name__ == "__main__":
     O.build()
     if not O.ref_available():
@@ -271,4 +297,5 @@ if __name__ == "__main__":
     elements()
     assembly()
     zz()
+    vtu()
     print("golden fixtures written to", HERE)

@@ -558,6 +558,23 @@ def ZZGradientRecovery(physics, feSystem):
     return feSystem
 
 
+class SimulationOutput:
+    """SimulationOutput(fname_base, BackendType::VTU) (include/output/SimulationOutput.hpp:22-116):
+    captureFrame(feSystem) writes fname_base.vtu -- the dof nodes, the linear
+    sub-cells of every element and the solution's components as Solution_0..
+    (the reference's default capture), in the reference's ASCII format."""
+
+    def __init__(self, fname_base="output", backend="VTU"):
+        if backend != "VTU":
+            raise ValueError("only the VTU backend is provided (no HDF5 library)")
+        self.fname_base = fname_base
+
+    def captureFrame(self, feSystem, solution=None):
+        sol = feSystem.solution if solution is None else solution
+        check(lib().yg_output_vtu(feSystem.dofm.h, self.fname_base.encode(), sol.h if sol is not None else None),
+              "SimulationOutput.captureFrame")
+
+
 class DirichletBC:
     """DirichletBC(dofm, value, comp) (include/boundary_conditions/DirichletBC.hpp:23-89);
     value is a number or a function f(x, t)."""

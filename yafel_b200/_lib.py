@@ -57,6 +57,7 @@ SIGNATURES = {
     "yg_dofmap_create_from_numbering": (i32, [vp, vp, i32, vp, vp, vp, i32, i32, i32, P(vp)]),
     "yg_element_table": (i32, [i32, i32, i32, P(i32), P(i32), vp, vp, vp, vp, vp]),
     "yg_zz_gradient_recovery": (i32, [vp, i32, vp, vp]),
+    "yg_output_vtu": (i32, [vp, C.c_char_p, vp]),
     "yg_assemble": (i32, [vp, P(Physics), u32, i32, P(vp), vp]),
     "yg_dirichlet_apply": (i32, [vp, vp, vp, vp, i64]),
     "yg_matrix_from_triplets": (i32, [vp, i32, vp, vp, vp, u64, P(vp)]),

@@ -651,6 +651,8 @@ __global__ void k_bc_zero(int64_t nbrows, int B, const int32_t *__restrict__ rp,
     }
 }
 
+const HostDofmap &dofmap_host(yg_dofmap d) { return d->host; }
+
 }  // namespace yg
 
 using namespace yg;
