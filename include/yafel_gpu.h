@@ -48,6 +48,7 @@ typedef struct yg_dofmap_t *yg_dofmap;
 typedef struct yg_matrix_t *yg_matrix;
 typedef struct yg_vector_t *yg_vector;
 typedef struct yg_precond_t *yg_precond;
+typedef struct yg_mesh_t *yg_mesh;
 
 /* ------------------------------------------------------------------ context */
 
@@ -81,7 +82,26 @@ YG_API yg_status yg_vector_axpy(double alpha, yg_vector x, yg_vector y);
 /* ------------------------------------------------------------------ DoFManager */
 
 /* Mesh cell types use the reference's CellType codes (include/mesh/mesh_typedefs.hpp:42-50). */
-enum { YG_CELL_LINE2 = 0, YG_CELL_TRI3 = 1, YG_CELL_TET4 = 2, YG_CELL_QUAD4 = 3, YG_CELL_HEX8 = 4, YG_CELL_POINT1 = 5 };
+enum { YG_CELL_LINE2 = 0, YG_CELL_TRI3 = 1, YG_CELL_TET4 = 2, YG_CELL_QUAD4 = 3, YG_CELL_HEX8 = 4, YG_CELL_POINT1 = 5,
+       YG_CELL_NONE = 6 };
+
+/* Mesh(const std::string &fname) (include/mesh/Mesh.hpp:56-59, src/mesh/parse_gmsh.cpp:80-193):
+ * reads a Gmsh 2.x ASCII file ($Nodes, $Elements; other sections skipped) into
+ * host arrays in the layout of Mesh(DefinitionScheme::Explicit, ...): node id-1
+ * gets its coordinates, element id-1 its CellType (Gmsh 1/2/3/4/5/15 ->
+ * Line2/Tri3/Quad4/Tet4/Hex8/Point1, else None), tags and node count, the node
+ * lists follow in file order, 0-based.  YG_BAD_ARG names the offending line. */
+YG_API yg_status yg_mesh_read_gmsh(const char *path, yg_mesh *out);
+/* Sizes: nodes, cells, entries of the cell-node list, entries of the tag list. */
+YG_API yg_status yg_mesh_sizes(yg_mesh m, int32_t *n_nodes, int32_t *n_cells, int64_t *n_cell_nodes,
+                        int64_t *n_tags);
+/* Copies of the arrays (any pointer may be NULL): nodes (3 per node), cell nodes,
+ * cell offsets (n_cells+1), CellType codes, and each cell's tags as
+ * tags[tag_offsets[c] .. tag_offsets[c+1]) (Mesh::getCellTags; the first tag is
+ * the region id DoFManager keeps, DoFManager.cpp:22-25). */
+YG_API yg_status yg_mesh_get(yg_mesh m, double *nodes_xyz, int32_t *cell_nodes, int32_t *cell_offsets,
+                      int32_t *cell_types, int32_t *tag_offsets, int32_t *tags);
+YG_API yg_status yg_mesh_destroy(yg_mesh m);
 /* Element topologies (include/element/ElementType.hpp:22-27). */
 enum { YG_TOPO_TENSOR = 0, YG_TOPO_SIMPLEX = 1, YG_TOPO_NONE = 2 };
 

@@ -183,6 +183,7 @@ def ref():
         R.refa_element.argtypes = [C.c_int] * 4 + [C.POINTER(C.c_int)] * 2 + [C.c_void_p] * 5
         R.refa_zz_gradient.argtypes = [C.c_void_p, C.c_int, f64p, f64p]
         R.refa_write_vtu.argtypes = [C.c_void_p, C.c_char_p, C.c_void_p, C.c_int]
+        R.refa_read_gmsh.argtypes = [C.c_char_p] + [C.POINTER(C.c_int)] * 4 + [C.c_void_p] * 6
         _REF = R
     return _REF
 
@@ -200,6 +201,26 @@ def ref_element(topology, dim, p, qrm=2):
     ptr = lambda x: x.ctypes.data_as(C.c_void_p)
     R.refa_element(topology, dim, p, qrm, C.byref(nen), C.byref(nq), ptr(L), ptr(X), ptr(W), ptr(N), ptr(dN))
     return L, X, W, N, dN
+
+
+def ref_read_gmsh(path):
+    """The reference's Mesh(fname) (src/mesh/parse_gmsh.cpp): dict of nodes,
+    cell_nodes, offsets, cell_types, tag_offsets, tags."""
+    R = ref()
+    a, b, c, d = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+    if R.refa_read_gmsh(path.encode(), C.byref(a), C.byref(b), C.byref(c), C.byref(d), None, None, None, None,
+                        None, None):
+        raise RuntimeError("Mesh::parse_gmsh failed")
+    out = {"nodes": np.zeros((a.value, 3)), "cell_nodes": np.zeros(max(1, c.value), np.int32),
+           "offsets": np.zeros(b.value + 1, np.int32), "cell_types": np.zeros(max(1, b.value), np.int32),
+           "tag_offsets": np.zeros(b.value + 1, np.int32), "tags": np.zeros(max(1, d.value), np.int32)}
+    ptr = lambda x: x.ctypes.data_as(C.c_void_p)
+    R.refa_read_gmsh(path.encode(), C.byref(a), C.byref(b), C.byref(c), C.byref(d), ptr(out["nodes"]),
+                     ptr(out["cell_nodes"]), ptr(out["offsets"]), ptr(out["cell_types"]), ptr(out["tag_offsets"]),
+                     ptr(out["tags"]))
+    out["cell_nodes"], out["cell_types"] = out["cell_nodes"][:c.value], out["cell_types"][:b.value]
+    out["tags"] = out["tags"][:d.value]
+    return out
 
 
 class RefDofManager:

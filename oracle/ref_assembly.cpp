@@ -186,6 +186,36 @@ void refa_set_threads(int n) {
 #endif
 }
 
+// Mesh(const std::string &fname) (parse_gmsh.cpp:80-171): sizes, then arrays
+// (call with NULL arrays first).  tag_offsets/tags hold each cell's tags.
+int refa_read_gmsh(const char *path, int *n_nodes, int *n_cells, int *n_cell_nodes, int *n_tags, double *xyz,
+                   int *cell_nodes, int *offsets, int *types, int *tag_offsets, int *tags) {
+    try {
+        Mesh m{std::string(path)};
+        *n_nodes = m.nNodes();
+        *n_cells = m.nCells();
+        *n_cell_nodes = static_cast<int>(m.getCellVector().size());
+        int nt = 0;
+        for (int c = 0; c < m.nCells(); ++c) nt += static_cast<int>(m.getCellTags(c).size());
+        *n_tags = nt;
+        if (!xyz) return 0;
+        for (int i = 0; i < m.nNodes(); ++i)
+            for (int k = 0; k < 3; ++k) xyz[3 * i + k] = m.getGeometryNodes()[i](k);
+        for (std::size_t i = 0; i < m.getCellVector().size(); ++i) cell_nodes[i] = m.getCellVector()[i];
+        for (std::size_t i = 0; i < m.getOffsetVector().size(); ++i) offsets[i] = m.getOffsetVector()[i];
+        int k = 0;
+        tag_offsets[0] = 0;
+        for (int c = 0; c < m.nCells(); ++c) {
+            types[c] = static_cast<int>(m.getCellType(c));
+            for (int t : m.getCellTags(c)) tags[k++] = t;
+            tag_offsets[c + 1] = k;
+        }
+        return 0;
+    } catch (...) {
+        return 1;
+    }
+}
+
 // Mesh(DefinitionScheme::Explicit, nodes, cells, offsets, types, tags) + DoFManager(M, CG, p, dpn).
 void *refa_dofmanager(const double *xyz, int n_nodes, const int *cells, const int *offsets, const int *types,
                       int n_cells, int p, int dpn) {

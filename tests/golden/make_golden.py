@@ -9,9 +9,10 @@ test_cg_solve.cpp, test_bicgstab_solve.cpp, test_ILU.cpp) and on a small
 assembled Poisson system (linalg.npz, quadrature.npz, poisson8.npz); and its
 assembly half -- Element tables, DoFManager numbering, CGAssembly values and
 residuals, DirichletBC::apply, LocalSmoothingGradient, ZZGradientRecovery and
-the VTU writer's text -- on small seeded quadrilateral, triangle, mixed,
-hexahedron and tetrahedron meshes at orders 1-3 (elements.npz,
-assembly_ref.npz, zz_ref.npz, vtu_ref.npz), built
+the VTU writer's text, and its Gmsh reader on files written here -- on small
+seeded quadrilateral, triangle, mixed, hexahedron and tetrahedron meshes at
+orders 1-3 (elements.npz, assembly_ref.npz, zz_ref.npz, vtu_ref.npz,
+gmsh_ref.npz), built
 against the from-scratch Eigen-API subset in oracle/ref_compat (Eigen itself is
 not installed).
 They pin the oracle without the reference tree being present.
@@ -287,6 +288,65 @@ def vtu():
     np.savez_compressed(os.path.join(HERE, "vtu_ref.npz"), **out)
 
 
+GMSH_TYPE = {0: 1, 1: 2, 3: 3, 2: 4, 4: 5, 5: 15}  # CellType code -> Gmsh element type
+
+
+def gmsh_text(mesh, extra_cells=(), seed=0):
+    """A Gmsh 2.2 ASCII file of `mesh` (written here, not taken from the
+    reference): a $MeshFormat header, $Nodes with 17 significant digits, and
+    $Elements with two tags each (physical, elementary) -- the mesh's cells, then
+    `extra_cells` (cell type code or raw Gmsh type as ("gmsh", t), node list)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    X = mesh["nodes"]
+    lines = ["$MeshFormat", "2.2 0 8", "$EndMeshFormat", "$Nodes", str(X.shape[0])]
+    lines += ["%d %.17g %.17g %.17g" % (i + 1, x, y, z) for i, (x, y, z) in enumerate(X)]
+    lines += ["$EndNodes"]
+    cells = []
+    off, cn, ct = mesh["offsets"], mesh["cell_nodes"], mesh["cell_types"]
+    for c in range(ct.size):
+        cells.append((GMSH_TYPE[int(ct[c])], list(cn[off[c]:off[c + 1]])))
+    for t, nodes in extra_cells:
+        cells.append((t[1] if isinstance(t, tuple) else GMSH_TYPE[t], list(nodes)))
+    lines += ["$Elements", str(len(cells))]
+    for i, (t, nodes) in enumerate(cells):
+        tags = rng.integers(1, 9, 2)
+        lines.append("%d %d 2 %d %d " % (i + 1, t, tags[0], tags[1]) + " ".join(str(n + 1) for n in nodes))
+    lines += ["$EndElements", "$PhysicalNames", "1", "2 1 \"domain\"", "$EndPhysicalNames"]
+    return "\n".join(lines) + "\n"
+
+
+def gmsh():
+    """The reference's Mesh(fname) on Gmsh files written by gmsh_text: a mixed
+    tri+quad mesh with boundary Line2 and corner Point1 cells, a hexahedron mesh,
+    a tetrahedron mesh and a file holding a second-order line (unknown to the
+    reference: CellType None); plus the reference's DoFManager numbering of the
+    mixed mesh at p = 2 (lower-dimensional cells included)."""
+    import tempfile
+    out = {}
+    m2 = meshgen.jittered_mixed(4, 3, seed=9, order="ccw")
+    X = m2["nodes"]
+    bottom = np.nonzero(np.abs(X[:, 1]) < 1e-12)[0]
+    bottom = bottom[np.argsort(X[bottom, 0])]
+    extra2 = [(0, [bottom[i], bottom[i + 1]]) for i in range(bottom.size - 1)] + [(5, [0]), (5, [4])]
+    files = {"mixed2d": gmsh_text(m2, extra2, seed=1),
+             "hex": gmsh_text(meshgen.structured_hex(2, 2, 1, order="ccw"), seed=2),
+             "tet": gmsh_text(meshgen.structured_tet(1, 2, 1, seed=3, jitter=0.1), seed=3),
+             "unknown_type": gmsh_text(meshgen.structured_quad(2, 1, order="ccw"), [(("gmsh", 8), [0, 1, 2])], seed=4)}
+    with tempfile.TemporaryDirectory() as tmp:
+        for name, text in files.items():
+            path = os.path.join(tmp, name + ".msh")
+            with open(path, "w") as f:
+                f.write(text)
+            r = O.ref_read_gmsh(path)
+            out[name + "/text"] = np.array(text)
+            for key, v in r.items():
+                out[name + "/" + key] = v
+        mesh = {k: out["mixed2d/" + k] for k in ("nodes", "cell_nodes", "offsets", "cell_types")}
+        dm = O.RefDofManager(mesh, 2, 1)
+        out["mixed2d/p2_dof_nodes"], out["mixed2d/p2_offsets"], out["mixed2d/p2_elements"] = dm.nodes, dm.offsets, dm.elements
+    np.savez_compressed(os.path.join(HERE, "gmsh_ref.npz"), **out)
+
+
 if __name__ == "__main__":
     O.build()
     if not O.ref_available():
@@ -298,4 +358,5 @@ if __name__ == "__main__":
     assembly()
     zz()
     vtu()
+    gmsh()
     print("golden fixtures written to", HERE)

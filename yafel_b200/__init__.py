@@ -160,6 +160,35 @@ class Mesh:
     def from_dict(cls, m):
         return cls(m["nodes"], m["cell_nodes"], m["offsets"], m["cell_types"], m.get("cell_tags"))
 
+    @classmethod
+    def from_gmsh(cls, path):
+        """Mesh(const std::string &fname) (src/mesh/parse_gmsh.cpp:80-193): a Gmsh
+        2.x ASCII file; cell_tags holds each cell's first tag (its region id) and
+        tags_all the full per-cell tag lists."""
+        h = C.c_void_p()
+        check(lib().yg_mesh_read_gmsh(str(path).encode(), C.byref(h)), "Mesh(gmsh)")
+        try:
+            a, b, c, d = C.c_int32(), C.c_int32(), C.c_int64(), C.c_int64()
+            check(lib().yg_mesh_sizes(h, C.byref(a), C.byref(b), C.byref(c), C.byref(d)))
+            nodes = np.zeros((a.value, 3))
+            cn = np.zeros(max(1, c.value), np.int32)
+            off = np.zeros(b.value + 1, np.int32)
+            ct = np.zeros(max(1, b.value), np.int32)
+            to = np.zeros(b.value + 1, np.int32)
+            tg = np.zeros(max(1, d.value), np.int32)
+            check(lib().yg_mesh_get(h, _ptr(nodes), _ptr(cn), _ptr(off), _ptr(ct), _ptr(to), _ptr(tg)))
+        finally:
+            lib().yg_mesh_destroy(h)
+        tags = [tg[to[i]:to[i + 1]].copy() for i in range(b.value)]
+        first = np.array([t[0] if t.size else 0 for t in tags], np.int32)
+        m = cls(nodes, cn[:c.value], off, ct[:b.value], first)
+        m.tags_all = tags
+        return m
+
+    def to_dict(self):
+        return {"nodes": self.nodes, "cell_nodes": self.cell_nodes, "offsets": self.offsets,
+                "cell_types": self.cell_types, "cell_tags": self.cell_tags}
+
     def nCells(self):
         return int(self.cell_types.size)
 

@@ -58,6 +58,10 @@ SIGNATURES = {
     "yg_element_table": (i32, [i32, i32, i32, P(i32), P(i32), vp, vp, vp, vp, vp]),
     "yg_zz_gradient_recovery": (i32, [vp, i32, vp, vp]),
     "yg_output_vtu": (i32, [vp, C.c_char_p, vp]),
+    "yg_mesh_read_gmsh": (i32, [C.c_char_p, P(vp)]),
+    "yg_mesh_sizes": (i32, [vp, P(i32), P(i32), P(i64), P(i64)]),
+    "yg_mesh_get": (i32, [vp, vp, vp, vp, vp, vp, vp]),
+    "yg_mesh_destroy": (i32, [vp]),
     "yg_assemble": (i32, [vp, P(Physics), u32, i32, P(vp), vp]),
     "yg_dirichlet_apply": (i32, [vp, vp, vp, vp, i64]),
     "yg_matrix_from_triplets": (i32, [vp, i32, vp, vp, vp, u64, P(vp)]),
