@@ -117,6 +117,20 @@ YG_API yg_status yg_dofmap_create(yg_context ctx, const double *nodes_xyz, int32
                            const int32_t *cell_nodes, const int32_t *cell_offsets,
                            const int32_t *cell_types, int32_t n_cells, int32_t poly_order,
                            int32_t dof_per_node, yg_dofmap *out);
+/* The same numbering computed on the GPU whatever the mesh size (p > 1; p = 1
+ * keeps the mesh numbering): raw nodes, snapped keys, a stable radix sort and
+ * the merge run on the device, the result is also copied to the host.
+ * yg_dofmap_create does this by itself for meshes of more than 2^20 raw nodes
+ * (no simplex/tensor mix at p >= 3), where its host path uses the same stable
+ * order, so both give identical bits.  On smaller meshes the host keeps the
+ * coincident node that the reference's std::sort leaves first; this entry keeps
+ * the first in raw order, so merged coordinates can differ in the last bits
+ * (numbering identical).  YG_UNSUPPORTED if the snapped keys need more than 64
+ * bits. */
+YG_API yg_status yg_dofmap_create_on_device(yg_context ctx, const double *nodes_xyz, int32_t n_nodes,
+                                     const int32_t *cell_nodes, const int32_t *cell_offsets,
+                                     const int32_t *cell_types, int32_t n_cells, int32_t poly_order,
+                                     int32_t dof_per_node, yg_dofmap *out);
 YG_API yg_status yg_dofmap_destroy(yg_dofmap d);
 /* Sizes of dof_nodes, cells, the elements array, and dofs = dof_nodes*dof_per_node. */
 YG_API yg_status yg_dofmap_sizes(yg_dofmap d, int32_t *n_dof_nodes, int32_t *n_cells,

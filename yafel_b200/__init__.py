@@ -200,10 +200,12 @@ class DoFManager:
     """DoFManager(M, ManagerType::CG, polyOrder, dof_per_node)
     (src/utils/DoFManager.cpp:11-36); numbering identical to the reference's."""
 
-    def __init__(self, mesh, polyOrder=1, dof_per_node=1, ctx=None, host_only=False, numbering=None):
+    def __init__(self, mesh, polyOrder=1, dof_per_node=1, ctx=None, host_only=False, numbering=None,
+                 on_device=False):
         """numbering: optional (dof_nodes n x 3, element_offsets, elements) of a
         DoFManager the caller already built (the reference's own, say); the
-        mesh then only supplies the cell types."""
+        mesh then only supplies the cell types.  on_device: number on the GPU
+        whatever the size (yg_dofmap_create_on_device)."""
         if isinstance(mesh, dict):
             mesh = Mesh.from_dict(mesh)
         self.ctx = None if host_only else (ctx or default_context())
@@ -211,7 +213,8 @@ class DoFManager:
         h = C.c_void_p()
         cx = self.ctx.h if self.ctx else None
         if numbering is None:
-            check(lib().yg_dofmap_create(cx, _ptr(mesh.nodes), mesh.nNodes(), _ptr(mesh.cell_nodes),
+            fn = lib().yg_dofmap_create_on_device if on_device else lib().yg_dofmap_create
+            check(fn(cx, _ptr(mesh.nodes), mesh.nNodes(), _ptr(mesh.cell_nodes),
                                          _ptr(mesh.offsets), _ptr(mesh.cell_types), mesh.nCells(), int(polyOrder),
                                          int(dof_per_node), C.byref(h)), "DoFManager")
         else:

@@ -653,6 +653,11 @@ __global__ void k_bc_zero(int64_t nbrows, int B, const int32_t *__restrict__ rp,
 
 const HostDofmap &dofmap_host(yg_dofmap d) { return d->host; }
 
+yg_status number_on_device(yg_context ctx, const double *xyz, int32_t n_nodes, const int32_t *cell_nodes,
+                           const int32_t *cell_offsets, const int32_t *cell_types, int32_t n_cells,
+                           const RawLayout &lay, int64_t N, HostDofmap &d, double **d_nodes_out,
+                           int32_t **d_elements_out);  // dofmap_gpu.cu
+
 }  // namespace yg
 
 using namespace yg;
@@ -696,14 +701,12 @@ static int cell_corner_count(int32_t ct) {
     }
 }
 
-extern "C" yg_status yg_dofmap_create(yg_context ctx, const double *nodes_xyz, int32_t n_nodes,
-                                      const int32_t *cell_nodes, const int32_t *cell_offsets,
-                                      const int32_t *cell_types, int32_t n_cells, int32_t poly_order,
-                                      int32_t dof_per_node, yg_dofmap *out) {
-    if (!out || n_nodes < 0 || n_cells < 0 || (n_nodes && !nodes_xyz) || (n_cells && (!cell_offsets || !cell_types)))
+static yg_status check_mesh(const double *nodes_xyz, int32_t n_nodes, const int32_t *cell_nodes,
+                            const int32_t *cell_offsets, const int32_t *cell_types, int32_t n_cells, int32_t poly_order,
+                            int32_t dof_per_node) {
+    if (n_nodes < 0 || n_cells < 0 || (n_nodes && !nodes_xyz) || (n_cells && (!cell_offsets || !cell_types)))
         return fail(YG_BAD_ARG, "yg_dofmap_create: bad argument");
     if (dof_per_node < 1 || dof_per_node > 3) return fail(YG_BAD_ARG, "dof_per_node must be 1..3");
-    *out = nullptr;
     for (int32_t c = 0; c < n_cells; ++c) {
         if (cell_offsets[c + 1] < cell_offsets[c]) return fail(YG_BAD_ARG, "cell offsets decrease at cell %d", c);
         for (int32_t i = cell_offsets[c]; i < cell_offsets[c + 1]; ++i)
@@ -712,13 +715,83 @@ extern "C" yg_status yg_dofmap_create(yg_context ctx, const double *nodes_xyz, i
         if (poly_order > 1 && nc > 0 && cell_offsets[c + 1] - cell_offsets[c] < nc)
             return fail(YG_BAD_ARG, "cell %d has %d corners, its type needs %d", c, cell_offsets[c + 1] - cell_offsets[c], nc);
     }
+    return YG_OK;
+}
+
+// The numbering on the device: the host lays out the raw nodes (element types,
+// offsets, local node tables) and the device does the rest (dofmap_gpu.cu).
+// YG_UNSUPPORTED when the host must number instead: a mesh the reference's own
+// comparison sort must order (unless forced: then the stable order is kept),
+// or keys wider than 64 bits.
+static yg_status try_number_on_device(yg_dofmap d, const double *xyz, int32_t n_nodes, const int32_t *cell_nodes,
+                                      const int32_t *cell_offsets, const int32_t *cell_types, int32_t n_cells,
+                                      int32_t p, int32_t dpn, bool forced) {
+    HostDofmap &h = d->host;
+    h.dof_per_node = dpn;
+    h.poly_order = p;
+    h.offsets.assign(n_cells + 1, 0);
+    h.topology.resize(n_cells);
+    h.topo_dim.resize(n_cells);
+    h.porder.assign(n_cells, (int8_t)p);
+    for (int32_t c = 0; c < n_cells; ++c) {
+        int t, td;
+        cell_element_type(cell_types[c], t, td);
+        h.topology[c] = (int8_t)t;
+        h.topo_dim[c] = (int8_t)td;
+    }
+    RawLayout lay;
+    const int64_t N = raw_node_layout(n_cells, p, h, lay);
+    if (N == 0 || (!forced && raw_mix_needs_reference_order(h, N))) return YG_UNSUPPORTED;
+    yg_context ctx = d->ctx;
+    YG_TRY(number_on_device(ctx, xyz, n_nodes, cell_nodes, cell_offsets, cell_types, n_cells, lay, N, h, &d->d_nodes,
+                            &d->d_elements));
+    YG_TRY(dev_alloc_t(ctx, &d->d_offsets, h.offsets.size() + 1));
+    YG_CUDA(cudaMemcpy(d->d_offsets, h.offsets.data(), sizeof(int32_t) * h.offsets.size(), cudaMemcpyHostToDevice));
+    return YG_OK;
+}
+
+extern "C" yg_status yg_dofmap_create(yg_context ctx, const double *nodes_xyz, int32_t n_nodes,
+                                      const int32_t *cell_nodes, const int32_t *cell_offsets,
+                                      const int32_t *cell_types, int32_t n_cells, int32_t poly_order,
+                                      int32_t dof_per_node, yg_dofmap *out) {
+    if (!out) return fail(YG_BAD_ARG, "yg_dofmap_create: bad argument");
+    *out = nullptr;
+    yg_status cs = check_mesh(nodes_xyz, n_nodes, cell_nodes, cell_offsets, cell_types, n_cells, poly_order, dof_per_node);
+    if (cs != YG_OK) return cs;
     auto *d = new yg_dofmap_t();
     d->ctx = ctx;
+    // large p > 1 meshes are numbered on the device (identical result, see dofmap_gpu.cu)
+    if (ctx && poly_order > 1) {
+        yg_status s = try_number_on_device(d, nodes_xyz, n_nodes, cell_nodes, cell_offsets, cell_types, n_cells,
+                                           poly_order, dof_per_node, false);
+        if (s == YG_OK) { *out = d; return YG_OK; }
+        if (s != YG_UNSUPPORTED) { yg_dofmap_destroy(d); return s; }
+        d->host = HostDofmap();
+    }
     if (!build_dofmap(nodes_xyz, n_nodes, cell_nodes, cell_offsets, cell_types, n_cells, poly_order, dof_per_node, d->host)) {
         delete d;
         return fail(YG_BAD_ARG, "DoFManager: Invalid polynomial order");
     }
     return upload_dofmap(d, out);
+}
+
+extern "C" yg_status yg_dofmap_create_on_device(yg_context ctx, const double *nodes_xyz, int32_t n_nodes,
+                                                const int32_t *cell_nodes, const int32_t *cell_offsets,
+                                                const int32_t *cell_types, int32_t n_cells, int32_t poly_order,
+                                                int32_t dof_per_node, yg_dofmap *out) {
+    if (!ctx) return fail(YG_BAD_ARG, "yg_dofmap_create_on_device: needs a context");
+    if (poly_order < 2) return yg_dofmap_create(ctx, nodes_xyz, n_nodes, cell_nodes, cell_offsets, cell_types, n_cells,
+                                                poly_order, dof_per_node, out);
+    yg_status s = check_mesh(nodes_xyz, n_nodes, cell_nodes, cell_offsets, cell_types, n_cells, poly_order, dof_per_node);
+    if (s != YG_OK) return s;
+    *out = nullptr;
+    auto *d = new yg_dofmap_t();
+    d->ctx = ctx;
+    s = try_number_on_device(d, nodes_xyz, n_nodes, cell_nodes, cell_offsets, cell_types, n_cells, poly_order,
+                             dof_per_node, true);
+    if (s != YG_OK) { yg_dofmap_destroy(d); return s; }
+    *out = d;
+    return YG_OK;
 }
 
 extern "C" yg_status yg_dofmap_create_from_numbering(yg_context ctx, const double *dof_nodes_xyz, int32_t n_dof_nodes,

@@ -574,10 +574,6 @@ static void interpolate_from_corners(const double *xl, const double *c, int ct, 
 // position of the j-th smallest key; equal keys keep their original order).  11-bit digits; each pass counts per thread and
 // scatters each thread's contiguous chunk in order, so the result does not
 // depend on the thread count.
-// Meshes with at most this many raw element nodes are numbered with the
-// reference's own comparison sort (see build_dofmap).
-constexpr int64_t kReferenceOrderMaxRawNodes = int64_t(1) << 20;
-
 static void radix_sort_index(uint64_t *ka, int64_t N, int nbits, int64_t *out_idx) {
     constexpr int D = 11, R = 1 << D;
     std::unique_ptr<uint64_t[]> kb(new uint64_t[N]);
@@ -626,6 +622,28 @@ static void radix_sort_index(uint64_t *ka, int64_t N, int nbits, int64_t *out_id
     for (int64_t i = 0; i < N; ++i) out_idx[i] = iin[i];
 }
 
+int64_t raw_node_layout(int32_t n_cells, int32_t p, HostDofmap &d, RawLayout &lay) {
+    int64_t offset = 0;
+    for (int c = 0; c < n_cells; ++c) {
+        const int t = d.topology[c], td = d.topo_dim[c];
+        d.offsets[c] = (int32_t)offset;
+        if (t == TOPO_NONE) continue;
+        if (!lay.nloc[t][td]) lay.nloc[t][td] = local_nodes(t, td, p, lay.loc[t][td]);
+        offset += lay.nloc[t][td];
+    }
+    d.offsets[n_cells] = (int32_t)offset;
+    return offset;
+}
+
+bool raw_mix_needs_reference_order(const HostDofmap &d, int64_t n_raw) {
+    bool has_simplex = false, has_tensor = false;
+    for (int32_t c = 0; c < d.n_cells(); ++c) {
+        has_simplex |= d.topology[c] == TOPO_SIMPLEX && d.topo_dim[c] >= 2;
+        has_tensor |= d.topology[c] == TOPO_TENSOR && d.topo_dim[c] >= 2;
+    }
+    return n_raw <= kReferenceOrderMaxRawNodes || (d.poly_order >= 3 && has_simplex && has_tensor);
+}
+
 bool build_dofmap(const double *xyz, int32_t n_nodes, const int32_t *cell_nodes, const int32_t *cell_offsets,
                   const int32_t *cell_types, int32_t n_cells, int32_t p, int32_t dpn, HostDofmap &d) {
     if (p < 1) return false;
@@ -650,18 +668,10 @@ bool build_dofmap(const double *xyz, int32_t n_nodes, const int32_t *cell_nodes,
     // make_raw_dofs (DoFManager.cpp:176-229): every element's nodes at the
     // element's local node coordinates, cells in mesh order (offsets first, then
     // the coordinates of all cells in parallel)
-    std::vector<double> tabs[3][4];
-    int nloc[3][4] = {{0}};
-    int64_t offset = 0;
-    for (int c = 0; c < n_cells; ++c) {
-        int t = d.topology[c], td = d.topo_dim[c];
-        d.offsets[c] = (int32_t)offset;
-        if (t == TOPO_NONE) continue;
-        if (!nloc[t][td]) nloc[t][td] = local_nodes(t, td, p, tabs[t][td]);
-        offset += nloc[t][td];
-    }
-    d.offsets[n_cells] = (int32_t)offset;
-    const int64_t N = offset;
+    RawLayout lay;
+    const int64_t N = raw_node_layout(n_cells, p, d, lay);
+    const auto &tabs = lay.loc;
+    const auto &nloc = lay.nloc;
     std::unique_ptr<double[]> raw(new double[3 * N]);  // written (first touched) in parallel below
 #pragma omp parallel for schedule(static)
     for (int c = 0; c < n_cells; ++c) {
@@ -736,12 +746,7 @@ bool build_dofmap(const double *xyz, int32_t n_nodes, const int32_t *cell_nodes,
     // identity permutation, which reproduces its order exactly; large meshes
     // use the stable parallel radix sort (same node numbering; merged
     // coordinates can differ from the reference's in the last bit).
-    bool has_simplex = false, has_tensor = false;
-    for (int c = 0; c < n_cells; ++c) {
-        has_simplex |= d.topology[c] == TOPO_SIMPLEX && d.topo_dim[c] >= 2;
-        has_tensor |= d.topology[c] == TOPO_TENSOR && d.topo_dim[c] >= 2;
-    }
-    const bool reference_order = N <= kReferenceOrderMaxRawNodes || (p >= 3 && has_simplex && has_tensor);
+    const bool reference_order = raw_mix_needs_reference_order(d, N);
     if (reference_order) {
         std::vector<int64_t> kq(3 * N);
 #pragma omp parallel for schedule(static)

@@ -40,6 +40,24 @@ struct HostDofmap {
     int32_t n_nodes() const { return (int32_t)(nodes.size() / 3); }
     int32_t n_cells() const { return (int32_t)topology.size(); }
 };
+// Meshes with at most this many raw element nodes are numbered with the
+// reference's own comparison sort (see build_dofmap).
+constexpr int64_t kReferenceOrderMaxRawNodes = int64_t(1) << 20;
+
+// The raw-node layout of make_raw_dofs for p > 1: the local node table of each
+// element type present, and d.offsets (the raw nodes of cell c start at
+// d.offsets[c]); d.topology and d.topo_dim must be set.  Returns the number of
+// raw nodes.
+struct RawLayout {
+    std::vector<double> loc[3][4];  // [topology][dim]: nloc x 3 local coordinates
+    int nloc[3][4] = {{0}};
+};
+int64_t raw_node_layout(int32_t n_cells, int32_t p, HostDofmap &d, RawLayout &lay);
+// True when the merge order must be the reference's own comparison sort
+// (meshes of at most kReferenceOrderMaxRawNodes raw nodes, or simplices mixed
+// with tensor cells at p >= 3); otherwise a stable sort gives the same numbering.
+bool raw_mix_needs_reference_order(const HostDofmap &d, int64_t n_raw);
+
 // DoFManager(M, CG, p, dpn): returns false for p < 1.
 bool build_dofmap(const double *xyz, int32_t n_nodes, const int32_t *cell_nodes, const int32_t *cell_offsets,
                   const int32_t *cell_types, int32_t n_cells, int32_t p, int32_t dpn, HostDofmap &out);
