@@ -131,6 +131,15 @@ YG_API yg_status yg_dofmap_create_on_device(yg_context ctx, const double *nodes_
                                      const int32_t *cell_nodes, const int32_t *cell_offsets,
                                      const int32_t *cell_types, int32_t n_cells, int32_t poly_order,
                                      int32_t dof_per_node, yg_dofmap *out);
+/* The DoFManager of a structured box generated on the device, with no mesh from
+ * the host: dim 2 gives nx*ny Quad4 cells on [0,lx]x[0,ly], dim 3 nx*ny*nz Hex8
+ * cells on [0,lx]x[0,ly]x[0,lz]; nodes x fastest at i*(lx/nx) (the last at lx);
+ * cell corners in the element's x-fastest order for p = 1 (the DoFManager keeps
+ * the mesh, DoFManager.cpp:153-160) and counter-clockwise, bottom face first,
+ * for p > 1 (the corner maps of DoFManager.cpp:296-338).  p > 1 is numbered on
+ * the device as by yg_dofmap_create_on_device. */
+YG_API yg_status yg_dofmap_create_box(yg_context ctx, int32_t dim, int32_t nx, int32_t ny, int32_t nz, double lx,
+                               double ly, double lz, int32_t poly_order, int32_t dof_per_node, yg_dofmap *out);
 YG_API yg_status yg_dofmap_destroy(yg_dofmap d);
 /* Sizes of dof_nodes, cells, the elements array, and dofs = dof_nodes*dof_per_node. */
 YG_API yg_status yg_dofmap_sizes(yg_dofmap d, int32_t *n_dof_nodes, int32_t *n_cells,

@@ -59,3 +59,21 @@ def test_device_numbered_mesh_assembles_and_solves(ctx):
     K = fe.getGlobalTangent()
     x, st = yb.solve(K, fe.getGlobalResidual(), M=yb.JacobiPreconditioner(K), tol=1e-10)
     assert st.status == 0 and st.rel_residual <= 1e-10
+
+
+@pytest.mark.parametrize("dim,n,p", [(3, (40, 40, 40), 2), (3, (5, 4, 3), 2), (3, (4, 3, 2), 3), (3, (6, 5, 4), 1),
+                                     (2, (13, 9), 2), (2, (7, 6), 3), (2, (8, 8), 1)])
+def test_box_generated_on_device(ctx, dim, n, p):
+    lengths = (1.0, 2.5, 0.75)
+    dev = yb.DoFManager.box(dim, n, lengths, p, 1, ctx=ctx)
+    order = meshgen.corner_order(p)
+    mesh = (meshgen.structured_hex(*n, *lengths, order=order) if dim == 3
+            else meshgen.structured_quad(*n, *lengths[:2], order=order))
+    host = yb.DoFManager(mesh, p, 1, host_only=True)
+    assert np.array_equal(dev.element_offsets, host.element_offsets)
+    assert np.array_equal(dev.elements, host.elements)
+    exact = p == 1 or np.prod(n) * (p + 1) ** dim > (1 << 20)  # the host's stable order
+    if exact:
+        assert np.array_equal(dev.dof_nodes, host.dof_nodes)
+    else:
+        assert np.abs(dev.dof_nodes - host.dof_nodes).max() <= 1e-15 * max(lengths)

@@ -232,6 +232,29 @@ class DoFManager:
         self._cache = None
         self.cell_region_idx = mesh.cell_tags
 
+    @classmethod
+    def box(cls, dim, n, lengths=(1.0, 1.0, 1.0), polyOrder=1, dof_per_node=1, ctx=None):
+        """The DoFManager of a structured box generated on the GPU
+        (yg_dofmap_create_box): n = (nx, ny[, nz]) cells, the mesh of
+        meshgen.structured_quad/hex in the corner order the element expects."""
+        self = cls.__new__(cls)
+        self.ctx = ctx or default_context()
+        self.mesh = None
+        nx, ny = int(n[0]), int(n[1])
+        nz = int(n[2]) if dim == 3 else 0
+        h = C.c_void_p()
+        check(lib().yg_dofmap_create_box(self.ctx.h, dim, nx, ny, nz, float(lengths[0]), float(lengths[1]),
+                                         float(lengths[2]) if dim == 3 else 0.0, int(polyOrder), int(dof_per_node),
+                                         C.byref(h)), "DoFManager.box")
+        self.h = h
+        self.polyOrder, self.dof_per_node = int(polyOrder), int(dof_per_node)
+        a, b, c, d = C.c_int32(), C.c_int32(), C.c_int64(), C.c_int64()
+        check(lib().yg_dofmap_sizes(h, C.byref(a), C.byref(b), C.byref(c), C.byref(d)))
+        self._n_nodes, self._n_cells, self._n_el, self.ndofs = a.value, b.value, c.value, d.value
+        self._cache = None
+        self.cell_region_idx = np.zeros(self._n_cells, np.int32)
+        return self
+
     def _fetch(self):
         if self._cache is None:
             nodes = np.empty((self._n_nodes, 3))

@@ -53,6 +53,7 @@ SIGNATURES = {
     "yg_dofmap_create": (i32, [vp, vp, i32, vp, vp, vp, i32, i32, i32, P(vp)]),
     "yg_dofmap_destroy": (i32, [vp]),
     "yg_dofmap_create_on_device": (i32, [vp, vp, i32, vp, vp, vp, i32, i32, i32, P(vp)]),
+    "yg_dofmap_create_box": (i32, [vp, i32, i32, i32, i32, f64, f64, f64, i32, i32, P(vp)]),
     "yg_dofmap_sizes": (i32, [vp, P(i32), P(i32), P(i64), P(i64)]),
     "yg_dofmap_get": (i32, [vp, vp, vp, vp, vp, vp, vp]),
     "yg_dofmap_create_from_numbering": (i32, [vp, vp, i32, vp, vp, vp, i32, i32, i32, P(vp)]),

@@ -656,7 +656,9 @@ const HostDofmap &dofmap_host(yg_dofmap d) { return d->host; }
 yg_status number_on_device(yg_context ctx, const double *xyz, int32_t n_nodes, const int32_t *cell_nodes,
                            const int32_t *cell_offsets, const int32_t *cell_types, int32_t n_cells,
                            const RawLayout &lay, int64_t N, HostDofmap &d, double **d_nodes_out,
-                           int32_t **d_elements_out);  // dofmap_gpu.cu
+                           int32_t **d_elements_out, bool device_mesh);  // dofmap_gpu.cu
+yg_status generate_box(yg_context ctx, int dim, int nx, int ny, int nz, double lx, double ly, double lz, bool ccw,
+                       double *xyz, int32_t *cell_nodes, int32_t *cell_offsets, int32_t *cell_types);
 
 }  // namespace yg
 
@@ -744,7 +746,7 @@ static yg_status try_number_on_device(yg_dofmap d, const double *xyz, int32_t n_
     if (N == 0 || (!forced && raw_mix_needs_reference_order(h, N))) return YG_UNSUPPORTED;
     yg_context ctx = d->ctx;
     YG_TRY(number_on_device(ctx, xyz, n_nodes, cell_nodes, cell_offsets, cell_types, n_cells, lay, N, h, &d->d_nodes,
-                            &d->d_elements));
+                            &d->d_elements, false));
     YG_TRY(dev_alloc_t(ctx, &d->d_offsets, h.offsets.size() + 1));
     YG_CUDA(cudaMemcpy(d->d_offsets, h.offsets.data(), sizeof(int32_t) * h.offsets.size(), cudaMemcpyHostToDevice));
     return YG_OK;
@@ -839,6 +841,72 @@ extern "C" yg_status yg_dofmap_create_from_numbering(yg_context ctx, const doubl
             }
     }
     return upload_dofmap(d, out);
+}
+
+extern "C" yg_status yg_dofmap_create_box(yg_context ctx, int32_t dim, int32_t nx, int32_t ny, int32_t nz, double lx,
+                                          double ly, double lz, int32_t poly_order, int32_t dof_per_node,
+                                          yg_dofmap *out) {
+    if (!ctx || !out || (dim != 2 && dim != 3) || nx < 1 || ny < 1 || (dim == 3 && nz < 1) || !(lx > 0) || !(ly > 0) ||
+        (dim == 3 && !(lz > 0)))
+        return fail(YG_BAD_ARG, "yg_dofmap_create_box: bad argument");
+    if (dof_per_node < 1 || dof_per_node > 3) return fail(YG_BAD_ARG, "dof_per_node must be 1..3");
+    if (poly_order < 1) return fail(YG_BAD_ARG, "DoFManager: Invalid polynomial order");
+    *out = nullptr;
+    const int64_t nnodes = (int64_t)(nx + 1) * (ny + 1) * (dim == 3 ? nz + 1 : 1);
+    const int64_t ncells = (int64_t)nx * ny * (dim == 3 ? nz : 1);
+    const int nc = dim == 3 ? 8 : 4;
+    if (nnodes > INT32_MAX || ncells * nc > INT32_MAX) return fail(YG_BAD_ARG, "yg_dofmap_create_box: box too large");
+    auto *d = new yg_dofmap_t();
+    d->ctx = ctx;
+    HostDofmap &h = d->host;
+    h.dof_per_node = dof_per_node;
+    h.poly_order = poly_order;
+    h.offsets.resize(ncells + 1);
+    for (int64_t c = 0; c <= ncells; ++c) h.offsets[c] = (int32_t)(c * nc);
+    h.topology.assign(ncells, (int8_t)TOPO_TENSOR);
+    h.topo_dim.assign(ncells, (int8_t)dim);
+    h.porder.assign(ncells, (int8_t)poly_order);
+    double *xyz = nullptr;
+    int32_t *cn = nullptr, *co = nullptr, *ct = nullptr;
+    auto done = [&](yg_status s) {
+        dev_free(ctx, xyz);
+        dev_free(ctx, cn);
+        dev_free(ctx, co);
+        dev_free(ctx, ct);
+        if (s != YG_OK) yg_dofmap_destroy(d);
+        else *out = d;
+        return s;
+    };
+    yg_status s;
+    if ((s = dev_alloc_t(ctx, &xyz, 3 * nnodes + 1)) != YG_OK || (s = dev_alloc_t(ctx, &cn, ncells * nc + 1)) != YG_OK ||
+        (s = dev_alloc_t(ctx, &co, ncells + 1)) != YG_OK || (s = dev_alloc_t(ctx, &ct, ncells + 1)) != YG_OK)
+        return done(s);
+    // p = 1 keeps the mesh numbering, whose cells must be in the element's
+    // x-fastest order; p > 1 places nodes with the counter-clockwise corner maps
+    if ((s = generate_box(ctx, dim, nx, ny, nz, lx, ly, lz, poly_order > 1, xyz, cn, co, ct)) != YG_OK) return done(s);
+    if (poly_order == 1) {  // DoFManager.cpp:153-160: the mesh itself
+        h.nodes.resize(3 * nnodes);
+        h.elements.resize(ncells * nc);
+        cudaError_t e = cudaMemcpyAsync(h.nodes.data(), xyz, sizeof(double) * 3 * nnodes, cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(h.elements.data(), cn, sizeof(int32_t) * ncells * nc, cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) return done(fail(YG_CUDA_ERROR, "yg_dofmap_create_box: %s", cudaGetErrorString(e)));
+        d->d_nodes = xyz;
+        d->d_elements = cn;
+        xyz = nullptr;
+        cn = nullptr;
+    } else {
+        RawLayout lay;
+        const int64_t N = raw_node_layout((int32_t)ncells, poly_order, h, lay);
+        if ((s = number_on_device(ctx, xyz, (int32_t)nnodes, cn, co, ct, (int32_t)ncells, lay, N, h, &d->d_nodes,
+                                  &d->d_elements, true)) != YG_OK)
+            return done(s);
+    }
+    if ((s = dev_alloc_t(ctx, &d->d_offsets, h.offsets.size() + 1)) != YG_OK) return done(s);
+    cudaError_t e = cudaMemcpy(d->d_offsets, h.offsets.data(), sizeof(int32_t) * h.offsets.size(), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return done(fail(YG_CUDA_ERROR, "yg_dofmap_create_box: %s", cudaGetErrorString(e)));
+    return done(YG_OK);
 }
 
 extern "C" yg_status yg_element_table(int32_t topology, int32_t dim, int32_t poly_order, int32_t *nen, int32_t *nq,

@@ -19,6 +19,8 @@
 //      its node number and each node the coordinates of its first raw node.
 // The numbering and coordinates are copied back to the host dofmap (the
 // element colouring and the host API read them) and kept on the device.
+// generate_box builds a structured quadrilateral or hexahedron box on the
+// device, so that a box's DoFManager needs no mesh from the host.
 #include "internal.h"
 #include "host_fe.h"
 
@@ -313,12 +315,62 @@ yg_status scan_counts(yg_context ctx, Scratch &S, const int32_t *in, int64_t n, 
     return YG_OK;
 }
 
+// Structured box: node (i, j, k) at (i dx, j dy, k dz), the last one of each
+// direction at exactly (lx, ly, lz) (numpy.linspace's values); nodes x fastest.
+__global__ void k_box_nodes(int64_t nnodes, int nx, int ny, int nz, double dx, double dy, double dz, double lx,
+                            double ly, double lz, double *__restrict__ xyz) {
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < nnodes; v += (int64_t)gridDim.x * blockDim.x) {
+        const int i = (int)(v % (nx + 1)), j = (int)((v / (nx + 1)) % (ny + 1)), k = (int)(v / ((int64_t)(nx + 1) * (ny + 1)));
+        xyz[3 * v + 0] = i == nx ? lx : __dmul_rn((double)i, dx);
+        xyz[3 * v + 1] = j == ny ? ly : __dmul_rn((double)j, dy);
+        xyz[3 * v + 2] = nz == 0 ? 0.0 : (k == nz ? lz : __dmul_rn((double)k, dz));
+    }
+}
+
+// Cells of the box: Quad4 (nz = 0) or Hex8, in counter-clockwise corner order
+// (bottom face first) or x-fastest tensor order; offsets and types alongside.
+__global__ void k_box_cells(int64_t ncells, int nx, int ny, int nz, int ccw, int32_t *__restrict__ cn,
+                            int32_t *__restrict__ off, int32_t *__restrict__ type) {
+    const int nc = nz == 0 ? 4 : 8;
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < ncells; c += (int64_t)gridDim.x * blockDim.x) {
+        const int i = (int)(c % nx), j = (int)((c / nx) % ny), k = nz == 0 ? 0 : (int)(c / ((int64_t)nx * ny));
+        const int32_t sx = 1, sy = nx + 1, sz = (nx + 1) * (ny + 1);
+        const int32_t n0 = k * sz + j * sy + i * sx;
+        int32_t *o = cn + c * nc;
+        if (ccw) {
+            o[0] = n0; o[1] = n0 + sx; o[2] = n0 + sx + sy; o[3] = n0 + sy;
+            if (nc == 8) { o[4] = n0 + sz; o[5] = n0 + sz + sx; o[6] = n0 + sz + sx + sy; o[7] = n0 + sz + sy; }
+        } else {
+            o[0] = n0; o[1] = n0 + sx; o[2] = n0 + sy; o[3] = n0 + sx + sy;
+            if (nc == 8) { o[4] = n0 + sz; o[5] = n0 + sz + sx; o[6] = n0 + sz + sy; o[7] = n0 + sz + sx + sy; }
+        }
+        off[c] = (int32_t)(c * nc);
+        type[c] = nc == 4 ? 3 : 4;
+        if (c == ncells - 1) off[ncells] = (int32_t)(ncells * nc);
+    }
+}
+
 }  // namespace
+
+// The box mesh on the device (into caller-held arrays sized for it).
+yg_status generate_box(yg_context ctx, int dim, int nx, int ny, int nz, double lx, double ly, double lz, bool ccw,
+                       double *xyz, int32_t *cell_nodes, int32_t *cell_offsets, int32_t *cell_types) {
+    const int64_t nnodes = (int64_t)(nx + 1) * (ny + 1) * (dim == 3 ? nz + 1 : 1);
+    const int64_t ncells = (int64_t)nx * ny * (dim == 3 ? nz : 1);
+    k_box_nodes<<<stream_grid(ctx, nnodes), kThreads, 0, ctx->stream>>>(
+        nnodes, nx, ny, dim == 3 ? nz : 0, lx / nx, ly / ny, dim == 3 ? lz / nz : 0.0, lx, ly, lz, xyz);
+    YG_LAUNCHED(ctx);
+    k_box_cells<<<stream_grid(ctx, ncells), kThreads, 0, ctx->stream>>>(ncells, nx, ny, dim == 3 ? nz : 0, ccw ? 1 : 0,
+                                                                       cell_nodes, cell_offsets, cell_types);
+    YG_LAUNCHED(ctx);
+    YG_CUDA(cudaGetLastError());
+    return YG_OK;
+}
 
 yg_status number_on_device(yg_context ctx, const double *xyz, int32_t n_nodes, const int32_t *cell_nodes,
                            const int32_t *cell_offsets, const int32_t *cell_types, int32_t n_cells,
                            const RawLayout &lay, int64_t N, HostDofmap &d, double **d_nodes_out,
-                           int32_t **d_elements_out) {
+                           int32_t **d_elements_out, bool device_mesh) {
     *d_nodes_out = nullptr;
     *d_elements_out = nullptr;
     cudaStream_t st = ctx->stream;
@@ -338,22 +390,37 @@ yg_status number_on_device(yg_context ctx, const double *xyz, int32_t n_nodes, c
         }
     for (int32_t c = 0; c < n_cells; ++c)
         if (d.topology[c] != TOPO_NONE) tab_of_cell[c] = tab_id[d.topology[c]][d.topo_dim[c]];
-    const int64_t ncn = cell_offsets[n_cells];
-    double *dxyz, *dtabs, *raw, *dnodes = nullptr;
-    int32_t *dcoff, *dcn, *dct, *droff, *dtoc, *dts, *delem = nullptr;
-    YG_TRY(S.get(&dxyz, 3 * (size_t)n_nodes + 1));
-    YG_TRY(S.get(&dcoff, (size_t)n_cells + 1));
-    YG_TRY(S.get(&dcn, (size_t)ncn + 1));
-    YG_TRY(S.get(&dct, (size_t)n_cells + 1));
+    const double *dxyz;
+    const int32_t *dcoff, *dcn, *dct;
+    double *dtabs, *raw, *dnodes = nullptr;
+    int32_t *droff, *dtoc, *dts, *delem = nullptr;
+    if (device_mesh) {  // the mesh arrays are already on the device
+        dxyz = xyz;
+        dcoff = cell_offsets;
+        dcn = cell_nodes;
+        dct = cell_types;
+    } else {
+        const int64_t ncn = cell_offsets[n_cells];
+        double *ux;
+        int32_t *uo, *un, *ut;
+        YG_TRY(S.get(&ux, 3 * (size_t)n_nodes + 1));
+        YG_TRY(S.get(&uo, (size_t)n_cells + 1));
+        YG_TRY(S.get(&un, (size_t)ncn + 1));
+        YG_TRY(S.get(&ut, (size_t)n_cells + 1));
+        YG_CUDA(cudaMemcpyAsync(ux, xyz, sizeof(double) * 3 * n_nodes, cudaMemcpyHostToDevice, st));
+        YG_CUDA(cudaMemcpyAsync(uo, cell_offsets, sizeof(int32_t) * (n_cells + 1), cudaMemcpyHostToDevice, st));
+        YG_CUDA(cudaMemcpyAsync(un, cell_nodes, sizeof(int32_t) * ncn, cudaMemcpyHostToDevice, st));
+        YG_CUDA(cudaMemcpyAsync(ut, cell_types, sizeof(int32_t) * n_cells, cudaMemcpyHostToDevice, st));
+        dxyz = ux;
+        dcoff = uo;
+        dcn = un;
+        dct = ut;
+    }
     YG_TRY(S.get(&droff, (size_t)n_cells + 1));
     YG_TRY(S.get(&dtoc, (size_t)n_cells + 1));
     YG_TRY(S.get(&dts, tab_start.size() + 1));
     YG_TRY(S.get(&dtabs, tabs.size() + 1));
     YG_TRY(S.get(&raw, 3 * (size_t)N));
-    YG_CUDA(cudaMemcpyAsync(dxyz, xyz, sizeof(double) * 3 * n_nodes, cudaMemcpyHostToDevice, st));
-    YG_CUDA(cudaMemcpyAsync(dcoff, cell_offsets, sizeof(int32_t) * (n_cells + 1), cudaMemcpyHostToDevice, st));
-    YG_CUDA(cudaMemcpyAsync(dcn, cell_nodes, sizeof(int32_t) * ncn, cudaMemcpyHostToDevice, st));
-    YG_CUDA(cudaMemcpyAsync(dct, cell_types, sizeof(int32_t) * n_cells, cudaMemcpyHostToDevice, st));
     YG_CUDA(cudaMemcpyAsync(droff, d.offsets.data(), sizeof(int32_t) * (n_cells + 1), cudaMemcpyHostToDevice, st));
     YG_CUDA(cudaMemcpyAsync(dtoc, tab_of_cell.data(), sizeof(int32_t) * n_cells, cudaMemcpyHostToDevice, st));
     YG_CUDA(cudaMemcpyAsync(dts, tab_start.data(), sizeof(int32_t) * tab_start.size(), cudaMemcpyHostToDevice, st));
