@@ -134,6 +134,8 @@ struct yg_precond_t {
     int32_t *d_lower_levels = nullptr, *d_upper_levels = nullptr;  // row lists grouped by level
     std::vector<int32_t> lower_level_ptr, upper_level_ptr;
     int32_t *d_csr_rowptr = nullptr, *d_csr_col = nullptr, *d_csr_diag = nullptr;  // scalar view
+    int32_t *d_lower_ptr = nullptr, *d_upper_ptr = nullptr;  // level pointers for the persistent sweeps
+    uint32_t *d_bar = nullptr;                              // their grid barrier (count, generation)
     int64_t n = 0, nnz = 0;
     double *d_tmp = nullptr;
 };

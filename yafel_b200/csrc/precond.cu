@@ -11,8 +11,9 @@
 // pivots (KIJ, O(N^2) row scans); here rows are factored in IKJ order, which
 // applies to every entry the same updates in the same order.  Rows are grouped
 // into dependency levels on the host (level = 1 + max level of the rows it
-// depends on); each level is one launch with a warp per row, for the
-// factorization and for both triangular solves.
+// depends on); the factorization and each triangular solve are one persistent
+// launch walking the levels with a grid-wide barrier between them, a warp per
+// row.
 #include "internal.h"
 #include "device_common.cuh"
 
@@ -88,89 +89,155 @@ __device__ __forceinline__ int find_col(const int32_t *__restrict__ col, int lo,
     return -1;
 }
 
-// Factor the rows of one level: warp per row, pivots in ascending order, the
-// lanes share the updates of one pivot row.
-__global__ void k_ilu_factor_level(const int32_t *__restrict__ rows, int nrows, const int32_t *__restrict__ rp,
-                                   const int32_t *__restrict__ col, const int32_t *__restrict__ diag,
-                                   double *__restrict__ lu, int *__restrict__ zero_pivots) {
+// ---------------------------------------------------------------------------
+// Persistent level sweeps.  One cooperative launch per factorization and per
+// triangular solve: the grid walks the levels in order with a grid-wide barrier
+// between them, instead of one launch per level (the levels of a 3-D mesh in
+// natural order number ~78 per cell layer, so launch latency dominated).  Values
+// written in earlier levels by other blocks are read through L2 (__ldcg).  The
+// barrier is bounded: after kSpinLimit polls a block records YG_TIMEOUT in the
+// context's error word and returns, so a sweep can only end.
+struct GridBarrier {
+    unsigned count, gen;
+};
+
+__device__ bool grid_barrier(GridBarrier *b) {
+    __shared__ int ok_s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        const unsigned g = atomicAdd(&b->gen, 0u);
+        __threadfence();
+        if (atomicAdd(&b->count, 1u) == gridDim.x - 1) {
+            atomicExch(&b->count, 0u);
+            __threadfence();
+            atomicAdd(&b->gen, 1u);
+        } else {
+            long long spins = 0;
+            while (atomicAdd(&b->gen, 0u) == g)
+                if (++spins > kSpinLimit) { ok = 0; break; }
+        }
+        __threadfence();
+        ok_s = ok;
+    }
+    __syncthreads();
+    return ok_s != 0;
+}
+
+// Factorization (IKJ): a warp per row of the level, pivots in ascending order,
+// the lanes share the updates of one pivot row.
+__global__ void __launch_bounds__(kThreads)
+k_ilu_factor_sweep(const int32_t *__restrict__ lev_ptr, int nlev, const int32_t *__restrict__ rows,
+                   const int32_t *__restrict__ rp, const int32_t *__restrict__ col, const int32_t *__restrict__ diag,
+                   double *__restrict__ lu, int *__restrict__ zero_pivots, GridBarrier *bar, int32_t *err) {
     const int lane = threadIdx.x & 31;
     const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nw = (gridDim.x * blockDim.x) >> 5;
-    for (int t = w; t < nrows; t += nw) {
-        const int i = rows[t];
-        const int rs = rp[i], re = rp[i + 1];
-        for (int kk = rs; kk < re; ++kk) {
-            const int k = col[kk];
-            if (k >= i) break;
-            const int dk = diag[k];
-            const double piv = dk >= 0 ? lu[dk] : 0.0;
-            if (piv == 0) {
-                if (lane == 0) atomicAdd(zero_pivots, 1);
-                continue;
+    for (int l = 0; l < nlev; ++l) {
+        for (int t = lev_ptr[l] + w; t < lev_ptr[l + 1]; t += nw) {
+            const int i = rows[t];
+            const int rs = rp[i], re = rp[i + 1];
+            for (int kk = rs; kk < re; ++kk) {
+                const int k = col[kk];
+                if (k >= i) break;
+                const int dk = diag[k];
+                const double piv = dk >= 0 ? __ldcg(lu + dk) : 0.0;
+                if (piv == 0) {
+                    if (lane == 0) atomicAdd(zero_pivots, 1);
+                    continue;
+                }
+                __syncwarp();
+                const double m = lu[kk] / piv;
+                const int ke = rp[k + 1];
+                for (int q = dk + 1 + lane; q < ke; q += 32) {
+                    const int pos = find_col(col, kk + 1, re, col[q]);
+                    if (pos >= 0) lu[pos] -= m * __ldcg(lu + q);
+                }
+                __syncwarp();
+                if (lane == 0) lu[kk] = m;
+                __syncwarp();
             }
-            __syncwarp();
-            const double m = lu[kk] / piv;
-            const int ke = rp[k + 1];
-            for (int q = dk + 1 + lane; q < ke; q += 32) {
-                int pos = find_col(col, kk + 1, re, col[q]);
-                if (pos >= 0) lu[pos] -= m * lu[q];
-            }
-            __syncwarp();
-            if (lane == 0) lu[kk] = m;
-            __syncwarp();
+        }
+        if (l + 1 < nlev && !grid_barrier(bar)) {
+            if (threadIdx.x == 0) atomicExch(err, (int32_t)YG_TIMEOUT);
+            return;
         }
     }
 }
 
-// Forward substitution with unit L for one level (f_subst, ILUPreconditioner.hpp:201-221).
-__global__ void k_ilu_lower_level(const int32_t *__restrict__ rows, int nrows, const int32_t *__restrict__ rp,
-                                  const int32_t *__restrict__ col, const int32_t *__restrict__ diag,
-                                  const double *__restrict__ lu, double *__restrict__ z) {
+// Forward substitution with unit L (f_subst, ILUPreconditioner.hpp:201-221).
+__global__ void __launch_bounds__(kThreads)
+k_ilu_lower_sweep(const int32_t *__restrict__ lev_ptr, int nlev, const int32_t *__restrict__ rows,
+                  const int32_t *__restrict__ rp, const int32_t *__restrict__ col, const int32_t *__restrict__ diag,
+                  const double *__restrict__ lu, double *__restrict__ z, GridBarrier *bar, int32_t *err) {
     const int lane = threadIdx.x & 31;
     const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nw = (gridDim.x * blockDim.x) >> 5;
-    for (int t = w; t < nrows; t += nw) {
-        const int i = rows[t];
-        const int rs = rp[i];
-        int re = diag[i] >= 0 ? diag[i] : rp[i + 1];
-        double s = 0;
-        for (int k = rs + lane; k < re; k += 32) {
-            int c = col[k];
-            if (c < i) s += lu[k] * z[c];
+    for (int l = 0; l < nlev; ++l) {
+        for (int t = lev_ptr[l] + w; t < lev_ptr[l + 1]; t += nw) {
+            const int i = rows[t];
+            const int rs = rp[i];
+            const int re = diag[i] >= 0 ? diag[i] : rp[i + 1];
+            double s = 0;
+            for (int k = rs + lane; k < re; k += 32) {
+                const int c = col[k];
+                if (c < i) s += lu[k] * __ldcg(z + c);
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+            if (lane == 0) z[i] = __ldcg(z + i) - s;
         }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        if (lane == 0) z[i] -= s;
+        if (l + 1 < nlev && !grid_barrier(bar)) {
+            if (threadIdx.x == 0) atomicExch(err, (int32_t)YG_TIMEOUT);
+            return;
+        }
     }
 }
 
-// Backward substitution for one level (b_subst, ILUPreconditioner.hpp:226-253);
-// a row without a diagonal uses its first entry, as the reference does.
-__global__ void k_ilu_upper_level(const int32_t *__restrict__ rows, int nrows, const int32_t *__restrict__ rp,
-                                  const int32_t *__restrict__ col, const int32_t *__restrict__ diag,
-                                  const double *__restrict__ lu, double *__restrict__ z) {
+// Backward substitution (b_subst, ILUPreconditioner.hpp:226-253); a row
+// without a diagonal uses its first entry, as the reference does.
+__global__ void __launch_bounds__(kThreads)
+k_ilu_upper_sweep(const int32_t *__restrict__ lev_ptr, int nlev, const int32_t *__restrict__ rows,
+                  const int32_t *__restrict__ rp, const int32_t *__restrict__ col, const int32_t *__restrict__ diag,
+                  const double *__restrict__ lu, double *__restrict__ z, GridBarrier *bar, int32_t *err) {
     const int lane = threadIdx.x & 31;
     const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nw = (gridDim.x * blockDim.x) >> 5;
-    for (int t = w; t < nrows; t += nw) {
-        const int i = rows[t];
-        const int id = diag[i] >= 0 ? diag[i] : rp[i];
-        const int re = rp[i + 1];
-        double s = 0;
-        for (int k = id + 1 + lane; k < re; k += 32) s += lu[k] * z[col[k]];
+    for (int l = 0; l < nlev; ++l) {
+        for (int t = lev_ptr[l] + w; t < lev_ptr[l + 1]; t += nw) {
+            const int i = rows[t];
+            const int id = diag[i] >= 0 ? diag[i] : rp[i];
+            const int re = rp[i + 1];
+            double s = 0;
+            for (int k = id + 1 + lane; k < re; k += 32) s += lu[k] * __ldcg(z + col[k]);
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        if (lane == 0) z[i] = (z[i] - s) / lu[id];
+            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+            if (lane == 0) z[i] = (__ldcg(z + i) - s) / lu[id];
+        }
+        if (l + 1 < nlev && !grid_barrier(bar)) {
+            if (threadIdx.x == 0) atomicExch(err, (int32_t)YG_TIMEOUT);
+            return;
+        }
     }
 }
 
-static int level_grid(yg_context ctx, int64_t rows) {
-    int64_t warps_per_block = kThreads / 32;
-    int64_t g = (rows + warps_per_block - 1) / warps_per_block;
-    int64_t cap = (int64_t)ctx->num_sms * 8;
-    if (g > cap) g = cap;
-    if (g < 1) g = 1;
-    return (int)g;
+// One block per SM: every block of the cooperative launch is resident at once.
+template <typename K, typename... Args>
+static yg_status launch_sweep(yg_context ctx, K kern, GridBarrier *bar, Args... args) {
+    YG_CUDA(cudaMemsetAsync(bar, 0, sizeof(GridBarrier), ctx->stream));
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)ctx->num_sms);
+    cfg.blockDim = dim3(kThreads);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = ctx->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    YG_CUDA(cudaLaunchKernelEx(&cfg, kern, args..., bar, ctx->d_err));
+    YG_LAUNCHED(ctx);
+    return YG_OK;
 }
 
 static yg_status build_ilu(yg_precond M) {
@@ -238,16 +305,22 @@ static yg_status build_ilu(yg_precond M) {
     YG_TRY(dev_alloc_t(ctx, &M->d_upper_levels, n));
     YG_CUDA(cudaMemcpyAsync(M->d_lower_levels, lrows.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, st));
     YG_CUDA(cudaMemcpyAsync(M->d_upper_levels, urows.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, st));
-    // factor level by level
+    // level pointers on the device for the persistent sweeps
+    YG_TRY(dev_alloc_t(ctx, &M->d_lower_ptr, M->lower_level_ptr.size()));
+    YG_TRY(dev_alloc_t(ctx, &M->d_upper_ptr, M->upper_level_ptr.size()));
+    YG_TRY(dev_alloc_t(ctx, &M->d_bar, 4));
+    YG_CUDA(cudaMemcpyAsync(M->d_lower_ptr, M->lower_level_ptr.data(), sizeof(int32_t) * M->lower_level_ptr.size(),
+                            cudaMemcpyHostToDevice, st));
+    YG_CUDA(cudaMemcpyAsync(M->d_upper_ptr, M->upper_level_ptr.data(), sizeof(int32_t) * M->upper_level_ptr.size(),
+                            cudaMemcpyHostToDevice, st));
+    // factor the levels in one persistent launch
     int *d_zero = reinterpret_cast<int *>(M->d_tmp);
     YG_CUDA(cudaMemsetAsync(d_zero, 0, sizeof(int), st));
-    for (size_t l = 0; l + 1 < M->lower_level_ptr.size(); ++l) {
-        int32_t a = M->lower_level_ptr[l], b = M->lower_level_ptr[l + 1];
-        if (b == a) continue;
-        k_ilu_factor_level<<<level_grid(ctx, b - a), kThreads, 0, st>>>(M->d_lower_levels + a, b - a, M->d_csr_rowptr,
-                                                                        M->d_csr_col, M->d_csr_diag, M->d_lu, d_zero);
-        YG_LAUNCHED(ctx);
-    }
+    GridBarrier *bar = reinterpret_cast<GridBarrier *>(M->d_bar);
+    YG_TRY(launch_sweep(ctx, k_ilu_factor_sweep, bar, (const int32_t *)M->d_lower_ptr,
+                        (int)M->lower_level_ptr.size() - 1, (const int32_t *)M->d_lower_levels,
+                        (const int32_t *)M->d_csr_rowptr, (const int32_t *)M->d_csr_col,
+                        (const int32_t *)M->d_csr_diag, M->d_lu, d_zero));
     YG_CUDA(cudaGetLastError());
     int zeros = 0;
     YG_CUDA(cudaMemcpyAsync(&zeros, d_zero, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -270,20 +343,13 @@ yg_status precond_apply_dev(yg_precond M, const double *r, double *z) {
         return YG_OK;
     }
     if (z != r) YG_CUDA(cudaMemcpyAsync(z, r, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
-    for (size_t l = 0; l + 1 < M->lower_level_ptr.size(); ++l) {
-        int32_t a = M->lower_level_ptr[l], b = M->lower_level_ptr[l + 1];
-        if (b == a) continue;
-        k_ilu_lower_level<<<level_grid(ctx, b - a), kThreads, 0, st>>>(M->d_lower_levels + a, b - a, M->d_csr_rowptr,
-                                                                       M->d_csr_col, M->d_csr_diag, M->d_lu, z);
-        YG_LAUNCHED(ctx);
-    }
-    for (size_t l = 0; l + 1 < M->upper_level_ptr.size(); ++l) {
-        int32_t a = M->upper_level_ptr[l], b = M->upper_level_ptr[l + 1];
-        if (b == a) continue;
-        k_ilu_upper_level<<<level_grid(ctx, b - a), kThreads, 0, st>>>(M->d_upper_levels + a, b - a, M->d_csr_rowptr,
-                                                                       M->d_csr_col, M->d_csr_diag, M->d_lu, z);
-        YG_LAUNCHED(ctx);
-    }
+    GridBarrier *bar = reinterpret_cast<GridBarrier *>(M->d_bar);
+    YG_TRY(launch_sweep(ctx, k_ilu_lower_sweep, bar, (const int32_t *)M->d_lower_ptr, (int)M->lower_level_ptr.size() - 1,
+                        (const int32_t *)M->d_lower_levels, (const int32_t *)M->d_csr_rowptr,
+                        (const int32_t *)M->d_csr_col, (const int32_t *)M->d_csr_diag, (const double *)M->d_lu, z));
+    YG_TRY(launch_sweep(ctx, k_ilu_upper_sweep, bar, (const int32_t *)M->d_upper_ptr, (int)M->upper_level_ptr.size() - 1,
+                        (const int32_t *)M->d_upper_levels, (const int32_t *)M->d_csr_rowptr,
+                        (const int32_t *)M->d_csr_col, (const int32_t *)M->d_csr_diag, (const double *)M->d_lu, z));
     YG_CUDA(cudaGetLastError());
     return YG_OK;
 }
@@ -337,7 +403,8 @@ extern "C" yg_status yg_precond_destroy(yg_precond M) {
     if (!M) return YG_OK;
     yg_context ctx = M->A->ctx;
     for (void *p : {(void *)M->d_dinv, (void *)M->d_lu, (void *)M->d_lower_levels, (void *)M->d_upper_levels,
-                    (void *)M->d_csr_rowptr, (void *)M->d_csr_col, (void *)M->d_csr_diag, (void *)M->d_tmp})
+                    (void *)M->d_csr_rowptr, (void *)M->d_csr_col, (void *)M->d_csr_diag, (void *)M->d_tmp,
+                    (void *)M->d_lower_ptr, (void *)M->d_upper_ptr, (void *)M->d_bar})
         dev_free(ctx, p);
     delete M;
     return YG_OK;
