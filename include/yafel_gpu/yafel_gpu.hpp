@@ -1,6 +1,7 @@
 // yafel_gpu.hpp -- header-only C++ adapters with the reference's spellings over
 // the C ABI of yafel_gpu.h.  Code written against the reference's
-//   DoFManager / FESystem / CGAssembly<Physics> / LocalSmoothingGradient<Physics> / DirichletBC
+//   DoFManager / FESystem / CGAssembly<Physics> / LocalSmoothingGradient<Physics> /
+//   ZZGradientRecovery<Physics> / SimulationOutput (VTU) / Mesh(gmsh file) / DirichletBC
 //   sparse_csr / sparse_bcsr / cg_solve / pcg_solve / bicgstab_solve /
 //   JacobiPreconditioner / ILUPreconditioner / IdentityPreconditioner
 // switches to the GPU by including this header and using namespace yafel::gpu.
@@ -403,6 +404,56 @@ void LocalSmoothingGradient(FESystem &fe) {
     check(yg_local_smoothing_gradient(fe.dofm.get(), Physics::nsd(), fe.getSolution().get(),
                                       fe.getSolutionGradient().get()),
           "LocalSmoothingGradient");
+}
+
+// ZZGradientRecovery<Physics>(FESystem&) (include/assembly/ZZGradientRecovery.hpp:33-140):
+// Zienkiewicz-Zhu patch recovery of the gradient of a p = 1 scalar solution;
+// read it with fe.getSolutionGradient() (n_nodes * nsd entries, row-major).
+template <typename Physics>
+void ZZGradientRecovery(FESystem &fe) {
+    fe.reset_gradient(Physics::nsd());
+    check(yg_zz_gradient_recovery(fe.dofm.get(), Physics::nsd(), fe.getSolution().get(),
+                                  fe.getSolutionGradient().get()),
+          "ZZGradientRecovery");
+}
+
+// SimulationOutput (include/output/SimulationOutput.hpp:22-116) with the VTU
+// backend: captureFrame(fe) writes fname_base.vtu, the reference's text.
+enum class BackendType { VTU };
+class SimulationOutput {
+public:
+    explicit SimulationOutput(std::string fname_base = "output", BackendType = BackendType::VTU)
+        : base_(std::move(fname_base)) {}
+    void captureFrame(FESystem &fe) {
+        check(yg_output_vtu(fe.getDoFManager().get(), base_.c_str(), fe.getSolution().get()),
+              "SimulationOutput::captureFrame");
+    }
+
+private:
+    std::string base_;
+};
+
+// Mesh(const std::string &fname) (src/mesh/parse_gmsh.cpp:80-193): a Gmsh 2.x file.
+inline Mesh read_gmsh(const std::string &fname) {
+    yg_mesh h = nullptr;
+    check(yg_mesh_read_gmsh(fname.c_str(), &h), "Mesh(fname)");
+    int32_t nn = 0, nc = 0;
+    int64_t ncn = 0, nt = 0;
+    yg_mesh_sizes(h, &nn, &nc, &ncn, &nt);
+    std::vector<double> xyz(3 * (size_t)nn);
+    std::vector<int32_t> cn(ncn), off(nc + 1), ct(nc), to(nc + 1), tg(nt);
+    yg_mesh_get(h, xyz.data(), cn.data(), off.data(), ct.data(), to.data(), tg.data());
+    yg_mesh_destroy(h);
+    Mesh m;
+    m.nodes.resize(nn);
+    for (int32_t i = 0; i < nn; ++i) m.nodes[i] = {xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]};
+    m.cellNodes.assign(cn.begin(), cn.end());
+    m.offsets.assign(off.begin(), off.end());
+    for (int32_t c = 0; c < nc; ++c) {
+        m.cellTypes.push_back(static_cast<CellType>(ct[c]));
+        m.cellTags.emplace_back(tg.begin() + to[c], tg.begin() + to[c + 1]);
+    }
+    return m;
 }
 
 // DirichletBC (include/boundary_conditions/DirichletBC.hpp:23-89)
