@@ -1,8 +1,10 @@
 """yg_dot_static_scratch, the dot product that allocates nothing, against
-yg_vector_dot on the same data: two calls in a row each agree within
-1e-12 * sum|x_i y_i| (both are fixed-order FP64 sums that differ only in
-order).  Calls go through the C ABI with device buffers that the test owns."""
+yg_vector_dot on the same data and against an exactly rounded host sum
+(math.fsum of the products): two calls in a row each agree within
+1e-12 * sum|x_i y_i| (fixed-order FP64 sums that differ only in order).  Calls
+go through the C ABI with device buffers that the test owns."""
 import ctypes as C
+import math
 
 import numpy as np
 import pytest
@@ -34,7 +36,9 @@ def test_static_scratch_dot_matches_vector_dot(ctx, n):
     rng = np.random.Generator(np.random.PCG64(n + 11))
     a, b = rng.standard_normal(n), rng.standard_normal(n)
     expect = vector_dot(a, b, ctx)
+    exact = math.fsum(a * b)
     scale = float(np.abs(a * b).sum())
+    assert abs(expect - exact) <= TOL * scale
     x = torch.from_numpy(a).to("cuda:0")
     y = torch.from_numpy(b).to("cuda:0")
     out = torch.full((2,), np.nan, dtype=torch.float64, device="cuda:0")
@@ -45,6 +49,7 @@ def test_static_scratch_dot_matches_vector_dot(ctx, n):
     got = out.cpu().numpy()
     for g in got:
         assert abs(g - expect) <= TOL * scale, (n, g, expect)
+        assert abs(g - exact) <= TOL * scale, (n, g, exact)
     assert got[0] == got[1]
 
 
