@@ -431,6 +431,23 @@ def assembly_flops_per_element(nq, nen, dpn, nsd):
     return 2 * nq * (s * s * n + s * n * n)
 
 
+def assembly_executed_flops_per_element(nq, nen, nsd):
+    """Flops k_assemble executes per 3D elasticity element: per quadrature point
+    the Jacobian (nen*nsd^2 multiply-adds) and its inverse (~60), the physical
+    gradients (nen*nsd^2 multiply-adds), and per node pair of the upper triangle
+    (nen(nen+1)/2) and point the dot product (6) and the scaled weight (1) plus
+    8 flops for each of the nsd^2 block entries."""
+    geometry = nq * (2 * nen * nsd * nsd + 60) + nq * nen * 2 * nsd * nsd
+    pairs = nen * (nen + 1) // 2
+    return geometry + pairs * nq * (7 + 8 * nsd * nsd)
+
+
+def assembly_scatter_bytes_per_element(nen, dpn):
+    """Bytes the element scatter moves per element: every one of its nen^2 node
+    blocks (dpn^2 FP64 values) read and written once."""
+    return nen * nen * dpn * dpn * 8 * 2
+
+
 def fp64_peak_tflops():
     """FP64 dense rate measured here: torch float64 8192^3 matmul (cuBLAS DGEMM),
     best of 5, CUDA events; None without torch CUDA."""
@@ -472,12 +489,20 @@ def run_assembly(ctx, dm, phys, nx, reps=5):
         ctx.synchronize()
         ts.append(time.perf_counter() - t0)
     t = min(ts)
-    flops = assembly_flops_per_element(27, 27, 3, 3) * nx ** 3
+    ne = nx ** 3
+    flops = assembly_flops_per_element(27, 27, 3, 3) * ne
+    executed = assembly_executed_flops_per_element(27, 27, 3) * ne
+    scatter = assembly_scatter_bytes_per_element(27, 3) * ne
     peak = fp64_peak_tflops()
     achieved = flops / t / 1e12
-    return {"elements": nx ** 3, "ms": t * 1e3, "algorithmic_flops": flops, "achieved_TFLOPs": achieved,
+    return {"elements": ne, "ms": t * 1e3, "algorithmic_flops": flops, "achieved_TFLOPs": achieved,
+            "executed_flops": executed, "executed_TFLOPs": executed / t / 1e12,
+            "scatter_bytes": scatter, "scatter_GBs": scatter / t / 1e9,
             "fp64_dgemm_TFLOPs_measured": peak, "frac_of_dgemm": (achieved / peak) if peak else None,
-            "bound": "FP64 FMA pipe (tcgen05 has no FP64 kind; element matrices use FP64 FMAs)"}
+            "executed_frac_of_dgemm": (executed / t / 1e12 / peak) if peak else None,
+            "note": "algorithmic = the B^T D B count; executed = what k_assemble does (node pairs of the upper "
+                    "triangle, 79 flops per pair and point, plus geometry); scatter = read-modify-write of every "
+                    "element block into the value array"}
 
 
 def run_ilu(ctx, nx=30):
