@@ -305,6 +305,8 @@ enum { YG_PRECOND_IDENTITY = 0, YG_PRECOND_JACOBI = 1, YG_PRECOND_ILU0 = 2 };
 YG_API yg_status yg_precond_create(yg_matrix A, int32_t kind, yg_precond *out);
 /* M.solve(z) in place (Preconditioner.hpp:9-21). */
 YG_API yg_status yg_precond_apply(yg_precond M, yg_vector z);
+/* Frees M; valid after A has been destroyed (M keeps A's context, not A), but
+ * not after that context has been destroyed. */
 YG_API yg_status yg_precond_destroy(yg_precond M);
 /* Number of zero pivots skipped while factoring (ILU(0)) or zero diagonals (Jacobi). */
 YG_API int64_t yg_precond_zero_pivots(yg_precond M);

@@ -88,6 +88,20 @@ def check_vector(v, ref, tol=VAL_TOL):
     assert np.abs(v - ref).max() <= tol * max(np.abs(ref).max(), 1e-300)
 
 
+def check_gradient(G, ref, tol=1e-12):
+    """The smoothed gradient at the nodes whose lumped volume is not zero.
+
+    A quadratic triangle's vertex shape functions integrate to zero, so a node
+    that is a vertex of quadratic triangles only divides a rounding-noise sum by
+    a rounding-noise volume (LocalSmoothingGradient.hpp:75-91): the reference
+    gives values of 1e9 and more there, whose digits carry nothing.  Those nodes
+    are told by the size of the reference value against the median."""
+    n = np.linalg.norm(ref, axis=1)
+    ok = n <= 1e4 * np.median(n)
+    assert ok.mean() > 0.5
+    check_vector(G[ok], ref[ok], tol)
+
+
 @pytest.mark.parametrize("name", CASES)
 @pytest.mark.parametrize("numbering", ["gpu", "reference"])
 @pytest.mark.parametrize("fmt", ["bcsr", "csr"])
@@ -122,7 +136,7 @@ def test_assembly_matches_reference(ctx, name, numbering, fmt):
     fe.getSolution().upload(c["grad_u"])
     yb.LocalSmoothingGradient(phys, fe)
     G = fe.solution_gradient.numpy().reshape(-1, c["nsd"])
-    check_vector(G, c["grad"], 1e-12)
+    check_gradient(G, c["grad"])
 
 
 def test_numbering_handed_over_is_checked(ctx):

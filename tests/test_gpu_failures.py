@@ -25,8 +25,8 @@ def poisson(n=32):
     return K, R
 
 
-@pytest.mark.parametrize("method", ["cg", "bicgstab"])
-@pytest.mark.parametrize("precision", [yb.PREC_FP64, yb.PREC_MIXED])
+@pytest.mark.parametrize("method,precision", [("cg", yb.PREC_FP64), ("cg", yb.PREC_MIXED),
+                                              ("bicgstab", yb.PREC_FP64)])
 def test_nan_rhs_reports_nan(ctx, method, precision):
     K, R = poisson()
     A = yb.sparse_csr.from_csr(K.row_ptr, K.col, K.val)
@@ -37,6 +37,32 @@ def test_nan_rhs_reports_nan(ctx, method, precision):
     # the context is still usable: the same system without the NaN converges
     x, st = yb.solve(A, R, M=yb.JacobiPreconditioner(A), method=method, tol=1e-10, precision=precision)
     assert st.status == _lib.YG_OK and st.rel_residual <= 1e-10
+
+
+def test_bicgstab_in_mixed_precision_is_unsupported(ctx):
+    """BiCGSTAB runs in FP64 only; another precision is refused before any launch."""
+    K, R = poisson()
+    A = yb.sparse_csr.from_csr(K.row_ptr, K.col, K.val)
+    with pytest.raises(yb.YafelError) as e:
+        yb.solve(A, R, M=yb.JacobiPreconditioner(A), method="bicgstab", precision=yb.PREC_MIXED)
+    assert e.value.status == _lib.YG_UNSUPPORTED
+
+
+def test_preconditioner_outlives_its_matrix(ctx):
+    """A garbage-collected cycle finalises objects in any order: a preconditioner
+    freed after its matrix touches only its own context."""
+    K, R = poisson()
+    A = yb.sparse_csr.from_csr(K.row_ptr, K.col, K.val)
+    for P in (yb.JacobiPreconditioner, yb.ILUPreconditioner):
+        M = P(A)
+        B = yb.sparse_csr.from_csr(K.row_ptr, K.col, K.val)
+        M2 = P(B)
+        _lib.check(_lib.lib().yg_matrix_destroy(B.h))
+        B.h = None
+        _lib.check(_lib.lib().yg_precond_destroy(M2.h))
+        M2.h = None
+    x, st = yb.solve(A, R, M=M, tol=1e-10)
+    assert st.status == _lib.YG_OK
 
 
 def test_budget_below_the_matrix_is_over_budget():

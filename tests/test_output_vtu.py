@@ -37,7 +37,7 @@ def test_mesh_text_matches_reference(tmp_path, name):
 def test_solution_text_matches_reference(ctx, tmp_path, name):
     mesh, p, dpn, u, _, text = case(name)
     dm = yb.DoFManager(mesh, p, dpn)
-    fe = yb.FESystem(dm, 2 if mesh["nodes"][:, 2].ptp() == 0 else 3)
+    fe = yb.FESystem(dm, 2 if np.ptp(mesh["nodes"][:, 2]) == 0 else 3)
     fe.getSolution().upload(u)
     base = str(tmp_path / "sol")
     yb.SimulationOutput(base).captureFrame(fe)

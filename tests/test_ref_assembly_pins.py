@@ -124,8 +124,13 @@ def test_oracle_matches_reference(name):
     assert_values(K.val, c["bc_val"], c["row_ptr"])
     assert np.abs(R - c["bc_rhs"]).max() <= VAL_TOL * max(np.abs(c["bc_rhs"]).max(), 1e-300)
     # LocalSmoothingGradient of a non-linear field
+    # (nodes that are vertices of quadratic triangles only have a zero lumped
+    # volume, LocalSmoothingGradient.hpp:75-91: noise over noise, not compared)
     G = O.local_smoothing_gradient(dm, c["dpn"], c["nsd"], c["grad_u"])
-    assert np.abs(G - c["grad"]).max() <= 1e-12 * np.abs(c["grad"]).max()
+    n = np.linalg.norm(c["grad"], axis=1)
+    ok = n <= 1e4 * np.median(n)
+    assert ok.mean() > 0.5
+    assert np.abs(G[ok] - c["grad"][ok]).max() <= 1e-12 * np.abs(c["grad"][ok]).max()
 
 
 def test_reference_quirks_visible_in_fixtures():

@@ -126,6 +126,7 @@ struct yg_matrix_t {
 
 struct yg_precond_t {
     yg_matrix A = nullptr;
+    yg_context ctx = nullptr;  // A's context: destroy must not touch A, which may already be gone
     int32_t kind = 0;
     double *d_dinv = nullptr;     // Jacobi: 1/a_ii (scalar diagonal)
     int64_t zero_pivots = 0;

@@ -367,6 +367,7 @@ extern "C" yg_status yg_precond_create(yg_matrix A, int32_t kind, yg_precond *ou
     *out = nullptr;
     auto *M = new yg_precond_t();
     M->A = A;
+    M->ctx = A->ctx;
     M->kind = kind;
     yg_context ctx = A->ctx;
     yg_status s = YG_OK;
@@ -401,7 +402,7 @@ extern "C" yg_status yg_precond_apply(yg_precond M, yg_vector z) {
 
 extern "C" yg_status yg_precond_destroy(yg_precond M) {
     if (!M) return YG_OK;
-    yg_context ctx = M->A->ctx;
+    yg_context ctx = M->ctx;
     for (void *p : {(void *)M->d_dinv, (void *)M->d_lu, (void *)M->d_lower_levels, (void *)M->d_upper_levels,
                     (void *)M->d_csr_rowptr, (void *)M->d_csr_col, (void *)M->d_csr_diag, (void *)M->d_tmp,
                     (void *)M->d_lower_ptr, (void *)M->d_upper_ptr, (void *)M->d_bar})
