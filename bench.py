@@ -103,10 +103,11 @@ TMA_CFG = {32: "64,3,4", 1: "32,4,8", 2: "32,3,8", 4: "32,2,8", 8: "32,3,12", 16
 
 
 def spmv_kernel_name(K, dot=1, vt="double"):
-    variant, lanes = K.get_spmv()
+    variant, lanes = K.get_spmv(0 if vt == "double" else 1)
     if variant == 2:
         cfg = TMA_CFG.get(lanes, "64,3,4")
-        return "k_bcsr_spmv_tma<3,%s,%d,TmaCfg<3,%s,%s>>" % (vt, dot, vt, cfg)
+        xf = ",true" if vt == "float" else ",false"
+        return "k_bcsr_spmv_tma<3,%s,%d,TmaCfg<3,%s,%s>%s>" % (vt, dot, vt, cfg, xf)
     if variant == 1:
         return "k_bcsr_spmv_staged<3,%s,%d>" % (vt, dot)
     return "k_bcsr_spmv<3,%d,%s,%d>" % (lanes, vt, dot)
@@ -127,6 +128,9 @@ def run_spmv_profile(args):
     K = fe.getGlobalTangent()
     if args.variant is not None:
         K.set_spmv(args.variant, args.lanes)
+    else:
+        K.make_fp32()
+        K.set_spmv(-1)  # the device autotuner, FP64 and FP32 values, as a solve runs it
     n = K.rows()
     x = yb.DeviceVector(np.random.default_rng(0).standard_normal(n), dm.ctx)
     if poisson:
@@ -137,7 +141,8 @@ def run_spmv_profile(args):
         cases = ((0, "fp64", nnz * 12 + 4 * (n + 1) + 16 * n), (1, "fp32_values", nnz * 8 + 4 * (n + 1) + 16 * n))
     else:
         nnzb = K.nnz() // 9
-        out = {"mesh": "%d^3 Q2 hex" % args.nx, "dofs": n, "blocks": nnzb, "kernel": spmv_kernel_name(K, 0)}
+        out = {"mesh": "%d^3 Q2 hex" % args.nx, "dofs": n, "blocks": nnzb, "kernel": spmv_kernel_name(K, 0),
+               "kernel_fp32": spmv_kernel_name(K, 0, "float"), "tuned": {"fp64": K.get_spmv(0), "fp32": K.get_spmv(1)}}
         cases = ((0, "fp64", bcsr3_spmv_bytes(nnzb, n)), (1, "fp32_values", nnzb * 40 + 4 * (n // 3 + 1) + 16 * n))
     for prec, name, nbytes in cases:
         if args.spmv_precision != "both" and name.split("_")[0] != args.spmv_precision:

@@ -289,6 +289,9 @@ YG_API yg_status yg_spmv_ex(yg_matrix A, yg_vector x, yg_vector y, int32_t preci
  * first SpMV or solve of a matrix). */
 YG_API yg_status yg_matrix_set_spmv(yg_matrix A, int32_t variant, int32_t lanes);
 YG_API yg_status yg_matrix_get_spmv(yg_matrix A, int32_t *variant, int32_t *lanes);
+/* The SpMV kernel used for FP64 values (precision YG_PREC_FP64) or for the FP32
+ * value copy (any other precision). */
+YG_API yg_status yg_matrix_get_spmv_for(yg_matrix A, int32_t precision, int32_t *variant, int32_t *lanes);
 /* Average device time of `reps` back-to-back SpMVs (CUDA events on the
  * context's stream), for roofline measurements. */
 YG_API yg_status yg_spmv_bench(yg_matrix A, yg_vector x, yg_vector y, int32_t precision, int32_t reps,

@@ -432,9 +432,11 @@ class _Matrix:
         row chunks (2x2/3x3 blocks), 3 bulk-copy row tiles (CSR), -1 autotune."""
         check(lib().yg_matrix_set_spmv(self.h, int(variant), int(lanes)))
 
-    def get_spmv(self):
+    def get_spmv(self, precision=PREC_FP64):
+        """(variant, lanes) of the SpMV kernel for FP64 values or, with another
+        precision, for the FP32 value copy."""
         v, l = C.c_int32(), C.c_int32()
-        check(lib().yg_matrix_get_spmv(self.h, C.byref(v), C.byref(l)))
+        check(lib().yg_matrix_get_spmv_for(self.h, int(precision), C.byref(v), C.byref(l)))
         return v.value, l.value
 
     def spmv_bench(self, reps=10, precision=PREC_FP64, x=None):

@@ -76,6 +76,7 @@ SIGNATURES = {
     "yg_spmv_ex": (i32, [vp, vp, vp, i32]),
     "yg_matrix_set_spmv": (i32, [vp, i32, i32]),
     "yg_matrix_get_spmv": (i32, [vp, P(i32), P(i32)]),
+    "yg_matrix_get_spmv_for": (i32, [vp, i32, P(i32), P(i32)]),
     "yg_spmv_bench": (i32, [vp, vp, vp, i32, i32, P(f64)]),
     "yg_precond_create": (i32, [vp, i32, P(vp)]),
     "yg_precond_apply": (i32, [vp, vp]),

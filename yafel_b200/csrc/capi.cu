@@ -156,6 +156,13 @@ __global__ void k_to_fp32(const double *__restrict__ v, float *__restrict__ o, i
         o[i] = (float)v[i];
 }
 
+// x rounded to FP32 in the node-padded gather layout of the FP32-value SpMV
+// (xs floats per node of B values; the padding stays zero).
+__global__ void k_to_x32(const double *__restrict__ x, float *__restrict__ x32, int64_t n, int B, int xs) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        x32[(i / B) * xs + i % B] = (float)x[i];
+}
+
 // A kernel whose bounded wait expired leaves YG_TIMEOUT in the context's error
 // word; report it (once) and clear it.
 yg_status check_device_error(yg_context ctx) {
@@ -555,6 +562,14 @@ extern "C" yg_status yg_matrix_get_spmv(yg_matrix A, int32_t *variant, int32_t *
     return YG_OK;
 }
 
+extern "C" yg_status yg_matrix_get_spmv_for(yg_matrix A, int32_t precision, int32_t *variant, int32_t *lanes) {
+    if (!A) return fail(YG_BAD_ARG, "NULL matrix");
+    const bool f32 = precision != YG_PREC_FP64;
+    if (variant) *variant = f32 ? A->variant32 : A->variant;
+    if (lanes) *lanes = f32 ? A->lanes32 : A->lanes;
+    return YG_OK;
+}
+
 extern "C" yg_status yg_spmv_bench(yg_matrix A, yg_vector x, yg_vector y, int32_t precision, int32_t reps,
                                    double *ms_per_launch) {
     if (!A || !x || !y || reps < 1 || !ms_per_launch) return fail(YG_BAD_ARG, "yg_spmv_bench: bad argument");
@@ -562,18 +577,34 @@ extern "C" yg_status yg_spmv_bench(yg_matrix A, yg_vector x, yg_vector y, int32_
     if (precision == YG_PREC_MIXED && !A->d_val32) YG_TRY(yg_matrix_make_fp32(A));
     yg_context ctx = A->ctx;
     int grid = spmv_grid_for(A, precision);
-    YG_TRY(spmv_launch(A, x->d, y->d, precision, nullptr, nullptr, grid));
-    cudaEvent_t e0, e1;
-    YG_CUDA(cudaEventCreate(&e0));
-    YG_CUDA(cudaEventCreate(&e1));
-    cudaEventRecord(e0, ctx->stream);
-    for (int r = 0; r < reps; ++r) YG_TRY(spmv_launch(A, x->d, y->d, precision, nullptr, nullptr, grid));
-    cudaEventRecord(e1, ctx->stream);
-    YG_CUDA(cudaEventSynchronize(e1));
+    // the FP32-value form the mixed-precision solvers run: with 2x2/3x3 blocks x
+    // is gathered from an FP32 node-padded copy
+    float *x32 = nullptr;
+    if (precision == YG_PREC_MIXED && (A->block == 2 || A->block == 3)) {
+        const int xs = spmv_x32_stride(A->block);
+        const int64_t m32 = (A->cols() / A->block + 1) * xs;
+        YG_TRY(dev_alloc_t(ctx, &x32, m32));
+        cudaMemsetAsync(x32, 0, sizeof(float) * m32, ctx->stream);
+        k_to_x32<<<stream_grid(ctx, x->n), kThreads, 0, ctx->stream>>>(x->d, x32, x->n, A->block, xs);
+        YG_LAUNCHED(ctx);
+    }
+    yg_status s = spmv_launch(A, x->d, y->d, precision, nullptr, nullptr, grid, x32);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (s == YG_OK && (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess))
+        s = fail(YG_CUDA_ERROR, "yg_spmv_bench: events");
     float ms = 0;
-    cudaEventElapsedTime(&ms, e0, e1);
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
+    if (s == YG_OK) {
+        cudaEventRecord(e0, ctx->stream);
+        for (int r = 0; r < reps && s == YG_OK; ++r) s = spmv_launch(A, x->d, y->d, precision, nullptr, nullptr, grid, x32);
+        cudaEventRecord(e1, ctx->stream);
+        if (cudaEventSynchronize(e1) != cudaSuccess) s = fail(YG_CUDA_ERROR, "yg_spmv_bench: launch");
+        cudaEventElapsedTime(&ms, e0, e1);
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaStreamSynchronize(ctx->stream);
+    dev_free(ctx, x32);
+    if (s != YG_OK) return s;
     *ms_per_launch = ms / reps;
     return check_device_error(ctx);
 }
