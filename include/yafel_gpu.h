@@ -271,9 +271,14 @@ YG_API yg_status yg_matrix_get(yg_matrix A, int64_t *brow_ptr, int64_t *bcol, do
 YG_API yg_status yg_matrix_make_fp32(yg_matrix A);
 
 /* y = A*x: csr_spmv / bcsr_spmv via operator* (include/old_handmade_linalg/csr_spmv.hpp:25-56,
- * bcsr_spmv.hpp:23-62, operators.hpp:117-131).  precision: YG_PREC_FP64 or
- * YG_PREC_MIXED (FP32 values, FP64 vectors and accumulation). */
-enum { YG_PREC_FP64 = 0, YG_PREC_MIXED = 1, YG_PREC_MIXED_IR = 2 };
+ * bcsr_spmv.hpp:23-62, operators.hpp:117-131).  precision: YG_PREC_FP64,
+ * YG_PREC_MIXED (FP32 values, FP64 vectors and accumulation) or
+ * YG_SPMV_MIXED_CORRECTED (no reference counterpart): FP32 values plus, per
+ * block row r, y_r += C_r x_r with C_r the FP64 sum over the row's blocks of
+ * A_rj - fl32(A_rj) -- the operator the mixed-precision solvers iterate with;
+ * it keeps A's block row sums, so it is exact on per-component constant x
+ * (square matrices only). */
+enum { YG_PREC_FP64 = 0, YG_PREC_MIXED = 1, YG_PREC_MIXED_IR = 2, YG_SPMV_MIXED_CORRECTED = 3 };
 YG_API yg_status yg_spmv(yg_matrix A, yg_vector x, yg_vector y);
 YG_API yg_status yg_spmv_ex(yg_matrix A, yg_vector x, yg_vector y, int32_t precision);
 
@@ -327,7 +332,8 @@ enum { YG_CRIT_REFERENCE = 0, YG_CRIT_RELRES = 1 };
 typedef struct yg_solve_opts {
     int32_t criterion;  /* YG_CRIT_* */
     int32_t precision;  /* YG_PREC_FP64; YG_PREC_MIXED: the iteration's SpMV reads FP32 values (FP64
-                           vectors, accumulation and dots) and the residual is replaced by the FP64
+                           vectors, accumulation and dots; the FP32 operator carries the row-sum
+                           correction of YG_SPMV_MIXED_CORRECTED) and the residual is replaced by the FP64
                            true residual b - A x whenever it fell 10x -- each replacement is an FP64
                            refinement step; YG_PREC_MIXED_IR: restarted FP64 iterative refinement
                            around FP32-SpMV PCG inner solves */

@@ -109,6 +109,51 @@ def test_csr_row_tiles_edge_cases(ctx):
         assert np.array_equal(A4 * x[:1].repeat(5000), d * x[0]), L
 
 
+def corrected_fp32_oracle(rp, col, val, B, x):
+    """A32 x + C x_own: FP32-rounded values, plus per block row the FP64 sum of
+    (A - fl32(A)) over its blocks times the row's own entries of x."""
+    v32 = val.astype(np.float32).astype(np.float64)
+    y = bcsr_to_oracle_csr(rp, col, v32, B).spmv(x)
+    nb = rp.size - 1
+    brow = np.repeat(np.arange(nb), np.diff(rp))
+    C = np.zeros((nb, B, B))
+    np.add.at(C, brow, (val - v32).reshape(-1, B, B))
+    return y + np.einsum("rik,rk->ri", C, x.reshape(nb, B)).ravel()
+
+
+@pytest.mark.parametrize("B,per_row", [(1, 30), (2, 9), (3, 40)])
+def test_spmv_mixed_corrected(ctx, B, per_row):
+    """The corrected FP32 operator of the mixed-precision solvers (FP32 values
+    plus the FP64 row-sum correction) in every SpMV variant against the same
+    operator in numpy; on a per-component constant x it reproduces the FP64
+    product to FP64 rounding, where the plain FP32 values are off by about
+    1e-8 of the scale."""
+    rp, col, val = random_block_matrix(2500, B, per_row, seed=40 + B)
+    A = yb.sparse_bcsr.from_bcsr(B, rp, col, val) if B > 1 else yb.sparse_csr.from_csr(rp, col, val)
+    rng = np.random.Generator(np.random.PCG64(5))
+    x = rng.standard_normal(A.cols())
+    yo = corrected_fp32_oracle(rp, col, val, B, x)
+    scale = np.abs(val).max() * np.abs(x).max() * (per_row + 1) * B
+    xc = np.tile(np.arange(1.0, B + 1.0), A.cols() // B)
+    y64c = bcsr_to_oracle_csr(rp, col, val, B).spmv(xc)
+    variants = [(0, 8), (0, 32)] + ([(1, 32), (2, 4), (2, 8), (2, 32)] if B > 1 else [(3, 2)]) + [(-1, 32)]
+    for v, L in variants:
+        A.set_spmv(v, L)
+        y = A.spmv(x, precision=yb.SPMV_MIXED_CORRECTED).numpy()
+        assert np.abs(y - yo).max() <= 1e-14 * scale, (v, L)
+        yc = A.spmv(xc, precision=yb.SPMV_MIXED_CORRECTED).numpy()
+        assert np.abs(yc - y64c).max() <= 1e-14 * scale, (v, L)
+    y32c = A.spmv(xc, precision=yb.PREC_MIXED).numpy()
+    assert np.abs(y32c - y64c).max() > 1e-12 * scale  # the plain FP32 values are not exact there
+    # a non-square matrix has no correction
+    if B == 1:
+        R = yb.sparse_csr.from_csr(np.array([0, 2, 3]), np.array([0, 2, 1]), np.array([1.0, 2.0, 3.0]), ncols=3)
+        with pytest.raises(Exception):
+            R.spmv(np.ones(3), precision=yb.SPMV_MIXED_CORRECTED)
+    with pytest.raises(Exception):
+        A.spmv(x, precision=7)
+
+
 @pytest.mark.parametrize("B", [1, 3])
 def test_spmv_mixed_precision(ctx, B):
     rp, col, val = random_block_matrix(2000, B, 20, seed=3 + B)

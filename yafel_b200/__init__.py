@@ -28,6 +28,7 @@ CG_SOLVER_TOL = 1.0e-14
 
 CSR, BCSR = 0, 1
 PREC_FP64, PREC_MIXED, PREC_MIXED_IR = 0, 1, 2
+SPMV_MIXED_CORRECTED = 3  # FP32 values + FP64 row-sum correction (the mixed solvers' operator)
 METHOD_CG, METHOD_BICGSTAB = 0, 1
 CRIT_REFERENCE, CRIT_RELRES = 0, 1
 POISSON, ELASTICITY, SUPG = 0, 1, 2

@@ -156,6 +156,42 @@ __global__ void k_to_fp32(const double *__restrict__ v, float *__restrict__ o, i
         o[i] = (float)v[i];
 }
 
+// Row-sum correction of the FP32 values: corr[r][i][k] = sum over the blocks
+// j of block row r of (A_rj[i][k] - fl32(A_rj[i][k])), in FP64.  A warp per
+// block row; each lane sums its blocks (lane-strided), then a fixed butterfly,
+// so the result does not change from run to run.  With it, A32 x + C x_r is
+// exact on fields that are constant per component (A's block row sums are
+// kept), which removes most of the FP32 rounding seen by the smooth error
+// components that limit the mixed-precision solvers.
+template <int B>
+__global__ void k_fp32_correction(int64_t nbrows, const int32_t *__restrict__ rowptr, const double *__restrict__ v,
+                                  double *__restrict__ corr) {
+    constexpr int B2 = B * B;
+    const int lane = threadIdx.x & 31;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t r = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; r < nbrows; r += nw) {
+        double s[B2];
+#pragma unroll
+        for (int e = 0; e < B2; ++e) s[e] = 0;
+        const int rs = rowptr[r], re = rowptr[r + 1];
+        for (int j = rs + lane; j < re; j += 32) {
+#pragma unroll
+            for (int e = 0; e < B2; ++e) {
+                const double a = v[(int64_t)j * B2 + e];
+                s[e] += a - (double)(float)a;
+            }
+        }
+#pragma unroll
+        for (int e = 0; e < B2; ++e) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) s[e] += __shfl_xor_sync(0xffffffffu, s[e], o);
+        }
+        if (lane == 0)
+#pragma unroll
+            for (int e = 0; e < B2; ++e) corr[r * B2 + e] = s[e];
+    }
+}
+
 // x rounded to FP32 in the node-padded gather layout of the FP32-value SpMV
 // (xs floats per node of B values; the padding stays zero).
 __global__ void k_to_x32(const double *__restrict__ x, float *__restrict__ x32, int64_t n, int B, int xs) {
@@ -473,6 +509,7 @@ extern "C" yg_status yg_matrix_destroy(yg_matrix A) {
     dev_free(ctx, A->d_col);
     dev_free(ctx, A->d_val);
     dev_free(ctx, A->d_val32);
+    dev_free(ctx, A->d_corr32);
     dev_free(ctx, A->d_diag);
     for (int k = 0; k < 3; ++k) dev_free(ctx, A->d_ctiles[k]);
     for (void *p : {(void *)A->d_bcmask, (void *)A->d_bcg, (void *)A->d_bcq, (void *)A->d_bcvals, (void *)A->d_bcdofs})
@@ -515,6 +552,16 @@ extern "C" yg_status yg_matrix_make_fp32(yg_matrix A) {
     if (!A->d_val32) YG_TRY(dev_alloc_t(ctx, &A->d_val32, n));
     k_to_fp32<<<stream_grid(ctx, n), kThreads, 0, ctx->stream>>>(A->d_val, A->d_val32, n);
     YG_LAUNCHED(ctx);
+    const int grid = (int)std::min<int64_t>((A->nbrows + kThreads / 32 - 1) / (kThreads / 32), (int64_t)ctx->num_sms * 8);
+    if (A->block <= 3 && A->nbrows == A->nbcols && grid > 0) {  // square, a block size the SpMV kernels take
+        if (!A->d_corr32) YG_TRY(dev_alloc_t(ctx, &A->d_corr32, A->nbrows * A->block * A->block));
+        switch (A->block) {
+        case 1: k_fp32_correction<1><<<grid, kThreads, 0, ctx->stream>>>(A->nbrows, A->d_rowptr, A->d_val, A->d_corr32); break;
+        case 2: k_fp32_correction<2><<<grid, kThreads, 0, ctx->stream>>>(A->nbrows, A->d_rowptr, A->d_val, A->d_corr32); break;
+        default: k_fp32_correction<3><<<grid, kThreads, 0, ctx->stream>>>(A->nbrows, A->d_rowptr, A->d_val, A->d_corr32); break;
+        }
+        YG_LAUNCHED(ctx);
+    }
     YG_CUDA(cudaGetLastError());
     return YG_OK;
 }
@@ -524,9 +571,15 @@ extern "C" yg_status yg_spmv_ex(yg_matrix A, yg_vector x, yg_vector y, int32_t p
     if (x->n != A->cols() || y->n != A->rows())
         return fail(YG_BAD_ARG, "yg_spmv: dimension mismatch (A %lldx%lld, x %lld, y %lld)", (long long)A->rows(),
                     (long long)A->cols(), (long long)x->n, (long long)y->n);
+    if (precision != YG_PREC_FP64 && precision != YG_PREC_MIXED && precision != YG_SPMV_MIXED_CORRECTED)
+        return fail(YG_BAD_ARG, "yg_spmv: precision %d is not an SpMV precision", (int)precision);
+    const bool corrected = precision == YG_SPMV_MIXED_CORRECTED;
+    if (corrected) precision = YG_PREC_MIXED;
     if (precision == YG_PREC_MIXED && !A->d_val32) YG_TRY(yg_matrix_make_fp32(A));
+    if (corrected && !A->d_corr32) return fail(YG_UNSUPPORTED, "yg_spmv: the row-sum correction needs a square matrix");
     YG_TRY(spmv_autotune_device(A));
-    YG_TRY(spmv_launch(A, x->d, y->d, precision, nullptr, nullptr, spmv_default_grid(A)));
+    YG_TRY(spmv_launch(A, x->d, y->d, precision, nullptr, nullptr, spmv_default_grid(A), nullptr,
+                       corrected ? A->d_corr32 : nullptr));
     YG_CUDA(cudaStreamSynchronize(A->ctx->stream));
     return check_device_error(A->ctx);
 }
@@ -574,7 +627,12 @@ extern "C" yg_status yg_spmv_bench(yg_matrix A, yg_vector x, yg_vector y, int32_
                                    double *ms_per_launch) {
     if (!A || !x || !y || reps < 1 || !ms_per_launch) return fail(YG_BAD_ARG, "yg_spmv_bench: bad argument");
     if (x->n != A->cols() || y->n != A->rows()) return fail(YG_BAD_ARG, "yg_spmv_bench: dimension mismatch");
+    if (precision != YG_PREC_FP64 && precision != YG_PREC_MIXED && precision != YG_SPMV_MIXED_CORRECTED)
+        return fail(YG_BAD_ARG, "yg_spmv_bench: precision %d is not an SpMV precision", (int)precision);
+    const bool corrected = precision == YG_SPMV_MIXED_CORRECTED;
+    if (corrected) precision = YG_PREC_MIXED;
     if (precision == YG_PREC_MIXED && !A->d_val32) YG_TRY(yg_matrix_make_fp32(A));
+    const double *corr = corrected ? A->d_corr32 : nullptr;
     yg_context ctx = A->ctx;
     int grid = spmv_grid_for(A, precision);
     // the FP32-value form the mixed-precision solvers run: with 2x2/3x3 blocks x
@@ -588,14 +646,15 @@ extern "C" yg_status yg_spmv_bench(yg_matrix A, yg_vector x, yg_vector y, int32_
         k_to_x32<<<stream_grid(ctx, x->n), kThreads, 0, ctx->stream>>>(x->d, x32, x->n, A->block, xs);
         YG_LAUNCHED(ctx);
     }
-    yg_status s = spmv_launch(A, x->d, y->d, precision, nullptr, nullptr, grid, x32);
+    yg_status s = spmv_launch(A, x->d, y->d, precision, nullptr, nullptr, grid, x32, corr);
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (s == YG_OK && (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess))
         s = fail(YG_CUDA_ERROR, "yg_spmv_bench: events");
     float ms = 0;
     if (s == YG_OK) {
         cudaEventRecord(e0, ctx->stream);
-        for (int r = 0; r < reps && s == YG_OK; ++r) s = spmv_launch(A, x->d, y->d, precision, nullptr, nullptr, grid, x32);
+        for (int r = 0; r < reps && s == YG_OK; ++r)
+            s = spmv_launch(A, x->d, y->d, precision, nullptr, nullptr, grid, x32, corr);
         cudaEventRecord(e1, ctx->stream);
         if (cudaEventSynchronize(e1) != cudaSuccess) s = fail(YG_CUDA_ERROR, "yg_spmv_bench: launch");
         cudaEventElapsedTime(&ms, e0, e1);

@@ -100,6 +100,10 @@ struct yg_matrix_t {
     int32_t *d_col = nullptr;     // nnzb
     double *d_val = nullptr;      // nnzb*block*block (row-major blocks)
     float *d_val32 = nullptr;     // optional FP32 copy
+    // with the FP32 copy: per block row, the FP64 sum over its blocks of
+    // (A_ij - fl32(A_ij)) (B*B per block row, row-major), so that the
+    // mixed-precision solvers' operator A32 x + C x_own keeps A's block row sums
+    double *d_corr32 = nullptr;
     int32_t *d_diag = nullptr;    // position of the diagonal block in each block row, -1 if absent
     int lanes = 32;               // SpMV lanes per block row (flat variant)
     int variant = 0;              // SpMV variant: 0 flat lane-strided, 1 cp.async staged, 2 TMA bulk staged (B = 2, 3),
@@ -154,11 +158,14 @@ yg_status dev_alloc_t(yg_context ctx, T **p, size_t count) {
 // x32 (optional, FP32-value precisions only): the same vector rounded to FP32 in
 // the node-padded layout of spmv_x32_stride(); the TMA kernels then gather it
 // with one vector load per block instead of B scalar FP64 loads.
+// corr (optional, FP32-value precisions only): the matrix's d_corr32; each
+// block row r then gets y_r += corr_r x_r (FP64), the corrected FP32 operator
+// of the mixed-precision solvers.
 yg_status spmv_launch(yg_matrix A, const double *x, double *y, int precision, double *partials_dot,
-                      const int32_t *flag, int grid, const float *x32 = nullptr);
+                      const int32_t *flag, int grid, const float *x32 = nullptr, const double *corr = nullptr);
 yg_status spmv_launch_ex(yg_matrix A, const double *x, double *y, int precision, const double *w, double *partials,
                          int dot_mode, const int32_t *flag, int grid, cudaStream_t stream = nullptr,
-                         const float *x32 = nullptr);
+                         const float *x32 = nullptr, const double *corr = nullptr);
 // Floats per block row of an FP32 gather copy: 4 for 3x3 blocks (16-byte rows),
 // else the block size.
 inline int spmv_x32_stride(int block) { return block == 3 ? 4 : block; }

@@ -361,11 +361,14 @@ static yg_status pcg_core(yg_matrix A, yg_precond M, const double *b, double *x,
     double *P = ctx->d_partials;  // [0,G): p.q ; [2G,4G): r.z/r.r pairs ; [4G, 7G): init triples
     KrylovScalars *S = ctx->d_scalars;
     cudaStream_t st = ctx->stream;
-    // the FP32 direction copy serves the FP32-value iteration SpMV only
-    const Dir32 d32 = (precision == YG_PREC_MIXED || precision == YG_PREC_MIXED_IR) ? w.d32 : Dir32{};
+    // the FP32 direction copy serves the FP32-value iteration SpMV only; so does
+    // the row-sum correction of the FP32 values (the operator A32 x + C x_own)
+    const bool f32 = precision == YG_PREC_MIXED || precision == YG_PREC_MIXED_IR;
+    const Dir32 d32 = f32 ? w.d32 : Dir32{};
+    const double *corr = f32 ? A->d_corr32 : nullptr;
 
     // r = b - A x ; z = M^-1 r ; p = z
-    YG_TRY(spmv_launch(A, x, w.q, precision, nullptr, nullptr, spmv_grid));
+    YG_TRY(spmv_launch(A, x, w.q, precision, nullptr, nullptr, spmv_grid, nullptr, corr));
     if (fused) {
         k_residual_init<<<G, kThreads, 0, st>>>(n, b, w.q, w.r, nullptr, dinv, P + 4 * G);
         YG_LAUNCHED(ctx);
@@ -387,7 +390,7 @@ static yg_status pcg_core(yg_matrix A, yg_precond M, const double *b, double *x,
     int slot = 0;
     auto one = [&](int parity) -> yg_status {
         if (prof && prof->on) YG_CUDA(cudaEventRecordWithFlags(prof->start[slot], st, cudaEventRecordExternal));
-        YG_TRY(spmv_launch(A, w.p, w.q, precision, P, &S->flag, spmv_grid, d32.p32));
+        YG_TRY(spmv_launch(A, w.p, w.q, precision, P, &S->flag, spmv_grid, d32.p32, corr));
         if (prof && prof->on) YG_CUDA(cudaEventRecordWithFlags(prof->stop[slot], st, cudaEventRecordExternal));
         ++slot;
         if (fused) {
@@ -587,6 +590,9 @@ extern "C" yg_status yg_cg(yg_matrix A, yg_precond M, yg_vector b, yg_vector x, 
     if (A->rows() != A->cols() || b->n != A->rows() || x->n != A->rows())
         return fail(YG_BAD_ARG, "yg_cg: dimension mismatch");
     if (M && M->A->rows() != A->rows()) return fail(YG_BAD_ARG, "yg_cg: preconditioner size mismatch");
+    if (opts && opts->precision != YG_PREC_FP64 && opts->precision != YG_PREC_MIXED &&
+        opts->precision != YG_PREC_MIXED_IR)
+        return fail(YG_BAD_ARG, "yg_cg: precision %d is not a solver precision", (int)opts->precision);
     YG_TRY(spmv_autotune_device(A));
     yg_status s = solve_cg(A, M, b, x, opts, stats);
     if (s != YG_OK && s != YG_NOT_CONVERGED && s != YG_BREAKDOWN && s != YG_NAN) return s;

@@ -21,13 +21,31 @@
 
 namespace yg {
 
+// Corrected FP32 operator: s += corr_r x_r, row i of the block row's FP64
+// correction (corr, B*B per block row) times the row's own entries of x (FP64).
+template <int B>
+__device__ __forceinline__ void add_corr(const double *__restrict__ corr, const double *__restrict__ x, int64_t r,
+                                         double (&s)[B]) {
+    double xr[B];
+#pragma unroll
+    for (int k = 0; k < B; ++k) xr[k] = x[(int64_t)B * r + k];
+#pragma unroll
+    for (int i = 0; i < B; ++i) {
+        const double *c = corr + ((int64_t)B * r + i) * B;
+        double t = c[0] * xr[0];
+#pragma unroll
+        for (int k = 1; k < B; ++k) t = fma(c[k], xr[k], t);
+        s[i] += t;
+    }
+}
+
 // DOT = 0: y = A x.  DOT = 1: also per-block sums of w.y.  DOT = 2: per-block
 // sums of w.y and y.y (partials[2b], partials[2b+1]).
 template <int B, int L, typename VT, int DOT>
 __global__ void __launch_bounds__(kThreads, B == 1 ? 8 : 1)
 k_bcsr_spmv(int64_t nbrows, const int32_t *__restrict__ rowptr, const int32_t *__restrict__ col,
             const VT *__restrict__ val, const double *__restrict__ x, double *__restrict__ y,
-            const double *__restrict__ w, double *__restrict__ partials, const int32_t *__restrict__ flag) {
+            const double *__restrict__ w, double *__restrict__ partials, const int32_t *__restrict__ flag, const double *__restrict__ corr) {
     __shared__ double sm[kThreads / 32 + 1];
     if (flag && read_flag(flag)) return;
     constexpr int B2 = B * B;
@@ -73,6 +91,7 @@ k_bcsr_spmv(int64_t nbrows, const int32_t *__restrict__ rowptr, const int32_t *_
 #pragma unroll
             for (int o = L / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
             if (r < nbrows && glane == 0) {
+                if (corr) acc = fma(corr[r], x[r], acc);
                 y[r] = acc;
                 if (DOT >= 1) dot = fma(acc, w[r], dot);
                 if (DOT == 2) yy = fma(acc, acc, yy);
@@ -114,6 +133,7 @@ k_bcsr_spmv(int64_t nbrows, const int32_t *__restrict__ rowptr, const int32_t *_
             for (int o = L / 2; o > 0; o >>= 1) acc[i] += __shfl_xor_sync(0xffffffffu, acc[i], o);
         }
         if (r < nbrows && glane == 0) {
+            if (corr) add_corr<B>(corr, x, r, acc);
 #pragma unroll
             for (int i = 0; i < B; ++i) {
                 y[B * r + i] = acc[i];
@@ -183,7 +203,7 @@ template <int B, typename VT, int DOT>
 __global__ void __launch_bounds__(Staged<B, VT>::WARPS * 32)
 k_bcsr_spmv_staged(int64_t nbrows, const int32_t *__restrict__ rowptr, const int32_t *__restrict__ col,
                    const VT *__restrict__ val, const double *__restrict__ x, double *__restrict__ y,
-                   const double *__restrict__ w, double *__restrict__ partials, const int32_t *__restrict__ flag) {
+                   const double *__restrict__ w, double *__restrict__ partials, const int32_t *__restrict__ flag, const double *__restrict__ corr) {
     using S = Staged<B, VT>;
     constexpr int B2 = B * B;
     constexpr int BB = B2 * (int)sizeof(VT);  // value bytes per block
@@ -256,6 +276,7 @@ k_bcsr_spmv_staged(int64_t nbrows, const int32_t *__restrict__ rowptr, const int
                 for (int o = 16; o > 0; o >>= 1) acc[i] += __shfl_xor_sync(0xffffffffu, acc[i], o);
             }
             if (lane == 0) {
+                if (corr) add_corr<B>(corr, x, cc.r, acc);
 #pragma unroll
                 for (int i = 0; i < B; ++i) {
                     y[B * cc.r + i] = acc[i];
@@ -336,7 +357,7 @@ __global__ void __launch_bounds__(C::WARPS * 32)
 k_bcsr_spmv_tma(int64_t nbrows, const int32_t *__restrict__ rowptr, const int32_t *__restrict__ col,
                 const VT *__restrict__ val, const double *__restrict__ x, const float *__restrict__ x32,
                 double *__restrict__ y, const double *__restrict__ w, double *__restrict__ partials,
-                const int32_t *__restrict__ flag, int32_t *__restrict__ err) {
+                const int32_t *__restrict__ flag, const double *__restrict__ corr, int32_t *__restrict__ err) {
     constexpr int B2 = B * B;
     constexpr int BB = B2 * (int)sizeof(VT);
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -390,6 +411,7 @@ k_bcsr_spmv_tma(int64_t nbrows, const int32_t *__restrict__ rowptr, const int32_
     double acc[B], acc2[B];
 #pragma unroll
     for (int i = 0; i < B; ++i) acc[i] = acc2[i] = 0;
+    double cv = 0, xo = 0;  // with corr: lane l < B*B holds corr_r[l], lane l < B holds x_r[l]
     int st = 0;
     unsigned phase = 0;  // bit k: parity of stage k's next completion
     bool timed_out = false;
@@ -411,6 +433,10 @@ k_bcsr_spmv_tma(int64_t nbrows, const int32_t *__restrict__ rowptr, const int32_
         phase ^= (1u << st);
         __syncwarp();
         const int nb = max(0, min(C::CH, cc.re - cc.rs - cc.b0));
+        if (corr && cc.b0 == 0) {  // first chunk of the row: its correction, used when the row completes
+            if (lane < B2) cv = corr[cc.r * B2 + lane];
+            if (lane < B) xo = x[B * cc.r + lane];
+        }
         const unsigned char *stg = ring + st * C::STAGE;
         const VT *blk = reinterpret_cast<const VT *>(stg + leads[wib][st][0]);
         const int32_t *cix = reinterpret_cast<const int32_t *>(stg + C::VBYTES + leads[wib][st][1]);
@@ -444,6 +470,15 @@ k_bcsr_spmv_tma(int64_t nbrows, const int32_t *__restrict__ rowptr, const int32_
                 acc[i] += acc2[i];
 #pragma unroll
                 for (int o = 16; o > 0; o >>= 1) acc[i] += __shfl_xor_sync(0xffffffffu, acc[i], o);
+            }
+            if (corr) {
+                // lane B*i+k holds corr_r[i][k]; row i's term sums lanes B*i .. B*i+B-1 in order
+                const double pr = cv * __shfl_sync(0xffffffffu, xo, lane % B);
+                double t = pr;
+#pragma unroll
+                for (int k = 1; k < B; ++k) t += __shfl_down_sync(0xffffffffu, pr, k);
+#pragma unroll
+                for (int i = 0; i < B; ++i) acc[i] += __shfl_sync(0xffffffffu, t, B * i);
             }
             if (lane == 0) {
 #pragma unroll
@@ -529,7 +564,7 @@ __global__ void __launch_bounds__(C::WARPS * 32)
 k_csr_spmv_tiles(int64_t ntiles, const int32_t *__restrict__ tiles, const int32_t *__restrict__ rowptr,
                  const int32_t *__restrict__ col, const VT *__restrict__ val, const double *__restrict__ x,
                  double *__restrict__ y, const double *__restrict__ w, double *__restrict__ partials,
-                 const int32_t *__restrict__ flag, int32_t *__restrict__ err) {
+                 const int32_t *__restrict__ flag, const double *__restrict__ corr, int32_t *__restrict__ err) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ double red[C::WARPS + 1];
     __shared__ int hdr[C::WARPS][C::NST][4];  // r0, r1, e0, e1 of the tile in each stage
@@ -635,6 +670,7 @@ k_csr_spmv_tiles(int64_t ntiles, const int32_t *__restrict__ tiles, const int32_
             const int a = rp[r] - e0, b = rp[r + 1] - e0;
             double sum = 0;
             for (int k = a; k < b; ++k) sum += prod[k];
+            if (corr) sum = fma(corr[r0 + r], x[r0 + r], sum);
             y[r0 + r] = sum;
             if (DOT >= 1) dot = fma(sum, w[r0 + r], dot);
             if (DOT == 2) yy = fma(sum, sum, yy);
@@ -778,14 +814,14 @@ yg_status spmv_prepare(yg_matrix A, int variant, int lanes) {
 
 template <typename VT, int DOT, typename C>
 static yg_status launch_csr_cfg(yg_matrix A, int k, const VT *val, const double *x, double *y, const double *w,
-                                double *partials, const int32_t *flag, int grid, cudaStream_t st) {
+                                double *partials, const int32_t *flag, const double *corr, int grid, cudaStream_t st) {
     static bool attr = false;
     if (!attr) {
         cudaFuncSetAttribute(k_csr_spmv_tiles<VT, DOT, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM);
         attr = true;
     }
     k_csr_spmv_tiles<VT, DOT, C><<<grid, C::WARPS * 32, C::SMEM, st>>>(A->nctiles[k], A->d_ctiles[k], A->d_rowptr,
-                                                                       A->d_col, val, x, y, w, partials, flag,
+                                                                       A->d_col, val, x, y, w, partials, flag, corr,
                                                                        A->ctx->d_err);
     YG_LAUNCHED(A->ctx);
     return YG_OK;
@@ -793,15 +829,15 @@ static yg_status launch_csr_cfg(yg_matrix A, int k, const VT *val, const double 
 
 template <typename VT, int DOT>
 static yg_status launch_csr(yg_matrix A, int lanes, const VT *val, const double *x, double *y, const double *w,
-                            double *partials, const int32_t *flag, int grid, cudaStream_t st) {
+                            double *partials, const int32_t *flag, const double *corr, int grid, cudaStream_t st) {
     const int k = csr_table(lanes);
     if (A->block != 1 || !csr_lanes_ok(lanes) || !A->d_ctiles[k])
         return fail(YG_BAD_ARG, "row-tile SpMV launched without its row tiles (block %d, lanes %d)", A->block, lanes);
     switch (lanes) {
-    case 1: return launch_csr_cfg<VT, DOT, CsrL1<VT>>(A, k, val, x, y, w, partials, flag, grid, st);
-    case 2: return launch_csr_cfg<VT, DOT, CsrL2<VT>>(A, k, val, x, y, w, partials, flag, grid, st);
-    case 4: return launch_csr_cfg<VT, DOT, CsrL4<VT>>(A, k, val, x, y, w, partials, flag, grid, st);
-    default: return launch_csr_cfg<VT, DOT, CsrL8<VT>>(A, k, val, x, y, w, partials, flag, grid, st);
+    case 1: return launch_csr_cfg<VT, DOT, CsrL1<VT>>(A, k, val, x, y, w, partials, flag, corr, grid, st);
+    case 2: return launch_csr_cfg<VT, DOT, CsrL2<VT>>(A, k, val, x, y, w, partials, flag, corr, grid, st);
+    case 4: return launch_csr_cfg<VT, DOT, CsrL4<VT>>(A, k, val, x, y, w, partials, flag, corr, grid, st);
+    default: return launch_csr_cfg<VT, DOT, CsrL8<VT>>(A, k, val, x, y, w, partials, flag, corr, grid, st);
     }
 }
 
@@ -817,7 +853,7 @@ static void csr_shape_v(int lanes, int *smem, int *wp) {
 
 template <int B, typename VT, int DOT, typename C, bool XF>
 static yg_status launch_tma_xf(yg_matrix A, const VT *val, const double *x, const float *x32, double *y,
-                               const double *w, double *partials, const int32_t *flag, int grid, cudaStream_t st) {
+                               const double *w, double *partials, const int32_t *flag, const double *corr, int grid, cudaStream_t st) {
     static bool attr = false;
     if (!attr) {
         cudaFuncSetAttribute(k_bcsr_spmv_tma<B, VT, DOT, C, XF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -825,7 +861,7 @@ static yg_status launch_tma_xf(yg_matrix A, const VT *val, const double *x, cons
         attr = true;
     }
     k_bcsr_spmv_tma<B, VT, DOT, C, XF><<<grid, C::WARPS * 32, C::SMEM, st>>>(
-        A->nbrows, A->d_rowptr, A->d_col, val, x, x32, y, w, partials, flag, A->ctx->d_err);
+        A->nbrows, A->d_rowptr, A->d_col, val, x, x32, y, w, partials, flag, corr, A->ctx->d_err);
     YG_LAUNCHED(A->ctx);
     return YG_OK;
 }
@@ -833,11 +869,11 @@ static yg_status launch_tma_xf(yg_matrix A, const VT *val, const double *x, cons
 // FP32 gathers only with FP32 values (the mixed-precision iteration SpMV).
 template <int B, typename VT, int DOT, typename C>
 static yg_status launch_tma_cfg(yg_matrix A, const VT *val, const double *x, const float *x32, double *y,
-                                const double *w, double *partials, const int32_t *flag, int grid, cudaStream_t st) {
+                                const double *w, double *partials, const int32_t *flag, const double *corr, int grid, cudaStream_t st) {
     if constexpr (std::is_same<VT, float>::value) {
-        if (x32) return launch_tma_xf<B, VT, DOT, C, true>(A, val, x, x32, y, w, partials, flag, grid, st);
+        if (x32) return launch_tma_xf<B, VT, DOT, C, true>(A, val, x, x32, y, w, partials, flag, corr, grid, st);
     }
-    return launch_tma_xf<B, VT, DOT, C, false>(A, val, x, nullptr, y, w, partials, flag, grid, st);
+    return launch_tma_xf<B, VT, DOT, C, false>(A, val, x, nullptr, y, w, partials, flag, corr, grid, st);
 }
 
 // TMA configurations (chunk blocks, ring depth, warps per CTA) the autotuner
@@ -851,14 +887,14 @@ template <int B, typename VT> using TmaL16 = TmaCfg<B, VT, 48, 3, 8>;
 
 template <int B, typename VT, int DOT>
 static yg_status launch_tma(yg_matrix A, int lanes, const VT *val, const double *x, const float *x32, double *y,
-                            const double *w, double *partials, const int32_t *flag, int grid, cudaStream_t st) {
+                            const double *w, double *partials, const int32_t *flag, const double *corr, int grid, cudaStream_t st) {
     switch (lanes) {
-    case 1: return launch_tma_cfg<B, VT, DOT, TmaL1<B, VT>>(A, val, x, x32, y, w, partials, flag, grid, st);
-    case 2: return launch_tma_cfg<B, VT, DOT, TmaL2<B, VT>>(A, val, x, x32, y, w, partials, flag, grid, st);
-    case 4: return launch_tma_cfg<B, VT, DOT, TmaL4<B, VT>>(A, val, x, x32, y, w, partials, flag, grid, st);
-    case 8: return launch_tma_cfg<B, VT, DOT, TmaL8<B, VT>>(A, val, x, x32, y, w, partials, flag, grid, st);
-    case 16: return launch_tma_cfg<B, VT, DOT, TmaL16<B, VT>>(A, val, x, x32, y, w, partials, flag, grid, st);
-    default: return launch_tma_cfg<B, VT, DOT, TmaL32<B, VT>>(A, val, x, x32, y, w, partials, flag, grid, st);
+    case 1: return launch_tma_cfg<B, VT, DOT, TmaL1<B, VT>>(A, val, x, x32, y, w, partials, flag, corr, grid, st);
+    case 2: return launch_tma_cfg<B, VT, DOT, TmaL2<B, VT>>(A, val, x, x32, y, w, partials, flag, corr, grid, st);
+    case 4: return launch_tma_cfg<B, VT, DOT, TmaL4<B, VT>>(A, val, x, x32, y, w, partials, flag, corr, grid, st);
+    case 8: return launch_tma_cfg<B, VT, DOT, TmaL8<B, VT>>(A, val, x, x32, y, w, partials, flag, corr, grid, st);
+    case 16: return launch_tma_cfg<B, VT, DOT, TmaL16<B, VT>>(A, val, x, x32, y, w, partials, flag, corr, grid, st);
+    default: return launch_tma_cfg<B, VT, DOT, TmaL32<B, VT>>(A, val, x, x32, y, w, partials, flag, corr, grid, st);
     }
 }
 
@@ -900,7 +936,7 @@ static void tma_shape(yg_matrix A, int lanes, bool f32, int *ctas_per_sm, int *w
 
 template <int B, typename VT, int DOT>
 static yg_status launch_staged(yg_matrix A, const VT *val, const double *x, double *y, const double *w,
-                               double *partials, const int32_t *flag, int grid, cudaStream_t st) {
+                               double *partials, const int32_t *flag, const double *corr, int grid, cudaStream_t st) {
     using S = Staged<B, VT>;
     static bool attr = false;
     if (!attr) {
@@ -908,20 +944,20 @@ static yg_status launch_staged(yg_matrix A, const VT *val, const double *x, doub
         attr = true;
     }
     k_bcsr_spmv_staged<B, VT, DOT><<<grid, S::WARPS * 32, S::SMEM, st>>>(A->nbrows, A->d_rowptr, A->d_col, val, x, y,
-                                                                        w, partials, flag);
+                                                                        w, partials, flag, corr);
     YG_LAUNCHED(A->ctx);
     return YG_OK;
 }
 
 template <int B, typename VT, int DOT>
 static yg_status launch_l(yg_matrix A, int lanes, const VT *val, const double *x, double *y, const double *w,
-                          double *partials, const int32_t *flag, int grid, cudaStream_t st) {
+                          double *partials, const int32_t *flag, const double *corr, int grid, cudaStream_t st) {
     switch (lanes) {
-    case 2: k_bcsr_spmv<B, 2, VT, DOT><<<grid, kThreads, 0, st>>>(A->nbrows, A->d_rowptr, A->d_col, val, x, y, w, partials, flag); break;
-    case 4: k_bcsr_spmv<B, 4, VT, DOT><<<grid, kThreads, 0, st>>>(A->nbrows, A->d_rowptr, A->d_col, val, x, y, w, partials, flag); break;
-    case 8: k_bcsr_spmv<B, 8, VT, DOT><<<grid, kThreads, 0, st>>>(A->nbrows, A->d_rowptr, A->d_col, val, x, y, w, partials, flag); break;
-    case 16: k_bcsr_spmv<B, 16, VT, DOT><<<grid, kThreads, 0, st>>>(A->nbrows, A->d_rowptr, A->d_col, val, x, y, w, partials, flag); break;
-    default: k_bcsr_spmv<B, 32, VT, DOT><<<grid, kThreads, 0, st>>>(A->nbrows, A->d_rowptr, A->d_col, val, x, y, w, partials, flag); break;
+    case 2: k_bcsr_spmv<B, 2, VT, DOT><<<grid, kThreads, 0, st>>>(A->nbrows, A->d_rowptr, A->d_col, val, x, y, w, partials, flag, corr); break;
+    case 4: k_bcsr_spmv<B, 4, VT, DOT><<<grid, kThreads, 0, st>>>(A->nbrows, A->d_rowptr, A->d_col, val, x, y, w, partials, flag, corr); break;
+    case 8: k_bcsr_spmv<B, 8, VT, DOT><<<grid, kThreads, 0, st>>>(A->nbrows, A->d_rowptr, A->d_col, val, x, y, w, partials, flag, corr); break;
+    case 16: k_bcsr_spmv<B, 16, VT, DOT><<<grid, kThreads, 0, st>>>(A->nbrows, A->d_rowptr, A->d_col, val, x, y, w, partials, flag, corr); break;
+    default: k_bcsr_spmv<B, 32, VT, DOT><<<grid, kThreads, 0, st>>>(A->nbrows, A->d_rowptr, A->d_col, val, x, y, w, partials, flag, corr); break;
     }
     YG_LAUNCHED(A->ctx);
     return YG_OK;
@@ -929,30 +965,30 @@ static yg_status launch_l(yg_matrix A, int lanes, const VT *val, const double *x
 
 template <typename VT, int DOT>
 static yg_status launch_b(yg_matrix A, int variant, int lanes, const VT *val, const double *x, const float *x32,
-                          double *y, const double *w, double *partials, const int32_t *flag, int grid,
+                          double *y, const double *w, double *partials, const int32_t *flag, const double *corr, int grid,
                           cudaStream_t st) {
-    if (variant == 3) return launch_csr<VT, DOT>(A, lanes, val, x, y, w, partials, flag, grid, st);
+    if (variant == 3) return launch_csr<VT, DOT>(A, lanes, val, x, y, w, partials, flag, corr, grid, st);
     if (variant == 2 && A->block == 3)
-        return launch_tma<3, VT, DOT>(A, lanes, val, x, x32, y, w, partials, flag, grid, st);
+        return launch_tma<3, VT, DOT>(A, lanes, val, x, x32, y, w, partials, flag, corr, grid, st);
     if (variant == 2 && A->block == 2)
-        return launch_tma<2, VT, DOT>(A, lanes, val, x, x32, y, w, partials, flag, grid, st);
-    if (variant == 1 && A->block == 3) return launch_staged<3, VT, DOT>(A, val, x, y, w, partials, flag, grid, st);
-    if (variant == 1 && A->block == 2) return launch_staged<2, VT, DOT>(A, val, x, y, w, partials, flag, grid, st);
+        return launch_tma<2, VT, DOT>(A, lanes, val, x, x32, y, w, partials, flag, corr, grid, st);
+    if (variant == 1 && A->block == 3) return launch_staged<3, VT, DOT>(A, val, x, y, w, partials, flag, corr, grid, st);
+    if (variant == 1 && A->block == 2) return launch_staged<2, VT, DOT>(A, val, x, y, w, partials, flag, corr, grid, st);
     switch (A->block) {
-    case 1: return launch_l<1, VT, DOT>(A, lanes, val, x, y, w, partials, flag, grid, st);
-    case 2: return launch_l<2, VT, DOT>(A, lanes, val, x, y, w, partials, flag, grid, st);
-    case 3: return launch_l<3, VT, DOT>(A, lanes, val, x, y, w, partials, flag, grid, st);
+    case 1: return launch_l<1, VT, DOT>(A, lanes, val, x, y, w, partials, flag, corr, grid, st);
+    case 2: return launch_l<2, VT, DOT>(A, lanes, val, x, y, w, partials, flag, corr, grid, st);
+    case 3: return launch_l<3, VT, DOT>(A, lanes, val, x, y, w, partials, flag, corr, grid, st);
     default: return fail(YG_UNSUPPORTED, "SpMV block size %d not supported (1, 2, 3)", A->block);
     }
 }
 
 template <typename VT>
 static yg_status launch_v(yg_matrix A, int variant, int lanes, const VT *val, const double *x, const float *x32,
-                          double *y, const double *w, double *partials, int dot_mode, const int32_t *flag, int grid,
+                          double *y, const double *w, double *partials, int dot_mode, const int32_t *flag, const double *corr, int grid,
                           cudaStream_t st) {
-    if (dot_mode == 0) return launch_b<VT, 0>(A, variant, lanes, val, x, x32, y, w, partials, flag, grid, st);
-    if (dot_mode == 1) return launch_b<VT, 1>(A, variant, lanes, val, x, x32, y, w, partials, flag, grid, st);
-    return launch_b<VT, 2>(A, variant, lanes, val, x, x32, y, w, partials, flag, grid, st);
+    if (dot_mode == 0) return launch_b<VT, 0>(A, variant, lanes, val, x, x32, y, w, partials, flag, corr, grid, st);
+    if (dot_mode == 1) return launch_b<VT, 1>(A, variant, lanes, val, x, x32, y, w, partials, flag, corr, grid, st);
+    return launch_b<VT, 2>(A, variant, lanes, val, x, x32, y, w, partials, flag, corr, grid, st);
 }
 
 // The kernel choice for a precision: FP32-value SpMVs have their own tuning.
@@ -971,7 +1007,8 @@ static void choice(yg_matrix A, int precision, int *variant, int *lanes) {
 // x) or of w.y and y.y (dot_mode 2).  The grid is persistent: `grid` blocks
 // stride over the block rows.
 yg_status spmv_launch_ex(yg_matrix A, const double *x, double *y, int precision, const double *w, double *partials,
-                         int dot_mode, const int32_t *flag, int grid, cudaStream_t stream, const float *x32) {
+                         int dot_mode, const int32_t *flag, int grid, cudaStream_t stream, const float *x32,
+                         const double *corr) {
     cudaStream_t st = stream ? stream : A->ctx->stream;
     if (grid > kMaxReduceBlocks) grid = kMaxReduceBlocks;
     if (!partials) dot_mode = 0;
@@ -981,9 +1018,9 @@ yg_status spmv_launch_ex(yg_matrix A, const double *x, double *y, int precision,
     choice(A, precision, &variant, &lanes);
     if (precision == YG_PREC_MIXED || precision == YG_PREC_MIXED_IR) {
         if (!A->d_val32) return fail(YG_BAD_ARG, "mixed-precision SpMV without FP32 values");
-        s = launch_v<float>(A, variant, lanes, A->d_val32, x, x32, y, w, partials, dot_mode, flag, grid, st);
+        s = launch_v<float>(A, variant, lanes, A->d_val32, x, x32, y, w, partials, dot_mode, flag, corr, grid, st);
     } else {
-        s = launch_v<double>(A, variant, lanes, A->d_val, x, nullptr, y, w, partials, dot_mode, flag, grid, st);
+        s = launch_v<double>(A, variant, lanes, A->d_val, x, nullptr, y, w, partials, dot_mode, flag, nullptr, grid, st);
     }
     if (s != YG_OK) return s;
     YG_CUDA(cudaGetLastError());
@@ -991,8 +1028,8 @@ yg_status spmv_launch_ex(yg_matrix A, const double *x, double *y, int precision,
 }
 
 yg_status spmv_launch(yg_matrix A, const double *x, double *y, int precision, double *partials,
-                      const int32_t *flag, int grid, const float *x32) {
-    return spmv_launch_ex(A, x, y, precision, x, partials, partials ? 1 : 0, flag, grid, nullptr, x32);
+                      const int32_t *flag, int grid, const float *x32, const double *corr) {
+    return spmv_launch_ex(A, x, y, precision, x, partials, partials ? 1 : 0, flag, grid, nullptr, x32, corr);
 }
 
 // Resident blocks per SM of the flat kernel (the heaviest, DOT = 2, form) for a
@@ -1107,6 +1144,7 @@ static yg_status tune_precision(yg_matrix A, int precision, double *x, const flo
         for (int L : {32, 1, 2, 4, 8, 16}) cands.push_back({2, L});  // TMA configurations
     }
     const bool f32 = precision != YG_PREC_FP64;
+    const double *corr = f32 ? A->d_corr32 : nullptr;
     int *pv = f32 ? &A->variant32 : &A->variant, *pl = f32 ? &A->lanes32 : &A->lanes;
     const int save_v = *pv, save_l = *pl;
     cudaEvent_t e0, e1;
@@ -1120,9 +1158,9 @@ static yg_status tune_precision(yg_matrix A, int precision, double *x, const flo
         *pv = c.variant;
         *pl = c.lanes;
         const int grid = spmv_grid_for(A, precision);
-        if ((s = spmv_launch(A, x, y, precision, nullptr, nullptr, grid, x32)) != YG_OK) break;  // warm-up
+        if ((s = spmv_launch(A, x, y, precision, nullptr, nullptr, grid, x32, corr)) != YG_OK) break;  // warm-up
         cudaEventRecord(e0, ctx->stream);
-        for (int r = 0; r < reps; ++r) spmv_launch(A, x, y, precision, nullptr, nullptr, grid, x32);
+        for (int r = 0; r < reps; ++r) spmv_launch(A, x, y, precision, nullptr, nullptr, grid, x32, corr);
         cudaEventRecord(e1, ctx->stream);
         cudaEventSynchronize(e1);
         float ms = 0;
