@@ -289,7 +289,10 @@ YG_API yg_status yg_spmv_ex(yg_matrix A, yg_vector x, yg_vector y, int32_t preci
  * row chunks into per-warp rings (2x2 and 3x3 blocks, `lanes` 1..32 selects the
  * ring shape); variant 3: bulk copies of tiles of whole rows with at most 256,
  * 512 or 1024 entries (CSR only, `lanes` 1, 2, 4, 8 selects the shape; every
- * row must hold 1..capacity entries).  variant -1 re-runs the device autotuner, which times
+ * row must hold 1..capacity entries); variant 4: one bulk copy pair per whole
+ * block row into per-warp rings, every lane's x gathers issued before its
+ * products, a transposed butterfly for the B row sums (2x2 and 3x3 blocks,
+ * `lanes` 1, 2: rows of up to 128 blocks, 4, 8: up to 64 blocks).  variant -1 re-runs the device autotuner, which times
  * the candidates on this matrix and keeps the fastest (it also runs on the
  * first SpMV or solve of a matrix). */
 YG_API yg_status yg_matrix_set_spmv(yg_matrix A, int32_t variant, int32_t lanes);

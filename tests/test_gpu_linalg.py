@@ -49,7 +49,8 @@ def test_spmv_matches_oracle(ctx, B, per_row):
     scale = np.abs(val).max() * np.abs(x).max() * (per_row + 1) * B
     tma = [(2, L) for L in (32, 1, 2, 4, 8, 16)]
     tiles = [(3, L) for L in (1, 2, 4, 8)]
-    variants = [(0, 4), (0, 32)] + ([(1, 32)] + tma if B in (2, 3) else tiles) + [(-1, 32)]
+    rows = [(4, L) for L in (1, 2, 4, 8) if per_row < (128 if L <= 2 else 64)]
+    variants = [(0, 4), (0, 32)] + ([(1, 32)] + tma + rows if B in (2, 3) else tiles) + [(-1, 32)]
     for v, L in variants:
         A.set_spmv(v, L)
         y = A * x
@@ -136,7 +137,7 @@ def test_spmv_mixed_corrected(ctx, B, per_row):
     scale = np.abs(val).max() * np.abs(x).max() * (per_row + 1) * B
     xc = np.tile(np.arange(1.0, B + 1.0), A.cols() // B)
     y64c = bcsr_to_oracle_csr(rp, col, val, B).spmv(xc)
-    variants = [(0, 8), (0, 32)] + ([(1, 32), (2, 4), (2, 8), (2, 32)] if B > 1 else [(3, 2)]) + [(-1, 32)]
+    variants = [(0, 8), (0, 32)] + ([(1, 32), (2, 4), (2, 8), (2, 32), (4, 1), (4, 2)] if B > 1 else [(3, 2)]) + [(-1, 32)]
     for v, L in variants:
         A.set_spmv(v, L)
         y = A.spmv(x, precision=yb.SPMV_MIXED_CORRECTED).numpy()
@@ -152,6 +153,87 @@ def test_spmv_mixed_corrected(ctx, B, per_row):
             R.spmv(np.ones(3), precision=yb.SPMV_MIXED_CORRECTED)
     with pytest.raises(Exception):
         A.spmv(x, precision=7)
+
+
+@pytest.mark.parametrize("B", [2, 3])
+def test_whole_row_edge_cases(ctx, B):
+    """Whole-row SpMV (variant 4): rows of 0 blocks (allowed), 1 block, exactly
+    a stage's capacity (64 and 128 blocks), a row longer than a capacity (only
+    the larger capacity remains), one row, fewer rows than warps; FP64 and FP32
+    values, plain and corrected; the same bits from run to run."""
+    rng = np.random.Generator(np.random.PCG64(70 + B))
+    n = 1200
+    lens = rng.integers(1, 60, n)
+    lens[::89] = 0      # empty block rows
+    lens[5::97] = 1
+    lens[11] = 64
+    lens[700] = 128     # longer than the 64-block stages
+    cols = [np.sort(rng.choice(n, L, replace=False)) for L in lens]
+    rp = np.concatenate([[0], np.cumsum(lens)]).astype(np.int64)
+    col = np.concatenate(cols).astype(np.int64)
+    val = rng.standard_normal(col.size * B * B)
+    A = yb.sparse_bcsr.from_bcsr(B, rp, col, val)
+    x = rng.standard_normal(n * B)
+    yo = bcsr_to_oracle_csr(rp, col, val, B).spmv(x)
+    yo32 = bcsr_to_oracle_csr(rp, col, val.astype(np.float32).astype(np.float64), B).spmv(x)
+    yoc = corrected_fp32_oracle(rp, col, val, B, x)
+    scale = np.abs(val).max() * np.abs(x).max() * 129 * B
+    for L in (4, 8):
+        with pytest.raises(Exception):
+            A.set_spmv(4, L)
+    for L in (1, 2):
+        A.set_spmv(4, L)
+        y = A * x
+        assert np.abs(y - yo).max() <= 1e-14 * scale, L
+        assert np.array_equal(y, A * x), L
+        assert np.all(y.reshape(-1, B)[lens == 0] == 0)
+        y32 = A.spmv(x, precision=yb.PREC_MIXED).numpy()
+        assert np.abs(y32 - yo32).max() <= 1e-14 * scale, L
+        yc = A.spmv(x, precision=yb.SPMV_MIXED_CORRECTED).numpy()
+        assert np.abs(yc - yoc).max() <= 1e-14 * scale, L
+        assert np.array_equal(yc, A.spmv(x, precision=yb.SPMV_MIXED_CORRECTED).numpy()), L
+    for nb in (1, 3, 31, 33, 700):
+        rp3 = np.arange(nb + 1, dtype=np.int64)
+        col3 = np.arange(nb, dtype=np.int64)
+        v3 = rng.standard_normal(nb * B * B)
+        A3 = yb.sparse_bcsr.from_bcsr(B, rp3, col3, v3)
+        x3 = rng.standard_normal(nb * B)
+        y3o = bcsr_to_oracle_csr(rp3, col3, v3, B).spmv(x3)
+        for L in (1, 2, 4, 8):
+            A3.set_spmv(4, L)
+            assert np.abs(A3 * x3 - y3o).max() <= 1e-14 * np.abs(v3).max() * np.abs(x3).max() * B, (nb, L)
+
+
+@pytest.mark.parametrize("lanes", [1, 2])
+def test_whole_row_in_solvers(ctx, lanes):
+    """The whole-row SpMV inside FP64 and mixed-precision Jacobi-PCG (fused p.Ap
+    partial sums; FP32 values gathering the FP32 copy of the direction, with the
+    row-sum correction) and inside BiCGSTAB (fused dot pairs) reaches the FP64
+    true relative residual of 1e-10 and agrees with the warp-per-row kernel."""
+    from yafel_b200 import meshgen
+    dm = O.dofmanager(meshgen.structured_hex(5, 5, 5, order="ccw"), 2)
+    K, _ = O.assemble(dm, 3, 3, O.ELASTICITY, [1.0, 0.5769230769230769, 0.3846153846153846])
+    X = dm.nodes
+    n = K.nrows
+    b = np.random.Generator(np.random.PCG64(2)).standard_normal(n)
+    mask = np.zeros(n, np.uint8)
+    clamp = np.nonzero(X[:, 0] < 1e-9)[0]
+    for c in range(3):
+        mask[clamp * 3 + c] = 1
+    O.dirichlet_apply(K, b, mask, np.zeros(n))
+    Bm = O.bcsr_from_triplets(3, *O.csr_to_triplets(K))
+    A = yb.sparse_bcsr.from_bcsr(3, Bm["brow_ptr"], Bm["bcol"], Bm["val"])
+    M = yb.JacobiPreconditioner(A)
+    A.set_spmv(2, 4)
+    x2, s2 = yb.solve(A, b, M=M, tol=1e-10)
+    A.set_spmv(4, lanes)
+    for prec in (yb.PREC_FP64, yb.PREC_MIXED, yb.PREC_MIXED_IR):
+        x4, s4 = yb.solve(A, b, M=M, tol=1e-10, precision=prec)
+        assert s4.status == 0 and s4.rel_residual <= 1e-10, prec
+        assert O.true_relres(K, b, x4.numpy()) <= 1e-10, prec
+        assert np.linalg.norm(x4.numpy() - x2.numpy()) <= 1e-8 * np.linalg.norm(x2.numpy()), prec
+    xb, sb = yb.solve(A, b, M=M, method="bicgstab", tol=1e-10)
+    assert sb.status == 0 and O.true_relres(K, b, xb.numpy()) <= 1e-10
 
 
 @pytest.mark.parametrize("B", [1, 3])

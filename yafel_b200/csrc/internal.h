@@ -107,7 +107,7 @@ struct yg_matrix_t {
     int32_t *d_diag = nullptr;    // position of the diagonal block in each block row, -1 if absent
     int lanes = 32;               // SpMV lanes per block row (flat variant)
     int variant = 0;              // SpMV variant: 0 flat lane-strided, 1 cp.async staged, 2 TMA bulk staged (B = 2, 3),
-                                  // 3 TMA row tiles (B = 1)
+                                  // 3 TMA row tiles (B = 1), 4 TMA whole rows (B = 2, 3)
     int variant32 = -1, lanes32 = 32;  // choice for FP32 values (-1: as for FP64)
     bool tuned32 = false;
     bool tuned = false;

@@ -766,6 +766,31 @@ __global__ void k_row_tiles(int64_t n, int64_t nt, int64_t per, const int32_t *_
     }
 }
 
+// Smallest and largest number of entries (blocks) per row of A, measured once.
+static yg_status row_extent(yg_matrix A) {
+    if (A->row_min >= 0) return YG_OK;
+    yg_context ctx = A->ctx;
+    cudaStreamCaptureStatus cs;
+    YG_CUDA(cudaStreamIsCapturing(ctx->stream, &cs));
+    if (cs != cudaStreamCaptureStatusNone) return fail(YG_BAD_ARG, "row extents cannot be measured during stream capture");
+    int32_t *d = nullptr;
+    YG_TRY(dev_alloc_t(ctx, &d, 2));
+    const int32_t init[2] = {INT32_MAX, 0};
+    int32_t h[2];
+    cudaMemcpyAsync(d, init, sizeof(init), cudaMemcpyHostToDevice, ctx->stream);
+    int blocks = (int)std::min<int64_t>((A->nbrows + kThreads - 1) / kThreads, (int64_t)ctx->num_sms * 4);
+    if (blocks < 1) blocks = 1;
+    k_row_extent<<<blocks, kThreads, 0, ctx->stream>>>(A->nbrows, A->d_rowptr, d);
+    YG_LAUNCHED(ctx);
+    cudaMemcpyAsync(h, d, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream);
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    dev_free(ctx, d);
+    if (e != cudaSuccess) return fail(YG_CUDA_ERROR, "row extent: %s", cudaGetErrorString(e));
+    A->row_min = h[0];
+    A->row_max = h[1];
+    return YG_OK;
+}
+
 // Row tiles of capacity 256 << k for A (block size 1).  Needs every row to hold
 // at least one and at most `cap` entries.
 static yg_status csr_tiles_build(yg_matrix A, int k) {
@@ -775,22 +800,7 @@ static yg_status csr_tiles_build(yg_matrix A, int k) {
     cudaStreamCaptureStatus cs;
     YG_CUDA(cudaStreamIsCapturing(ctx->stream, &cs));
     if (cs != cudaStreamCaptureStatusNone) return fail(YG_BAD_ARG, "row tiles cannot be built during stream capture");
-    if (A->row_min < 0) {
-        int32_t *d = nullptr;
-        YG_TRY(dev_alloc_t(ctx, &d, 2));
-        const int32_t init[2] = {INT32_MAX, 0};
-        int32_t h[2];
-        cudaMemcpyAsync(d, init, sizeof(init), cudaMemcpyHostToDevice, ctx->stream);
-        int blocks = (int)std::min<int64_t>((A->nbrows + kThreads - 1) / kThreads, (int64_t)ctx->num_sms * 4);
-        k_row_extent<<<blocks, kThreads, 0, ctx->stream>>>(A->nbrows, A->d_rowptr, d);
-        YG_LAUNCHED(ctx);
-        cudaMemcpyAsync(h, d, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream);
-        cudaError_t e = cudaStreamSynchronize(ctx->stream);
-        dev_free(ctx, d);
-        if (e != cudaSuccess) return fail(YG_CUDA_ERROR, "row extent: %s", cudaGetErrorString(e));
-        A->row_min = h[0];
-        A->row_max = h[1];
-    }
+    YG_TRY(row_extent(A));
     const int cap = 256 << k;
     if (A->row_min < 1 || A->row_max > cap)
         return fail(YG_UNSUPPORTED, "row-tile SpMV needs 1..%d entries per row (rows hold %d..%d)", cap, A->row_min,
@@ -806,7 +816,20 @@ static yg_status csr_tiles_build(yg_matrix A, int k) {
     return YG_OK;
 }
 
+static int rows_capacity_of(int lanes) { return lanes <= 2 ? 128 : 64; }
+
 yg_status spmv_prepare(yg_matrix A, int variant, int lanes) {
+    if (variant == 4) {  // whole rows: every block row must fit one stage
+        if (lanes != 1 && lanes != 2 && lanes != 4 && lanes != 8)
+            return fail(YG_BAD_ARG, "whole-row SpMV configurations are lanes 1, 2, 4, 8");
+        if (A->block != 2 && A->block != 3) return fail(YG_UNSUPPORTED, "whole-row SpMV needs 2x2 or 3x3 blocks");
+        if (A->nbrows >= INT32_MAX) return fail(YG_UNSUPPORTED, "whole-row SpMV needs fewer than 2^31 block rows");
+        YG_TRY(row_extent(A));
+        if (A->row_max > rows_capacity_of(lanes))
+            return fail(YG_UNSUPPORTED, "whole-row SpMV (lanes %d) holds rows of up to %d blocks; the longest has %d",
+                        lanes, rows_capacity_of(lanes), A->row_max);
+        return YG_OK;
+    }
     if (variant != 3) return YG_OK;
     if (!csr_lanes_ok(lanes)) return fail(YG_BAD_ARG, "row-tile SpMV configurations are lanes 1, 2, 4, 8");
     return csr_tiles_build(A, csr_table(lanes));
@@ -915,6 +938,304 @@ static void tma_shape_bv(int lanes, int *smem, int *wp) {
     }
 }
 
+// ---------------------------------------------------------------------------
+// Whole-row variant for B = 2, 3 (variant 4).  The chunked TMA variant above
+// spends most of its instructions outside the block products: per chunk the
+// copy issue, a cursor with two row-pointer loads, the stage offsets through
+// shared memory, a lane-divergent tail, and per row a 5-step butterfly of B
+// sums.  With FP32 values that bookkeeping, not HBM, sets its speed.  Here
+// every block row fits one stage (the matrix's longest row is at most CH
+// blocks), so a row costs one copy pair, one bounded wait and one reduction:
+// * the warp's next 32 rows' bounds are loaded at once, lane k holding row
+//   r + k*stride, and handed out by shuffles;
+// * stage offsets are recomputed from the row's first block, not stored;
+// * each lane issues the x gathers of all its blocks (lane + 32u) before its
+//   products, accumulating even and odd u in separate sums;
+// * the B row sums are reduced by a transposed butterfly (the halves of the
+//   warp first exchange different sums, then one sum per lane is reduced), so
+//   sum i ends in lanes 32i/Bp .. (the lane groups of the padded B), whose
+//   first lane writes y[B r + i] (and its dot terms).
+// The summation order is fixed (lane order, then the butterfly), so results are
+// reproducible.  Waits are bounded as in the variants above.
+template <int B, typename VT, int CH_, int NST_, int WARPS_>
+struct RowCfg {
+    static constexpr int CH = CH_, NST = NST_, WARPS = WARPS_, U = CH / 32;
+    static constexpr int VBYTES = (CH * B * B * (int)sizeof(VT) + 32 + 15) & ~15;
+    static constexpr int CBYTES = (CH * 4 + 32 + 15) & ~15;
+    static constexpr int STAGE = VBYTES + CBYTES;
+    static constexpr int SMEM = WARPS * NST * STAGE + WARPS * NST * 8;  // stages + mbarriers
+    static_assert(CH % 32 == 0, "whole 32-block groups per stage");
+};
+
+// Transposed butterfly of B (2 or 3) sums over the warp: returns, in every lane,
+// the full sum of component comp_of_lane(lane) = lane / (32 / Bp), Bp = 2 or 4.
+template <int B>
+__device__ __forceinline__ double reduce_rows_t(const double (&a)[B], int lane) {
+    if constexpr (B == 2) {
+        const bool up = lane & 16;
+        double k = up ? a[1] : a[0];
+        k += __shfl_xor_sync(0xffffffffu, up ? a[0] : a[1], 16);
+#pragma unroll
+        for (int o = 8; o > 0; o >>= 1) k += __shfl_xor_sync(0xffffffffu, k, o);
+        return k;
+    } else {
+        const bool up = lane & 16, mid = lane & 8;
+        // step 1: the lower half keeps sums 0 and 1, the upper half sums 2 and 3 (3 is 0)
+        double s0 = up ? a[2] : a[0];
+        double s1 = up ? 0.0 : a[1];
+        const double t0 = up ? a[0] : a[2];
+        const double t1 = up ? a[1] : 0.0;
+        s0 += __shfl_xor_sync(0xffffffffu, t0, 16);
+        s1 += __shfl_xor_sync(0xffffffffu, t1, 16);
+        // step 2: lanes with bit 3 keep the second of the two
+        double k = mid ? s1 : s0;
+        k += __shfl_xor_sync(0xffffffffu, mid ? s0 : s1, 8);
+#pragma unroll
+        for (int o = 4; o > 0; o >>= 1) k += __shfl_xor_sync(0xffffffffu, k, o);
+        return k;
+    }
+}
+
+template <int B, typename VT, int DOT, typename C, bool XF>
+__global__ void __launch_bounds__(C::WARPS * 32)
+k_bcsr_spmv_rows(int32_t nbrows, const int32_t *__restrict__ rowptr, const int32_t *__restrict__ col,
+                 const VT *__restrict__ val, const double *__restrict__ x, const float *__restrict__ x32,
+                 double *__restrict__ y, const double *__restrict__ w, double *__restrict__ partials,
+                 const int32_t *__restrict__ flag, const double *__restrict__ corr, int32_t *__restrict__ err) {
+    constexpr int B2 = B * B;
+    constexpr int BB = B2 * (int)sizeof(VT);
+    constexpr int GL = B == 2 ? 16 : 8;  // lanes per reduced component
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ double red[C::WARPS + 1];
+    __shared__ int hdr[C::WARPS][C::NST][2];  // first block and block count of the row in each stage
+    if (flag && read_flag(flag)) return;
+    const uint64_t pol = evict_first_policy();
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    unsigned char *ring = smem_raw + (size_t)wib * C::NST * C::STAGE;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw + (size_t)C::WARPS * C::NST * C::STAGE) + wib * C::NST;
+    if (lane == 0)
+        for (int k = 0; k < C::NST; ++k) mbar_init(&bars[k], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    __syncwarp();
+    const int stride = gridDim.x * C::WARPS;
+    const char *vbytes = reinterpret_cast<const char *>(val);
+    const char *cbytes = reinterpret_cast<const char *>(col);
+
+    // bounds of the warp's next 32 rows to issue: lane k holds row pf_base + k*stride
+    int64_t pf_base = (int64_t)blockIdx.x * C::WARPS + wib;
+    int pf_used = 32, pf_rs = 0, pf_re = 0;
+    // lane 0 issues the copies of the next row into stage st (an empty copy past the end)
+    auto issue = [&](int st) {
+        if (pf_used == 32) {
+            const int64_t r = pf_base + (int64_t)lane * stride;
+            pf_rs = pf_re = 0;
+            if (r < nbrows) {
+                pf_rs = __ldg(rowptr + r);
+                pf_re = __ldg(rowptr + r + 1);
+            }
+            pf_used = 0;
+        }
+        const int rs = __shfl_sync(0xffffffffu, pf_rs, pf_used), re = __shfl_sync(0xffffffffu, pf_re, pf_used);
+        if (++pf_used == 32) pf_base += 32 * (int64_t)stride;
+        if (lane == 0) {
+            hdr[wib][st][0] = rs;
+            hdr[wib][st][1] = re - rs;
+            if (re > rs) {
+                const int64_t vs = (int64_t)rs * BB, va = vs & ~(int64_t)15, ve = ((int64_t)re * BB + 15) & ~(int64_t)15;
+                const int64_t cs = (int64_t)rs * 4, ca = cs & ~(int64_t)15, ce = ((int64_t)re * 4 + 15) & ~(int64_t)15;
+                unsigned char *dst = ring + st * C::STAGE;
+                mbar_expect_tx(&bars[st], (unsigned)((ve - va) + (ce - ca)));
+                bulk_g2s(dst, vbytes + va, (unsigned)(ve - va), &bars[st], pol);
+                bulk_g2s(dst + C::VBYTES, cbytes + ca, (unsigned)(ce - ca), &bars[st], pol);
+            } else {
+                mbar_expect_tx(&bars[st], 0);  // completes the phase with no transfer
+            }
+        }
+    };
+
+#pragma unroll
+    for (int k = 0; k < C::NST - 1; ++k) issue(k);
+    double dot = 0, yy = 0;
+    int st = 0;
+    unsigned phase = 0;  // bit k: parity of stage k's next completion
+    bool timed_out = false;
+    const int comp = lane / GL;               // the sum this lane holds after the reduction
+    const bool writer = (lane % GL) == 0 && comp < B;
+    for (int64_t r = (int64_t)blockIdx.x * C::WARPS + wib; r < nbrows; r += stride) {
+        issue((st + C::NST - 1) % C::NST);
+        // the writer lanes fetch the row's correction and own x early (used at the end)
+        double cr[B], xr[B];
+        if (corr && writer) {
+#pragma unroll
+            for (int k = 0; k < B; ++k) {
+                cr[k] = corr[(r * B + comp) * B + k];
+                xr[k] = x[r * B + k];
+            }
+        }
+        int ok = 1;
+        if (lane == 0) {
+            long long spins = 0;
+            while (!mbar_try_wait(&bars[st], (phase >> st) & 1u))
+                if (++spins > kSpinLimit) { ok = 0; break; }
+        }
+        ok = __shfl_sync(0xffffffffu, ok, 0);
+        if (!ok) { timed_out = true; break; }
+        if (lane != 0) mbar_try_wait(&bars[st], (phase >> st) & 1u);
+        phase ^= (1u << st);
+        __syncwarp();
+        const int rs = hdr[wib][st][0], nb = hdr[wib][st][1];
+        const unsigned char *stg = ring + st * C::STAGE;
+        const VT *blk = reinterpret_cast<const VT *>(stg + (((unsigned)rs * (unsigned)BB) & 15u));
+        const int32_t *cix = reinterpret_cast<const int32_t *>(stg + C::VBYTES + (((unsigned)rs * 4u) & 15u));
+        double xv[C::U][B];
+#pragma unroll
+        for (int u = 0; u < C::U; ++u) {
+            if (32 * u < nb) {  // warp-uniform
+                const int j = lane + 32 * u;
+                if (j < nb) {
+                    gather_x<B, XF>(x, x32, cix[j], xv[u]);
+                } else {
+#pragma unroll
+                    for (int k = 0; k < B; ++k) xv[u][k] = 0;
+                }
+            }
+        }
+        double acc[B], acc2[B];
+#pragma unroll
+        for (int i = 0; i < B; ++i) acc[i] = acc2[i] = 0;
+#pragma unroll
+        for (int u = 0; u < C::U; ++u) {
+            if (32 * u < nb) {
+                const int j = lane + 32 * u;
+                if (j < nb) {
+#pragma unroll
+                    for (int i = 0; i < B; ++i)
+#pragma unroll
+                        for (int k = 0; k < B; ++k) {
+                            if (u & 1) acc2[i] = fma((double)blk[j * B2 + i * B + k], xv[u][k], acc2[i]);
+                            else acc[i] = fma((double)blk[j * B2 + i * B + k], xv[u][k], acc[i]);
+                        }
+                }
+            }
+        }
+        __syncwarp();  // the stage is free again
+#pragma unroll
+        for (int i = 0; i < B; ++i) acc[i] += acc2[i];
+        double s = reduce_rows_t<B>(acc, lane);
+        if (writer) {
+            if (corr) {
+                double t = cr[0] * xr[0];
+#pragma unroll
+                for (int k = 1; k < B; ++k) t = fma(cr[k], xr[k], t);
+                s += t;
+            }
+            const int64_t yi = r * B + comp;
+            y[yi] = s;
+            if (DOT >= 1) dot = fma(s, w[yi], dot);
+            if (DOT == 2) yy = fma(s, s, yy);
+        }
+        st = (st + 1) % C::NST;
+    }
+    if (timed_out && lane == 0 && err) atomicExch(err, (int32_t)YG_TIMEOUT);
+    // drain the copies still in flight into this warp's stages (bounded): NST-1
+    // after the loop, all NST after a timeout (the failed stage included)
+    if (lane == 0) {
+        const int outstanding = timed_out ? C::NST : C::NST - 1;
+        for (int k = 0; k < outstanding; ++k) {
+            const int s2 = (st + k) % C::NST;
+            long long spins = 0;
+            while (!mbar_try_wait(&bars[s2], (phase >> s2) & 1u) && ++spins <= kSpinLimit) {
+            }
+            phase ^= (1u << s2);
+        }
+    }
+    __syncwarp();
+    if (DOT) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            dot += __shfl_xor_sync(0xffffffffu, dot, o);
+            if (DOT == 2) yy += __shfl_xor_sync(0xffffffffu, yy, o);
+        }
+        if (lane == 0) red[wib] = dot;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double sum = 0;
+            for (int i = 0; i < C::WARPS; ++i) sum += red[i];
+            if (DOT == 1) partials[blockIdx.x] = sum;
+            else partials[2 * blockIdx.x] = sum;
+        }
+        if (DOT == 2) {
+            __syncthreads();
+            if (lane == 0) red[wib] = yy;
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                double sum = 0;
+                for (int i = 0; i < C::WARPS; ++i) sum += red[i];
+                partials[2 * blockIdx.x + 1] = sum;
+            }
+        }
+    }
+}
+
+// Whole-row configurations (longest row in blocks, ring depth, warps per CTA),
+// selected by the `lanes` field of a variant-4 matrix.
+template <int B, typename VT> using RowL1 = RowCfg<B, VT, 128, 2, 4>;
+template <int B, typename VT> using RowL2 = RowCfg<B, VT, 128, 3, 4>;
+template <int B, typename VT> using RowL4 = RowCfg<B, VT, 64, 2, 8>;
+template <int B, typename VT> using RowL8 = RowCfg<B, VT, 64, 3, 8>;
+static bool rows_lanes_ok(int lanes) { return lanes == 1 || lanes == 2 || lanes == 4 || lanes == 8; }
+
+template <int B, typename VT, int DOT, typename C, bool XF>
+static yg_status launch_rows_xf(yg_matrix A, const VT *val, const double *x, const float *x32, double *y,
+                                const double *w, double *partials, const int32_t *flag, const double *corr, int grid,
+                                cudaStream_t st) {
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_bcsr_spmv_rows<B, VT, DOT, C, XF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             C::SMEM);
+        attr = true;
+    }
+    k_bcsr_spmv_rows<B, VT, DOT, C, XF><<<grid, C::WARPS * 32, C::SMEM, st>>>(
+        (int32_t)A->nbrows, A->d_rowptr, A->d_col, val, x, x32, y, w, partials, flag, corr, A->ctx->d_err);
+    YG_LAUNCHED(A->ctx);
+    return YG_OK;
+}
+
+template <int B, typename VT, int DOT, typename C>
+static yg_status launch_rows_cfg(yg_matrix A, const VT *val, const double *x, const float *x32, double *y,
+                                 const double *w, double *partials, const int32_t *flag, const double *corr, int grid,
+                                 cudaStream_t st) {
+    if constexpr (std::is_same<VT, float>::value) {
+        if (x32) return launch_rows_xf<B, VT, DOT, C, true>(A, val, x, x32, y, w, partials, flag, corr, grid, st);
+    }
+    return launch_rows_xf<B, VT, DOT, C, false>(A, val, x, nullptr, y, w, partials, flag, corr, grid, st);
+}
+
+template <int B, typename VT, int DOT>
+static yg_status launch_rows(yg_matrix A, int lanes, const VT *val, const double *x, const float *x32, double *y,
+                             const double *w, double *partials, const int32_t *flag, const double *corr, int grid,
+                             cudaStream_t st) {
+    if (!rows_lanes_ok(lanes) || A->row_max < 0 || A->row_max > rows_capacity_of(lanes))
+        return fail(YG_BAD_ARG, "whole-row SpMV launched on rows it does not hold (lanes %d, longest row %d)", lanes,
+                    A->row_max);
+    switch (lanes) {
+    case 1: return launch_rows_cfg<B, VT, DOT, RowL1<B, VT>>(A, val, x, x32, y, w, partials, flag, corr, grid, st);
+    case 2: return launch_rows_cfg<B, VT, DOT, RowL2<B, VT>>(A, val, x, x32, y, w, partials, flag, corr, grid, st);
+    case 4: return launch_rows_cfg<B, VT, DOT, RowL4<B, VT>>(A, val, x, x32, y, w, partials, flag, corr, grid, st);
+    default: return launch_rows_cfg<B, VT, DOT, RowL8<B, VT>>(A, val, x, x32, y, w, partials, flag, corr, grid, st);
+    }
+}
+
+template <int B, typename VT>
+static void rows_shape_bv(int lanes, int *smem, int *wp) {
+    switch (lanes) {
+    case 1: shape_of<RowL1<B, VT>>(smem, wp); break;
+    case 2: shape_of<RowL2<B, VT>>(smem, wp); break;
+    case 4: shape_of<RowL4<B, VT>>(smem, wp); break;
+    default: shape_of<RowL8<B, VT>>(smem, wp); break;
+    }
+}
+
 // CTAs per SM and warps per CTA of a TMA configuration (for the grid size): as
 // many CTAs as the shared memory holds, at most 64 warps and 8 CTAs per SM (the
 // Krylov kernels reserve 8 partial sums per SM for the SpMV).
@@ -968,6 +1289,10 @@ static yg_status launch_b(yg_matrix A, int variant, int lanes, const VT *val, co
                           double *y, const double *w, double *partials, const int32_t *flag, const double *corr, int grid,
                           cudaStream_t st) {
     if (variant == 3) return launch_csr<VT, DOT>(A, lanes, val, x, y, w, partials, flag, corr, grid, st);
+    if (variant == 4 && A->block == 3)
+        return launch_rows<3, VT, DOT>(A, lanes, val, x, x32, y, w, partials, flag, corr, grid, st);
+    if (variant == 4 && A->block == 2)
+        return launch_rows<2, VT, DOT>(A, lanes, val, x, x32, y, w, partials, flag, corr, grid, st);
     if (variant == 2 && A->block == 3)
         return launch_tma<3, VT, DOT>(A, lanes, val, x, x32, y, w, partials, flag, corr, grid, st);
     if (variant == 2 && A->block == 2)
@@ -1079,6 +1404,24 @@ int spmv_grid_for(yg_matrix A, int precision) {
         if (need < g) g = need;
         return (int)(g < 1 ? 1 : g);
     }
+    if (variant == 4) {  // whole rows: as many CTAs as the shared memory holds, a warp per row
+        int smem = 0, wp = 1;
+        if (A->block == 3) {
+            if (f32) rows_shape_bv<3, float>(lanes, &smem, &wp);
+            else rows_shape_bv<3, double>(lanes, &smem, &wp);
+        } else {
+            if (f32) rows_shape_bv<2, float>(lanes, &smem, &wp);
+            else rows_shape_bv<2, double>(lanes, &smem, &wp);
+        }
+        int per = (220 * 1024) / (smem + 1024);
+        if (per * wp > 64) per = 64 / wp;
+        if (per > 8) per = 8;
+        if (per < 1) per = 1;
+        int64_t need = (A->nbrows + wp - 1) / wp;
+        int64_t g = (int64_t)A->ctx->num_sms * per;
+        if (need < g) g = need;
+        return (int)(g < 1 ? 1 : g);
+    }
     if (variant == 2) {  // TMA: as many CTAs as fit, a warp per row
         int per, wp;
         tma_shape(A, lanes, f32, &per, &wp);
@@ -1142,6 +1485,8 @@ static yg_status tune_precision(yg_matrix A, int precision, double *x, const flo
     if (A->block == 2 || A->block == 3) {
         cands.push_back({1, 32});
         for (int L : {32, 1, 2, 4, 8, 16}) cands.push_back({2, L});  // TMA configurations
+        for (int L : {1, 2, 4, 8})  // whole-row configurations, where the longest row fits a stage
+            if (spmv_prepare(A, 4, L) == YG_OK) cands.push_back({4, L});
     }
     const bool f32 = precision != YG_PREC_FP64;
     const double *corr = f32 ? A->d_corr32 : nullptr;
