@@ -879,7 +879,7 @@ class _NumberingView:
         self.ndofs = rd.n_nodes * rd.dpn
 
 
-def cpu_sample(nx, threads, tol=1e-20):
+def cpu_sample(nx, threads, tol=1e-20, split=False):
     """The reference's own CPU path on an nx^3 Q2 sample of the workload, every
     step in its code compiled in place (oracle/_ref; no yafel_b200 library is
     loaded): Mesh + DoFManager(M, CG, 2, 3), CGAssembly<elasticity> on all
@@ -888,7 +888,8 @@ def cpu_sample(nx, threads, tol=1e-20):
     handed to its handmade sparse_csr(triplets), and pcg_solve with
     JacobiPreconditioner (OpenMP csr_spmv).  pcg_solve stops when
     r.z / r0.z0 < tol (a squared, preconditioned ratio).
-    Returns (dofs, seconds, FP64 true relative residual, kind)."""
+    Returns (dofs, seconds, FP64 true relative residual, kind), and with
+    `split` also the seconds up to the solve and of the solve."""
     os.environ["OMP_NUM_THREADS"] = str(threads)
     from oracle import oracle as O
     from yafel_b200 import loads
@@ -906,9 +907,12 @@ def cpu_sample(nx, threads, tol=1e-20):
     for c in range(3):
         rs.dirichlet_plane(c, 0, 0.0, 0.0)
     A, b = rs.to_ref_csr()
+    t1 = time.perf_counter()
     x = A.pcg_jacobi(b, np.zeros(b.size), tol)
-    dt = time.perf_counter() - t0
-    return b.size, dt, A.true_relres(b, x), "reference"
+    t2 = time.perf_counter()
+    if split:
+        return b.size, t2 - t0, A.true_relres(b, x), "reference", t1 - t0, t2 - t1
+    return b.size, t2 - t0, A.true_relres(b, x), "reference"
 
 
 def calibrate_cpu_tol(nx, threads, target=8e-11):
@@ -981,49 +985,84 @@ def cpu_problems(specs, meshes=None, budget_s=30.0, max_dofs=None):
 
 def cpu_baseline(args):
     """One calibrated sample of the reference's CPU path (untimed probe solve
-    first), reported beside the GPU numbers."""
+    first) on the whole cpu_nx^3 cube, scaled to the configured size the way
+    the reference arm scales its sample (phases up to the solve by the element
+    count, the solve by stored entries times iterations), reported beside the
+    GPU numbers."""
     threads = os.cpu_count() or 1
     nx = args.cpu_nx
     tol, _ = calibrate_cpu_tol(nx, threads)
-    ndofs, dt, rel, kind = cpu_sample(nx, threads, tol)
-    return {"value": ndofs / dt, "unit": "dofs/s", "cores": threads, "kind": kind,
-            "sample": cpu_sample_text(nx, ndofs, rel, tol, dt)}
-
-
-def cpu_sample_text(nx, ndofs, rel, tol, dt):
-    return ("%d^3 Q2 hex (%d dofs), every step in the reference's own code (DoFManager, CGAssembly on all "
-            "cores, DirichletBC, sparse_csr, pcg_solve+Jacobi with TOL %.2e on r.z/r0.z0) to a true relative "
-            "residual of %.1e in %.2f s; at 60^3 PCG needs ~3.8x the iterations per dof, so this sample's "
-            "rate is above the full-size rate" % (nx, ndofs, tol, rel, dt))
+    ndofs, dt, rel, kind, t_setup, t_solve = cpu_sample(nx, threads, tol, split=True)
+    elem_ratio = (args.nx / nx) ** 3
+    nnz_ratio = base_config(args.nx, 1)["blocks"] / base_config(nx, 1)["blocks"]
+    iter_ratio = args.nx / nx
+    est = t_setup * elem_ratio + t_solve * nnz_ratio * iter_ratio
+    return {"value": base_config(args.nx, 1)["dofs"] / est, "unit": "dofs/s", "cores": threads, "kind": kind,
+            "sample_rate_dofs_per_s": ndofs / dt,
+            "sample": ("the reference's own code on the whole %d^3 Q2 cube (%d dofs: DoFManager, CGAssembly on "
+                       "all cores, DirichletBC, sparse_csr, pcg_solve+Jacobi with TOL %.2e on r.z/r0.z0, true "
+                       "relative residual %.1e): %.2f s to the solve + %.2f s of solve; scaled to %d^3 by elements "
+                       "x%.1f and stored entries x%.1f times iterations x%.2f" %
+                       (nx, ndofs, tol, rel, t_setup, t_solve, args.nx, elem_ratio, nnz_ratio, iter_ratio))}
 
 
 def run_reference(args):
+    """The reference's own CPU path (oracle/_ref: its DoFManager, CGAssembly,
+    DirichletBC, sparse_csr and pcg_solve compiled in place; no yafel_b200
+    library is loaded) on the benchmark's workload, on all host cores.  The
+    full nx^3 = 60^3 system takes minutes per step on the CPU, so each step runs
+    the same pipeline on the whole --ref-nx^3 cube (default 30^3: the same
+    elements, physics, loads and tolerance) and the value is scaled to the
+    configured size by the measured phases: everything up to the solve grows
+    with the element count (x (nx/ref_nx)^3), and the solve with the stored
+    entries times the iteration count, which grows as 1/h for this system
+    (x nnz ratio x nx/ref_nx; Jacobi-PCG takes 583 and 1169 iterations to
+    1e-10 at 30^3 and 60^3).  Warm-up: the tolerance probe at ref_nx^3, then
+    W-1 runs at 16^3."""
     ws, rank, _ = dist_env()
     if rank != 0:
         return
     threads = os.cpu_count() or 1
+    rnx = args.ref_nx
     # warm-up: the first one is the tolerance probe (pcg_solve's test is on a
     # squared preconditioned ratio; the probe rescales it so that every timed
     # solve ends near a 1e-10 true relative residual, like the GPU's)
-    tol, _ = calibrate_cpu_tol(args.cpu_nx, threads)
-    for _ in range(max(0, args.warmup - 1)):
-        cpu_sample(args.cpu_nx, threads, tol)
-    vals, rels, dts, kind, ndofs = [], [], [], "reference", 0
+    tol, _ = calibrate_cpu_tol(rnx, threads)
+    if args.warmup > 1:
+        wtol, _ = calibrate_cpu_tol(16, threads)
+        for _ in range(args.warmup - 2):
+            cpu_sample(16, threads, wtol)
+    cfg = base_config(args.nx, ws)
+    elem_ratio = (args.nx / rnx) ** 3
+    nnz_ratio = base_config(args.nx, ws)["blocks"] / base_config(rnx, ws)["blocks"]
+    iter_ratio = args.nx / rnx
+    vals, rels, setups, solves, ndofs = [], [], [], [], 0
     for _ in range(args.steps):
-        ndofs, dt, rel, kind = cpu_sample(args.cpu_nx, threads, tol)
-        vals.append(ndofs / dt)
+        ndofs, dt, rel, kind, t_setup, t_solve = cpu_sample(rnx, threads, tol, split=True)
+        est = t_setup * elem_ratio + t_solve * nnz_ratio * iter_ratio
+        vals.append(cfg["dofs"] / est)
         rels.append(rel)
-        dts.append(dt)
+        setups.append(t_setup)
+        solves.append(t_solve)
     value = statistics.mean(vals)
+    ms_step = (statistics.mean(setups) * elem_ratio + statistics.mean(solves) * nnz_ratio * iter_ratio) * 1e3
+    sample_rate = ndofs / (statistics.mean(setups) + statistics.mean(solves))
+    text = ("the reference's own code on the whole %d^3 Q2 cube (%d dofs: DoFManager, CGAssembly on all cores, "
+            "DirichletBC, sparse_csr, pcg_solve+Jacobi with TOL %.2e on r.z/r0.z0, true relative residual %.1e): "
+            "%.2f s to the solve + %.2f s of solve, %.0f dofs/s there; scaled to %d^3 by elements x%.2f "
+            "(to the solve) and stored entries x%.2f times iterations x%.2f (the solve)" %
+            (rnx, ndofs, tol, max(rels), statistics.mean(setups), statistics.mean(solves), sample_rate, args.nx,
+             elem_ratio, nnz_ratio, iter_ratio))
     out = {"impl": "reference", "metric": METRIC, "value": value, "unit": "dofs/s", "n_gpus": ws,
-           "steps": args.steps, "warmup": args.warmup, "ms_per_step": statistics.mean(dts) * 1e3,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
            "data": "synthetic (structured mesh)",
-           "config": base_config(args.nx, ws),
-           "sample": {"mesh": "%d^3 Q2 hex" % args.cpu_nx, "dofs": ndofs, "tol_rz_ratio": tol,
-                      "relres_min": min(rels), "relres_max": max(rels)},
-           "cpu_baseline": {"value": value, "unit": "dofs/s", "cores": threads, "kind": kind,
-                            "sample": cpu_sample_text(args.cpu_nx, ndofs, max(rels), tol, statistics.mean(dts))},
+           "config": cfg,
+           "sample": {"ran": "%d^3 Q2 hex, full pipeline, converged" % rnx, "dofs": ndofs, "tol_rz_ratio": tol,
+                      "relres_min": min(rels), "relres_max": max(rels), "setup_s": statistics.mean(setups),
+                      "solve_s": statistics.mean(solves), "rate_at_sample_dofs_per_s": sample_rate,
+                      "scale_elements": elem_ratio, "scale_entries": nnz_ratio, "scale_iterations": iter_ratio},
+           "cpu_baseline": {"value": value, "unit": "dofs/s", "cores": threads, "kind": kind, "sample": text},
            "e2e": {"value": value, "unit": "dofs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
 
@@ -1053,6 +1092,7 @@ def main():
     ap.add_argument("--impl", default="yafel_b200")
     ap.add_argument("--nx", type=int, default=NX)
     ap.add_argument("--cpu-nx", type=int, default=16)
+    ap.add_argument("--ref-nx", type=int, default=30, help="cube the reference arm runs whole (scaled to --nx)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extra", action="store_true", help="skip the 64x64 Poisson, 30^3 Q3 and ILU(0) side measurements")
     ap.add_argument("--spmv-profile", action="store_true", help="time the SpMV kernel alone (roofline/ncu)")

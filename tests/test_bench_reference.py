@@ -1,8 +1,9 @@
 """The reference arm of bench.py (`--impl reference`) on the host: one JSON line
 with the contract's keys and the GPU arm's config, the reference's own CPU path
 (its DoFManager, CGAssembly, DirichletBC, sparse_csr and pcg_solve) reaching a
-1e-10 relative residual on a small sample of the workload, with no part of the
-yafel_b200 library loaded (no GPU needed)."""
+1e-10 relative residual on a whole smaller cube of the workload, scaled to the
+configured size by its measured phases, with no part of the yafel_b200 library
+loaded (no GPU needed)."""
 import json
 import os
 import subprocess
@@ -14,7 +15,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 def test_reference_arm_prints_one_contract_line():
     env = dict(os.environ, OMP_NUM_THREADS="2")
     out = subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--steps", "1", "--warmup", "1",
-                          "--cpu-nx", "3"], cwd=ROOT, env=env, capture_output=True, text=True, timeout=600)
+                          "--ref-nx", "3"], cwd=ROOT, env=env, capture_output=True, text=True, timeout=600)
     assert out.returncode == 0, out.stderr[-2000:]
     lines = [l for l in out.stdout.splitlines() if l.startswith("{")]
     assert len(lines) == 1
@@ -27,7 +28,13 @@ def test_reference_arm_prints_one_contract_line():
     assert d["cpu_baseline"]["kind"] in ("reference", "port")
     assert d["config"] == bench_config()
     assert 1e-12 <= d["sample"]["relres_min"] and d["sample"]["relres_max"] <= 1e-10
-    assert d["sample"]["mesh"] == "3^3 Q2 hex" and d["sample"]["dofs"] == 3 * 7 ** 3
+    smp = d["sample"]
+    assert smp["ran"] == "3^3 Q2 hex, full pipeline, converged" and smp["dofs"] == 3 * 7 ** 3
+    # the value is the configured size's dofs over the scaled phases of the sample
+    est = smp["setup_s"] * smp["scale_elements"] + smp["solve_s"] * smp["scale_entries"] * smp["scale_iterations"]
+    assert abs(d["value"] - d["config"]["dofs"] / est) <= 1e-9 * d["value"]
+    assert smp["scale_elements"] == 8000.0 and smp["scale_iterations"] == 20.0
+    assert abs(smp["scale_entries"] - (481 / 25) ** 3) < 1e-9
 
 
 def bench_config():
