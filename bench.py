@@ -553,6 +553,10 @@ def run_ilu(ctx, nx=30):
         t2 = time.perf_counter()
         out[name] = {"setup_s": t1 - t0, "solve_s": t2 - t1, "iterations": st.iterations,
                      "relres": st.rel_residual, "status": st.status}
+        if name == "ilu0":
+            lo, up = M.levels
+            out[name]["levels_forward_backward"] = [lo, up]
+            out[name]["ms_per_iteration"] = 1e3 * (t2 - t1) / max(1, st.iterations)
         del M, x
     return out
 
@@ -1103,8 +1107,9 @@ def main():
     ap.add_argument("--reps", type=int, default=10)
     ap.add_argument("--spmv-precision", default="both", choices=["both", "fp64", "fp32"],
                     help="value precisions timed by --spmv-profile")
-    ap.add_argument("--workload", default="fem", choices=["fem", "batch", "serve"],
-                    help="fem: 60^3 Q2 elasticity assemble+solve; batch: many 2D problems solved together")
+    ap.add_argument("--workload", default="fem", choices=["fem", "batch", "serve", "ilu"],
+                    help="fem: 60^3 Q2 elasticity assemble+solve; batch: many 2D problems solved together; "
+                         "serve: the serving loop; ilu: ILU(0)- beside Jacobi-PCG on the --nx^3 problem")
     ap.add_argument("--problems", type=int, default=512, help="problems in the batched workload")
     ap.add_argument("--no-side-workloads", action="store_true",
                     help="skip the batched (512 problems) and served objects of the default line")
@@ -1131,6 +1136,9 @@ def main():
         run_batch(args)
     elif args.workload == "serve":
         run_serve(args)
+    elif args.workload == "ilu":
+        import yafel_b200 as yb
+        print(json.dumps(run_ilu(yb.Context(0), args.nx)), flush=True)
     else:
         run_gpu(args)
 

@@ -321,6 +321,10 @@ YG_API yg_status yg_precond_apply(yg_precond M, yg_vector z);
 YG_API yg_status yg_precond_destroy(yg_precond M);
 /* Number of zero pivots skipped while factoring (ILU(0)) or zero diagonals (Jacobi). */
 YG_API int64_t yg_precond_zero_pivots(yg_precond M);
+/* ILU(0) only (no reference counterpart): the dependency levels of its forward
+ * and backward triangular sweeps -- the grid-wide barriers each apply waits
+ * on; 0 and 0 for the other kinds. */
+YG_API yg_status yg_precond_levels(yg_precond M, int64_t *lower, int64_t *upper);
 
 /* ------------------------------------------------------------------ solvers */
 

@@ -699,6 +699,13 @@ class _Precond:
         self.h = h
         self.zero_pivots = lib().yg_precond_zero_pivots(h)
 
+    @property
+    def levels(self):
+        """(forward, backward) dependency levels of an ILU(0) apply; (0, 0) otherwise."""
+        lo, up = C.c_int64(), C.c_int64()
+        check(lib().yg_precond_levels(self.h, C.byref(lo), C.byref(up)))
+        return lo.value, up.value
+
     def solve(self, z):
         """M.solve(z) in place (Preconditioner.hpp:9-21); z is a DeviceVector or a
         numpy array (modified in place)."""

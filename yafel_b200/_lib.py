@@ -82,6 +82,7 @@ SIGNATURES = {
     "yg_precond_apply": (i32, [vp, vp]),
     "yg_precond_destroy": (i32, [vp]),
     "yg_precond_zero_pivots": (i64, [vp]),
+    "yg_precond_levels": (i32, [vp, P(i64), P(i64)]),
     "yg_cg": (i32, [vp, vp, vp, vp, P(SolveOpts), P(SolveStats)]),
     "yg_bicgstab": (i32, [vp, vp, vp, vp, P(SolveOpts), P(SolveStats)]),
     "yg_batch_create": (i32, [vp, i32, P(vp)]),

@@ -412,3 +412,10 @@ extern "C" yg_status yg_precond_destroy(yg_precond M) {
 }
 
 extern "C" int64_t yg_precond_zero_pivots(yg_precond M) { return M ? M->zero_pivots : -1; }
+
+extern "C" yg_status yg_precond_levels(yg_precond M, int64_t *lower, int64_t *upper) {
+    if (!M || !lower || !upper) return fail(YG_BAD_ARG, "yg_precond_levels: NULL argument");
+    *lower = M->lower_level_ptr.empty() ? 0 : (int64_t)M->lower_level_ptr.size() - 1;
+    *upper = M->upper_level_ptr.empty() ? 0 : (int64_t)M->upper_level_ptr.size() - 1;
+    return YG_OK;
+}
