@@ -197,6 +197,9 @@ def run_gpu(args):
         yb.CGAssembly(phys, fe)
         K, F = fe.getGlobalTangent(), fe.getGlobalResidual()
         F.axpy(1.0, trac_dev)
+        for prec, pin in ((yb.PREC_FP64, args.spmv), (yb.PREC_MIXED, args.spmv32)):
+            if pin:  # pinned kernels (a profiler distorts the autotuner's timings)
+                K.set_spmv_for(prec, *[int(v) for v in pin.split(":")])
         ctx.synchronize()
         t1 = time.perf_counter()
         for bc in bcs:
@@ -297,6 +300,7 @@ def run_gpu(args):
                      "frac": (achieved / peak) if achieved else None, "traffic": traffic,
                      "kernel": kname, "bytes_per_launch": spmv_bytes,
                      "ms_per_launch": spmv_ms, "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback",
+                     "spmv_choice": {"fp64": list(K.get_spmv(0)), "fp32": list(K.get_spmv(1))},
                      "fp32_values_kernel_GBs": spmv32_bytes / (spmv32_ms * 1e-3) / 1e9 if spmv32_ms > 0 else None},
         "solver": {"fp64_iterations": iters64, "fp64_relres": max(s.rel_residual for s in st64),
                    "mixed_iterations": itersmx, "mixed_relres": max(s.rel_residual for s in stmx),
@@ -1097,6 +1101,8 @@ def main():
     ap.add_argument("--nx", type=int, default=NX)
     ap.add_argument("--cpu-nx", type=int, default=16)
     ap.add_argument("--ref-nx", type=int, default=30, help="cube the reference arm runs whole (scaled to --nx)")
+    ap.add_argument("--spmv", default=None, help="pin the FP64-value SpMV as variant:lanes (default: autotuned)")
+    ap.add_argument("--spmv32", default=None, help="pin the FP32-value SpMV as variant:lanes (default: autotuned)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extra", action="store_true", help="skip the 64x64 Poisson, 30^3 Q3 and ILU(0) side measurements")
     ap.add_argument("--spmv-profile", action="store_true", help="time the SpMV kernel alone (roofline/ncu)")

@@ -296,6 +296,10 @@ YG_API yg_status yg_spmv_ex(yg_matrix A, yg_vector x, yg_vector y, int32_t preci
  * the candidates on this matrix and keeps the fastest (it also runs on the
  * first SpMV or solve of a matrix). */
 YG_API yg_status yg_matrix_set_spmv(yg_matrix A, int32_t variant, int32_t lanes);
+/* As yg_matrix_set_spmv for one value precision only: YG_PREC_FP64 sets the
+ * kernel of FP64 values, any other precision that of the FP32 copy (no
+ * reference counterpart; pins the autotuner's choice, e.g. under a profiler). */
+YG_API yg_status yg_matrix_set_spmv_for(yg_matrix A, int32_t precision, int32_t variant, int32_t lanes);
 YG_API yg_status yg_matrix_get_spmv(yg_matrix A, int32_t *variant, int32_t *lanes);
 /* The SpMV kernel used for FP64 values (precision YG_PREC_FP64) or for the FP32
  * value copy (any other precision). */

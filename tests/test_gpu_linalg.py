@@ -236,6 +236,26 @@ def test_whole_row_in_solvers(ctx, lanes):
     assert sb.status == 0 and O.true_relres(K, b, xb.numpy()) <= 1e-10
 
 
+def test_spmv_choice_per_precision(ctx):
+    """yg_matrix_set_spmv_for pins the kernel of one value precision and leaves
+    the other alone; the autotuner is not a choice it takes; both kernels give
+    the oracle's product."""
+    rp, col, val = random_block_matrix(1500, 3, 20, seed=77)
+    A = yb.sparse_bcsr.from_bcsr(3, rp, col, val)
+    x = np.random.Generator(np.random.PCG64(8)).standard_normal(A.cols())
+    A.set_spmv(0, 8)
+    A.set_spmv_for(yb.PREC_MIXED, 4, 1)
+    assert A.get_spmv(yb.PREC_FP64) == (0, 8) and A.get_spmv(yb.PREC_MIXED) == (4, 1)
+    A.set_spmv_for(yb.PREC_FP64, 2, 4)
+    assert A.get_spmv(yb.PREC_FP64) == (2, 4) and A.get_spmv(yb.PREC_MIXED) == (4, 1)
+    with pytest.raises(Exception):
+        A.set_spmv_for(yb.PREC_FP64, -1, 32)
+    yo = bcsr_to_oracle_csr(rp, col, val, 3).spmv(x)
+    assert np.abs(A * x - yo).max() <= 1e-13 * np.abs(yo).max()
+    yo32 = bcsr_to_oracle_csr(rp, col, val.astype(np.float32).astype(np.float64), 3).spmv(x)
+    assert np.abs(A.spmv(x, precision=yb.PREC_MIXED).numpy() - yo32).max() <= 1e-13 * np.abs(yo32).max()
+
+
 @pytest.mark.parametrize("B", [1, 3])
 def test_spmv_mixed_precision(ctx, B):
     rp, col, val = random_block_matrix(2000, B, 20, seed=3 + B)

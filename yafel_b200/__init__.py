@@ -434,6 +434,10 @@ class _Matrix:
         whole rows (2x2/3x3 blocks, rows of up to 128 or 64 blocks), -1 autotune."""
         check(lib().yg_matrix_set_spmv(self.h, int(variant), int(lanes)))
 
+    def set_spmv_for(self, precision, variant, lanes):
+        """Pin the SpMV kernel of one value precision (PREC_FP64, or the FP32 copy)."""
+        check(lib().yg_matrix_set_spmv_for(self.h, int(precision), int(variant), int(lanes)))
+
     def get_spmv(self, precision=PREC_FP64):
         """(variant, lanes) of the SpMV kernel for FP64 values or, with another
         precision, for the FP32 value copy."""

@@ -75,6 +75,7 @@ SIGNATURES = {
     "yg_spmv": (i32, [vp, vp, vp]),
     "yg_spmv_ex": (i32, [vp, vp, vp, i32]),
     "yg_matrix_set_spmv": (i32, [vp, i32, i32]),
+    "yg_matrix_set_spmv_for": (i32, [vp, i32, i32, i32]),
     "yg_matrix_get_spmv": (i32, [vp, P(i32), P(i32)]),
     "yg_matrix_get_spmv_for": (i32, [vp, i32, P(i32), P(i32)]),
     "yg_spmv_bench": (i32, [vp, vp, vp, i32, i32, P(f64)]),

@@ -586,7 +586,8 @@ extern "C" yg_status yg_spmv_ex(yg_matrix A, yg_vector x, yg_vector y, int32_t p
 
 extern "C" yg_status yg_spmv(yg_matrix A, yg_vector x, yg_vector y) { return yg_spmv_ex(A, x, y, YG_PREC_FP64); }
 
-extern "C" yg_status yg_matrix_set_spmv(yg_matrix A, int32_t variant, int32_t lanes) {
+// Checks a (variant, lanes) choice for A and builds what it needs.
+static yg_status spmv_choice_check(yg_matrix A, int32_t variant, int32_t lanes) {
     if (!A || variant < -1 || variant > 4 ||
         (lanes != 1 && lanes != 2 && lanes != 4 && lanes != 8 && lanes != 16 && lanes != 32))
         return fail(YG_BAD_ARG, "yg_matrix_set_spmv: bad variant/lanes");
@@ -594,6 +595,26 @@ extern "C" yg_status yg_matrix_set_spmv(yg_matrix A, int32_t variant, int32_t la
         return fail(YG_UNSUPPORTED, "staged SpMV needs 2x2 or 3x3 blocks");
     if (variant == 0 && lanes == 1) return fail(YG_BAD_ARG, "flat SpMV needs 2..32 lanes");
     if (variant == 3 || variant == 4) YG_TRY(spmv_prepare(A, variant, lanes));
+    return YG_OK;
+}
+
+extern "C" yg_status yg_matrix_set_spmv_for(yg_matrix A, int32_t precision, int32_t variant, int32_t lanes) {
+    if (variant < 0) return fail(YG_BAD_ARG, "yg_matrix_set_spmv_for: a variant (0..4), not the autotuner");
+    YG_TRY(spmv_choice_check(A, variant, lanes));
+    if (precision == YG_PREC_FP64) {
+        A->variant = variant;
+        A->lanes = lanes;
+        A->tuned = true;
+    } else {
+        A->variant32 = variant;
+        A->lanes32 = lanes;
+        A->tuned32 = true;
+    }
+    return YG_OK;
+}
+
+extern "C" yg_status yg_matrix_set_spmv(yg_matrix A, int32_t variant, int32_t lanes) {
+    YG_TRY(spmv_choice_check(A, variant, lanes));
     if (variant < 0) {  // re-run the device autotuner
         A->tuned = false;
         A->tuned32 = false;

@@ -73,6 +73,17 @@ __device__ __forceinline__ void block_chunk(int64_t n, int64_t &lo, int64_t &hi)
     if (lo > n) lo = n;
 }
 
+// As block_chunk, with chunk starts on even indices (16-byte aligned doubles) so
+// that a block can stream its chunk as double2.
+__device__ __forceinline__ void block_chunk2(int64_t n, int64_t &lo, int64_t &hi) {
+    int64_t per = (n + gridDim.x - 1) / gridDim.x;
+    per += per & 1;
+    lo = (int64_t)blockIdx.x * per;
+    hi = lo + per;
+    if (hi > n) hi = n;
+    if (lo > n) lo = n;
+}
+
 __device__ __forceinline__ int read_flag(const int32_t *flag) {
     return *reinterpret_cast<const volatile int32_t *>(flag);
 }

@@ -135,9 +135,10 @@ k_cg_update(int64_t n, const double *__restrict__ pq_partials, int np, KrylovSca
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) S->iter_seen = S->iter;  // for k_cg_pupdate's iteration cap test
     int64_t lo, hi;
-    block_chunk(n, lo, hi);
+    block_chunk2(n, lo, hi);
     double srz = 0, srr = 0;
-    for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+    // pairs of entries as 16-byte loads (the chunk starts on an even index)
+    auto one = [&](int64_t i) {
         x[i] += p[i] * alpha;
         double ri = r[i] + (-alpha) * q[i];
         r[i] = ri;
@@ -146,7 +147,34 @@ k_cg_update(int64_t n, const double *__restrict__ pq_partials, int np, KrylovSca
             double zi = dinv ? dinv[i] * ri : ri;
             srz += ri * zi;
         }
+    };
+    const int64_t v1 = hi >> 1;
+#pragma unroll 2
+    for (int64_t v = (lo >> 1) + threadIdx.x; v < v1; v += blockDim.x) {
+        double2 xv = reinterpret_cast<const double2 *>(x)[v];
+        const double2 pv = reinterpret_cast<const double2 *>(p)[v];
+        double2 rv = reinterpret_cast<const double2 *>(r)[v];
+        const double2 qv = reinterpret_cast<const double2 *>(q)[v];
+        xv.x += pv.x * alpha;
+        xv.y += pv.y * alpha;
+        rv.x = rv.x + (-alpha) * qv.x;
+        rv.y = rv.y + (-alpha) * qv.y;
+        reinterpret_cast<double2 *>(x)[v] = xv;
+        reinterpret_cast<double2 *>(r)[v] = rv;
+        srr += rv.x * rv.x;
+        srr += rv.y * rv.y;
+        if (FUSED) {
+            double2 zv = rv;
+            if (dinv) {
+                const double2 dv = reinterpret_cast<const double2 *>(dinv)[v];
+                zv.x = dv.x * rv.x;
+                zv.y = dv.y * rv.y;
+            }
+            srz += rv.x * zv.x;
+            srz += rv.y * zv.y;
+        }
     }
+    if ((hi & 1) && hi > lo && threadIdx.x == 0) one(hi - 1);  // odd n: the last entry
     srr = block_sum<kThreads>(srr, sm);
     if (FUSED) srz = block_sum<kThreads>(srz, sm);
     if (threadIdx.x == 0) {
@@ -200,8 +228,26 @@ k_cg_pupdate(int64_t n, const double *__restrict__ partials_in, int np, KrylovSc
     if (done) return;
     const double beta = rz_new / rz_old;
     int64_t lo, hi;
-    block_chunk(n, lo, hi);
-    for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+    block_chunk2(n, lo, hi);
+    const int64_t v1 = hi >> 1;
+#pragma unroll 2
+    for (int64_t v = (lo >> 1) + threadIdx.x; v < v1; v += blockDim.x) {
+        const double2 rv = reinterpret_cast<const double2 *>(FUSED ? r : z)[v];
+        double2 zv = rv;
+        if (FUSED && dinv) {
+            const double2 dv = reinterpret_cast<const double2 *>(dinv)[v];
+            zv.x = dv.x * rv.x;
+            zv.y = dv.y * rv.y;
+        }
+        double2 pv = reinterpret_cast<const double2 *>(p)[v];
+        pv.x = zv.x + beta * pv.x;
+        pv.y = zv.y + beta * pv.y;
+        reinterpret_cast<double2 *>(p)[v] = pv;
+        d32.put(2 * v, pv.x);
+        d32.put(2 * v + 1, pv.y);
+    }
+    if ((hi & 1) && hi > lo && threadIdx.x == 0) {  // odd n: the last entry
+        const int64_t i = hi - 1;
         double zi = FUSED ? (dinv ? dinv[i] * r[i] : r[i]) : z[i];
         const double pi = zi + beta * p[i];
         p[i] = pi;
@@ -354,6 +400,8 @@ static yg_status pcg_core(yg_matrix A, yg_precond M, const double *b, double *x,
                           SpmvProfile *prof = nullptr, int64_t *replacements = nullptr) {
     yg_context ctx = A->ctx;
     const int64_t n = A->rows();
+    // the update kernels stream pairs of entries as 16-byte loads
+    if (((uintptr_t)b | (uintptr_t)x) & 15) return fail(YG_BAD_ARG, "solver vectors must be 16-byte aligned");
     const bool fused = !M || precond_fusable(M);
     const double *dinv = M ? precond_dinv(M) : nullptr;
     const int G = ctx->reduce_blocks;
