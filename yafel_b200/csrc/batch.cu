@@ -61,6 +61,7 @@ struct BatchSys {
     const int32_t *rowptr, *col;
     const double *val;
     const float *val32;
+    const double *corr32;         // mixed precision: the FP32 values' row-sum correction (else NULL)
     const double *b, *dinv;
     double *x, *r, *p, *q;        // q: SpMV output of PCG and of the verification (BiCGSTAB: q is t)
     double *r0, *v, *s, *t, *ph, *sh;  // BiCGSTAB only
@@ -278,7 +279,8 @@ constexpr int kMaxItems = 16384;
 template <int B, int L, int KIND, typename VT>
 __device__ __forceinline__ void tile_rows(const int32_t *rowptr, int r0, int r1, int b0, const VT *vals,
                                           const int32_t *cols, const double *__restrict__ xin, double *__restrict__ out,
-                                          const double *__restrict__ w, double &dot1, double &dot2, int lane) {
+                                          const double *__restrict__ w, double &dot1, double &dot2, int lane,
+                                          const double *__restrict__ corr) {
     constexpr int B2 = B * B;
     constexpr int G = 32 / L;
     const int glane = lane % L, grp = lane / L;
@@ -320,6 +322,7 @@ __device__ __forceinline__ void tile_rows(const int32_t *rowptr, int r0, int r1,
 #pragma unroll
             for (int o = L / 2; o > 0; o >>= 1) acc[i] += __shfl_xor_sync(0xffffffffu, acc[i], o);
         if (r < r1 && glane == 0) {
+            if (corr) add_corr<B>(corr, xin, r, acc);
 #pragma unroll
             for (int i = 0; i < B; ++i) {
                 out[(int64_t)B * r + i] = acc[i];
@@ -344,7 +347,7 @@ template <int B, int KIND, typename VT>
 __device__ __forceinline__ void tile_rows_seg(const int32_t *rows, int r0, int r1, int b0, const VT *vals,
                                               const int32_t *cols, const double *__restrict__ xin,
                                               double *__restrict__ out, const double *__restrict__ w, double &dot1,
-                                              double &dot2, int lane) {
+                                              double &dot2, int lane, const double *__restrict__ corr) {
     constexpr int B2 = B * B;
     const int nrows = r1 - r0;
     const int nb = rows[nrows] - b0;
@@ -391,6 +394,7 @@ __device__ __forceinline__ void tile_rows_seg(const int32_t *rows, int r0, int r
         const bool row_done = seg_end && (rows[myrow + 1] - b0 - 1 == j);
         if (row_done) {
             const int r = r0 + myrow;
+            if (corr) add_corr<B>(corr, xin, r, v);
 #pragma unroll
             for (int i = 0; i < B; ++i) {
                 out[(int64_t)B * r + i] = v[i];
@@ -616,7 +620,7 @@ __device__ __forceinline__ void direct_rows(const int32_t *__restrict__ rowptr, 
                                             const VT *__restrict__ val, const int32_t *__restrict__ col,
                                             const double *__restrict__ xin, double *__restrict__ out,
                                             const double *__restrict__ w, double &dot1, double &dot2, int lane,
-                                            uint64_t pol) {
+                                            uint64_t pol, const double *__restrict__ corr) {
     constexpr int B2 = B * B;
     constexpr int G = 32 / L;
     constexpr int U = B == 1 ? 4 : (B == 2 ? 2 : 1);
@@ -662,6 +666,7 @@ __device__ __forceinline__ void direct_rows(const int32_t *__restrict__ rowptr, 
 #pragma unroll
             for (int o = L / 2; o > 0; o >>= 1) acc[i] += __shfl_xor_sync(0xffffffffu, acc[i], o);
         if (r < r1 && glane == 0) {
+            if (corr) add_corr<B>(corr, xin, r, acc);
 #pragma unroll
             for (int i = 0; i < B; ++i) {
                 out[(int64_t)B * r + i] = acc[i];
@@ -699,9 +704,11 @@ k_batch_spmv_direct(const BatchMItem *__restrict__ items, const int32_t *__restr
             const double *w = KIND == SP_CG ? d.p : KIND == SP_BICG_V ? d.r0 : d.s;
             double dot1 = 0, dot2 = 0;
             if (KIND != SP_VERIFY && d.precision == YG_PREC_MIXED)
-                direct_rows<B, L, KIND, float>(d.rowptr, r0, r1, d.val32, d.col, xin, out, w, dot1, dot2, lane, pol);
+                direct_rows<B, L, KIND, float>(d.rowptr, r0, r1, d.val32, d.col, xin, out, w, dot1, dot2, lane, pol,
+                                               d.corr32);
             else
-                direct_rows<B, L, KIND, double>(d.rowptr, r0, r1, d.val, d.col, xin, out, w, dot1, dot2, lane, pol);
+                direct_rows<B, L, KIND, double>(d.rowptr, r0, r1, d.val, d.col, xin, out, w, dot1, dot2, lane, pol,
+                                                nullptr);
             if (KIND != SP_VERIFY && commit)
                 finish_item<KIND>(sys, scal, part, cticket, it, s, parity, dot1, dot2, lane);
         }
@@ -790,6 +797,7 @@ k_batch_spmv(const BatchMItem *__restrict__ items, const int32_t *__restrict__ r
     const int32_t *c_rowptr = nullptr, *c_col = nullptr;
     const double *c_val = nullptr;
     const float *c_val32 = nullptr;
+    const double *c_corr = nullptr;
     bool c_f32 = false;
     double dot1 = 0, dot2 = 0;
     bool timed_out = false;
@@ -812,6 +820,7 @@ k_batch_spmv(const BatchMItem *__restrict__ items, const int32_t *__restrict__ r
             c_col = d.col;
             c_val = d.val;
             c_val32 = d.val32;
+            c_corr = c_f32 ? d.corr32 : nullptr;
             xin = KIND == SP_CG ? d.p : KIND == SP_VERIFY ? d.x : KIND == SP_BICG_V ? d.ph : d.sh;
             out = (KIND == SP_CG || KIND == SP_VERIFY) ? d.q : KIND == SP_BICG_V ? d.v : d.t;
             w = KIND == SP_CG ? d.p : KIND == SP_BICG_V ? d.r0 : d.s;
@@ -825,12 +834,16 @@ k_batch_spmv(const BatchMItem *__restrict__ items, const int32_t *__restrict__ r
                                          : c_rowptr + h.r0;
             if (c_f32) {
                 const float *v = staged ? reinterpret_cast<const float *>(stg + lv) : c_val32 + (int64_t)h.b0 * B2;
-                if (L == 1) tile_rows_seg<B, KIND, float>(rows, h.r0, h.r1, h.b0, v, cols, xin, out, w, dot1, dot2, lane);
-                else tile_rows<B, L, KIND, float>(rows, h.r0, h.r1, h.b0, v, cols, xin, out, w, dot1, dot2, lane);
+                if (L == 1)
+                    tile_rows_seg<B, KIND, float>(rows, h.r0, h.r1, h.b0, v, cols, xin, out, w, dot1, dot2, lane, c_corr);
+                else
+                    tile_rows<B, L, KIND, float>(rows, h.r0, h.r1, h.b0, v, cols, xin, out, w, dot1, dot2, lane, c_corr);
             } else {
                 const double *v = staged ? reinterpret_cast<const double *>(stg + lv) : c_val + (int64_t)h.b0 * B2;
-                if (L == 1) tile_rows_seg<B, KIND, double>(rows, h.r0, h.r1, h.b0, v, cols, xin, out, w, dot1, dot2, lane);
-                else tile_rows<B, L, KIND, double>(rows, h.r0, h.r1, h.b0, v, cols, xin, out, w, dot1, dot2, lane);
+                if (L == 1)
+                    tile_rows_seg<B, KIND, double>(rows, h.r0, h.r1, h.b0, v, cols, xin, out, w, dot1, dot2, lane, nullptr);
+                else
+                    tile_rows<B, L, KIND, double>(rows, h.r0, h.r1, h.b0, v, cols, xin, out, w, dot1, dot2, lane, nullptr);
             }
         }
         ++seq_wait;
@@ -1322,14 +1335,15 @@ static void launch_solo(yg_batch bt, int kind, int parity) {
         const int32_t *flag = &bt->d_scal[s].flag;
         const int64_t l0 = A->ctx->launches;
         yg_status st;
+        const double *corr = prec == YG_PREC_MIXED ? A->d_corr32 : nullptr;
         if (kind == SP_CG) {
-            st = spmv_launch_ex(A, d.p, d.q, prec, d.p, bt->d_solo_part, 1, flag, grid, ctx->stream);
+            st = spmv_launch_ex(A, d.p, d.q, prec, d.p, bt->d_solo_part, 1, flag, grid, ctx->stream, nullptr, corr);
             k_batch_solo_finish<SP_CG><<<1, 32, 0, ctx->stream>>>(bt->d_scal, bt->d_solo_part, grid, s, parity);
         } else if (kind == SP_BICG_V) {
-            st = spmv_launch_ex(A, d.ph, d.v, prec, d.r0, bt->d_solo_part, 1, flag, grid, ctx->stream);
+            st = spmv_launch_ex(A, d.ph, d.v, prec, d.r0, bt->d_solo_part, 1, flag, grid, ctx->stream, nullptr, corr);
             k_batch_solo_finish<SP_BICG_V><<<1, 32, 0, ctx->stream>>>(bt->d_scal, bt->d_solo_part, grid, s, parity);
         } else {
-            st = spmv_launch_ex(A, d.sh, d.t, prec, d.s, bt->d_solo_part, 2, flag, grid, ctx->stream);
+            st = spmv_launch_ex(A, d.sh, d.t, prec, d.s, bt->d_solo_part, 2, flag, grid, ctx->stream, nullptr, corr);
             k_batch_solo_finish<SP_BICG_T><<<1, 32, 0, ctx->stream>>>(bt->d_scal, bt->d_solo_part, grid, s, parity);
         }
         if (st != YG_OK && bt->solo_err == YG_OK) bt->solo_err = st;
@@ -1659,6 +1673,7 @@ extern "C" yg_status yg_batch_add(yg_batch bt, yg_matrix A, yg_vector b, yg_vect
     d.col = A->d_col;
     d.val = A->d_val;
     d.val32 = A->d_val32;
+    d.corr32 = o.precision == YG_PREC_MIXED ? A->d_corr32 : nullptr;
     d.b = b->d;
     d.x = x->d;
     d.precision = o.precision;

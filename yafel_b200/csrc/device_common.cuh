@@ -73,6 +73,25 @@ __device__ __forceinline__ void block_chunk(int64_t n, int64_t &lo, int64_t &hi)
     if (lo > n) lo = n;
 }
 
+// Corrected FP32 operator: s += corr_r x_r, row i of the block row's FP64
+// correction (corr, B*B per block row: the sum over the row's blocks of
+// A - fl32(A)) times the row's own entries of x (FP64).
+template <int B>
+__device__ __forceinline__ void add_corr(const double *__restrict__ corr, const double *__restrict__ x, int64_t r,
+                                         double (&s)[B]) {
+    double xr[B];
+#pragma unroll
+    for (int k = 0; k < B; ++k) xr[k] = x[(int64_t)B * r + k];
+#pragma unroll
+    for (int i = 0; i < B; ++i) {
+        const double *c = corr + ((int64_t)B * r + i) * B;
+        double t = c[0] * xr[0];
+#pragma unroll
+        for (int k = 1; k < B; ++k) t = fma(c[k], xr[k], t);
+        s[i] += t;
+    }
+}
+
 // As block_chunk, with chunk starts on even indices (16-byte aligned doubles) so
 // that a block can stream its chunk as double2.
 __device__ __forceinline__ void block_chunk2(int64_t n, int64_t &lo, int64_t &hi) {

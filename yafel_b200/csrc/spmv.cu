@@ -21,24 +21,6 @@
 
 namespace yg {
 
-// Corrected FP32 operator: s += corr_r x_r, row i of the block row's FP64
-// correction (corr, B*B per block row) times the row's own entries of x (FP64).
-template <int B>
-__device__ __forceinline__ void add_corr(const double *__restrict__ corr, const double *__restrict__ x, int64_t r,
-                                         double (&s)[B]) {
-    double xr[B];
-#pragma unroll
-    for (int k = 0; k < B; ++k) xr[k] = x[(int64_t)B * r + k];
-#pragma unroll
-    for (int i = 0; i < B; ++i) {
-        const double *c = corr + ((int64_t)B * r + i) * B;
-        double t = c[0] * xr[0];
-#pragma unroll
-        for (int k = 1; k < B; ++k) t = fma(c[k], xr[k], t);
-        s[i] += t;
-    }
-}
-
 // DOT = 0: y = A x.  DOT = 1: also per-block sums of w.y.  DOT = 2: per-block
 // sums of w.y and y.y (partials[2b], partials[2b+1]).
 template <int B, int L, typename VT, int DOT>
