@@ -1131,8 +1131,9 @@ def main():
                          "own SpMV launch in the batch (default: the library's)")
     ap.add_argument("--build-per-block", type=int, default=0,
                     help="most requests the serving loop builds while a block runs (0 = while it runs)")
-    ap.add_argument("--solo-rows", type=int, default=0,
-                    help="served systems of at least this many rows are solved alone (0: batch all)")
+    ap.add_argument("--solo-rows", type=int, default=100000,
+                    help="served systems of at least this many rows are solved alone by the single-system "
+                         "solvers, whose SpMV runs at the HBM rate (0: batch all)")
     args = ap.parse_args()
     if args.spmv_profile:
         run_spmv_profile(args)

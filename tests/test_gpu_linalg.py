@@ -336,6 +336,16 @@ def test_ilu_apply_matches_reference(ctx):
     L.solve(z)
     assert np.allclose(z, g["ilu5_apply"], rtol=1e-13, atol=1e-14)
     assert L.zero_pivots == 0
+    # dependency levels of the sweeps: at least 1, at most one per row; none for Jacobi
+    lo, up = L.levels
+    assert 1 <= lo <= A.rows() and 1 <= up <= A.rows()
+    assert yb.JacobiPreconditioner(A).levels == (0, 0)
+    # a diagonal matrix: every row is independent, one level each way
+    D = yb.sparse_csr([(i, i, 1.0 + i) for i in range(7)])
+    assert yb.ILUPreconditioner(D).levels == (1, 1)
+    # a bidiagonal (lower) chain: each row waits for the previous one
+    Lc = yb.sparse_csr([(i, i, 2.0) for i in range(6)] + [(i + 1, i, 1.0) for i in range(5)])
+    assert yb.ILUPreconditioner(Lc).levels[0] == 6
 
 
 def test_jacobi_zero_diagonal_gives_inf_like_reference(ctx):
