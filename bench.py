@@ -300,7 +300,7 @@ def run_gpu(args):
                      "frac": (achieved / peak) if achieved else None, "traffic": traffic,
                      "kernel": kname, "bytes_per_launch": spmv_bytes,
                      "ms_per_launch": spmv_ms, "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback",
-                     "spmv_choice": {"fp64": list(K.get_spmv(0)), "fp32": list(K.get_spmv(1))},
+                     "spmv_choice": {"fp64": list(K.get_spmv(0)), "fp32": list(Kmx.get_spmv(1))},
                      "fp32_values_kernel_GBs": spmv32_bytes / (spmv32_ms * 1e-3) / 1e9 if spmv32_ms > 0 else None},
         "solver": {"fp64_iterations": iters64, "fp64_relres": max(s.rel_residual for s in st64),
                    "mixed_iterations": itersmx, "mixed_relres": max(s.rel_residual for s in stmx),
