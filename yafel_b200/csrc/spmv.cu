@@ -334,6 +334,35 @@ __device__ __forceinline__ void gather_x(const double *__restrict__ x, const flo
     }
 }
 
+// Transposed butterfly of B (2 or 3) sums over the warp: returns, in every lane,
+// the full sum of component comp_of_lane(lane) = lane / (32 / Bp), Bp = 2 or 4.
+template <int B>
+__device__ __forceinline__ double reduce_rows_t(const double (&a)[B], int lane) {
+    if constexpr (B == 2) {
+        const bool up = lane & 16;
+        double k = up ? a[1] : a[0];
+        k += __shfl_xor_sync(0xffffffffu, up ? a[0] : a[1], 16);
+#pragma unroll
+        for (int o = 8; o > 0; o >>= 1) k += __shfl_xor_sync(0xffffffffu, k, o);
+        return k;
+    } else {
+        const bool up = lane & 16, mid = lane & 8;
+        // step 1: the lower half keeps sums 0 and 1, the upper half sums 2 and 3 (3 is 0)
+        double s0 = up ? a[2] : a[0];
+        double s1 = up ? 0.0 : a[1];
+        const double t0 = up ? a[0] : a[2];
+        const double t1 = up ? a[1] : 0.0;
+        s0 += __shfl_xor_sync(0xffffffffu, t0, 16);
+        s1 += __shfl_xor_sync(0xffffffffu, t1, 16);
+        // step 2: lanes with bit 3 keep the second of the two
+        double k = mid ? s1 : s0;
+        k += __shfl_xor_sync(0xffffffffu, mid ? s0 : s1, 8);
+#pragma unroll
+        for (int o = 4; o > 0; o >>= 1) k += __shfl_xor_sync(0xffffffffu, k, o);
+        return k;
+    }
+}
+
 template <int B, typename VT, int DOT, typename C, bool XF>
 __global__ void __launch_bounds__(C::WARPS * 32)
 k_bcsr_spmv_tma(int64_t nbrows, const int32_t *__restrict__ rowptr, const int32_t *__restrict__ col,
@@ -394,6 +423,9 @@ k_bcsr_spmv_tma(int64_t nbrows, const int32_t *__restrict__ rowptr, const int32_
 #pragma unroll
     for (int i = 0; i < B; ++i) acc[i] = acc2[i] = 0;
     double cv = 0, xo = 0;  // with corr: lane l < B*B holds corr_r[l], lane l < B holds x_r[l]
+    constexpr int GL = B == 2 ? 16 : 8;  // lanes per reduced component
+    const int comp = lane / GL;
+    const bool writer = (lane % GL) == 0 && comp < B;
     int st = 0;
     unsigned phase = 0;  // bit k: parity of stage k's next completion
     bool timed_out = false;
@@ -448,27 +480,23 @@ k_bcsr_spmv_tma(int64_t nbrows, const int32_t *__restrict__ rowptr, const int32_
         __syncwarp();
         if (cc.b0 + C::CH >= cc.re - cc.rs) {  // row complete
 #pragma unroll
-            for (int i = 0; i < B; ++i) {
-                acc[i] += acc2[i];
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) acc[i] += __shfl_xor_sync(0xffffffffu, acc[i], o);
-            }
+            for (int i = 0; i < B; ++i) acc[i] += acc2[i];
+            // transposed butterfly: lane l ends with the row's sum l / GL, and the
+            // first lane of each of the B groups writes that component
+            double sr = reduce_rows_t<B>(acc, lane);
             if (corr) {
                 // lane B*i+k holds corr_r[i][k]; row i's term sums lanes B*i .. B*i+B-1 in order
                 const double pr = cv * __shfl_sync(0xffffffffu, xo, lane % B);
                 double t = pr;
 #pragma unroll
                 for (int k = 1; k < B; ++k) t += __shfl_down_sync(0xffffffffu, pr, k);
-#pragma unroll
-                for (int i = 0; i < B; ++i) acc[i] += __shfl_sync(0xffffffffu, t, B * i);
+                sr += __shfl_sync(0xffffffffu, t, B * (comp < B ? comp : 0));
             }
-            if (lane == 0) {
-#pragma unroll
-                for (int i = 0; i < B; ++i) {
-                    y[B * cc.r + i] = acc[i];
-                    if (DOT >= 1) dot = fma(acc[i], w[B * cc.r + i], dot);
-                    if (DOT == 2) yy = fma(acc[i], acc[i], yy);
-                }
+            if (writer) {
+                const int64_t yi = B * cc.r + comp;
+                y[yi] = sr;
+                if (DOT >= 1) dot = fma(sr, w[yi], dot);
+                if (DOT == 2) yy = fma(sr, sr, yy);
             }
 #pragma unroll
             for (int i = 0; i < B; ++i) acc[i] = acc2[i] = 0;
@@ -490,6 +518,11 @@ k_bcsr_spmv_tma(int64_t nbrows, const int32_t *__restrict__ rowptr, const int32_
     }
     __syncwarp();
     if (DOT) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            dot += __shfl_xor_sync(0xffffffffu, dot, o);
+            if (DOT == 2) yy += __shfl_xor_sync(0xffffffffu, yy, o);
+        }
         if (lane == 0) red[wib] = dot;
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -948,35 +981,6 @@ struct RowCfg {
     static constexpr int SMEM = WARPS * NST * STAGE + WARPS * NST * 8;  // stages + mbarriers
     static_assert(CH % 32 == 0, "whole 32-block groups per stage");
 };
-
-// Transposed butterfly of B (2 or 3) sums over the warp: returns, in every lane,
-// the full sum of component comp_of_lane(lane) = lane / (32 / Bp), Bp = 2 or 4.
-template <int B>
-__device__ __forceinline__ double reduce_rows_t(const double (&a)[B], int lane) {
-    if constexpr (B == 2) {
-        const bool up = lane & 16;
-        double k = up ? a[1] : a[0];
-        k += __shfl_xor_sync(0xffffffffu, up ? a[0] : a[1], 16);
-#pragma unroll
-        for (int o = 8; o > 0; o >>= 1) k += __shfl_xor_sync(0xffffffffu, k, o);
-        return k;
-    } else {
-        const bool up = lane & 16, mid = lane & 8;
-        // step 1: the lower half keeps sums 0 and 1, the upper half sums 2 and 3 (3 is 0)
-        double s0 = up ? a[2] : a[0];
-        double s1 = up ? 0.0 : a[1];
-        const double t0 = up ? a[0] : a[2];
-        const double t1 = up ? a[1] : 0.0;
-        s0 += __shfl_xor_sync(0xffffffffu, t0, 16);
-        s1 += __shfl_xor_sync(0xffffffffu, t1, 16);
-        // step 2: lanes with bit 3 keep the second of the two
-        double k = mid ? s1 : s0;
-        k += __shfl_xor_sync(0xffffffffu, mid ? s0 : s1, 8);
-#pragma unroll
-        for (int o = 4; o > 0; o >>= 1) k += __shfl_xor_sync(0xffffffffu, k, o);
-        return k;
-    }
-}
 
 template <int B, typename VT, int DOT, typename C, bool XF>
 __global__ void __launch_bounds__(C::WARPS * 32)
