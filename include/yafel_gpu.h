@@ -475,7 +475,9 @@ YG_API yg_status yg_server_info(yg_server S, int64_t *queued, int64_t *active, u
  * and the next launch). */
 YG_API yg_status yg_server_tune(yg_server S);
 /* Systems of at least `rows` rows (0: none) skip the batch: each wait solves
- * one of them alone, to completion, with yg_cg or yg_bicgstab (Jacobi). */
+ * one of them alone, to completion, with yg_cg or yg_bicgstab (Jacobi), before
+ * it waits for the block in flight; on the matrix's own context, so with the
+ * systems built on another context the solve and the block overlap. */
 YG_API yg_status yg_server_set_solo_rows(yg_server S, int64_t rows);
 
 /* ------------------------------------------------------------------ allocation-free dot product */

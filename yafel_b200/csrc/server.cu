@@ -15,7 +15,9 @@
 // Inside the batch, systems with a large matrix run their iteration SpMV as
 // their own single-system launch (yg_server_set_solo_spmv_bytes).  Systems of
 // at least `solo_rows` rows (when set; off by default) skip the batch instead
-// and are solved one at a time, after a block, by the single-system solvers.
+// and are solved one at a time by the single-system solvers, one per wait,
+// before the wait for the block in flight (so the two overlap when the
+// system's context has its own stream).
 #include "internal.h"
 
 #include <deque>
@@ -163,9 +165,35 @@ extern "C" yg_status yg_server_launch(yg_server S) {
     return YG_OK;
 }
 
+// One system of the solo queue solved alone by the single-system solvers (on
+// its matrix's context: with the requests built on the server's second context
+// this solve runs beside a block in flight on the batch's stream).
+static yg_status solve_one_solo(yg_server S, int32_t *done) {
+    if (S->solo.empty()) return YG_OK;
+    const int64_t r = S->solo.front();
+    S->solo.pop_front();
+    Request &q = S->reqs[r];
+    yg_precond M = nullptr;
+    YG_TRY(yg_precond_create(q.A, YG_PRECOND_JACOBI, &M));
+    yg_solve_stats st{};
+    yg_status e = q.method == YG_METHOD_BICGSTAB ? yg_bicgstab(q.A, M, q.b, q.x, &q.opts, &st)
+                                                  : yg_cg(q.A, M, q.b, q.x, &q.opts, &st);
+    yg_precond_destroy(M);
+    if (e != YG_OK && e != YG_NOT_CONVERGED && e != YG_BREAKDOWN && e != YG_NAN) return e;
+    q.stats = st;
+    q.state = RQ_DONE;
+    q.A = nullptr;
+    q.b = q.x = nullptr;
+    S->finished.push_back(r);
+    ++*done;
+    return YG_OK;
+}
+
 extern "C" yg_status yg_server_wait(yg_server S, int32_t *n_finished) {
     if (!S) return fail(YG_BAD_ARG, "yg_server_wait: NULL server");
     int32_t done = 0;
+    // one system solved alone per wait, while the block (if any) is still running
+    YG_TRY(solve_one_solo(S, &done));
     if (S->in_flight) {
         S->in_flight = false;
         int32_t active = 0;
@@ -183,25 +211,6 @@ extern "C" yg_status yg_server_wait(yg_server S, int32_t *n_finished) {
             S->finished.push_back(r);
             ++done;
         }
-    }
-    // one system solved alone per wait
-    if (!S->solo.empty()) {
-        const int64_t r = S->solo.front();
-        S->solo.pop_front();
-        Request &q = S->reqs[r];
-        yg_precond M = nullptr;
-        YG_TRY(yg_precond_create(q.A, YG_PRECOND_JACOBI, &M));
-        yg_solve_stats st{};
-        yg_status e = q.method == YG_METHOD_BICGSTAB ? yg_bicgstab(q.A, M, q.b, q.x, &q.opts, &st)
-                                                      : yg_cg(q.A, M, q.b, q.x, &q.opts, &st);
-        yg_precond_destroy(M);
-        if (e != YG_OK && e != YG_NOT_CONVERGED && e != YG_BREAKDOWN && e != YG_NAN) return e;
-        q.stats = st;
-        q.state = RQ_DONE;
-        q.A = nullptr;
-        q.b = q.x = nullptr;
-        S->finished.push_back(r);
-        ++done;
     }
     if (n_finished) *n_finished = done;
     return YG_OK;
