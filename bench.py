@@ -319,6 +319,7 @@ def run_gpu(args):
         out["small_poisson64"] = run_small_poisson(ctx)
         out["q3_30cubed"] = run_q3(ctx)
         out["ilu0_vs_jacobi_30cubed"] = run_ilu(ctx)
+        out["gradient_recovery"] = run_gradient(ctx, dm, x, args.nx)
     if ws == 1 and not args.no_side_workloads:
         # configurations 4 and 5 (batched and served solves), one timed pass each
         del K, Kmx, x
@@ -562,6 +563,40 @@ def run_ilu(ctx, nx=30):
             out[name]["levels_forward_backward"] = [lo, up]
             out[name]["ms_per_iteration"] = 1e3 * (t2 - t1) / max(1, st.iterations)
         del M, x
+    return out
+
+
+def run_gradient(ctx, dm, x, nx, reps=5):
+    """Gradient recovery on the benchmark's solution: LocalSmoothingGradient of
+    the 60^3 Q2 elasticity displacement (nodal 3x3 gradients), and ZZ patch
+    recovery of a smooth scalar field on a Q1 hex mesh of the same cell count
+    (ZZ takes p = 1 scalar fields); device-synchronised wall time, best of reps."""
+    import yafel_b200 as yb
+    out = {}
+    fe = yb.FESystem(dm, 3, format=yb.BCSR)
+    fe.getSolution().axpy(1.0, x)
+    ts = []
+    for _ in range(reps):
+        ctx.synchronize()
+        t0 = time.perf_counter()
+        yb.LocalSmoothingGradient(yb.LinearElasticity(3, E=E, nu=NU), fe)
+        ctx.synchronize()
+        ts.append(time.perf_counter() - t0)
+    out["local_smoothing_q2_%dcubed" % nx] = {"cells": nx ** 3, "dofs": dm.ndofs, "ms": 1e3 * min(ts),
+                                              "dofs_per_s": dm.ndofs / min(ts)}
+    dm1 = yb.DoFManager(problem(nx), 1, 1, ctx=ctx)
+    X = dm1.dof_nodes
+    fe1 = yb.FESystem(dm1, 3)
+    fe1.getSolution().upload(np.sin(2 * X[:, 0]) * np.cos(X[:, 1]) + X[:, 2] ** 2)
+    ts = []
+    for _ in range(reps):
+        ctx.synchronize()
+        t0 = time.perf_counter()
+        yb.ZZGradientRecovery(yb.PoissonEquation(3), fe1)
+        ctx.synchronize()
+        ts.append(time.perf_counter() - t0)
+    out["zz_q1_%dcubed" % nx] = {"cells": nx ** 3, "nodes": dm1.ndofs, "ms": 1e3 * min(ts),
+                                 "nodes_per_s": dm1.ndofs / min(ts)}
     return out
 
 
