@@ -109,7 +109,7 @@ def bcsr3_spmv32_bytes(nnzb, n):
 
 
 TMA_CFG = {32: "64,3,4", 1: "32,4,8", 2: "32,3,8", 4: "32,2,8", 8: "32,3,12", 16: "48,3,8"}
-ROW_CFG = {1: "128,2,4,5", 2: "128,3,4,3", 4: "64,2,8,4", 8: "64,2,4,8", 16: "96,2,4,6"}
+ROW_CFG = {1: "128,2,4", 2: "128,3,4", 4: "64,2,8", 8: "64,3,8"}
 
 
 def spmv_kernel_name(K, dot=1, vt="double"):
@@ -120,7 +120,7 @@ def spmv_kernel_name(K, dot=1, vt="double"):
         return "k_bcsr_spmv_tma<3,%s,%d,TmaCfg<3,%s,%s>%s>" % (vt, dot, vt, cfg, xf)
     if variant == 4:
         xf = ",true" if vt == "float" else ",false"
-        return "k_bcsr_spmv_rows<3,%s,%d,RowCfg<3,%s,%s>%s>" % (vt, dot, vt, ROW_CFG.get(lanes, "128,2,4,5"), xf)
+        return "k_bcsr_spmv_rows<3,%s,%d,RowCfg<3,%s,%s>%s>" % (vt, dot, vt, ROW_CFG.get(lanes, "128,2,4"), xf)
     if variant == 1:
         return "k_bcsr_spmv_staged<3,%s,%d>" % (vt, dot)
     return "k_bcsr_spmv<3,%d,%s,%d>" % (lanes, vt, dot)

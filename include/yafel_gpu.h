@@ -292,8 +292,7 @@ YG_API yg_status yg_spmv_ex(yg_matrix A, yg_vector x, yg_vector y, int32_t preci
  * row must hold 1..capacity entries); variant 4: one bulk copy pair per whole
  * block row into per-warp rings, every lane's x gathers issued before its
  * products, a transposed butterfly for the B row sums (2x2 and 3x3 blocks,
- * `lanes` 1, 2, 4, 8, 16 selects stages of 128, 128, 64, 64, 96 blocks; a
- * longer row is fetched in pieces of a stage).  variant -1 re-runs the device autotuner, which times
+ * `lanes` 1, 2: rows of up to 128 blocks, 4, 8: up to 64 blocks).  variant -1 re-runs the device autotuner, which times
  * the candidates on this matrix and keeps the fastest (it also runs on the
  * first SpMV or solve of a matrix). */
 YG_API yg_status yg_matrix_set_spmv(yg_matrix A, int32_t variant, int32_t lanes);

@@ -431,7 +431,7 @@ class _Matrix:
     def set_spmv(self, variant, lanes=32):
         """variant 0 flat (lanes per row), 1 shared-memory staged, 2 bulk-copy
         row chunks (2x2/3x3 blocks), 3 bulk-copy row tiles (CSR), 4 bulk-copy
-        whole rows (2x2/3x3 blocks; rows longer than a stage in pieces), -1 autotune."""
+        whole rows (2x2/3x3 blocks, rows of up to 128 or 64 blocks), -1 autotune."""
         check(lib().yg_matrix_set_spmv(self.h, int(variant), int(lanes)))
 
     def set_spmv_for(self, precision, variant, lanes):

@@ -831,12 +831,18 @@ static yg_status csr_tiles_build(yg_matrix A, int k) {
     return YG_OK;
 }
 
+static int rows_capacity_of(int lanes) { return lanes <= 2 ? 128 : 64; }
+
 yg_status spmv_prepare(yg_matrix A, int variant, int lanes) {
-    if (variant == 4) {  // whole rows (longer rows in pieces of a stage)
-        if (lanes != 1 && lanes != 2 && lanes != 4 && lanes != 8 && lanes != 16)
-            return fail(YG_BAD_ARG, "whole-row SpMV configurations are lanes 1, 2, 4, 8, 16");
+    if (variant == 4) {  // whole rows: every block row must fit one stage
+        if (lanes != 1 && lanes != 2 && lanes != 4 && lanes != 8)
+            return fail(YG_BAD_ARG, "whole-row SpMV configurations are lanes 1, 2, 4, 8");
         if (A->block != 2 && A->block != 3) return fail(YG_UNSUPPORTED, "whole-row SpMV needs 2x2 or 3x3 blocks");
         if (A->nbrows >= INT32_MAX) return fail(YG_UNSUPPORTED, "whole-row SpMV needs fewer than 2^31 block rows");
+        YG_TRY(row_extent(A));
+        if (A->row_max > rows_capacity_of(lanes))
+            return fail(YG_UNSUPPORTED, "whole-row SpMV (lanes %d) holds rows of up to %d blocks; the longest has %d",
+                        lanes, rows_capacity_of(lanes), A->row_max);
         return YG_OK;
     }
     if (variant != 3) return YG_OK;
@@ -966,9 +972,9 @@ static void tma_shape_bv(int lanes, int *smem, int *wp) {
 //   first lane writes y[B r + i] (and its dot terms).
 // The summation order is fixed (lane order, then the butterfly), so results are
 // reproducible.  Waits are bounded as in the variants above.
-template <int B, typename VT, int CH_, int NST_, int WARPS_, int MINB_>
+template <int B, typename VT, int CH_, int NST_, int WARPS_>
 struct RowCfg {
-    static constexpr int CH = CH_, NST = NST_, WARPS = WARPS_, U = CH / 32, MINB = MINB_;
+    static constexpr int CH = CH_, NST = NST_, WARPS = WARPS_, U = CH / 32;
     static constexpr int VBYTES = (CH * B * B * (int)sizeof(VT) + 32 + 15) & ~15;
     static constexpr int CBYTES = (CH * 4 + 32 + 15) & ~15;
     static constexpr int STAGE = VBYTES + CBYTES;
@@ -977,7 +983,7 @@ struct RowCfg {
 };
 
 template <int B, typename VT, int DOT, typename C, bool XF>
-__global__ void __launch_bounds__(C::WARPS * 32, C::MINB)
+__global__ void __launch_bounds__(C::WARPS * 32)
 k_bcsr_spmv_rows(int32_t nbrows, const int32_t *__restrict__ rowptr, const int32_t *__restrict__ col,
                  const VT *__restrict__ val, const double *__restrict__ x, const float *__restrict__ x32,
                  double *__restrict__ y, const double *__restrict__ w, double *__restrict__ partials,
@@ -1021,9 +1027,8 @@ k_bcsr_spmv_rows(int32_t nbrows, const int32_t *__restrict__ rowptr, const int32
             hdr[wib][st][0] = rs;
             hdr[wib][st][1] = re - rs;
             if (re > rs) {
-                const int pe = min(re, rs + C::CH);  // the first piece of a longer row
-                const int64_t vs = (int64_t)rs * BB, va = vs & ~(int64_t)15, ve = ((int64_t)pe * BB + 15) & ~(int64_t)15;
-                const int64_t cs = (int64_t)rs * 4, ca = cs & ~(int64_t)15, ce = ((int64_t)pe * 4 + 15) & ~(int64_t)15;
+                const int64_t vs = (int64_t)rs * BB, va = vs & ~(int64_t)15, ve = ((int64_t)re * BB + 15) & ~(int64_t)15;
+                const int64_t cs = (int64_t)rs * 4, ca = cs & ~(int64_t)15, ce = ((int64_t)re * 4 + 15) & ~(int64_t)15;
                 unsigned char *dst = ring + st * C::STAGE;
                 mbar_expect_tx(&bars[st], (unsigned)((ve - va) + (ce - ca)));
                 bulk_g2s(dst, vbytes + va, (unsigned)(ve - va), &bars[st], pol);
@@ -1065,68 +1070,40 @@ k_bcsr_spmv_rows(int32_t nbrows, const int32_t *__restrict__ rowptr, const int32
         phase ^= (1u << st);
         __syncwarp();
         const int rs = hdr[wib][st][0], nb = hdr[wib][st][1];
-        unsigned char *stg = ring + st * C::STAGE;
+        const unsigned char *stg = ring + st * C::STAGE;
+        const VT *blk = reinterpret_cast<const VT *>(stg + (((unsigned)rs * (unsigned)BB) & 15u));
+        const int32_t *cix = reinterpret_cast<const int32_t *>(stg + C::VBYTES + (((unsigned)rs * 4u) & 15u));
+        double xv[C::U][B];
+#pragma unroll
+        for (int u = 0; u < C::U; ++u) {
+            if (32 * u < nb) {  // warp-uniform
+                const int j = lane + 32 * u;
+                if (j < nb) {
+                    gather_x<B, XF>(x, x32, cix[j], xv[u]);
+                } else {
+#pragma unroll
+                    for (int k = 0; k < B; ++k) xv[u][k] = 0;
+                }
+            }
+        }
         double acc[B], acc2[B];
 #pragma unroll
         for (int i = 0; i < B; ++i) acc[i] = acc2[i] = 0;
-        // a row longer than the stage is taken in pieces of CH blocks: after the
-        // first, each piece is fetched into the same stage and waited for here
-        for (int b0 = 0;;) {
-            const int nbp = min(C::CH, nb - b0);
-            const VT *blk = reinterpret_cast<const VT *>(stg + (((unsigned)(rs + b0) * (unsigned)BB) & 15u));
-            const int32_t *cix = reinterpret_cast<const int32_t *>(stg + C::VBYTES + (((unsigned)(rs + b0) * 4u) & 15u));
-            double xv[C::U][B];
 #pragma unroll
-            for (int u = 0; u < C::U; ++u) {
-                if (32 * u < nbp) {  // warp-uniform
-                    const int j = lane + 32 * u;
-                    if (j < nbp) {
-                        gather_x<B, XF>(x, x32, cix[j], xv[u]);
-                    } else {
+        for (int u = 0; u < C::U; ++u) {
+            if (32 * u < nb) {
+                const int j = lane + 32 * u;
+                if (j < nb) {
 #pragma unroll
-                        for (int k = 0; k < B; ++k) xv[u][k] = 0;
-                    }
+                    for (int i = 0; i < B; ++i)
+#pragma unroll
+                        for (int k = 0; k < B; ++k) {
+                            if (u & 1) acc2[i] = fma((double)blk[j * B2 + i * B + k], xv[u][k], acc2[i]);
+                            else acc[i] = fma((double)blk[j * B2 + i * B + k], xv[u][k], acc[i]);
+                        }
                 }
             }
-#pragma unroll
-            for (int u = 0; u < C::U; ++u) {
-                if (32 * u < nbp) {
-                    const int j = lane + 32 * u;
-                    if (j < nbp) {
-#pragma unroll
-                        for (int i = 0; i < B; ++i)
-#pragma unroll
-                            for (int k = 0; k < B; ++k) {
-                                if (u & 1) acc2[i] = fma((double)blk[j * B2 + i * B + k], xv[u][k], acc2[i]);
-                                else acc[i] = fma((double)blk[j * B2 + i * B + k], xv[u][k], acc[i]);
-                            }
-                    }
-                }
-            }
-            b0 += C::CH;
-            if (b0 >= nb) break;
-            __syncwarp();  // the piece is consumed: fetch the next one into this stage
-            if (lane == 0) {
-                const int ps = rs + b0, pe = min(rs + nb, ps + C::CH);
-                const int64_t vs = (int64_t)ps * BB, va = vs & ~(int64_t)15, ve = ((int64_t)pe * BB + 15) & ~(int64_t)15;
-                const int64_t cs = (int64_t)ps * 4, ca = cs & ~(int64_t)15, ce = ((int64_t)pe * 4 + 15) & ~(int64_t)15;
-                mbar_expect_tx(&bars[st], (unsigned)((ve - va) + (ce - ca)));
-                bulk_g2s(stg, vbytes + va, (unsigned)(ve - va), &bars[st], pol);
-                bulk_g2s(stg + C::VBYTES, cbytes + ca, (unsigned)(ce - ca), &bars[st], pol);
-            }
-            int pok = 1;
-            if (lane == 0) {
-                long long spins = 0;
-                while (!mbar_try_wait(&bars[st], (phase >> st) & 1u))
-                    if (++spins > kSpinLimit) { pok = 0; break; }
-            }
-            pok = __shfl_sync(0xffffffffu, pok, 0);
-            if (!pok) { timed_out = true; break; }
-            if (lane != 0) mbar_try_wait(&bars[st], (phase >> st) & 1u);
-            phase ^= (1u << st);
-            __syncwarp();
         }
-        if (timed_out) break;
         __syncwarp();  // the stage is free again
 #pragma unroll
         for (int i = 0; i < B; ++i) acc[i] += acc2[i];
@@ -1186,15 +1163,13 @@ k_bcsr_spmv_rows(int32_t nbrows, const int32_t *__restrict__ rowptr, const int32
     }
 }
 
-// Whole-row configurations (stage capacity in blocks, ring depth, warps per CTA,
-// CTAs per SM the registers are sized for), selected by the `lanes` field of a
-// variant-4 matrix; rows longer than the stage are taken in pieces.
-template <int B, typename VT> using RowL1 = RowCfg<B, VT, 128, 2, 4, 5>;
-template <int B, typename VT> using RowL2 = RowCfg<B, VT, 128, 3, 4, 3>;
-template <int B, typename VT> using RowL4 = RowCfg<B, VT, 64, 2, 8, 4>;
-template <int B, typename VT> using RowL8 = RowCfg<B, VT, 64, 2, 4, 8>;
-template <int B, typename VT> using RowL16 = RowCfg<B, VT, 96, 2, 4, 6>;
-static bool rows_lanes_ok(int lanes) { return lanes == 1 || lanes == 2 || lanes == 4 || lanes == 8 || lanes == 16; }
+// Whole-row configurations (longest row in blocks, ring depth, warps per CTA),
+// selected by the `lanes` field of a variant-4 matrix.
+template <int B, typename VT> using RowL1 = RowCfg<B, VT, 128, 2, 4>;
+template <int B, typename VT> using RowL2 = RowCfg<B, VT, 128, 3, 4>;
+template <int B, typename VT> using RowL4 = RowCfg<B, VT, 64, 2, 8>;
+template <int B, typename VT> using RowL8 = RowCfg<B, VT, 64, 3, 8>;
+static bool rows_lanes_ok(int lanes) { return lanes == 1 || lanes == 2 || lanes == 4 || lanes == 8; }
 
 template <int B, typename VT, int DOT, typename C, bool XF>
 static yg_status launch_rows_xf(yg_matrix A, const VT *val, const double *x, const float *x32, double *y,
@@ -1226,13 +1201,14 @@ template <int B, typename VT, int DOT>
 static yg_status launch_rows(yg_matrix A, int lanes, const VT *val, const double *x, const float *x32, double *y,
                              const double *w, double *partials, const int32_t *flag, const double *corr, int grid,
                              cudaStream_t st) {
-    if (!rows_lanes_ok(lanes)) return fail(YG_BAD_ARG, "whole-row SpMV configurations are lanes 1, 2, 4, 8, 16");
+    if (!rows_lanes_ok(lanes) || A->row_max < 0 || A->row_max > rows_capacity_of(lanes))
+        return fail(YG_BAD_ARG, "whole-row SpMV launched on rows it does not hold (lanes %d, longest row %d)", lanes,
+                    A->row_max);
     switch (lanes) {
     case 1: return launch_rows_cfg<B, VT, DOT, RowL1<B, VT>>(A, val, x, x32, y, w, partials, flag, corr, grid, st);
     case 2: return launch_rows_cfg<B, VT, DOT, RowL2<B, VT>>(A, val, x, x32, y, w, partials, flag, corr, grid, st);
     case 4: return launch_rows_cfg<B, VT, DOT, RowL4<B, VT>>(A, val, x, x32, y, w, partials, flag, corr, grid, st);
-    case 8: return launch_rows_cfg<B, VT, DOT, RowL8<B, VT>>(A, val, x, x32, y, w, partials, flag, corr, grid, st);
-    default: return launch_rows_cfg<B, VT, DOT, RowL16<B, VT>>(A, val, x, x32, y, w, partials, flag, corr, grid, st);
+    default: return launch_rows_cfg<B, VT, DOT, RowL8<B, VT>>(A, val, x, x32, y, w, partials, flag, corr, grid, st);
     }
 }
 
@@ -1242,8 +1218,7 @@ static void rows_shape_bv(int lanes, int *smem, int *wp) {
     case 1: shape_of<RowL1<B, VT>>(smem, wp); break;
     case 2: shape_of<RowL2<B, VT>>(smem, wp); break;
     case 4: shape_of<RowL4<B, VT>>(smem, wp); break;
-    case 8: shape_of<RowL8<B, VT>>(smem, wp); break;
-    default: shape_of<RowL16<B, VT>>(smem, wp); break;
+    default: shape_of<RowL8<B, VT>>(smem, wp); break;
     }
 }
 
@@ -1496,7 +1471,7 @@ static yg_status tune_precision(yg_matrix A, int precision, double *x, const flo
     if (A->block == 2 || A->block == 3) {
         cands.push_back({1, 32});
         for (int L : {32, 1, 2, 4, 8, 16}) cands.push_back({2, L});  // TMA configurations
-        for (int L : {1, 2, 4, 8, 16})  // whole-row configurations
+        for (int L : {1, 2, 4, 8})  // whole-row configurations, where the longest row fits a stage
             if (spmv_prepare(A, 4, L) == YG_OK) cands.push_back({4, L});
     }
     const bool f32 = precision != YG_PREC_FP64;
