@@ -18,6 +18,17 @@
 #include "device_common.cuh"
 
 #include <type_traits>
+#include <atomic>
+
+// cudaFuncSetAttribute sets a kernel's shared-memory limit on the current device
+// only: each launcher keeps one bit per device (0..63) it has been set on.  Two
+// threads that both see the bit clear both set the same value.
+static bool smem_attr_due(const std::atomic<uint64_t> &done, int device) {
+    return device < 0 || device >= 64 || !(done.load(std::memory_order_acquire) & (1ull << device));
+}
+static void smem_attr_done(std::atomic<uint64_t> &done, int device) {
+    if (device >= 0 && device < 64) done.fetch_or(1ull << device, std::memory_order_release);
+}
 
 namespace yg {
 
@@ -853,10 +864,10 @@ yg_status spmv_prepare(yg_matrix A, int variant, int lanes) {
 template <typename VT, int DOT, typename C>
 static yg_status launch_csr_cfg(yg_matrix A, int k, const VT *val, const double *x, double *y, const double *w,
                                 double *partials, const int32_t *flag, const double *corr, int grid, cudaStream_t st) {
-    static bool attr = false;
-    if (!attr) {
+    static std::atomic<uint64_t> attr{0};
+    if (smem_attr_due(attr, A->ctx->device)) {
         cudaFuncSetAttribute(k_csr_spmv_tiles<VT, DOT, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM);
-        attr = true;
+        smem_attr_done(attr, A->ctx->device);
     }
     k_csr_spmv_tiles<VT, DOT, C><<<grid, C::WARPS * 32, C::SMEM, st>>>(A->nctiles[k], A->d_ctiles[k], A->d_rowptr,
                                                                        A->d_col, val, x, y, w, partials, flag, corr,
@@ -892,11 +903,11 @@ static void csr_shape_v(int lanes, int *smem, int *wp) {
 template <int B, typename VT, int DOT, typename C, bool XF>
 static yg_status launch_tma_xf(yg_matrix A, const VT *val, const double *x, const float *x32, double *y,
                                const double *w, double *partials, const int32_t *flag, const double *corr, int grid, cudaStream_t st) {
-    static bool attr = false;
-    if (!attr) {
+    static std::atomic<uint64_t> attr{0};
+    if (smem_attr_due(attr, A->ctx->device)) {
         cudaFuncSetAttribute(k_bcsr_spmv_tma<B, VT, DOT, C, XF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              C::SMEM);
-        attr = true;
+        smem_attr_done(attr, A->ctx->device);
     }
     k_bcsr_spmv_tma<B, VT, DOT, C, XF><<<grid, C::WARPS * 32, C::SMEM, st>>>(
         A->nbrows, A->d_rowptr, A->d_col, val, x, x32, y, w, partials, flag, corr, A->ctx->d_err);
@@ -1175,11 +1186,11 @@ template <int B, typename VT, int DOT, typename C, bool XF>
 static yg_status launch_rows_xf(yg_matrix A, const VT *val, const double *x, const float *x32, double *y,
                                 const double *w, double *partials, const int32_t *flag, const double *corr, int grid,
                                 cudaStream_t st) {
-    static bool attr = false;
-    if (!attr) {
+    static std::atomic<uint64_t> attr{0};
+    if (smem_attr_due(attr, A->ctx->device)) {
         cudaFuncSetAttribute(k_bcsr_spmv_rows<B, VT, DOT, C, XF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              C::SMEM);
-        attr = true;
+        smem_attr_done(attr, A->ctx->device);
     }
     k_bcsr_spmv_rows<B, VT, DOT, C, XF><<<grid, C::WARPS * 32, C::SMEM, st>>>(
         (int32_t)A->nbrows, A->d_rowptr, A->d_col, val, x, x32, y, w, partials, flag, corr, A->ctx->d_err);
@@ -1245,10 +1256,10 @@ template <int B, typename VT, int DOT>
 static yg_status launch_staged(yg_matrix A, const VT *val, const double *x, double *y, const double *w,
                                double *partials, const int32_t *flag, const double *corr, int grid, cudaStream_t st) {
     using S = Staged<B, VT>;
-    static bool attr = false;
-    if (!attr) {
+    static std::atomic<uint64_t> attr{0};
+    if (smem_attr_due(attr, A->ctx->device)) {
         cudaFuncSetAttribute(k_bcsr_spmv_staged<B, VT, DOT>, cudaFuncAttributeMaxDynamicSharedMemorySize, S::SMEM);
-        attr = true;
+        smem_attr_done(attr, A->ctx->device);
     }
     k_bcsr_spmv_staged<B, VT, DOT><<<grid, S::WARPS * 32, S::SMEM, st>>>(A->nbrows, A->d_rowptr, A->d_col, val, x, y,
                                                                         w, partials, flag, corr);
